@@ -1,0 +1,140 @@
+/*
+ * vshe_gpu.h -- C ABI of the B200 SHE linear-solve backend (libvshe_b200.so).
+ *
+ * This is the library a ViennaSHE build binds for its reserved
+ * gpu_parallel_linear_solver slot.  Every entry point takes plain pointers and
+ * sizes; no C++, CUDA or PyTorch types cross the boundary.  All functions
+ * return VSHE_OK (0) on success and a negative VSHE_E* code on failure; the
+ * message of the last failure on a context is available from vshe_last_error().
+ *
+ * Reference interfaces this library replaces (paths inside viennashe-dev):
+ *   - viennashe::solvers::solve(sparse_matrix<double>&, std::vector<double> const&,
+ *     linear_solver_config const&) with config.id() == gpu_parallel_linear_solver
+ *       src/solver.cpp:34-38, dispatched at src/solvers/solve.hpp:68-86, slot
+ *       reserved at viennashe/solvers/config.hpp:46 / viennashe/forwards.h:215-216
+ *       -> vshe_solve_csr / vshe_system_*
+ *   - viennashe::she::assemble(...)   viennashe/she/assemble_all.hpp:46-424
+ *   - viennashe::she::solve(...)      viennashe/she/linear_solver.hpp:100-189
+ *       -> vshe_she_*
+ *   - error codes: libviennashe/include/error.h:25-31 (int codes, 0 = success)
+ */
+#ifndef VSHE_GPU_H
+#define VSHE_GPU_H
+
+#include "vshe_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes (0 = success, as viennasheErrorCode) ---- */
+#define VSHE_OK                   0
+#define VSHE_E_INVALID_ARGUMENT  -1   /* bad size, null pointer, bad option */
+#define VSHE_E_EMPTY_ROW         -2   /* src/solvers/solve.hpp:54-58 (matrix_consistency_check) */
+#define VSHE_E_NAN               -3   /* NaN/Inf in rhs or matrix (util/checks.hpp:111-130) */
+#define VSHE_E_ODD_DIAGONAL      -4   /* non-positive S^oo diagonal (she/eliminate.hpp:265-270) */
+#define VSHE_E_BREAKDOWN         -5   /* BiCGStab breakdown (rho or (r^,v) == 0) */
+#define VSHE_E_NOT_CONVERGED     -6   /* iteration limit reached above tolerance */
+#define VSHE_E_OUT_OF_MEMORY     -7   /* device allocation failed */
+#define VSHE_E_BUDGET            -8   /* request exceeds the context's HBM budget */
+#define VSHE_E_CUDA              -9   /* CUDA runtime error */
+#define VSHE_E_TIMEOUT          -10   /* a device-side wait ran out of iterations */
+#define VSHE_E_ZERO_PIVOT       -11   /* zero pivot in the incomplete factorisation */
+#define VSHE_E_NOT_FOUND        -12   /* unknown handle */
+#define VSHE_E_UNSUPPORTED      -13   /* option not available in this build */
+
+/* ---- solver options ---- */
+#define VSHE_PRECISION_FP64   0   /* FP64 BiCGStab, FP64 preconditioner */
+#define VSHE_PRECISION_MIXED  1   /* FP32 BiCGStab + FP32 preconditioner inside FP64 iterative refinement */
+
+#define VSHE_PRECOND_NONE        0
+#define VSHE_PRECOND_ILU0        1   /* ILU(0) on the whole system (serial_linear_solver's choice) */
+#define VSHE_PRECOND_BLOCK_ILU0  2   /* ILU(0) per block (energy slabs: block_preconditioner_boundaries) */
+
+#define VSHE_ORDER_NATURAL 0
+
+#define VSHE_TRSV_AUTO        0
+#define VSHE_TRSV_PERSISTENT  1   /* one cooperative launch per triangular solve, grid barrier per level */
+#define VSHE_TRSV_PER_LEVEL   2   /* one launch per level */
+
+typedef struct vshe_solve_opts {
+  int32_t precision;        /* VSHE_PRECISION_* */
+  int32_t precond;          /* VSHE_PRECOND_* */
+  int32_t ordering;         /* VSHE_ORDER_* */
+  double  tol;              /* FP64 relative residual ||b - A x|| / ||b|| to reach (e.g. 1e-10) */
+  int32_t max_iters;        /* cap on BiCGStab iterations (all refinement sweeps together) */
+  double  inner_tol;        /* mixed: relative reduction asked of each FP32 sweep (e.g. 1e-5) */
+  int32_t max_refinements;  /* mixed: cap on FP64 refinement sweeps */
+  int64_t n_blocks;         /* BLOCK_ILU0: number of blocks; 0 = one block per ... see block_ptr */
+  const int64_t *block_ptr; /* n_blocks + 1 row offsets (block_preconditioner_boundaries) */
+  int32_t trsv_mode;        /* VSHE_TRSV_* */
+  int32_t check_every;      /* iterations between host-side convergence checks (0 = default 8) */
+} vshe_solve_opts;
+
+typedef struct vshe_solve_stats {
+  int32_t status;           /* VSHE_OK or an error code */
+  int32_t iterations;       /* BiCGStab iterations (all sweeps) */
+  int32_t refinements;      /* FP64 refinement sweeps (mixed) */
+  double  rel_residual;     /* final FP64 ||b - A x|| / ||b|| */
+  double  setup_ms;         /* factorisation time (device) */
+  double  solve_ms;         /* Krylov + refinement time (device) */
+  int32_t levels_L;         /* level-schedule depth of the L and U solves */
+  int32_t levels_U;
+  int64_t bytes_device;     /* device memory held by the system */
+} vshe_solve_stats;
+
+/* Fills opts with the defaults: mixed precision, block ILU0 per energy slab
+ * when blocks are given (ILU0 otherwise), tol 1e-10, max_iters 1000,
+ * inner_tol 1e-5, max_refinements 10. */
+void vshe_default_opts(vshe_solve_opts *opts);
+
+/* ---- context ---- */
+typedef struct vshe_ctx vshe_ctx;
+
+/* Creates a context on CUDA device `device`; hbm_budget_bytes = 0 means 150 GB. */
+int vshe_create(vshe_ctx **ctx, int device, size_t hbm_budget_bytes);
+int vshe_destroy(vshe_ctx *ctx);
+const char *vshe_errstr(int code);
+const char *vshe_last_error(vshe_ctx *ctx);
+/* Bytes of device memory currently held by the context's systems. */
+size_t vshe_bytes_in_use(vshe_ctx *ctx);
+
+/* ---- drop-in linear solve: viennashe::solvers::solve(A, b, config), gpu slot ----
+ * A is n x n CSR (int64 row offsets, int32 column indices ascending per row,
+ * FP64 values), rhs and x are host arrays of length n.  Checks, in the
+ * reference's order (src/solvers/solve.hpp:54-66): empty rows -> VSHE_E_EMPTY_ROW,
+ * non-finite rhs -> VSHE_E_NAN, ||rhs|| == 0 -> x = 0.  Host buffers are copied
+ * in and out inside the call. */
+int vshe_solve_csr(vshe_ctx *ctx, int64_t n, int64_t nnz, const int64_t *row_ptr, const int32_t *col,
+                   const double *val, const double *rhs, const vshe_solve_opts *opts, double *x,
+                   vshe_solve_stats *stats);
+
+/* ---- resident systems: upload once, refactor/solve many times ----
+ * vshe_system_create copies the CSR (host) to the device and builds the
+ * preconditioner's schedule for `opts`.  The pattern is fixed for the life of
+ * the handle; vshe_system_set_values replaces values and rhs (host arrays). */
+int vshe_system_create(vshe_ctx *ctx, int64_t n, int64_t nnz, const int64_t *row_ptr, const int32_t *col,
+                       const double *val, const double *rhs, const vshe_solve_opts *opts, int64_t *handle);
+int vshe_system_set_values(vshe_ctx *ctx, int64_t handle, const double *val, const double *rhs);
+/* Factorises and solves on the device; x (host, may be NULL) receives the solution. */
+int vshe_system_solve(vshe_ctx *ctx, int64_t handle, double *x, vshe_solve_stats *stats);
+/* Solves several resident systems together (one batched pass; per-system
+ * Krylov scalars, so each result equals the one it would get alone). */
+int vshe_batch_solve(vshe_ctx *ctx, int32_t count, const int64_t *handles, vshe_solve_stats *stats);
+int vshe_system_get_x(vshe_ctx *ctx, int64_t handle, double *x);
+int vshe_system_free(vshe_ctx *ctx, int64_t handle);
+
+/* Kernel-level entry points on a resident system (used by parity tests and
+ * the bench): y = A x in FP64 (precision 0) or FP32 (1), host x/y of length n;
+ * the incomplete factor values in A's pattern (FP64, host array of length nnz). */
+int vshe_system_spmv(vshe_ctx *ctx, int64_t handle, int32_t precision, const double *x, double *y);
+int vshe_system_factor_values(vshe_ctx *ctx, int64_t handle, double *lu);
+/* Device-timed kernel throughput on a resident system: runs `reps` SpMVs in the
+ * given precision and returns the mean time per SpMV (ms) from CUDA events. */
+int vshe_system_time_spmv(vshe_ctx *ctx, int64_t handle, int32_t precision, int32_t reps, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VSHE_GPU_H */

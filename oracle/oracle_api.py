@@ -1,0 +1,241 @@
+"""ctypes binding of the CPU oracle (oracle/she_oracle.cpp).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, always as the checker or the timed CPU
+reference, never as part of the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "_build", "libvshe_oracle.so")
+sys.path.insert(0, os.path.join(ROOT, "viennashe-dev_b200"))
+from vshe.abi import DeviceDesc, she_config_c, Coupling, ptr  # noqa: E402
+
+i32p = C.POINTER(C.c_int32)
+i64p = C.POINTER(C.c_int64)
+f64p = C.POINTER(C.c_double)
+
+_lib = None
+
+
+def build():
+    subprocess.check_call(["sh", os.path.join(HERE, "build.sh")])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.vsheo_create.restype = C.c_void_p
+        L.vsheo_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]
+        L.vsheo_destroy.argtypes = [C.c_void_p]
+        L.vsheo_info.argtypes = [C.c_void_p, i64p]
+        L.vsheo_energies.argtypes = [C.c_void_p, f64p, f64p, f64p, f64p]
+        L.vsheo_mapping.argtypes = [C.c_void_p, i64p, i64p, i32p, i32p, f64p]
+        L.vsheo_matrix.argtypes = [C.c_void_p, C.c_int, i64p, i32p, f64p, f64p]
+        L.vsheo_scaling.argtypes = [C.c_void_p, f64p, f64p]
+        L.vsheo_blocks.argtypes = [C.c_void_p, i64p]
+        L.vsheo_finish.argtypes = [C.c_void_p, f64p, f64p, f64p, f64p, C.c_int, f64p]
+        L.vsheo_csr_solve.argtypes = [C.c_int64, i64p, i32p, f64p, f64p, f64p, C.c_int, C.c_int, C.c_double,
+                                      C.c_int64, i64p, C.c_double, C.c_int, i32p, f64p, f64p, f64p]
+        L.vsheo_ilu0_values.argtypes = [C.c_int64, i64p, i32p, f64p, C.c_int64, i64p, f64p]
+        L.vsheo_ilu0_apply.argtypes = [C.c_int64, i64p, i32p, f64p, C.c_int64, i64p, f64p, f64p]
+        L.vsheo_dense_solve.argtypes = [C.c_int64, i64p, i32p, f64p, f64p, f64p]
+        L.vsheo_spmv.argtypes = [C.c_int64, i64p, i32p, f64p, f64p, f64p]
+        L.vsheo_harmonics.argtypes = [C.c_int, C.c_int, i64p, C.c_int]
+        L.vsheo_harmonics.restype = C.c_int
+        L.vsheo_bench_serial.argtypes = [C.c_int64, i64p, i32p, f64p, f64p, C.c_int, f64p, f64p, f64p]
+        _lib = L
+    return _lib
+
+
+class CSR:
+    def __init__(self, rp, ci, v, rhs=None):
+        self.rp = np.ascontiguousarray(rp, np.int64)
+        self.ci = np.ascontiguousarray(ci, np.int32)
+        self.v = np.ascontiguousarray(v, np.float64)
+        self.rhs = None if rhs is None else np.ascontiguousarray(rhs, np.float64)
+
+    @property
+    def n(self):
+        return len(self.rp) - 1
+
+    @property
+    def nnz(self):
+        return int(self.rp[-1])
+
+    def dense(self):
+        A = np.zeros((self.n, self.n))
+        for i in range(self.n):
+            A[i, self.ci[self.rp[i]:self.rp[i + 1]]] += self.v[self.rp[i]:self.rp[i + 1]]
+        return A
+
+
+class OracleProblem:
+    """setup + assembly + elimination + scaling/normalisation on the CPU."""
+
+    def __init__(self, dev, cfg, coupling: Coupling):
+        self.dev = dev
+        self._desc = DeviceDesc(dev)
+        self._cfg = she_config_c(cfg)
+        self._cpl = coupling
+        err = C.create_string_buffer(512)
+        h = lib().vsheo_create(C.byref(self._desc.c), C.byref(self._cfg), C.byref(coupling.c), err, 512)
+        if not h:
+            raise RuntimeError("oracle: " + err.value.decode())
+        self.h = h
+        info = np.zeros(9, np.int64)
+        lib().vsheo_info(h, ptr(info, C.c_int64))
+        self.NH, self.n_even, self.n_odd = int(info[0]), int(info[1]), int(info[2])
+        self.nnz = {0: int(info[3]), 1: int(info[4]), 2: int(info[5]), 3: int(info[6])}
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().vsheo_destroy(self.h)
+        except Exception:
+            pass
+
+    def energies(self):
+        H = np.zeros(self.NH)
+        sc = np.zeros(self.dev.n_cells)
+        sf = np.zeros(self.dev.n_facets)
+        w = np.zeros(1)
+        lib().vsheo_energies(self.h, ptr(H, C.c_double), ptr(sc, C.c_double), ptr(sf, C.c_double), ptr(w, C.c_double))
+        return H, sc, sf, float(w[0])
+
+    def mapping(self):
+        nc, nf, NH = self.dev.n_cells, self.dev.n_facets, self.NH
+        ic = np.zeros(nc * NH, np.int64)
+        jf = np.zeros(nf * NH, np.int64)
+        oc = np.zeros(nc * NH, np.int32)
+        of = np.zeros(nf * NH, np.int32)
+        bc = np.zeros(nc * NH)
+        lib().vsheo_mapping(self.h, ptr(ic, C.c_int64), ptr(jf, C.c_int64), ptr(oc, C.c_int32), ptr(of, C.c_int32), ptr(bc, C.c_double))
+        return ic, jf, oc, of, bc
+
+    def matrix(self, which):
+        n = self.n_even + self.n_odd if which in (0, 1) else self.n_even
+        nnz = self.nnz[which]
+        rp = np.zeros(n + 1, np.int64)
+        ci = np.zeros(nnz, np.int32)
+        v = np.zeros(nnz)
+        b = np.zeros(n)
+        lib().vsheo_matrix(self.h, which, ptr(rp, C.c_int64), ptr(ci, C.c_int32), ptr(v, C.c_double), ptr(b, C.c_double))
+        return CSR(rp, ci, v, b)
+
+    def scaling(self):
+        s = np.zeros(self.n_even)
+        f = np.zeros(self.n_even)
+        lib().vsheo_scaling(self.h, ptr(s, C.c_double), ptr(f, C.c_double))
+        return s, f
+
+    def blocks(self):
+        b = np.zeros(self.NH + 1, np.int64)
+        lib().vsheo_blocks(self.h, ptr(b, C.c_int64))
+        return b
+
+    def finish(self, x_red):
+        x_red = np.ascontiguousarray(x_red, np.float64)
+        xf = np.zeros(self.n_even + self.n_odd)
+        dens = np.zeros(self.dev.n_cells)
+        nct = max(self.dev.n_contacts, 1)
+        cur = np.zeros(nct)
+        res = np.zeros(1)
+        lib().vsheo_finish(self.h, ptr(x_red, C.c_double), ptr(xf, C.c_double), ptr(dens, C.c_double),
+                           ptr(cur, C.c_double), nct, ptr(res, C.c_double))
+        return xf, dens, cur, float(res[0])
+
+
+def csr_solve(A: CSR, b, precond=1, tol=1e-10, maxit=5000, ilut_p=20, ilut_tau=1e-3, blocks=None):
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(A.n)
+    it = np.zeros(1, np.int32)
+    rr = np.zeros(1)
+    ts = np.zeros(1)
+    tv = np.zeros(1)
+    bp = None if blocks is None else np.ascontiguousarray(blocks, np.int64)
+    nb = 0 if bp is None else len(bp) - 1
+    rc = lib().vsheo_csr_solve(A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double),
+                               ptr(b, C.c_double), ptr(x, C.c_double), precond, ilut_p, ilut_tau, nb,
+                               None if bp is None else ptr(bp, C.c_int64), tol, maxit,
+                               ptr(it, C.c_int32), ptr(rr, C.c_double), ptr(ts, C.c_double), ptr(tv, C.c_double))
+    return x, dict(rc=rc, iters=int(it[0]), relres=float(rr[0]), t_setup=float(ts[0]), t_solve=float(tv[0]))
+
+
+def ilu0_values(A: CSR, blocks=None):
+    lu = np.zeros(A.nnz)
+    bp = None if blocks is None else np.ascontiguousarray(blocks, np.int64)
+    nb = 0 if bp is None else len(bp) - 1
+    rc = lib().vsheo_ilu0_values(A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double), nb,
+                                 None if bp is None else ptr(bp, C.c_int64), ptr(lu, C.c_double))
+    if rc:
+        raise RuntimeError("oracle ilu0 failed")
+    return lu
+
+
+def ilu0_apply(A: CSR, lu, b, blocks=None):
+    lu = np.ascontiguousarray(lu, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(A.n)
+    bp = None if blocks is None else np.ascontiguousarray(blocks, np.int64)
+    nb = 0 if bp is None else len(bp) - 1
+    lib().vsheo_ilu0_apply(A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(lu, C.c_double), nb,
+                           None if bp is None else ptr(bp, C.c_int64), ptr(b, C.c_double), ptr(x, C.c_double))
+    return x
+
+
+def dense_solve(A: CSR, b):
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(A.n)
+    rc = lib().vsheo_dense_solve(A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double), ptr(b, C.c_double), ptr(x, C.c_double))
+    if rc:
+        raise RuntimeError("singular")
+    return x
+
+
+def spmv(A: CSR, x):
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.zeros(A.n)
+    lib().vsheo_spmv(A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double), ptr(x, C.c_double), ptr(y, C.c_double))
+    return y
+
+
+def bench_serial(A: CSR, b, iters):
+    b = np.ascontiguousarray(b, np.float64)
+    tf = np.zeros(1)
+    ti = np.zeros(1)
+    rr = np.zeros(1)
+    done = lib().vsheo_bench_serial(A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double),
+                                    ptr(b, C.c_double), iters, ptr(tf, C.c_double), ptr(ti, C.c_double), ptr(rr, C.c_double))
+    return dict(iters=int(done), t_factor=float(tf[0]), t_per_iter=float(ti[0]), relres=float(rr[0]))
+
+
+def golden_coupling(L):
+    """The reference's tabulated coupling tables (tests/golden/coupling_L*.json)."""
+    import json
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "coupling_L%d.json" % L)))
+    D = d["dim"]
+    data = np.zeros((6, D, D))
+    for t, name in enumerate(["a_x", "a_y", "a_z", "b_x", "b_y", "b_z"]):
+        for r, c, v in d["entries"][name]:
+            data[t, r, c] = v
+    return Coupling(L, data)
+
+
+def harmonics(L, kind):
+    """Index sequence l*l + l + m of the reference's spherical_harmonics_iterator."""
+    t = {"all": 0, "even": 1, "odd": 2}[kind]
+    out = np.zeros(256, np.int64)
+    k = lib().vsheo_harmonics(L, t, ptr(out, C.c_int64), 256)
+    return out[:k].tolist()

@@ -1,0 +1,38 @@
+"""Small seeded SHE problems shared by the tests (sizes the CPU oracle builds in well under a second)."""
+import numpy as np
+
+from vshe import devices as D
+import oracle_api as O
+
+
+def resistor_2d(T=300.0, nx=9, ny=1):
+    """The reference's equilibrium resistor (tests/src/equilibrium_resistor.cpp:176-190): 600 x 600 nm,
+    doping n = p = 1e16 m^-3, zero bias, contact potential on cells with x < 0.1 L and x > 0.9 L."""
+    lx = ly = 6.0e-7
+    vol, cen, fc, fvol, fn, cfp, cfi = D._mesh_2d(nx, ny, lx / nx, ly / ny)
+    n = nx * ny
+    mat = np.zeros(n, np.int32)
+    nd = np.full(n, 1e16)
+    na = np.full(n, 1e16)
+    contact = np.full(n, -1, np.int32)
+    contact[cen[:, 0] < 0.1 * lx] = 0
+    contact[cen[:, 0] > 0.9 * lx] = 1
+    phi = D._built_in_potential(T, nd, na)
+    dev = D.Device(2, mat, vol, cen, nd, na, phi, contact, fc, fvol, fn, cfp, cfi, T, np.zeros(2), "resistor")
+    cfg = D.SheConfig(max_expansion_order=1, energy_spacing=6.2 * D.Q / 1000.0)
+    return dev, cfg
+
+
+def diode_small(L=1, boxes=40, bias=0.3, n_energy_range=0.5):
+    dev = D.nin_diode_1d(lengths=(10e-9, 30e-9, 10e-9), dopings=(1e25, 1e22, 1e25), boxes=boxes, bias=bias, name="diode_small")
+    cfg = D.SheConfig(max_expansion_order=L, energy_spacing=D.HBAR_OMEGA_OP / 4.0, min_kinetic_energy_range=n_energy_range * D.Q)
+    return dev, cfg
+
+
+def bar_small(L=3, nx=16, ny=6, n_energies=40):
+    dev, cfg = D.config2(nx=nx, ny=ny, n_energies=n_energies, L=L)
+    return dev, cfg
+
+
+def oracle_problem(dev, cfg):
+    return O.OracleProblem(dev, cfg, O.golden_coupling(cfg.max_expansion_order))

@@ -1,0 +1,132 @@
+"""CUDA solver path (through the C ABI) against the CPU oracle.
+
+Tolerances: SpMV FP64 1e-13 relative (summation order differs), FP32 1e-6;
+ILU(0) factor values 1e-11 relative to the row scale; solutions to the
+stated FP64 residual 1e-10, and within 1e-7 of the oracle's direct solution.
+"""
+import numpy as np
+import pytest
+
+from vshe import devices as D
+from vshe import gpu
+import oracle_api as O
+import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _problems():
+    out = []
+    dev, cfg = cases.diode_small(L=1, boxes=40)
+    out.append(("diode_L1", dev, cfg))
+    dev, cfg = cases.diode_small(L=3, boxes=30)
+    out.append(("diode_L3", dev, cfg))
+    dev, cfg = cases.bar_small(L=3, nx=12, ny=5, n_energies=30)
+    out.append(("bar_L3", dev, cfg))
+    return out
+
+
+PROBLEMS = _problems()
+
+
+@pytest.fixture(scope="module", params=PROBLEMS, ids=[p[0] for p in PROBLEMS])
+def prob(request):
+    name, dev, cfg = request.param
+    P = cases.oracle_problem(dev, cfg)
+    A = P.matrix(3)
+    return name, P, A
+
+
+def test_spmv_parity(gpu_ctx, prob):
+    name, P, A = prob
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(A.n)
+    S = gpu_ctx.system(A.rp, A.ci, A.v, A.rhs, precision="mixed")
+    try:
+        y_ref = O.spmv(A, x)
+        y = S.spmv(x, "fp64")
+        assert np.max(np.abs(y - y_ref)) <= 1e-13 * np.max(np.abs(y_ref))
+        y32 = S.spmv(x, "mixed")
+        assert np.max(np.abs(y32 - y_ref)) <= 1e-6 * np.max(np.abs(y_ref))
+    finally:
+        S.free()
+
+
+@pytest.mark.parametrize("block", [False, True])
+def test_ilu0_factor_parity(gpu_ctx, prob, block):
+    name, P, A = prob
+    bl = P.blocks() if block else None
+    S = gpu_ctx.system(A.rp, A.ci, A.v, A.rhs, precision="fp64", precond="block_ilu0" if block else "ilu0", blocks=bl)
+    try:
+        lu = S.factor_values()
+        lu_ref = O.ilu0_values(A, blocks=bl)
+        if block:
+            blk = np.zeros(A.n, np.int64)
+            for k in range(len(bl) - 1):
+                blk[bl[k]:bl[k + 1]] = k
+            rows = np.repeat(np.arange(A.n), np.diff(A.rp))
+            lu_ref = np.where(blk[A.ci] == blk[rows], lu_ref, 0.0)
+        scale = np.maximum(np.abs(lu_ref), 1.0)
+        assert np.max(np.abs(lu - lu_ref) / scale) < 1e-11
+    finally:
+        S.free()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precond", ["ilu0", "block_ilu0"])
+def test_solve_parity(gpu_ctx, prob, precision, precond):
+    name, P, A = prob
+    xd = O.dense_solve(A, A.rhs) if A.n <= 4000 else O.csr_solve(A, A.rhs, tol=1e-14, maxit=20000)[0]
+    bl = P.blocks() if precond == "block_ilu0" else None
+    x, st = gpu_ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision=precision, precond=precond, blocks=bl, tol=1e-10, max_iters=4000)
+    assert st["status"] == 0, st
+    r = O.spmv(A, x) - A.rhs
+    assert np.linalg.norm(r) / np.linalg.norm(A.rhs) < 1e-10
+    assert st["rel_residual"] < 1e-10
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-7
+    # downstream quantities through the oracle's post-processing: terminal currents 1e-8
+    _, dens, cur, res = P.finish(x)
+    _, dens_r, cur_r, _ = P.finish(xd)
+    assert np.max(np.abs(cur - cur_r)) <= 1e-8 * np.max(np.abs(cur_r))
+    assert np.max(np.abs(dens - dens_r) / dens_r) < 1e-8
+
+
+def test_batch_equals_alone(gpu_ctx):
+    probs = [cases.oracle_problem(*cases.diode_small(L=L, boxes=b, bias=v)) for L, b, v in ((1, 30, 0.2), (3, 24, 0.5), (1, 50, 0.8))]
+    mats = [P.matrix(3) for P in probs]
+    alone = []
+    for A in mats:
+        S = gpu_ctx.system(A.rp, A.ci, A.v, A.rhs, precision="mixed")
+        x, st = S.solve()
+        assert st["status"] == 0
+        alone.append(x)
+        S.free()
+    systems = [gpu_ctx.system(A.rp, A.ci, A.v, A.rhs, precision="mixed") for A in mats]
+    try:
+        stats = gpu_ctx.batch_solve(systems)
+        for S, st, xa, A in zip(systems, stats, alone, mats):
+            assert st["status"] == 0 and st["rel_residual"] < 1e-10
+            xb = S.x()
+            assert np.array_equal(xb, xa), np.max(np.abs(xb - xa))
+    finally:
+        for S in systems:
+            S.free()
+
+
+def test_reference_error_behaviour(gpu_ctx):
+    # empty row -> solve(): Found empty row (src/solvers/solve.hpp:54-58)
+    rp = np.array([0, 1, 1, 2]); ci = np.array([0, 2]); v = np.array([1.0, 1.0])
+    with pytest.raises(gpu.VsheError) as e:
+        gpu_ctx.solve_csr(rp, ci, v, np.ones(3))
+    assert e.value.code == -2
+    # non-finite rhs -> error
+    rp = np.array([0, 1, 2]); ci = np.array([0, 1]); v = np.array([2.0, 4.0])
+    with pytest.raises(gpu.VsheError) as e:
+        gpu_ctx.solve_csr(rp, ci, v, np.array([1.0, np.nan]))
+    assert e.value.code == -3
+    # ||b|| = 0 -> x = 0
+    x, st = gpu_ctx.solve_csr(rp, ci, v, np.zeros(2))
+    assert np.all(x == 0) and st["status"] == 0
+    # diagonal system solves exactly
+    x, st = gpu_ctx.solve_csr(rp, ci, v, np.array([1.0, 1.0]), precision="fp64")
+    assert np.allclose(x, [0.5, 0.25], rtol=1e-14)
