@@ -45,13 +45,15 @@ extern "C" {
 
 /* ---- solver options ---- */
 #define VSHE_PRECISION_FP64   0   /* FP64 BiCGStab, FP64 preconditioner */
-#define VSHE_PRECISION_MIXED  1   /* FP32 BiCGStab + FP32 preconditioner inside FP64 iterative refinement */
+#define VSHE_PRECISION_MIXED  1   /* FP32 BiCGStab recurrences + FP32 preconditioner; x and the
+                                     true residual kept in FP64 (reliable updates every 10x drop) */
 
 #define VSHE_PRECOND_NONE        0
 #define VSHE_PRECOND_ILU0        1   /* ILU(0) on the whole system (serial_linear_solver's choice) */
 #define VSHE_PRECOND_BLOCK_ILU0  2   /* ILU(0) per block (energy slabs: block_preconditioner_boundaries) */
 
-#define VSHE_ORDER_NATURAL 0
+#define VSHE_ORDER_NATURAL     0   /* the caller's row order (the reference's) */
+#define VSHE_ORDER_MULTICOLOR  1   /* greedy colouring of the matrix graph, rows grouped by colour */
 
 #define VSHE_TRSV_AUTO        0
 #define VSHE_TRSV_PERSISTENT  1   /* one cooperative launch per triangular solve, grid barrier per level */
@@ -63,12 +65,14 @@ typedef struct vshe_solve_opts {
   int32_t ordering;         /* VSHE_ORDER_* */
   double  tol;              /* FP64 relative residual ||b - A x|| / ||b|| to reach (e.g. 1e-10) */
   int32_t max_iters;        /* cap on BiCGStab iterations (all refinement sweeps together) */
-  double  inner_tol;        /* mixed: relative reduction asked of each FP32 sweep (e.g. 1e-5) */
-  int32_t max_refinements;  /* mixed: cap on FP64 refinement sweeps */
+  double  inner_tol;        /* reserved (mixed precision uses reliable updates, see below) */
+  int32_t max_refinements;  /* reserved */
   int64_t n_blocks;         /* BLOCK_ILU0: number of blocks; 0 = one block per ... see block_ptr */
   const int64_t *block_ptr; /* n_blocks + 1 row offsets (block_preconditioner_boundaries) */
   int32_t trsv_mode;        /* VSHE_TRSV_* */
   int32_t check_every;      /* iterations between host-side convergence checks (0 = default 8) */
+  const int32_t *perm;      /* optional symmetric permutation for the preconditioner: perm[i] is the
+                               original row placed at position i (overrides ordering); NULL = none */
 } vshe_solve_opts;
 
 typedef struct vshe_solve_stats {
@@ -83,9 +87,8 @@ typedef struct vshe_solve_stats {
   int64_t bytes_device;     /* device memory held by the system */
 } vshe_solve_stats;
 
-/* Fills opts with the defaults: mixed precision, block ILU0 per energy slab
- * when blocks are given (ILU0 otherwise), tol 1e-10, max_iters 1000,
- * inner_tol 1e-5, max_refinements 10. */
+/* Fills opts with the defaults: mixed precision, ILU0, natural order, tol 1e-10,
+ * max_iters 1000, persistent triangular solves. */
 void vshe_default_opts(vshe_solve_opts *opts);
 
 /* ---- context ---- */
@@ -98,6 +101,16 @@ const char *vshe_errstr(int code);
 const char *vshe_last_error(vshe_ctx *ctx);
 /* Bytes of device memory currently held by the context's systems. */
 size_t vshe_bytes_in_use(vshe_ctx *ctx);
+/* Per-kernel-class device timing (CUDA events around every launch of the next
+ * solves; off by default).  vshe_get_profile returns, for the last solve, ms spent
+ * in [0] SpMV, [1] triangular solves, [2] vector updates, [3] FP64 reliable updates,
+ * [4] factorisation, and counts[0] SpMV launches, counts[1] triangular-solve launches. */
+int vshe_set_profiling(vshe_ctx *ctx, int32_t on);
+int vshe_get_profile(vshe_ctx *ctx, double *ms, int64_t *counts);
+/* Number of this library's own kernel launches in the process so far (all
+ * contexts; library kernels such as CUB scans are not counted).  No reference
+ * counterpart: instrumentation. */
+int64_t vshe_kernel_launches(void);
 
 /* ---- drop-in linear solve: viennashe::solvers::solve(A, b, config), gpu slot ----
  * A is n x n CSR (int64 row offsets, int32 column indices ascending per row,
@@ -132,6 +145,58 @@ int vshe_system_factor_values(vshe_ctx *ctx, int64_t handle, double *lu);
 /* Device-timed kernel throughput on a resident system: runs `reps` SpMVs in the
  * given precision and returns the mean time per SpMV (ms) from CUDA events. */
 int vshe_system_time_spmv(vshe_ctx *ctx, int64_t handle, int32_t precision, int32_t reps, double *ms);
+
+/* ---- SHE path on the device: she::assemble + she::solve (secondary boundary) ----
+ * vshe_she_create runs the host setup of the (x, H) space (energies, expansion
+ * orders, unknown mapping, boundary values: viennashe/she/setup_energies.hpp:61-153,
+ * expansion_order.hpp:262-364, mapping.hpp:97-393, boundary_conditions.hpp:57-134),
+ * then builds the patterns of the full and the reduced system on the device and
+ * the preconditioner schedule for `opts` (BLOCK_ILU0 with no block_ptr uses one
+ * block per energy slab, as fill_block_indices, linear_solver.hpp:44-83).
+ * `coupling` carries the spherical-harmonics coupling tables a_{x,y,z}, b_{x,y,z}
+ * of order cfg->max_expansion_order (fill_coupling_matrices,
+ * viennashe/she/harmonics_coupling.hpp:1050-1073); vshe_coupling_tables_compute
+ * fills them by quadrature when the caller has none. */
+typedef struct vshe_she_info {
+  int32_t n_energies;       /* N_H */
+  int64_t n_even, n_odd;    /* unknowns (even = reduced system size) */
+  int64_t nnz_full, nnz_reduced;
+  int32_t n_cells, n_facets, n_contacts;
+  double  hbar_omega;       /* optical phonon energy snapped to the grid, J */
+  int64_t bytes_device;
+  int32_t levels_L, levels_U;
+} vshe_she_info;
+
+/* 6 * ((L+1)^2)^2 doubles, layout of vshe_coupling_tables.data; no GPU needed. */
+int vshe_coupling_tables_compute(int32_t L, double *out);
+int vshe_she_create(vshe_ctx *ctx, const vshe_device_desc *dev, const vshe_she_config *cfg,
+                    const vshe_coupling_tables *coupling, const vshe_solve_opts *opts, int64_t *handle);
+int vshe_she_info_get(vshe_ctx *ctx, int64_t handle, vshe_she_info *info);
+/* Device assembly with the current potential-independent tables: upto = 1 assembles the
+ * full even+odd system (assemble_all.hpp:46-424), 2 also eliminates the odd unknowns
+ * (eliminate.hpp:80-293), 3 also scales and normalises (rescaling.hpp:50-107,
+ * linalg_util.hpp:202-282) -- the state vshe_she_solve needs. */
+int vshe_she_assemble(vshe_ctx *ctx, int64_t handle, int32_t upto);
+/* ILU(0)/BiCGStab (FP64 or mixed) on the reduced system, on the device. */
+int vshe_she_solve(vshe_ctx *ctx, int64_t handle, vshe_solve_stats *stats);
+/* Unscale, recover the odd unknowns, full-system residual (linear_solver.hpp:172-186,
+ * eliminate.hpp:305-354), carrier density per cell and terminal current per contact
+ * (carrier_density.hpp:68-130, terminal_current.hpp:47-105), on the device. */
+int vshe_she_finish(vshe_ctx *ctx, int64_t handle, double *full_residual);
+/* assemble(3) + solve + finish. */
+int vshe_she_run(vshe_ctx *ctx, int64_t handle, vshe_solve_stats *stats, double *full_residual);
+/* Device-timed throughput of vshe_she_run: `warmup` untimed runs, then `steps` runs each
+ * bracketed by a device synchronisation and timed with CUDA events on the library's
+ * stream; step_ms[k] receives the duration of run k, *last the stats of the last run. */
+int vshe_she_bench(vshe_ctx *ctx, int64_t handle, int32_t warmup, int32_t steps, double *step_ms, vshe_solve_stats *last);
+/* Host copies of the results (any pointer may be NULL): x_full (n_even + n_odd),
+ * density (n_cells), currents (n_contacts). */
+int vshe_she_results(vshe_ctx *ctx, int64_t handle, double *x_full, double *density, double *currents);
+/* Host copy of the current full (which = 0) or reduced (which = 1) system, CSR + rhs. */
+int vshe_she_export(vshe_ctx *ctx, int64_t handle, int32_t which, int64_t *row_ptr, int32_t *col, double *val, double *rhs);
+/* Unknown scaling s and column scale factors of the reduced system (length n_even). */
+int vshe_she_scaling(vshe_ctx *ctx, int64_t handle, double *scaling, double *scale_factors);
+int vshe_she_free(vshe_ctx *ctx, int64_t handle);
 
 #ifdef __cplusplus
 }

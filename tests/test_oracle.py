@@ -154,3 +154,15 @@ def test_ilu0_block_variants_solve():
         assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-8
     x, st = O.csr_solve(A, A.rhs, precond=2, ilut_p=20, ilut_tau=1e-4, tol=1e-12, maxit=5000)
     assert st["rc"] == 0 and np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-8
+
+
+@pytest.mark.parametrize("L", [1, 3, 5, 7])
+def test_library_coupling_quadrature_matches_reference_tables(L):
+    """The library's own quadrature of the coupling integrals (harmonics_coupling.hpp:39-278)
+    against the reference's tabulated literals (harmonics_coupling.hpp:282-1048): same
+    pattern, values within the literals' precision (they carry ~12 digits)."""
+    from vshe import gpu
+    c = gpu.coupling_tables(L)
+    g = O.golden_coupling(L)
+    assert np.array_equal(c.data != 0, g.data != 0)
+    assert np.max(np.abs(c.data - g.data)) < 1e-7

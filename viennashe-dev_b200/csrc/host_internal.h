@@ -17,11 +17,6 @@ namespace vshe {
 
 const char *errstr(int code);
 
-template <typename T>
-using BiStateHost = BiState<T>;
-typedef RefDev RefHost;
-typedef FactDev FactHost;
-
 // Device allocations owned by one object, freed together.
 struct DevArena {
   std::vector<void *> ptrs;
@@ -33,31 +28,52 @@ struct DevArena {
 
 struct Ctx;
 
-// One resident linear system.
+// One resident linear system.  A stays in the caller's order for the SpMV; the
+// incomplete factors belong to P A P^T (P from opts.perm or the ordering) and
+// are stored level by level for the triangular solves.
 struct System {
   int64_t n = 0, nnz = 0;
   vshe_solve_opts opts{};
   bool mixed = true;
-  bool factored = false;
+  bool borrowed = false;  // A and b live in the caller's device memory
+  bool has_pc = true;
   double bnorm_host = 0.0;
-  // host copies of the pattern and schedules
-  std::vector<int64_t> rp, diag, lrp, urp;
-  std::vector<int32_t> ci, blk, lci, uci, levL, levU;
+  // host: pattern, permutation and schedules
+  std::vector<int64_t> rp;
+  std::vector<int32_t> ci;
+  std::vector<int32_t> perm, blk;       // perm[i] = original row of permuted row i; blk in permuted order
+  std::vector<int64_t> prp, pdiag;      // permuted pattern
+  std::vector<int32_t> pci;
+  std::vector<int32_t> levL, levU;      // level of each permuted row
+  std::vector<int64_t> lvlptrL, lvlptrU;// per level, positions in the level-ordered arrays
+  std::vector<int32_t> lrow, urow;      // level-ordered permuted row ids
   int32_t nlevL = 0, nlevU = 0;
+  int64_t nnzL = 0, nnzU = 0;
   int spmv_group = 8, trsv_group = 4;
+  bool identity_perm = true;
   // device
   DevArena arena;
   int64_t *d_rp = nullptr; int32_t *d_ci = nullptr;
   double *d_av64 = nullptr; float *d_av32 = nullptr;
   double *d_b64 = nullptr, *d_x64 = nullptr, *d_r64 = nullptr;
-  double *d_lu64 = nullptr; int64_t *d_diag = nullptr; int32_t *d_blk = nullptr;
-  int64_t *d_lrp = nullptr, *d_urp = nullptr; int32_t *d_lci = nullptr, *d_uci = nullptr;
-  void *d_lv = nullptr, *d_uv = nullptr, *d_dinv = nullptr;
+  int32_t *d_perm = nullptr, *d_blk = nullptr;
+  int64_t *d_prp = nullptr, *d_pdiag = nullptr, *d_amap = nullptr, *d_fmap = nullptr, *d_dpos = nullptr;
+  int32_t *d_pci = nullptr;
+  double *d_lu64 = nullptr;
+  int32_t *d_lrow = nullptr, *d_urow = nullptr, *d_lcol = nullptr, *d_ucol = nullptr;
+  int64_t *d_lptr = nullptr, *d_uptr = nullptr, *d_lvlptrL = nullptr, *d_lvlptrU = nullptr;
+  void *d_lval = nullptr, *d_uval = nullptr, *d_udinv = nullptr, *d_ytmp = nullptr;
   void *kv[9] = {nullptr};  // x r rh p v s t ph sh in the Krylov precision
 
   int create(Ctx &ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *v,
              const double *rhs, const vshe_solve_opts &o);
+  // A system whose CSR and rhs already live on the device (owned by the caller): the host
+  // pattern is used for the schedules, values are read from the device at solve time.
+  int create_borrowed(Ctx &ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, int64_t *d_rp_,
+                      int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o);
+  int refresh_device_values(Ctx &ctx);  // after the borrowed values changed
   int set_values(Ctx &ctx, const double *v, const double *rhs);
+  int setup_pattern(Ctx &ctx);          // ordering, schedules, device buffers
   void fill_sysdev(void *out) const;
 };
 
@@ -76,10 +92,14 @@ struct Batch {
   unsigned *d_bar = nullptr;
   void *d_sysdev = nullptr, *d_state = nullptr, *d_refdev = nullptr, *d_factdev = nullptr;
   int64_t *d_lptrL = nullptr, *d_lptrU = nullptr;
-  int32_t *d_esL = nullptr, *d_erL = nullptr, *d_esU = nullptr, *d_erU = nullptr;
+  int32_t *d_esL = nullptr, *d_erL = nullptr, *d_esU = nullptr, *d_erU = nullptr, *d_efR = nullptr;
   VkTiles tiles{};
-  VkLevels levL{}, levU{};
+  VkLevels levL{}, levU{}, levF{};
   std::vector<char> last_state;
+  // per-kernel-class device time of the last solve (CUDA events), when profiling is on
+  bool profile = false;
+  double t_spmv = 0, t_trsv = 0, t_vec = 0, t_reliable = 0, t_factor = 0;
+  int64_t n_spmv = 0, n_trsv = 0;
 
   int build(Ctx &ctx, const std::vector<System *> &members);
   int factor(Ctx &ctx);
@@ -88,7 +108,7 @@ struct Batch {
   int set_active(Ctx &ctx, const std::vector<int32_t> &act);
   int solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats);
   int check_err(Ctx &ctx, const char *what);
-  int state_of(int k, int32_t &status, int32_t &iter, double &res) const;
+  int state_of(int k, int32_t &status, int32_t &iter, int32_t &nupd, double &res) const;
 };
 
 struct Ctx {
@@ -98,10 +118,19 @@ struct Ctx {
   std::string last_error;
   std::mutex mu;
   int64_t next_handle = 0;
+  bool profile = false;
   std::map<int64_t, std::unique_ptr<System>> systems;
   std::map<std::vector<int64_t>, std::unique_ptr<Batch>> batches;
+  // kernel-class timings of the last profiled solve (ms): spmv, trsv, vector, reliable, factor
+  double prof[5] = {0, 0, 0, 0, 0};
+  int64_t prof_counts[2] = {0, 0};
   int fail(int code, const std::string &msg);
   int cuda_fail(cudaError_t e, const char *what);
 };
 
+// releases the SHE problems of a context (she_pipeline.cpp)
+void she_release_all(Ctx *ctx);
+
 }  // namespace vshe
+
+struct vshe_ctx : public vshe::Ctx {};

@@ -1,10 +1,10 @@
 // host_solver.cpp -- C++ host side of the SHE linear-solve backend.
 //
 // Owns resident systems (CSR on the device, incomplete factors, Krylov
-// vectors), builds their level schedules and tiles, merges several systems
-// into one batch, and drives the batched BiCGStab / FP64 iterative refinement
-// through the thin kernel launchers of kernels.h.  Exposes the public C ABI
-// of include/vshe_gpu.h.
+// vectors), builds their orderings, level schedules and tiles, merges several
+// systems into one batch, and drives the batched BiCGStab (FP64, or FP32 with
+// FP64 reliable updates) through the thin kernel launchers of kernels.h.
+// Exposes the public C ABI of include/vshe_gpu.h.
 //
 // Reference semantics mirrored here:
 //   * input checks of src/solvers/solve.hpp:54-66 (empty rows, non-finite
@@ -24,6 +24,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -79,7 +80,6 @@ static int trsv_group_for(double avg) {
   return 8;
 }
 
-// ---------------------------------------------------------------- DevBuf
 void *DevArena::alloc(size_t bytes, cudaError_t &e) {
   if (bytes == 0) bytes = 16;
   void *p = nullptr;
@@ -93,37 +93,6 @@ void DevArena::release() {
   for (void *p : ptrs) cudaFree(p);
   ptrs.clear();
   total = 0;
-}
-
-// ------------------------------------------------------------- schedules
-// Level of each row in the forward (L) and backward (U) solves of a
-// block-restricted incomplete factorisation with A's pattern.
-static void compute_levels(int64_t n, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci,
-                           const std::vector<int32_t> &blk, std::vector<int32_t> &levL, std::vector<int32_t> &levU,
-                           int32_t &nL, int32_t &nU) {
-  levL.assign(size_t(n), 0);
-  levU.assign(size_t(n), 0);
-  nL = 0; nU = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    int32_t m = -1;
-    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
-      int32_t j = ci[k];
-      if (j >= i) break;
-      if (blk[j] == blk[i] && levL[j] > m) m = levL[j];
-    }
-    levL[i] = m + 1;
-    nL = std::max(nL, m + 2);
-  }
-  for (int64_t i = n - 1; i >= 0; --i) {
-    int32_t m = -1;
-    for (int64_t k = rp[i + 1] - 1; k >= rp[i]; --k) {
-      int32_t j = ci[k];
-      if (j <= i) break;
-      if (blk[j] == blk[i] && levU[j] > m) m = levU[j];
-    }
-    levU[i] = m + 1;
-    nU = std::max(nU, m + 2);
-  }
 }
 
 // ----------------------------------------------------------------- System
@@ -140,7 +109,6 @@ int System::create(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_, const
     if (rp[i + 1] < rp[i]) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "row_ptr not monotone");
     if (rp[i + 1] == rp[i]) return ctx.fail(VSHE_E_EMPTY_ROW, "row " + std::to_string(i));
   }
-  diag.assign(size_t(n), -1);
   for (int64_t i = 0; i < n; ++i) {
     int32_t prev = -1;
     for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
@@ -148,110 +116,48 @@ int System::create(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_, const
       if (j < 0 || j >= n) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "column index out of range");
       if (j <= prev) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "columns not strictly ascending in row " + std::to_string(i));
       prev = j;
-      if (j == i) diag[size_t(i)] = k;
     }
   }
   for (int64_t k = 0; k < nnz; ++k)
     if (!std::isfinite(v[k])) return ctx.fail(VSHE_E_NAN, "matrix entry " + std::to_string(k));
   for (int64_t i = 0; i < n; ++i)
     if (!std::isfinite(rhs[i])) return ctx.fail(VSHE_E_NAN, "rhs entry " + std::to_string(i));
-
-  const bool has_pc = opts.precond != VSHE_PRECOND_NONE;
-  if (has_pc)
-    for (int64_t i = 0; i < n; ++i)
-      if (diag[size_t(i)] < 0) return ctx.fail(VSHE_E_ZERO_PIVOT, "no diagonal entry in row " + std::to_string(i));
-
-  // block ids
-  blk.assign(size_t(n), 0);
-  if (opts.precond == VSHE_PRECOND_BLOCK_ILU0 && opts.n_blocks > 0 && opts.block_ptr) {
-    const int64_t *bp = opts.block_ptr;
-    if (bp[0] != 0 || bp[opts.n_blocks] != n) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "block_ptr must span [0, n]");
-    for (int64_t b = 0; b < opts.n_blocks; ++b) {
-      if (bp[b + 1] < bp[b]) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "block_ptr not monotone");
-      for (int64_t i = bp[b]; i < bp[b + 1]; ++i) blk[size_t(i)] = int32_t(b);
-    }
-  }
-  // factor patterns and level schedules
-  if (has_pc) {
-    compute_levels(n, rp, ci, blk, levL, levU, nlevL, nlevU);
-    lrp.assign(size_t(n) + 1, 0);
-    urp.assign(size_t(n) + 1, 0);
-    for (int64_t i = 0; i < n; ++i) {
-      int64_t nl = 0, nu = 0;
-      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
-        int32_t j = ci[k];
-        if (j == i || blk[j] != blk[i]) continue;
-        if (j < i) ++nl; else ++nu;
-      }
-      lrp[i + 1] = lrp[i] + nl;
-      urp[i + 1] = urp[i] + nu;
-    }
-    lci.resize(size_t(lrp[n]));
-    uci.resize(size_t(urp[n]));
-    for (int64_t i = 0; i < n; ++i) {
-      int64_t lp = lrp[i], up = urp[i];
-      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
-        int32_t j = ci[k];
-        if (j == i || blk[j] != blk[i]) continue;
-        if (j < i) lci[size_t(lp++)] = j; else uci[size_t(up++)] = j;
-      }
-    }
-  }
-  mixed = opts.precision == VSHE_PRECISION_MIXED;
-  spmv_group = group_for(double(nnz) / double(n));
-  trsv_group = has_pc ? trsv_group_for(double(lrp[n] + urp[n]) / (2.0 * double(n))) : 1;
-
-  // ---- device buffers ----
   cudaError_t e;
-#define ALLOC(ptr, type, count)                                              \
-  ptr = (type *)arena.alloc(sizeof(type) * size_t(count), e);               \
-  if (!ptr) return ctx.cuda_fail(e, "cudaMalloc " #ptr);
-  ALLOC(d_rp, int64_t, n + 1);
-  ALLOC(d_ci, int32_t, nnz);
-  ALLOC(d_av64, double, nnz);
-  ALLOC(d_b64, double, n);
-  ALLOC(d_x64, double, n);
-  ALLOC(d_r64, double, n);
-  ALLOC(d_blk, int32_t, n);
-  if (mixed) { ALLOC(d_av32, float, nnz); }
-  const size_t tsz = mixed ? sizeof(float) : sizeof(double);
-  for (int k = 0; k < 9; ++k) {
-    kv[k] = arena.alloc(tsz * size_t(n), e);
-    if (!kv[k]) return ctx.cuda_fail(e, "cudaMalloc krylov");
-  }
-  if (has_pc) {
-    ALLOC(d_lu64, double, nnz);
-    ALLOC(d_diag, int64_t, n);
-    ALLOC(d_lrp, int64_t, n + 1);
-    ALLOC(d_urp, int64_t, n + 1);
-    ALLOC(d_lci, int32_t, std::max<int64_t>(lrp[n], 1));
-    ALLOC(d_uci, int32_t, std::max<int64_t>(urp[n], 1));
-    d_lv = arena.alloc(tsz * size_t(std::max<int64_t>(lrp[n], 1)), e);
-    if (!d_lv) return ctx.cuda_fail(e, "cudaMalloc lv");
-    d_uv = arena.alloc(tsz * size_t(std::max<int64_t>(urp[n], 1)), e);
-    if (!d_uv) return ctx.cuda_fail(e, "cudaMalloc uv");
-    d_dinv = arena.alloc(tsz * size_t(n), e);
-    if (!d_dinv) return ctx.cuda_fail(e, "cudaMalloc dinv");
-  }
-#undef ALLOC
-  cudaStream_t s = ctx.stream;
-#define H2D(dst, src, bytes)                                                             \
-  if ((e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) \
-    return ctx.cuda_fail(e, "upload " #dst);
-  H2D(d_rp, rp.data(), sizeof(int64_t) * size_t(n + 1));
-  H2D(d_ci, ci.data(), sizeof(int32_t) * size_t(nnz));
-  H2D(d_blk, blk.data(), sizeof(int32_t) * size_t(n));
-  if (has_pc) {
-    H2D(d_diag, diag.data(), sizeof(int64_t) * size_t(n));
-    H2D(d_lrp, lrp.data(), sizeof(int64_t) * size_t(n + 1));
-    H2D(d_urp, urp.data(), sizeof(int64_t) * size_t(n + 1));
-    if (lrp[n]) H2D(d_lci, lci.data(), sizeof(int32_t) * size_t(lrp[n]));
-    if (urp[n]) H2D(d_uci, uci.data(), sizeof(int32_t) * size_t(urp[n]));
-  }
-#undef H2D
-  int rc = set_values(ctx, v, rhs);
+  d_rp = (int64_t *)arena.alloc(sizeof(int64_t) * size_t(n + 1), e);
+  if (!d_rp) return ctx.cuda_fail(e, "cudaMalloc rp");
+  d_ci = (int32_t *)arena.alloc(sizeof(int32_t) * size_t(nnz), e);
+  if (!d_ci) return ctx.cuda_fail(e, "cudaMalloc ci");
+  d_av64 = (double *)arena.alloc(sizeof(double) * size_t(nnz), e);
+  if (!d_av64) return ctx.cuda_fail(e, "cudaMalloc values");
+  d_b64 = (double *)arena.alloc(sizeof(double) * size_t(n), e);
+  if (!d_b64) return ctx.cuda_fail(e, "cudaMalloc rhs");
+  if ((e = cudaMemcpyAsync(d_rp, rp.data(), sizeof(int64_t) * rp.size(), cudaMemcpyHostToDevice, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "upload rp");
+  if ((e = cudaMemcpyAsync(d_ci, ci.data(), sizeof(int32_t) * ci.size(), cudaMemcpyHostToDevice, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "upload ci");
+  int rc = setup_pattern(ctx);
   if (rc) return rc;
-  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx.cuda_fail(e, "upload");
+  rc = set_values(ctx, v, rhs);
+  if (rc) return rc;
+  if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "upload");
+  return VSHE_OK;
+}
+
+int System::create_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_, const int32_t *ci_, int64_t *d_rp_,
+                            int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o) {
+  n = n_; nnz = nnz_; opts = o; borrowed = true;
+  if (n <= 0 || nnz <= 0) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "empty system");
+  rp.assign(rp_, rp_ + n + 1);
+  ci.assign(ci_, ci_ + nnz);
+  for (int64_t i = 0; i < n; ++i)
+    if (rp[i + 1] == rp[i]) return ctx.fail(VSHE_E_EMPTY_ROW, "row " + std::to_string(i));
+  d_rp = d_rp_; d_ci = d_ci_; d_av64 = d_val; d_b64 = d_rhs;
+  int rc = setup_pattern(ctx);
+  if (rc) return rc;
+  bnorm_host = 1.0;  // the trivial-rhs test uses the device-side norm
+  return refresh_device_values(ctx);
+}
+
+int System::refresh_device_values(Ctx &ctx) {
+  if (mixed) vk_cast_f64_f32(nnz, d_av64, d_av32, ctx.stream);
   return VSHE_OK;
 }
 
@@ -268,22 +174,265 @@ int System::set_values(Ctx &ctx, const double *v, const double *rhs) {
   bnorm_host = std::sqrt(bnorm_host);
   if ((e = cudaMemcpyAsync(d_av64, v, sizeof(double) * size_t(nnz), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "upload values");
   if ((e = cudaMemcpyAsync(d_b64, rhs, sizeof(double) * size_t(n), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "upload rhs");
-  if (mixed) vk_cast_f64_f32(nnz, d_av64, d_av32, s);
-  factored = false;
+  return refresh_device_values(ctx);
+}
+
+// greedy colouring of the symmetrised pattern, rows grouped by block
+static void greedy_colours(int64_t n, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci, const std::vector<int32_t> &blk,
+                           std::vector<int32_t> &col) {
+  std::vector<int64_t> tcnt((size_t)(n) + 1, 0);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tcnt[size_t(ci[k]) + 1]++;
+  for (int64_t i = 0; i < n; ++i) tcnt[size_t(i) + 1] += tcnt[size_t(i)];
+  std::vector<int32_t> tci(size_t(tcnt[size_t(n)]));
+  std::vector<int64_t> pos(tcnt.begin(), tcnt.end() - 1);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tci[size_t(pos[size_t(ci[k])]++)] = int32_t(i);
+  col.assign(size_t(n), -1);
+  std::vector<int64_t> mark(64, -1);
+  for (int64_t i = 0; i < n; ++i) {
+    auto visit = [&](int32_t j) {
+      if (j == i || col[size_t(j)] < 0 || blk[size_t(j)] != blk[size_t(i)]) return;
+      int32_t c = col[size_t(j)];
+      if (c >= int32_t(mark.size())) mark.resize(size_t(c) + 1, -1);
+      mark[size_t(c)] = i;
+    };
+    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) visit(ci[k]);
+    for (int64_t k = tcnt[size_t(i)]; k < tcnt[size_t(i) + 1]; ++k) visit(tci[size_t(k)]);
+    int32_t c = 0;
+    while (c < int32_t(mark.size()) && mark[size_t(c)] == i) ++c;
+    col[size_t(i)] = c;
+  }
+}
+
+int System::setup_pattern(Ctx &ctx) {
+  has_pc = opts.precond != VSHE_PRECOND_NONE;
+  mixed = opts.precision == VSHE_PRECISION_MIXED;
+  cudaError_t e;
+  // block ids in the original order
+  std::vector<int32_t> blk0((size_t)(n), 0);
+  if (opts.precond == VSHE_PRECOND_BLOCK_ILU0 && opts.n_blocks > 0 && opts.block_ptr) {
+    const int64_t *bp = opts.block_ptr;
+    if (bp[0] != 0 || bp[opts.n_blocks] != n) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "block_ptr must span [0, n]");
+    for (int64_t b = 0; b < opts.n_blocks; ++b) {
+      if (bp[b + 1] < bp[b]) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "block_ptr not monotone");
+      for (int64_t i = bp[b]; i < bp[b + 1]; ++i) blk0[size_t(i)] = int32_t(b);
+    }
+  }
+  // ordering
+  perm.resize(size_t(n));
+  if (opts.perm) {
+    std::vector<char> seen((size_t)(n), 0);
+    for (int64_t i = 0; i < n; ++i) {
+      int32_t o = opts.perm[i];
+      if (o < 0 || o >= n || seen[size_t(o)]) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "perm is not a permutation");
+      seen[size_t(o)] = 1;
+      perm[size_t(i)] = o;
+    }
+  } else if (has_pc && opts.ordering == VSHE_ORDER_MULTICOLOR) {
+    std::vector<int32_t> col;
+    greedy_colours(n, rp, ci, blk0, col);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) {
+      if (blk0[size_t(a)] != blk0[size_t(b)]) return blk0[size_t(a)] < blk0[size_t(b)];
+      return col[size_t(a)] < col[size_t(b)];
+    });
+  } else {
+    std::iota(perm.begin(), perm.end(), 0);
+  }
+  identity_perm = true;
+  for (int64_t i = 0; i < n; ++i) if (perm[size_t(i)] != i) { identity_perm = false; break; }
+  std::vector<int32_t> inv((size_t)(n));
+  for (int64_t i = 0; i < n; ++i) inv[size_t(perm[size_t(i)])] = int32_t(i);
+  blk.resize(size_t(n));
+  for (int64_t i = 0; i < n; ++i) blk[size_t(i)] = blk0[size_t(perm[size_t(i)])];
+
+  std::vector<int64_t> amap, fmap, dpos, lptr, uptr;
+  std::vector<int32_t> lcol, ucol;
+  if (has_pc) {
+    // permuted pattern P A P^T with the map back to A's entries
+    prp.assign(size_t(n) + 1, 0);
+    pci.resize(size_t(nnz));
+    amap.resize(size_t(nnz));
+    pdiag.assign(size_t(n), -1);
+    std::vector<std::pair<int32_t, int64_t>> row;
+    for (int64_t i = 0; i < n; ++i) {
+      const int64_t o = perm[size_t(i)];
+      row.clear();
+      for (int64_t k = rp[o]; k < rp[o + 1]; ++k) row.push_back({inv[size_t(ci[k])], k});
+      std::sort(row.begin(), row.end());
+      int64_t p = prp[size_t(i)];
+      for (auto &x : row) {
+        if (x.first == i) pdiag[size_t(i)] = p;
+        pci[size_t(p)] = x.first;
+        amap[size_t(p)] = x.second;
+        ++p;
+      }
+      prp[size_t(i) + 1] = p;
+      if (pdiag[size_t(i)] < 0) return ctx.fail(VSHE_E_ZERO_PIVOT, "no diagonal entry in row " + std::to_string(o));
+    }
+    // levels of the forward / backward solves (block-restricted)
+    levL.assign(size_t(n), 0);
+    levU.assign(size_t(n), 0);
+    nlevL = nlevU = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      int32_t m = -1;
+      for (int64_t k = prp[size_t(i)]; k < pdiag[size_t(i)]; ++k) {
+        int32_t j = pci[size_t(k)];
+        if (blk[size_t(j)] == blk[size_t(i)] && levL[size_t(j)] > m) m = levL[size_t(j)];
+      }
+      levL[size_t(i)] = m + 1;
+      nlevL = std::max(nlevL, m + 2);
+    }
+    for (int64_t i = n - 1; i >= 0; --i) {
+      int32_t m = -1;
+      for (int64_t k = pdiag[size_t(i)] + 1; k < prp[size_t(i) + 1]; ++k) {
+        int32_t j = pci[size_t(k)];
+        if (blk[size_t(j)] == blk[size_t(i)] && levU[size_t(j)] > m) m = levU[size_t(j)];
+      }
+      levU[size_t(i)] = m + 1;
+      nlevU = std::max(nlevU, m + 2);
+    }
+    // level-ordered rows (stable: by level, then row)
+    auto order = [&](const std::vector<int32_t> &lev, int32_t nl, std::vector<int64_t> &lvp, std::vector<int32_t> &rows) {
+      lvp.assign(size_t(nl) + 1, 0);
+      for (int32_t l : lev) lvp[size_t(l) + 1]++;
+      for (size_t k = 1; k < lvp.size(); ++k) lvp[k] += lvp[k - 1];
+      rows.resize(size_t(n));
+      std::vector<int64_t> cur(lvp.begin(), lvp.end() - 1);
+      for (int64_t i = 0; i < n; ++i) rows[size_t(cur[size_t(lev[size_t(i)])]++)] = int32_t(i);
+    };
+    order(levL, nlevL, lvlptrL, lrow);
+    order(levU, nlevU, lvlptrU, urow);
+    fmap.assign(size_t(nnz), -1);
+    lptr.assign(size_t(n) + 1, 0);
+    uptr.assign(size_t(n) + 1, 0);
+    dpos.resize(size_t(n));
+    for (int64_t q = 0; q < n; ++q) {
+      const int32_t r = lrow[size_t(q)];
+      int64_t c = 0;
+      for (int64_t k = prp[size_t(r)]; k < pdiag[size_t(r)]; ++k)
+        if (blk[size_t(pci[size_t(k)])] == blk[size_t(r)]) ++c;
+      lptr[size_t(q) + 1] = lptr[size_t(q)] + c;
+    }
+    nnzL = lptr[size_t(n)];
+    lcol.resize(size_t(nnzL));
+    for (int64_t q = 0; q < n; ++q) {
+      const int32_t r = lrow[size_t(q)];
+      int64_t p = lptr[size_t(q)];
+      for (int64_t k = prp[size_t(r)]; k < pdiag[size_t(r)]; ++k) {
+        const int32_t j = pci[size_t(k)];
+        if (blk[size_t(j)] != blk[size_t(r)]) continue;
+        lcol[size_t(p)] = j;
+        fmap[size_t(k)] = p;
+        ++p;
+      }
+    }
+    for (int64_t q = 0; q < n; ++q) {
+      const int32_t r = urow[size_t(q)];
+      dpos[size_t(r)] = q;
+      int64_t c = 0;
+      for (int64_t k = pdiag[size_t(r)] + 1; k < prp[size_t(r) + 1]; ++k)
+        if (blk[size_t(pci[size_t(k)])] == blk[size_t(r)]) ++c;
+      uptr[size_t(q) + 1] = uptr[size_t(q)] + c;
+    }
+    nnzU = uptr[size_t(n)];
+    ucol.resize(size_t(nnzU));
+    for (int64_t q = 0; q < n; ++q) {
+      const int32_t r = urow[size_t(q)];
+      int64_t p = uptr[size_t(q)];
+      for (int64_t k = pdiag[size_t(r)] + 1; k < prp[size_t(r) + 1]; ++k) {
+        const int32_t j = pci[size_t(k)];
+        if (blk[size_t(j)] != blk[size_t(r)]) continue;
+        ucol[size_t(p)] = j;
+        fmap[size_t(k)] = -(p + 2);
+        ++p;
+      }
+    }
+  }
+  spmv_group = group_for(double(nnz) / double(n));
+  trsv_group = has_pc ? trsv_group_for(double(nnzL + nnzU) / (2.0 * double(n))) : 1;
+
+  // ---- device buffers ----
+  const size_t tsz = mixed ? sizeof(float) : sizeof(double);
+#define ALLOC(ptr, type, count)                                              \
+  ptr = (type *)arena.alloc(sizeof(type) * size_t(count), e);               \
+  if (!ptr) return ctx.cuda_fail(e, "cudaMalloc " #ptr);
+#define ALLOCT(ptr, count)                                                   \
+  ptr = arena.alloc(tsz * size_t(count), e);                                 \
+  if (!ptr) return ctx.cuda_fail(e, "cudaMalloc " #ptr);
+  ALLOC(d_x64, double, n);
+  ALLOC(d_r64, double, n);
+  if (mixed) { ALLOC(d_av32, float, nnz); }
+  for (int k = 0; k < 9; ++k) { ALLOCT(kv[k], n); }
+  if (has_pc) {
+    ALLOC(d_blk, int32_t, n);
+    ALLOC(d_prp, int64_t, n + 1);
+    ALLOC(d_pci, int32_t, nnz);
+    ALLOC(d_pdiag, int64_t, n);
+    ALLOC(d_amap, int64_t, nnz);
+    ALLOC(d_fmap, int64_t, nnz);
+    ALLOC(d_dpos, int64_t, n);
+    ALLOC(d_lu64, double, nnz);
+    ALLOC(d_lrow, int32_t, n);
+    ALLOC(d_urow, int32_t, n);
+    ALLOC(d_lptr, int64_t, n + 1);
+    ALLOC(d_uptr, int64_t, n + 1);
+    ALLOC(d_lvlptrL, int64_t, nlevL + 1);
+    ALLOC(d_lvlptrU, int64_t, nlevU + 1);
+    ALLOC(d_lcol, int32_t, std::max<int64_t>(nnzL, 1));
+    ALLOC(d_ucol, int32_t, std::max<int64_t>(nnzU, 1));
+    ALLOCT(d_lval, std::max<int64_t>(nnzL, 1));
+    ALLOCT(d_uval, std::max<int64_t>(nnzU, 1));
+    ALLOCT(d_udinv, n);
+    ALLOCT(d_ytmp, n);
+    if (!identity_perm) { ALLOC(d_perm, int32_t, n); }
+  }
+#undef ALLOC
+#undef ALLOCT
+  cudaStream_t s = ctx.stream;
+#define H2D(dst, vec)                                                                                        \
+  if (!vec.empty() && (e = cudaMemcpyAsync(dst, vec.data(), sizeof(vec[0]) * vec.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess) \
+    return ctx.cuda_fail(e, "upload " #dst);
+  if (has_pc) {
+    H2D(d_blk, blk);
+    H2D(d_prp, prp);
+    H2D(d_pci, pci);
+    H2D(d_pdiag, pdiag);
+    H2D(d_amap, amap);
+    H2D(d_fmap, fmap);
+    H2D(d_dpos, dpos);
+    H2D(d_lrow, lrow);
+    H2D(d_urow, urow);
+    H2D(d_lptr, lptr);
+    H2D(d_uptr, uptr);
+    H2D(d_lvlptrL, lvlptrL);
+    H2D(d_lvlptrU, lvlptrU);
+    H2D(d_lcol, lcol);
+    H2D(d_ucol, ucol);
+    if (!identity_perm) { H2D(d_perm, perm); }
+  }
+#undef H2D
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx.cuda_fail(e, "upload pattern");
+  // the permuted host pattern is only needed to build the device tables
+  prp.clear(); prp.shrink_to_fit(); pci.clear(); pci.shrink_to_fit();
   return VSHE_OK;
 }
 
 void System::fill_sysdev(void *out) const {
   // SysDev<T> has the same layout for both T (pointers); fill through the float view
   SysDev<float> d;
+  std::memset(&d, 0, sizeof(d));
   d.n = n;
   d.rp = d_rp; d.ci = d_ci;
   d.av = mixed ? d_av32 : (const float *)d_av64;
-  d.lrp = d_lrp; d.lci = d_lci; d.lv = (const float *)d_lv;
-  d.urp = d_urp; d.uci = d_uci; d.uv = (const float *)d_uv;
-  d.dinv = (const float *)d_dinv;
+  d.perm = identity_perm ? nullptr : d_perm;
+  d.lrow = d_lrow; d.lptr = d_lptr; d.lcol = d_lcol; d.lval = (const float *)d_lval;
+  d.urow = d_urow; d.uptr = d_uptr; d.ucol = d_ucol; d.uval = (const float *)d_uval; d.udinv = (const float *)d_udinv;
+  d.ytmp = (float *)d_ytmp;
   d.x = (float *)kv[0]; d.r = (float *)kv[1]; d.rh = (float *)kv[2]; d.p = (float *)kv[3];
   d.v = (float *)kv[4]; d.s = (float *)kv[5]; d.t = (float *)kv[6]; d.ph = (float *)kv[7]; d.sh = (float *)kv[8];
+  d.av64 = d_av64; d.b64 = d_b64; d.x64 = d_x64; d.r64 = d_r64;
   std::memcpy(out, &d, sizeof(d));
 }
 
@@ -292,12 +441,10 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   sys = members;
   nsys = int(sys.size());
   mixed = sys[0]->mixed;
-  has_pc = sys[0]->opts.precond != VSHE_PRECOND_NONE;
-  for (System *S : sys) {
-    if (S->mixed != mixed || (S->opts.precond != VSHE_PRECOND_NONE) != has_pc)
+  has_pc = sys[0]->has_pc;
+  for (System *S : sys)
+    if (S->mixed != mixed || S->has_pc != has_pc)
       return ctx.fail(VSHE_E_INVALID_ARGUMENT, "systems in one batch need the same precision and preconditioner kind");
-  }
-  // tiles
   const int64_t TILE = 2048;
   std::vector<int32_t> tsys, st0;
   std::vector<int64_t> tr0, tr1;
@@ -311,35 +458,39 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   }
   st0.push_back(int32_t(tsys.size()));
   ntiles = int(tsys.size());
-  // merged level schedules
+  // merged level schedules: trsv entries are level-ordered positions, factorisation entries row ids
   std::vector<int64_t> lptrL, lptrU;
-  std::vector<int32_t> esL, erL, esU, erU;
-  if (has_pc) {
-    auto merge = [&](bool lower, std::vector<int64_t> &lptr, std::vector<int32_t> &es, std::vector<int32_t> &er, int32_t &nlev) {
-      nlev = 0;
-      for (System *S : sys) nlev = std::max(nlev, lower ? S->nlevL : S->nlevU);
-      std::vector<int64_t> cnt(size_t(nlev) + 1, 0);
-      for (System *S : sys) {
-        const auto &lev = lower ? S->levL : S->levU;
-        for (int32_t l : lev) cnt[size_t(l) + 1]++;
-      }
-      for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
-      lptr = cnt;
-      int64_t total = cnt.back();
-      es.resize(size_t(total));
-      er.resize(size_t(total));
-      std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
-      for (int s = 0; s < nsys; ++s) {
-        const auto &lev = lower ? sys[s]->levL : sys[s]->levU;
-        if (lower) {
-          for (int64_t i = 0; i < sys[s]->n; ++i) { int64_t p = pos[size_t(lev[size_t(i)])]++; es[size_t(p)] = s; er[size_t(p)] = int32_t(i); }
-        } else {
-          for (int64_t i = sys[s]->n - 1; i >= 0; --i) { int64_t p = pos[size_t(lev[size_t(i)])]++; es[size_t(p)] = s; er[size_t(p)] = int32_t(i); }
+  std::vector<int32_t> esL, erL, esU, erU, efR;
+  if (has_pc && nsys > 1) {
+    auto merge = [&](bool lower, std::vector<int64_t> &lptr, std::vector<int32_t> &es, std::vector<int32_t> &er, int32_t &nl) {
+      nl = 0;
+      for (System *S : sys) nl = std::max(nl, lower ? S->nlevL : S->nlevU);
+      lptr.assign(size_t(nl) + 1, 0);
+      for (int32_t l = 0; l < nl; ++l) {
+        int64_t c = 0;
+        for (System *S : sys) {
+          const auto &vp = lower ? S->lvlptrL : S->lvlptrU;
+          if (l + 1 < int32_t(vp.size())) c += vp[size_t(l) + 1] - vp[size_t(l)];
         }
+        lptr[size_t(l) + 1] = lptr[size_t(l)] + c;
       }
+      es.resize(size_t(lptr.back()));
+      er.resize(size_t(lptr.back()));
+      int64_t p = 0;
+      for (int32_t l = 0; l < nl; ++l)
+        for (int s = 0; s < nsys; ++s) {
+          const auto &vp = lower ? sys[s]->lvlptrL : sys[s]->lvlptrU;
+          if (l + 1 >= int32_t(vp.size())) continue;
+          for (int64_t q = vp[size_t(l)]; q < vp[size_t(l) + 1]; ++q) { es[size_t(p)] = s; er[size_t(p)] = int32_t(q); ++p; }
+        }
     };
     merge(true, lptrL, esL, erL, nlevL);
     merge(false, lptrU, esU, erU, nlevU);
+    efR.resize(erL.size());
+    for (size_t e = 0; e < erL.size(); ++e) efR[e] = sys[size_t(esL[e])]->lrow[size_t(erL[e])];
+  } else if (has_pc) {
+    nlevL = sys[0]->nlevL;
+    nlevU = sys[0]->nlevU;
   }
   cudaError_t e;
 #define ALLOC(ptr, type, count)                                              \
@@ -364,13 +515,14 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   if (!d_refdev) return ctx.cuda_fail(e, "cudaMalloc refdev");
   d_factdev = arena.alloc(vk_factdev_size() * size_t(nsys), e);
   if (!d_factdev) return ctx.cuda_fail(e, "cudaMalloc factdev");
-  if (has_pc) {
+  if (has_pc && nsys > 1) {
     ALLOC(d_lptrL, int64_t, lptrL.size());
     ALLOC(d_lptrU, int64_t, lptrU.size());
     ALLOC(d_esL, int32_t, std::max<size_t>(esL.size(), 1));
     ALLOC(d_erL, int32_t, std::max<size_t>(erL.size(), 1));
     ALLOC(d_esU, int32_t, std::max<size_t>(esU.size(), 1));
     ALLOC(d_erU, int32_t, std::max<size_t>(erU.size(), 1));
+    ALLOC(d_efR, int32_t, std::max<size_t>(efR.size(), 1));
   }
 #undef ALLOC
   cudaStream_t s = ctx.stream;
@@ -378,13 +530,14 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   std::vector<char> rd(vk_refdev_size() * size_t(nsys));
   std::vector<char> fd(vk_factdev_size() * size_t(nsys));
   for (int k = 0; k < nsys; ++k) {
-    sys[k]->fill_sysdev(sd.data() + vk_sysdev_size_f32() * size_t(k));
-    RefHost r{sys[k]->n, sys[k]->d_rp, sys[k]->d_ci, sys[k]->d_av64, sys[k]->d_b64, sys[k]->d_x64, sys[k]->d_r64};
+    System *S = sys[size_t(k)];
+    S->fill_sysdev(sd.data() + vk_sysdev_size_f32() * size_t(k));
+    RefDev r{S->n, S->d_rp, S->d_ci, S->d_av64, S->d_b64, S->d_x64, S->d_r64};
     std::memcpy(rd.data() + vk_refdev_size() * size_t(k), &r, sizeof(r));
-    FactHost f{sys[k]->n, sys[k]->d_rp, sys[k]->d_ci, sys[k]->d_lu64, sys[k]->d_diag, sys[k]->d_blk};
+    FactDev f{S->n, S->d_prp, S->d_pci, S->d_lu64, S->d_pdiag, S->d_blk};
     std::memcpy(fd.data() + vk_factdev_size() * size_t(k), &f, sizeof(f));
   }
-  std::vector<int32_t> ones(size_t(nsys), 1), zeros(size_t(nsys), 0);
+  std::vector<int32_t> ones((size_t)(nsys), 1), zeros(size_t(nsys), 0);
 #define H2D(dst, src, bytes)                                                             \
   if ((e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) \
     return ctx.cuda_fail(e, "upload batch " #dst);
@@ -397,21 +550,30 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   H2D(d_sysdev, sd.data(), sd.size());
   H2D(d_refdev, rd.data(), rd.size());
   H2D(d_factdev, fd.data(), fd.size());
-  if (has_pc) {
+  if (has_pc && nsys > 1) {
     H2D(d_lptrL, lptrL.data(), sizeof(int64_t) * lptrL.size());
     H2D(d_lptrU, lptrU.data(), sizeof(int64_t) * lptrU.size());
-    if (!esL.empty()) { H2D(d_esL, esL.data(), sizeof(int32_t) * esL.size()); H2D(d_erL, erL.data(), sizeof(int32_t) * erL.size()); }
+    if (!esL.empty()) { H2D(d_esL, esL.data(), sizeof(int32_t) * esL.size()); H2D(d_erL, erL.data(), sizeof(int32_t) * erL.size()); H2D(d_efR, efR.data(), sizeof(int32_t) * efR.size()); }
     if (!esU.empty()) { H2D(d_esU, esU.data(), sizeof(int32_t) * esU.size()); H2D(d_erU, erU.data(), sizeof(int32_t) * erU.size()); }
   }
 #undef H2D
   if ((e = cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   if ((e = cudaMemsetAsync(d_err, 0, sizeof(int32_t), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+  if ((e = cudaMemsetAsync(d_state, 0, vk_bistate_size_f64() * size_t(nsys), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   tiles = VkTiles{ntiles, d_tile_sys, d_tile_r0, d_tile_r1, d_sys_tile0};
-  levL = VkLevels{nlevL, d_lptrL, nsys > 1 ? d_esL : nullptr, d_erL};
-  levU = VkLevels{nlevU, d_lptrU, nsys > 1 ? d_esU : nullptr, d_erU};
-  // execution shapes
+  if (has_pc) {
+    if (nsys > 1) {
+      levL = VkLevels{nlevL, d_lptrL, d_esL, d_erL};
+      levU = VkLevels{nlevU, d_lptrU, d_esU, d_erU};
+      levF = VkLevels{nlevL, d_lptrL, d_esL, d_efR};
+    } else {
+      levL = VkLevels{nlevL, sys[0]->d_lvlptrL, nullptr, nullptr};
+      levU = VkLevels{nlevU, sys[0]->d_lvlptrU, nullptr, nullptr};
+      levF = VkLevels{nlevL, sys[0]->d_lvlptrL, nullptr, sys[0]->d_lrow};
+    }
+  }
   int64_t tot_nnz = 0, tot_n = 0, tot_lu = 0;
-  for (System *S : sys) { tot_nnz += S->nnz; tot_n += S->n; if (has_pc) tot_lu += S->lrp[S->n] + S->urp[S->n]; }
+  for (System *S : sys) { tot_nnz += S->nnz; tot_n += S->n; tot_lu += S->nnzL + S->nnzU; }
   spmv_group = group_for(double(tot_nnz) / double(tot_n));
   trsv_group = has_pc ? trsv_group_for(double(tot_lu) / (2.0 * double(tot_n))) : 1;
   int dev = 0;
@@ -419,10 +581,12 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
   int bps = 0;
   if (mixed) vk_trsv_occupancy_f32(trsv_group, &bps); else vk_trsv_occupancy_f64(trsv_group, &bps);
-  trsv_grid = std::max(1, bps) * num_sms;
+  trsv_grid = std::max(1, std::min(bps, 4)) * num_sms;
   int bpf = 0;
   vk_ilu0_occupancy(&bpf);
-  ilu_grid = std::max(1, bpf) * num_sms;
+  ilu_grid = std::max(1, std::min(bpf, 4)) * num_sms;
+  cudaError_t es = cudaStreamSynchronize(s);
+  if (es != cudaSuccess) return ctx.cuda_fail(es, "batch upload");
   return VSHE_OK;
 }
 
@@ -442,73 +606,126 @@ int Batch::check_err(Ctx &ctx, const char *what) {
 int Batch::factor(Ctx &ctx) {
   if (!has_pc) return VSHE_OK;
   cudaStream_t s = ctx.stream;
-  cudaError_t e;
-  for (System *S : sys)
-    if ((e = cudaMemcpyAsync(S->d_lu64, S->d_av64, sizeof(double) * size_t(S->nnz), cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
-      return ctx.cuda_fail(e, "copy factor values");
+  for (System *S : sys) vk_gather_values(S->nnz, S->d_amap, S->d_av64, S->d_lu64, s);
   const int mode = (sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) ? 2 : 1;
-  int rc = vk_ilu0(mode, mode == 1 ? ilu_grid : std::max(1, num_sms * 8), d_factdev, &levL, d_bar, d_err, s);
+  int rc = vk_ilu0(mode, mode == 1 ? ilu_grid : std::max(1, num_sms * 8), d_factdev, &levF, d_bar, d_err, s);
   if (rc) return ctx.cuda_fail(cudaError_t(rc), "ilu0 launch");
   for (System *S : sys) {
     if (mixed)
-      vk_split_factor_f32(S->n, S->d_rp, S->d_ci, S->d_lu64, S->d_blk, S->d_lrp, (float *)S->d_lv, S->d_urp, (float *)S->d_uv, (float *)S->d_dinv, s);
+      vk_split_factor_f32(S->nnz, S->n, S->d_lu64, S->d_fmap, S->d_pdiag, S->d_dpos, (float *)S->d_lval, (float *)S->d_uval, (float *)S->d_udinv, s);
     else
-      vk_split_factor_f64(S->n, S->d_rp, S->d_ci, S->d_lu64, S->d_blk, S->d_lrp, (double *)S->d_lv, S->d_urp, (double *)S->d_uv, (double *)S->d_dinv, s);
+      vk_split_factor_f64(S->nnz, S->n, S->d_lu64, S->d_fmap, S->d_pdiag, S->d_dpos, (double *)S->d_lval, (double *)S->d_uval, (double *)S->d_udinv, s);
   }
-  rc = check_err(ctx, "ilu0 factorisation");
-  if (rc) return rc;
-  for (System *S : sys) S->factored = true;
-  return VSHE_OK;
+  return check_err(ctx, "ilu0 factorisation");
 }
 
-// One BiCGStab solve on every active system, rhs in r (precision of the batch),
-// to relative tolerance `tol`.  Returns the total iterations of the slowest system.
+// A small pool of CUDA events for the per-kernel-class timing of a profiled solve.
+struct EventProf {
+  bool on = false;
+  cudaStream_t s = nullptr;
+  std::vector<cudaEvent_t> pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> recs;
+  size_t used = 0;
+  cudaEvent_t get() {
+    if (used == pool.size()) { cudaEvent_t e; cudaEventCreate(&e); pool.push_back(e); }
+    return pool[used++];
+  }
+  cudaEvent_t begin() {
+    if (!on) return nullptr;
+    cudaEvent_t a = get();
+    cudaEventRecord(a, s);
+    return a;
+  }
+  void end(int cls, cudaEvent_t a) {
+    if (!on) return;
+    cudaEvent_t b = get();
+    cudaEventRecord(b, s);
+    recs.push_back({cls, {a, b}});
+  }
+  void collect(double *out, int64_t *counts) {
+    for (auto &r : recs) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, r.second.first, r.second.second);
+      out[r.first] += ms;
+      if (r.first < 2) counts[r.first] += 1;
+    }
+    recs.clear();
+    used = 0;
+  }
+  ~EventProf() { for (auto e : pool) cudaEventDestroy(e); }
+};
+static thread_local EventProf g_prof;
+
+// BiCGStab on every active system to relative tolerance `tol` (FP64), or with
+// FP32 recurrences and FP64 reliable updates (mixed).  Iteration chunks of
+// `check_every` run without host synchronisation.
 int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, int &iters_out) {
   cudaStream_t s = ctx.stream;
   const int every = sys[0]->opts.check_every > 0 ? sys[0]->opts.check_every : 8;
   const int mode = (sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) ? 2 : 1;
   const int lvl_grid = mode == 1 ? trsv_grid : std::max(1, num_sms * 8);
-  // state: tolerance and iteration cap (host writes, before init)
-  std::vector<char> stbuf(vk_bistate_size_f64() * size_t(nsys), 0);
+  const size_t bsz = mixed ? vk_bistate_size_f32() : vk_bistate_size_f64();
+  std::vector<char> stbuf(bsz * size_t(nsys), 0);
   cudaError_t e = cudaMemcpyAsync(stbuf.data(), d_state, stbuf.size(), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return ctx.cuda_fail(e, "read state");
   for (int k = 0; k < nsys; ++k) {
     if (mixed) {
-      BiStateHost<float> *b = (BiStateHost<float> *)(stbuf.data() + vk_bistate_size_f32() * size_t(k));
-      b->tol = float(tol); b->max_iter = max_iter; b->done = 0;
+      BiState<float> *b = (BiState<float> *)(stbuf.data() + bsz * size_t(k));
+      b->tol = float(tol); b->max_iter = max_iter; b->done = 0; b->upd = 0; b->iter = 0;
     } else {
-      BiStateHost<double> *b = (BiStateHost<double> *)(stbuf.data() + vk_bistate_size_f64() * size_t(k));
-      b->tol = tol; b->max_iter = max_iter; b->done = 0;
+      BiState<double> *b = (BiState<double> *)(stbuf.data() + bsz * size_t(k));
+      b->tol = tol; b->max_iter = max_iter; b->done = 0; b->upd = 0; b->iter = 0;
     }
   }
   if ((e = cudaMemcpyAsync(d_state, stbuf.data(), stbuf.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "write state");
-  if (mixed) vk_bicg_init_f32(ntiles, d_sysdev, d_state, &tiles, (float *)d_partials, d_counters, d_active, s);
-  else vk_bicg_init_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s);
+  EventProf &P = g_prof;
+  P.on = profile; P.s = s;
+  if (mixed) {
+    // r64 = b - A x64 (x64 = 0 here), r32 = r64, then the FP32 recurrences start from it
+    vk_reliable_r(spmv_group, ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, tol, 1, s);
+    vk_bicg_init_f32(ntiles, d_sysdev, d_state, &tiles, (float *)d_partials, d_counters, d_active, s);
+  } else {
+    vk_bicg_init_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s);
+  }
   int done_iters = 0;
   while (true) {
     for (int it = 0; it < every; ++it) {
       int rc = 0;
+      cudaEvent_t a;
       if (mixed) {
-        vk_update_p_f32(ntiles, d_sysdev, d_state, &tiles, d_active, s);
+        float *pf = (float *)d_partials;
+        a = P.begin(); vk_update_p_f32(ntiles, d_sysdev, d_state, &tiles, d_active, s); P.end(2, a);
+        a = P.begin();
         if (has_pc) rc = vk_trsv_f32(mode, trsv_group, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
         else vk_precond_copy_f32(ntiles, d_sysdev, d_state, &tiles, d_active, 0, s);
-        vk_spmv_dot_f32(spmv_group, ntiles, d_sysdev, d_state, &tiles, (float *)d_partials, d_counters, d_active, 0, s);
-        vk_update_s_f32(ntiles, d_sysdev, d_state, &tiles, (float *)d_partials, d_counters, d_active, s);
+        P.end(1, a);
+        a = P.begin(); vk_spmv_dot_f32(spmv_group, ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 0, s); P.end(0, a);
+        a = P.begin(); vk_update_s_f32(ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, s); P.end(2, a);
+        a = P.begin();
         if (has_pc) rc |= vk_trsv_f32(mode, trsv_group, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 1, d_bar, d_err, s);
         else vk_precond_copy_f32(ntiles, d_sysdev, d_state, &tiles, d_active, 1, s);
-        vk_spmv_dot_f32(spmv_group, ntiles, d_sysdev, d_state, &tiles, (float *)d_partials, d_counters, d_active, 1, s);
-        vk_update_xr_f32(ntiles, d_sysdev, d_state, &tiles, (float *)d_partials, d_counters, d_active, s);
+        P.end(1, a);
+        a = P.begin(); vk_spmv_dot_f32(spmv_group, ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 1, s); P.end(0, a);
+        a = P.begin(); vk_update_xr_f32(ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 1, s); P.end(2, a);
+        a = P.begin();
+        vk_reliable_x(ntiles, d_sysdev, d_state, &tiles, d_active, s);
+        vk_reliable_r(spmv_group, ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, tol, 0, s);
+        P.end(3, a);
       } else {
-        vk_update_p_f64(ntiles, d_sysdev, d_state, &tiles, d_active, s);
+        a = P.begin(); vk_update_p_f64(ntiles, d_sysdev, d_state, &tiles, d_active, s); P.end(2, a);
+        a = P.begin();
         if (has_pc) rc = vk_trsv_f64(mode, trsv_group, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
         else vk_precond_copy_f64(ntiles, d_sysdev, d_state, &tiles, d_active, 0, s);
-        vk_spmv_dot_f64(spmv_group, ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 0, s);
-        vk_update_s_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s);
+        P.end(1, a);
+        a = P.begin(); vk_spmv_dot_f64(spmv_group, ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 0, s); P.end(0, a);
+        a = P.begin(); vk_update_s_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s); P.end(2, a);
+        a = P.begin();
         if (has_pc) rc |= vk_trsv_f64(mode, trsv_group, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 1, d_bar, d_err, s);
         else vk_precond_copy_f64(ntiles, d_sysdev, d_state, &tiles, d_active, 1, s);
-        vk_spmv_dot_f64(spmv_group, ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 1, s);
-        vk_update_xr_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s);
+        P.end(1, a);
+        a = P.begin(); vk_spmv_dot_f64(spmv_group, ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 1, s); P.end(0, a);
+        a = P.begin(); vk_update_xr_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 0, s); P.end(2, a);
       }
       if (rc) return ctx.cuda_fail(cudaError_t(rc), "trsv launch");
     }
@@ -520,27 +737,39 @@ int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, int &iters_out) {
     int maxit = 0;
     for (int k = 0; k < nsys; ++k) {
       int32_t d, it;
-      if (mixed) { auto *b = (BiStateHost<float> *)(stbuf.data() + vk_bistate_size_f32() * size_t(k)); d = b->done; it = b->iter; }
-      else { auto *b = (BiStateHost<double> *)(stbuf.data() + vk_bistate_size_f64() * size_t(k)); d = b->done; it = b->iter; }
+      if (mixed) { auto *b = (BiState<float> *)(stbuf.data() + bsz * size_t(k)); d = b->done; it = b->iter; }
+      else { auto *b = (BiState<double> *)(stbuf.data() + bsz * size_t(k)); d = b->done; it = b->iter; }
       if (!d) all_done = false;
       maxit = std::max(maxit, it);
     }
     iters_out = maxit;
-    if (all_done || done_iters >= max_iter + every) break;
+    if (all_done || done_iters >= max_iter + 2 * every) break;
   }
-  // per-system status
+  if (profile) {
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx.cuda_fail(e, "profile");
+    double t[5] = {0, 0, 0, 0, 0};
+    int64_t c[2] = {0, 0};
+    P.collect(t, c);
+    t_spmv += t[0]; t_trsv += t[1]; t_vec += t[2]; t_reliable += t[3];
+    n_spmv += c[0]; n_trsv += c[1];
+  }
   last_state.assign(stbuf.begin(), stbuf.end());
   return VSHE_OK;
 }
 
-int Batch::state_of(int k, int32_t &status, int32_t &iter, double &res) const {
-  if (last_state.empty()) { status = 0; iter = 0; res = 0; return 0; }
-  if (mixed) { auto *b = (const BiStateHost<float> *)(last_state.data() + vk_bistate_size_f32() * size_t(k)); status = b->status; iter = b->iter; res = b->res; }
-  else { auto *b = (const BiStateHost<double> *)(last_state.data() + vk_bistate_size_f64() * size_t(k)); status = b->status; iter = b->iter; res = b->res; }
+int Batch::state_of(int k, int32_t &status, int32_t &iter, int32_t &nupd, double &res) const {
+  if (last_state.empty()) { status = 0; iter = 0; nupd = 0; res = 0; return 0; }
+  if (mixed) {
+    auto *b = (const BiState<float> *)(last_state.data() + vk_bistate_size_f32() * size_t(k));
+    status = b->status; iter = b->iter; nupd = b->nupd; res = b->res64;
+  } else {
+    auto *b = (const BiState<double> *)(last_state.data() + vk_bistate_size_f64() * size_t(k));
+    status = b->status; iter = b->iter; nupd = 0; res = b->res;
+  }
   return 0;
 }
 
-// FP64 residual r = b - A x for all members; returns per-system ||r|| / ||b||.
+// FP64 residual r = b - A x64 for all members; returns per-system ||r|| / ||b||.
 int Batch::residual(Ctx &ctx, std::vector<double> &rel) {
   cudaStream_t s = ctx.stream;
   vk_residual64(spmv_group, ntiles, d_refdev, &tiles, d_partials, d_counters, d_active, d_rnorm2, d_bnorm2, s);
@@ -561,15 +790,18 @@ int Batch::set_active(Ctx &ctx, const std::vector<int32_t> &act) {
 }
 
 // Full solve of every member: factorisation, then FP64 BiCGStab or FP32 BiCGStab
-// inside FP64 iterative refinement, to each member's tolerance.
+// with FP64 reliable updates, to each member's tolerance.
 int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
   cudaStream_t s = ctx.stream;
   cudaError_t e;
   stats.assign(size_t(nsys), vshe_solve_stats{});
+  profile = ctx.profile;
+  t_spmv = t_trsv = t_vec = t_reliable = t_factor = 0;
+  n_spmv = n_trsv = 0;
   cudaEvent_t e0, e1, e2;
   cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
   struct EvGuard { cudaEvent_t a, b, c; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); } } guard{e0, e1, e2};
-  std::vector<int32_t> act(size_t(nsys), 1);
+  std::vector<int32_t> act((size_t)(nsys), 1);
   int rc = set_active(ctx, act);
   if (rc) return rc;
   cudaEventRecord(e0, s);
@@ -577,87 +809,44 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
   if (rc) return rc;
   cudaEventRecord(e1, s);
   const vshe_solve_opts &o = sys[0]->opts;
-  std::vector<int32_t> status(size_t(nsys), 0), iters(size_t(nsys), 0), refs(size_t(nsys), 0);
-  std::vector<double> rel(size_t(nsys), 1.0);
-  // x64 = 0, r64 = b
-  for (System *S : sys) {
+  for (System *S : sys)
     if ((e = cudaMemsetAsync(S->d_x64, 0, sizeof(double) * size_t(S->n), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset x");
-  }
-  // trivial rhs -> x = 0 (src/solvers/solve.hpp:60-66)
-  for (int k = 0; k < nsys; ++k)
-    if (sys[size_t(k)]->bnorm_host == 0.0) { act[size_t(k)] = 0; rel[size_t(k)] = 0.0; }
-  if (!mixed) {
-    for (int k = 0; k < nsys; ++k) {
-      System *S = sys[size_t(k)];
+  if (!mixed)
+    for (System *S : sys)
       if ((e = cudaMemcpyAsync(S->kv[1], S->d_b64, sizeof(double) * size_t(S->n), cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "rhs");
-    }
-    if ((rc = set_active(ctx, act))) return rc;
-    int it = 0;
-    rc = bicgstab(ctx, o.tol, o.max_iters, it);
-    if (rc) return rc;
-    for (int k = 0; k < nsys; ++k) {
-      System *S = sys[size_t(k)];
-      int32_t stt, itk; double res;
-      state_of(k, stt, itk, res);
-      status[size_t(k)] = act[size_t(k)] ? stt : 0;
-      iters[size_t(k)] = act[size_t(k)] ? itk : 0;
-      if (act[size_t(k)] && (e = cudaMemcpyAsync(S->d_x64, S->kv[0], sizeof(double) * size_t(S->n), cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "x");
-    }
-    std::vector<int32_t> all(size_t(nsys), 1);
-    if ((rc = set_active(ctx, all))) return rc;
-    if ((rc = residual(ctx, rel))) return rc;
-  } else {
-    std::vector<int32_t> all(size_t(nsys), 1);
-    const int max_ref = o.max_refinements > 0 ? o.max_refinements : 10;
-    const double inner = o.inner_tol > 0 ? o.inner_tol : 1e-5;
-    for (int sweep = 0; sweep <= max_ref; ++sweep) {
-      if ((rc = set_active(ctx, all))) return rc;
-      if ((rc = residual(ctx, rel))) return rc;  // r64 = b - A x64
-      bool any = false;
-      for (int k = 0; k < nsys; ++k) {
-        if (sys[size_t(k)]->bnorm_host == 0.0) { act[size_t(k)] = 0; rel[size_t(k)] = 0.0; continue; }
-        act[size_t(k)] = (rel[size_t(k)] >= o.tol && status[size_t(k)] == 0 && iters[size_t(k)] < o.max_iters) ? 1 : 0;
-        if (act[size_t(k)]) any = true;
-      }
-      if (!any || sweep == max_ref) break;
-      if ((rc = set_active(ctx, act))) return rc;
-      vk_scale_to_f32(ntiles, d_refdev, d_sysdev, &tiles, d_active, d_rnorm2, s);
-      int it = 0;
-      int budget = 0;
-      for (int k = 0; k < nsys; ++k) if (act[size_t(k)]) budget = std::max(budget, o.max_iters - iters[size_t(k)]);
-      rc = bicgstab(ctx, inner, std::max(1, budget), it);
-      if (rc) return rc;
-      vk_accumulate_x(ntiles, d_refdev, d_sysdev, &tiles, d_active, d_rnorm2, s);
-      for (int k = 0; k < nsys; ++k) {
-        if (!act[size_t(k)]) continue;
-        int32_t stt, itk; double res;
-        state_of(k, stt, itk, res);
-        iters[size_t(k)] += itk;
-        refs[size_t(k)] += 1;
-        // an inner breakdown / stall is not fatal while refinement still makes progress
-        if (stt == VSHE_E_BREAKDOWN && itk <= 1) status[size_t(k)] = VSHE_E_BREAKDOWN;
-      }
-    }
-  }
+  int it = 0;
+  rc = bicgstab(ctx, o.tol, o.max_iters, it);
+  if (rc) return rc;
+  if (!mixed)
+    for (System *S : sys)
+      if ((e = cudaMemcpyAsync(S->d_x64, S->kv[0], sizeof(double) * size_t(S->n), cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "x");
+  std::vector<double> rel;
+  if ((rc = residual(ctx, rel))) return rc;  // true FP64 residual of the final x
   cudaEventRecord(e2, s);
   if ((e = cudaEventSynchronize(e2)) != cudaSuccess) return ctx.cuda_fail(e, "solve");
   float ms_setup = 0, ms_solve = 0;
   cudaEventElapsedTime(&ms_setup, e0, e1);
   cudaEventElapsedTime(&ms_solve, e1, e2);
+  if (profile) {
+    ctx.prof[0] = t_spmv; ctx.prof[1] = t_trsv; ctx.prof[2] = t_vec; ctx.prof[3] = t_reliable; ctx.prof[4] = ms_setup;
+    ctx.prof_counts[0] = n_spmv; ctx.prof_counts[1] = n_trsv;
+  }
   for (int k = 0; k < nsys; ++k) {
     vshe_solve_stats &st = stats[size_t(k)];
     System *S = sys[size_t(k)];
-    st.iterations = iters[size_t(k)];
-    st.refinements = refs[size_t(k)];
+    int32_t status, iters, nupd; double res;
+    state_of(k, status, iters, nupd, res);
+    st.iterations = iters;
+    st.refinements = nupd;
     st.rel_residual = rel[size_t(k)];
     st.setup_ms = ms_setup;
     st.solve_ms = ms_solve;
     st.levels_L = S->nlevL;
     st.levels_U = S->nlevU;
     st.bytes_device = int64_t(S->arena.total);
-    int32_t code = status[size_t(k)];
+    int32_t code = status;
     if (code == 0 && rel[size_t(k)] >= o.tol) code = VSHE_E_NOT_CONVERGED;
-    if (code == VSHE_E_BREAKDOWN && rel[size_t(k)] < o.tol) code = 0;
+    if (code != 0 && rel[size_t(k)] < o.tol) code = 0;
     st.status = code;
   }
   return VSHE_OK;
@@ -669,8 +858,6 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
 // public C ABI
 // =======================================================================
 using namespace vshe;
-
-struct vshe_ctx : public vshe::Ctx {};
 
 extern "C" {
 
@@ -709,6 +896,7 @@ int vshe_destroy(vshe_ctx *ctx) {
   if (!ctx) return VSHE_E_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  vshe::she_release_all(ctx);
   ctx->batches.clear();
   ctx->systems.clear();
   cudaStreamDestroy(ctx->stream);
@@ -726,6 +914,21 @@ size_t vshe_bytes_in_use(vshe_ctx *ctx) {
   return t;
 }
 
+int vshe_set_profiling(vshe_ctx *ctx, int32_t on) {
+  if (!ctx) return VSHE_E_INVALID_ARGUMENT;
+  ctx->profile = on != 0;
+  return VSHE_OK;
+}
+
+int64_t vshe_kernel_launches(void) { return (int64_t)vk_launches_total(); }
+
+int vshe_get_profile(vshe_ctx *ctx, double *ms, int64_t *counts) {
+  if (!ctx || !ms) return VSHE_E_INVALID_ARGUMENT;
+  for (int k = 0; k < 5; ++k) ms[k] = ctx->prof[k];
+  if (counts) { counts[0] = ctx->prof_counts[0]; counts[1] = ctx->prof_counts[1]; }
+  return VSHE_OK;
+}
+
 int vshe_system_create(vshe_ctx *ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *v,
                        const double *rhs, const vshe_solve_opts *opts, int64_t *handle) {
   if (!ctx || !handle) return VSHE_E_INVALID_ARGUMENT;
@@ -734,11 +937,13 @@ int vshe_system_create(vshe_ctx *ctx, int64_t n, int64_t nnz, const int64_t *rp,
   vshe_solve_opts o;
   if (opts) o = *opts; else vshe_default_opts(&o);
   // admission against the HBM budget (upper estimate of the system's footprint)
-  const size_t est = size_t(nnz) * (4 + 8 + 8 + 4 + 16) + size_t(n) * (8 * 8 + 9 * 8 + 16);
+  const size_t est = size_t(nnz) * (4 + 8 + 8 + 4 + 8 + 8 + 8 + 8) + size_t(n) * (8 * 8 + 9 * 8 + 32);
   if (vshe_bytes_in_use(ctx) + est > ctx->budget) return ctx->fail(VSHE_E_BUDGET, std::to_string(est) + " bytes requested");
   std::unique_ptr<System> S(new System);
   int rc = S->create(*ctx, n, nnz, rp, ci, v, rhs, o);
   if (rc) return rc;
+  S->opts.block_ptr = nullptr;  // read during creation only
+  S->opts.perm = nullptr;
   int64_t h = ++ctx->next_handle;
   ctx->systems[h] = std::move(S);
   *handle = h;
@@ -880,11 +1085,11 @@ int vshe_system_time_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, int32_t r
   auto it = ctx->systems.find(h);
   if (it == ctx->systems.end()) return ctx->fail(VSHE_E_NOT_FOUND, "");
   System *S = it->second.get();
+  if (precision == 1 && !S->mixed) return ctx->fail(VSHE_E_UNSUPPORTED, "");
   cudaStream_t s = ctx->stream;
   const int grid = std::max(1, int(std::min<int64_t>((S->n * S->spmv_group + 255) / 256, 65535 * 8)));
   cudaEvent_t a, b;
   cudaEventCreate(&a); cudaEventCreate(&b);
-  if (precision == 1 && !S->mixed) return ctx->fail(VSHE_E_UNSUPPORTED, "");
   for (int w = 0; w < 3; ++w) {
     if (precision == 1) vk_spmv_plain_f32(S->spmv_group, grid, S->n, S->d_rp, S->d_ci, S->d_av32, (float *)S->kv[0], (float *)S->kv[1], s);
     else vk_spmv_plain_f64(S->spmv_group, grid, S->n, S->d_rp, S->d_ci, S->d_av64, S->d_x64, S->d_r64, s);
@@ -904,27 +1109,35 @@ int vshe_system_time_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, int32_t r
   return VSHE_OK;
 }
 
+// Factor values of P A P^T in A's entry order (FP64, host array of length nnz);
+// entries coupling two blocks are not part of the factor and read 0.
 int vshe_system_factor_values(vshe_ctx *ctx, int64_t h, double *lu) {
   if (!ctx || !lu) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  std::vector<int64_t> hs{h};
   int rc;
-  {
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    cudaSetDevice(ctx->device);
-    std::vector<int64_t> hs{h};
-    Batch *B = get_batch(ctx, hs, rc);
-    if (!B) return rc;
-    if (!B->has_pc) return ctx->fail(VSHE_E_UNSUPPORTED, "no preconditioner");
-    rc = B->factor(*ctx);
-    if (rc) return rc;
-    System *S = B->sys[0];
-    cudaError_t e = cudaMemcpyAsync(lu, S->d_lu64, sizeof(double) * size_t(S->nnz), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) return ctx->cuda_fail(e, "download factor");
-    // entries coupling two blocks are not part of the factor
-    for (int64_t i = 0; i < S->n; ++i)
-      for (int64_t k = S->rp[i]; k < S->rp[i + 1]; ++k)
-        if (S->blk[size_t(S->ci[k])] != S->blk[size_t(i)]) lu[k] = 0.0;
-  }
+  Batch *B = get_batch(ctx, hs, rc);
+  if (!B) return rc;
+  if (!B->has_pc) return ctx->fail(VSHE_E_UNSUPPORTED, "no preconditioner");
+  rc = B->factor(*ctx);
+  if (rc) return rc;
+  System *S = B->sys[0];
+  std::vector<double> lp((size_t)S->nnz);
+  std::vector<int64_t> amap((size_t)S->nnz);
+  std::vector<int32_t> pci((size_t)S->nnz);
+  std::vector<int64_t> prp((size_t)S->n + 1);
+  cudaError_t e = cudaMemcpyAsync(lp.data(), S->d_lu64, sizeof(double) * lp.size(), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(amap.data(), S->d_amap, sizeof(int64_t) * amap.size(), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(pci.data(), S->d_pci, sizeof(int32_t) * pci.size(), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(prp.data(), S->d_prp, sizeof(int64_t) * prp.size(), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "download factor");
+  for (int64_t i = 0; i < S->n; ++i)
+    for (int64_t k = prp[size_t(i)]; k < prp[size_t(i) + 1]; ++k) {
+      const bool in_factor = S->blk[size_t(pci[size_t(k)])] == S->blk[size_t(i)];
+      lu[amap[size_t(k)]] = in_factor ? lp[size_t(k)] : 0.0;
+    }
   return VSHE_OK;
 }
 

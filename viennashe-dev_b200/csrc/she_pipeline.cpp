@@ -1,0 +1,521 @@
+// she_pipeline.cpp -- C++ host orchestration of the device-side SHE path:
+// setup on the host (she_host.cpp), then on the GPU: assembly (K1/K2),
+// odd elimination (K3), unknown scaling + row/column normalisation (K4),
+// ILU(0)/BiCGStab solve of the reduced system (host_solver.cpp), and
+// recovery + post-processing (K10).  Implements the vshe_she_* C ABI.
+//
+// Mirrors viennashe::she::assemble (viennashe/she/assemble_all.hpp:46-424) followed by
+// viennashe::she::solve (viennashe/she/linear_solver.hpp:100-189).
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/vshe_gpu.h"
+#include "host_internal.h"
+#include "she_host.h"
+#include "she_kernels.h"
+
+namespace vshe {
+
+struct SheProblem {
+  SheSetup H;
+  DevArena arena;
+  SheDev P{};
+  vshe_solve_opts opts{};
+  int ncontacts = 0;
+  // full (even + odd) system
+  int64_t n_full = 0, nnz_full = 0;
+  int64_t *d_frp = nullptr; int32_t *d_fci = nullptr; double *d_fval = nullptr, *d_frhs = nullptr;
+  // reduced system
+  int64_t n_red = 0, nnz_red = 0;
+  int64_t *d_rrp = nullptr; int32_t *d_rci = nullptr; double *d_rval = nullptr, *d_rrhs = nullptr;
+  uint8_t *d_ins = nullptr;
+  double *d_s = nullptr, *d_sf = nullptr;
+  int64_t *d_dpos = nullptr, *d_cptr = nullptr, *d_cursor = nullptr, *d_cpos = nullptr;
+  void *d_tmp = nullptr; size_t tmp_bytes = 0;
+  int32_t *d_err = nullptr;
+  // outputs
+  double *d_xf = nullptr, *d_dens = nullptr, *d_cur = nullptr, *d_part = nullptr;
+  std::vector<int64_t> slab_ptr;
+  std::unique_ptr<System> sys;
+  std::unique_ptr<Batch> batch;
+  double full_residual = -1.0;
+  int stage = 0;
+
+  int create(Ctx &ctx, const vshe_device_desc &d, const vshe_she_config &c, const vshe_coupling_tables &ct, const vshe_solve_opts &o);
+  int symbolic_full(Ctx &ctx);
+  int fill_full(Ctx &ctx);
+  int assemble(Ctx &ctx, int upto);
+  int finish(Ctx &ctx);
+  int check(Ctx &ctx, const char *what);
+};
+
+template <typename T>
+static T *upload(Ctx &ctx, DevArena &ar, const std::vector<T> &v, int &rc) {
+  cudaError_t e;
+  T *p = (T *)ar.alloc(sizeof(T) * std::max<size_t>(v.size(), 1), e);
+  if (!p) { rc = ctx.cuda_fail(e, "cudaMalloc she table"); return nullptr; }
+  if (!v.empty() && (e = cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, ctx.stream)) != cudaSuccess) {
+    rc = ctx.cuda_fail(e, "upload she table");
+    return nullptr;
+  }
+  rc = 0;
+  return p;
+}
+
+int SheProblem::check(Ctx &ctx, const char *what) {
+  int32_t err = 0;
+  cudaError_t e = cudaMemcpyAsync(&err, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+  if (e != cudaSuccess) return ctx.cuda_fail(e, what);
+  if (err) {
+    cudaMemsetAsync(d_err, 0, sizeof(int32_t), ctx.stream);
+    if (err == -100) return -100;
+    if (err == -4) return ctx.fail(VSHE_E_ODD_DIAGONAL, what);
+    return ctx.fail(VSHE_E_INVALID_ARGUMENT, std::string(what) + ": per-row capacity exceeded");
+  }
+  return VSHE_OK;
+}
+
+int SheProblem::create(Ctx &ctx, const vshe_device_desc &d, const vshe_she_config &c, const vshe_coupling_tables &ct, const vshe_solve_opts &o) {
+  std::string msg = H.build(d, c, ct);
+  if (!msg.empty()) return ctx.fail(VSHE_E_INVALID_ARGUMENT, msg);
+  opts = o;
+  for (int i = 0; i < H.nc; ++i) ncontacts = std::max(ncontacts, H.contact[i] + 1);
+  int rc = 0;
+  cudaError_t e;
+#define UP(dst, vec) dst = upload(ctx, arena, vec, rc); if (rc) return rc;
+  P.dim = H.dim; P.nc = H.nc; P.nf = H.nf; P.NH = H.NH; P.D = H.D; P.L = H.L; P.T = H.T;
+  const int32_t *i32; const double *f64; const int64_t *i64; const char *ch;
+  UP(i32, H.mat); P.mat = i32;
+  UP(i32, H.contact); P.contact = i32;
+  UP(i32, H.cf_ptr); P.cf_ptr = i32;
+  UP(i32, H.cf_idx); P.cf_idx = i32;
+  UP(i32, H.inc_dir_even); P.inc_dir_even = i32;
+  UP(f64, H.vol); P.vol = f64;
+  UP(f64, H.cen); P.cen = f64;
+  UP(f64, H.shift_c); P.shift_c = f64;
+  UP(ch, H.mask_c); P.mask_c = ch;
+  UP(i32, H.fcell); P.fcell = i32;
+  UP(i32, H.inc_dir_odd); P.inc_dir_odd = i32;
+  UP(f64, H.fvol); P.fvol = f64;
+  UP(f64, H.fnorm); P.fnorm = f64;
+  UP(f64, H.shift_f); P.shift_f = f64;
+  UP(f64, H.Hval); P.Hval = f64;
+  UP(f64, H.bnd_c); P.bnd_c = f64;
+  UP(i32, H.ord_c); P.ord_c = i32;
+  UP(i32, H.ord_f); P.ord_f = i32;
+  UP(i64, H.idx_c); P.idx_c = i64;
+  UP(i64, H.idx_f); P.idx_f = i64;
+  UP(i32, H.even_nodes); P.even_nodes = i32;
+  UP(i32, H.odd_nodes); P.odd_nodes = i32;
+  UP(i32, H.even_harm); P.even_harm = i32;
+  UP(i32, H.odd_harm); P.odd_harm = i32;
+  UP(f64, H.cblocks); P.cblocks = f64;
+#undef UP
+  P.n_even_nodes = int64_t(H.even_nodes.size() / 2);
+  P.n_odd_nodes = int64_t(H.odd_nodes.size() / 2);
+  P.n_even = H.n_even; P.n_odd = H.n_odd;
+  P.acoustic = H.cfg.acoustic_phonon; P.optical = H.cfg.optical_phonon;
+  P.bnd_type = H.cfg.boundary_type == VSHE_BOUNDARY_DIRICHLET ? 1 : 0;
+  P.scaling_type = H.cfg.scaling_type;
+  P.tau = H.cfg.gr_tau;
+  P.hbar_omega = H.hbar_omega;
+  {
+    // rates: acoustic_phonon_scattering.hpp:98-114, optical_phonon_scattering.hpp:162-179, physics.hpp:71-75
+    const double PI = SheConst::PI, Q = SheConst::Q, KB = SheConst::KB;
+    const double hbar = 6.62606896e-34 / (2.0 * 3.1415926535897932384626433832795);
+    const double ul = 9040.0, rho = 2330.0, E1 = 8.9 * Q, DtK = 5e10 * Q;
+    P.rate_ac = H.cfg.acoustic_fit_factor * (2.0 * PI * KB * H.T * E1 * E1 / (hbar * ul * ul * rho));
+    P.rate_op = H.cfg.optical_fit_factor * (PI * DtK * DtK * hbar / (2.0 * rho * H.hbar_omega));
+    P.n_op = 1.0 / (std::exp(H.hbar_omega / (KB * H.T)) - 1.0);
+  }
+  for (int j = 0; j < 3; ++j) { P.ax01[j] = H.a_x01[j]; P.ay01[j] = H.a_y01[j]; }
+  n_full = H.n_even + H.n_odd;
+  n_red = H.n_even;
+  slab_ptr = H.slab_ptr;
+#define ALLOC(ptr, type, count) \
+  ptr = (type *)arena.alloc(sizeof(type) * size_t(count), e); if (!ptr) return ctx.cuda_fail(e, "cudaMalloc she " #ptr);
+  ALLOC(d_err, int32_t, 1);
+  ALLOC(d_frp, int64_t, n_full + 1);
+  ALLOC(d_rrp, int64_t, n_red + 1);
+  if ((e = cudaMemsetAsync(d_err, 0, sizeof(int32_t), ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+  // scan scratch sized for the larger of the scans
+  {
+    size_t t1 = 0;
+    vk_scan_rowptr(d_frp, n_full, nullptr, &t1, ctx.stream);
+    tmp_bytes = std::max<size_t>(t1, 256) * 2;
+    d_tmp = arena.alloc(tmp_bytes, e);
+    if (!d_tmp) return ctx.cuda_fail(e, "cudaMalloc scan scratch");
+  }
+  rc = symbolic_full(ctx);
+  if (rc) return rc;
+  // reduced pattern: count pass of K3 needs the assembled full system
+  rc = fill_full(ctx);
+  if (rc) return rc;
+  FullDev A{d_frp, d_fci, d_fval, d_frhs};
+  if ((e = cudaMemsetAsync(d_rrp, 0, sizeof(int64_t), ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+  if ((rc = vk_she_schur(&A, n_red, 0, d_rrp + 1, nullptr, nullptr, nullptr, nullptr, nullptr, d_err, ctx.stream))) return ctx.cuda_fail(cudaError_t(rc), "schur count");
+  if ((rc = check(ctx, "eliminate_odd_unknowns (count)"))) return rc;
+  {
+    size_t tb = tmp_bytes;
+    if ((rc = vk_scan_rowptr(d_rrp, n_red, d_tmp, &tb, ctx.stream))) return ctx.cuda_fail(cudaError_t(rc), "scan");
+  }
+  if ((e = cudaMemcpyAsync(&nnz_red, d_rrp + n_red, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "nnz");
+  if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "nnz");
+  if (nnz_red >= (int64_t(1) << 40)) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "reduced system too large");
+  ALLOC(d_rci, int32_t, nnz_red);
+  ALLOC(d_rval, double, nnz_red);
+  ALLOC(d_rrhs, double, n_red);
+  ALLOC(d_ins, uint8_t, n_red);
+  ALLOC(d_s, double, n_red);
+  ALLOC(d_sf, double, n_red);
+  ALLOC(d_dpos, int64_t, n_red);
+  ALLOC(d_cptr, int64_t, n_red + 1);
+  ALLOC(d_cursor, int64_t, n_red);
+  ALLOC(d_cpos, int64_t, nnz_red);
+  ALLOC(d_xf, double, n_full);
+  ALLOC(d_dens, double, H.nc);
+  ALLOC(d_cur, double, std::max(ncontacts, 1));
+  ALLOC(d_part, double, 2 * size_t(vk_she_residual_blocks(n_full)));
+#undef ALLOC
+  {
+    std::vector<double> ones((size_t)(n_red), 1.0);
+    if ((e = cudaMemcpyAsync(d_s, ones.data(), sizeof(double) * ones.size(), cudaMemcpyHostToDevice, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "scaling");
+    if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "scaling");
+  }
+  rc = assemble(ctx, 3);
+  if (rc) return rc;
+  // reduced pattern on the host for the preconditioner's schedules
+  std::vector<int64_t> hrp((size_t)n_red + 1);
+  std::vector<int32_t> hci((size_t)nnz_red);
+  if ((e = cudaMemcpyAsync(hrp.data(), d_rrp, sizeof(int64_t) * hrp.size(), cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "pattern");
+  if ((e = cudaMemcpyAsync(hci.data(), d_rci, sizeof(int32_t) * hci.size(), cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "pattern");
+  if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "pattern");
+  vshe_solve_opts so = opts;
+  std::vector<int32_t> node_perm;
+  if (so.ordering == VSHE_ORDER_MULTICOLOR && !so.perm && so.precond != VSHE_PRECOND_NONE) {
+    // Colour the (cell, H) nodes so that no two coupled nodes share a colour: cells by a
+    // greedy colouring of the mesh graph, energies by the parity of H / n_op (in-scattering
+    // couples H and H +- n_op).  All harmonics of a node share its colour; rows are ordered
+    // by colour, then by their original position.
+    std::vector<int32_t> ccol((size_t)H.nc, -1);
+    for (int c = 0; c < H.nc; ++c) {
+      uint64_t used = 0;
+      for (int k = H.cf_ptr[c]; k < H.cf_ptr[c + 1]; ++k) {
+        const int o = H.other_cell(H.cf_idx[k], c);
+        if (o >= 0 && ccol[(size_t)o] >= 0 && ccol[(size_t)o] < 64) used |= (uint64_t(1) << ccol[(size_t)o]);
+      }
+      int col = 0;
+      while (col < 63 && (used >> col) & 1) ++col;
+      ccol[(size_t)c] = col;
+    }
+    const int nop = std::max(1, int(std::lround(H.hbar_omega / H.cfg.energy_spacing)));
+    std::vector<int32_t> rowcol((size_t)n_red);
+    for (size_t k = 0; k + 1 < H.even_nodes.size(); k += 2) {
+      const int c = H.even_nodes[k], h = H.even_nodes[k + 1];
+      const int64_t base = H.idx_c[(size_t)c * H.NH + h];
+      int ne = 0;
+      for (int l = 0; l <= H.ord_c[(size_t)c * H.NH + h]; l += 2) ne += 2 * l + 1;
+      const int32_t col = ccol[(size_t)c] * 2 + ((h / nop) & 1);
+      for (int q = 0; q < ne; ++q) rowcol[(size_t)(base + q)] = col;
+    }
+    node_perm.resize((size_t)n_red);
+    for (int64_t i = 0; i < n_red; ++i) node_perm[(size_t)i] = int32_t(i);
+    std::stable_sort(node_perm.begin(), node_perm.end(), [&](int32_t a, int32_t b) { return rowcol[(size_t)a] < rowcol[(size_t)b]; });
+    so.perm = node_perm.data();
+  }
+  if (so.precond == VSHE_PRECOND_BLOCK_ILU0 && (so.n_blocks <= 0 || !so.block_ptr)) {
+    // energy slabs (fill_block_indices, linear_solver.hpp:44-83): one block per H with unknowns
+    so.n_blocks = int64_t(slab_ptr.size()) - 1;
+    so.block_ptr = slab_ptr.data();
+  }
+  sys.reset(new System);
+  rc = sys->create_borrowed(ctx, n_red, nnz_red, hrp.data(), hci.data(), d_rrp, d_rci, d_rval, d_rrhs, so);
+  if (rc) return rc;
+  sys->opts.block_ptr = nullptr;  // the pointers above are only read during creation
+  sys->opts.perm = nullptr;
+  batch.reset(new Batch);
+  std::vector<System *> mem{sys.get()};
+  return batch->build(ctx, mem);
+}
+
+int SheProblem::symbolic_full(Ctx &ctx) {
+  cudaError_t e;
+  int rc;
+  if ((e = cudaMemsetAsync(d_frp, 0, sizeof(int64_t), ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+  if ((rc = vk_she_assemble_even(&P, 0, d_frp + 1, nullptr, nullptr, nullptr, nullptr, d_err, ctx.stream))) return ctx.cuda_fail(cudaError_t(rc), "assemble even (count)");
+  if ((rc = vk_she_assemble_odd(&P, 0, d_frp + 1, nullptr, nullptr, nullptr, nullptr, d_err, ctx.stream))) return ctx.cuda_fail(cudaError_t(rc), "assemble odd (count)");
+  size_t tb = tmp_bytes;
+  if ((rc = vk_scan_rowptr(d_frp, n_full, d_tmp, &tb, ctx.stream))) return ctx.cuda_fail(cudaError_t(rc), "scan");
+  if ((e = cudaMemcpyAsync(&nnz_full, d_frp + n_full, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "nnz");
+  if ((rc = check(ctx, "assemble (count)"))) return rc;
+  if (d_fci) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "full pattern already allocated");
+  d_fci = (int32_t *)arena.alloc(sizeof(int32_t) * size_t(nnz_full), e);
+  if (!d_fci) return ctx.cuda_fail(e, "cudaMalloc full ci");
+  d_fval = (double *)arena.alloc(sizeof(double) * size_t(nnz_full), e);
+  if (!d_fval) return ctx.cuda_fail(e, "cudaMalloc full val");
+  d_frhs = (double *)arena.alloc(sizeof(double) * size_t(n_full), e);
+  if (!d_frhs) return ctx.cuda_fail(e, "cudaMalloc full rhs");
+  return VSHE_OK;
+}
+
+int SheProblem::fill_full(Ctx &ctx) {
+  int rc;
+  if ((rc = vk_she_assemble_even(&P, 1, nullptr, d_frp, d_fci, d_fval, d_frhs, d_err, ctx.stream))) return ctx.cuda_fail(cudaError_t(rc), "assemble even");
+  if ((rc = vk_she_assemble_odd(&P, 1, nullptr, d_frp, d_fci, d_fval, d_frhs, d_err, ctx.stream))) return ctx.cuda_fail(cudaError_t(rc), "assemble odd");
+  rc = check(ctx, "assemble");
+  if (rc == -100) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "the assembled pattern changed (an entry cancelled to zero); recreate the problem");
+  return rc;
+}
+
+// upto: 1 = assemble the full system, 2 = + eliminate odd unknowns, 3 = + scaling/normalisation
+int SheProblem::assemble(Ctx &ctx, int upto) {
+  int rc;
+  if (stage > 0 || upto >= 1) {
+    if ((rc = fill_full(ctx))) return rc;
+  }
+  stage = 1;
+  if (upto < 2) return VSHE_OK;
+  FullDev A{d_frp, d_fci, d_fval, d_frhs};
+  if ((rc = vk_she_schur(&A, n_red, 1, nullptr, d_rrp, d_rci, d_rval, d_rrhs, d_ins, d_err, ctx.stream))) return ctx.cuda_fail(cudaError_t(rc), "schur");
+  rc = check(ctx, "eliminate_odd_unknowns");
+  if (rc == -100) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "reduced pattern changed; recreate the problem");
+  if (rc) return rc;
+  stage = 2;
+  if (upto < 3) return VSHE_OK;
+  if ((rc = vk_she_normalise(&P, n_red, d_rrp, d_rci, d_rval, d_rrhs, d_ins, H.cfg.scale ? 1 : 0, d_s, d_sf, d_dpos, d_cptr, d_cursor, d_cpos, d_tmp, tmp_bytes, ctx.stream)))
+    return ctx.cuda_fail(cudaError_t(rc), "normalise");
+  stage = 3;
+  if (sys) sys->refresh_device_values(ctx);
+  return VSHE_OK;
+}
+
+int SheProblem::finish(Ctx &ctx) {
+  FullDev A{d_frp, d_fci, d_fval, d_frhs};
+  int rc = vk_she_finish(&P, &A, sys->d_x64, d_s, d_sf, H.cfg.scale ? 1 : 0, d_xf, d_part, d_dens, ncontacts, d_cur, ctx.stream);
+  if (rc) return ctx.cuda_fail(cudaError_t(rc), "finish");
+  const int nb = vk_she_residual_blocks(n_full);
+  std::vector<double> part(2 * size_t(nb));
+  cudaError_t e = cudaMemcpyAsync(part.data(), d_part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, ctx.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+  if (e != cudaSuccess) return ctx.cuda_fail(e, "finish");
+  double r2 = 0, b2 = 0;
+  for (int k = 0; k < nb; ++k) { r2 += part[2 * size_t(k)]; b2 += part[2 * size_t(k) + 1]; }
+  full_residual = b2 > 0 ? std::sqrt(r2) / std::sqrt(b2) : 0.0;
+  return VSHE_OK;
+}
+
+}  // namespace vshe
+
+using namespace vshe;
+
+static std::map<vshe::Ctx *, std::map<int64_t, std::unique_ptr<SheProblem>>> g_she;
+static std::mutex g_she_mu;
+
+static SheProblem *find_she(vshe_ctx *ctx, int64_t h) {
+  std::lock_guard<std::mutex> lk(g_she_mu);
+  auto it = g_she.find(ctx);
+  if (it == g_she.end()) return nullptr;
+  auto jt = it->second.find(h);
+  return jt == it->second.end() ? nullptr : jt->second.get();
+}
+
+namespace vshe {
+void she_release_all(Ctx *ctx) {
+  std::lock_guard<std::mutex> lk(g_she_mu);
+  g_she.erase(ctx);
+}
+}  // namespace vshe
+
+extern "C" {
+
+int vshe_coupling_tables_compute(int32_t L, double *out) {
+  if (L < 1 || L > 9 || !out) return VSHE_E_INVALID_ARGUMENT;
+  vshe::coupling_quadrature(L, out);
+  return VSHE_OK;
+}
+
+int vshe_she_create(vshe_ctx *ctx, const vshe_device_desc *d, const vshe_she_config *c, const vshe_coupling_tables *ct,
+                    const vshe_solve_opts *opts, int64_t *handle) {
+  if (!ctx || !d || !c || !ct || !handle) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  vshe_solve_opts o;
+  if (opts) o = *opts; else vshe_default_opts(&o);
+  std::unique_ptr<SheProblem> S(new SheProblem);
+  int rc = S->create(*ctx, *d, *c, *ct, o);
+  if (rc) return rc;
+  int64_t h = ++ctx->next_handle;
+  std::lock_guard<std::mutex> lk2(g_she_mu);
+  g_she[ctx][h] = std::move(S);
+  *handle = h;
+  return VSHE_OK;
+}
+
+int vshe_she_info_get(vshe_ctx *ctx, int64_t h, vshe_she_info *info) {
+  if (!ctx || !info) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  SheProblem *S = find_she(ctx, h);
+  if (!S) return ctx->fail(VSHE_E_NOT_FOUND, "");
+  info->n_energies = S->H.NH;
+  info->n_even = S->H.n_even;
+  info->n_odd = S->H.n_odd;
+  info->nnz_full = S->nnz_full;
+  info->nnz_reduced = S->nnz_red;
+  info->n_cells = S->H.nc;
+  info->n_facets = S->H.nf;
+  info->n_contacts = S->ncontacts;
+  info->hbar_omega = S->H.hbar_omega;
+  info->bytes_device = int64_t(S->arena.total + (S->sys ? S->sys->arena.total : 0) + (S->batch ? S->batch->arena.total : 0));
+  info->levels_L = S->sys ? S->sys->nlevL : 0;
+  info->levels_U = S->sys ? S->sys->nlevU : 0;
+  return VSHE_OK;
+}
+
+int vshe_she_assemble(vshe_ctx *ctx, int64_t h, int32_t upto) {
+  if (!ctx) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  SheProblem *S = find_she(ctx, h);
+  if (!S) return ctx->fail(VSHE_E_NOT_FOUND, "");
+  if (upto < 1 || upto > 3) return ctx->fail(VSHE_E_INVALID_ARGUMENT, "upto must be 1, 2 or 3");
+  return S->assemble(*ctx, upto);
+}
+
+int vshe_she_solve(vshe_ctx *ctx, int64_t h, vshe_solve_stats *stats) {
+  if (!ctx) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  SheProblem *S = find_she(ctx, h);
+  if (!S) return ctx->fail(VSHE_E_NOT_FOUND, "");
+  if (S->stage < 3) return ctx->fail(VSHE_E_INVALID_ARGUMENT, "assemble the system first");
+  std::vector<vshe_solve_stats> st;
+  int rc = S->batch->solve(*ctx, st);
+  if (rc) return rc;
+  if (stats) *stats = st[0];
+  if (st[0].status) return ctx->fail(st[0].status, "");
+  return VSHE_OK;
+}
+
+int vshe_she_finish(vshe_ctx *ctx, int64_t h, double *full_residual) {
+  if (!ctx) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  SheProblem *S = find_she(ctx, h);
+  if (!S) return ctx->fail(VSHE_E_NOT_FOUND, "");
+  int rc = S->finish(*ctx);
+  if (rc) return rc;
+  if (full_residual) *full_residual = S->full_residual;
+  return VSHE_OK;
+}
+
+int vshe_she_run(vshe_ctx *ctx, int64_t h, vshe_solve_stats *stats, double *full_residual) {
+  int rc = vshe_she_assemble(ctx, h, 3);
+  if (rc) return rc;
+  rc = vshe_she_solve(ctx, h, stats);
+  if (rc && rc != VSHE_E_NOT_CONVERGED) return rc;
+  int rc2 = vshe_she_finish(ctx, h, full_residual);
+  return rc ? rc : rc2;
+}
+
+int vshe_she_bench(vshe_ctx *ctx, int64_t h, int32_t warmup, int32_t steps, double *step_ms, vshe_solve_stats *last) {
+  if (!ctx || steps <= 0 || !step_ms) return VSHE_E_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  int rc = VSHE_OK;
+  for (int k = 0; k < warmup + steps && rc == VSHE_OK; ++k) {
+    cudaDeviceSynchronize();
+    cudaEventRecord(a, ctx->stream);
+    vshe_solve_stats st;
+    double fr = 0;
+    rc = vshe_she_run(ctx, h, &st, &fr);
+    cudaEventRecord(b, ctx->stream);
+    cudaEventSynchronize(b);
+    cudaDeviceSynchronize();
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (k >= warmup) step_ms[k - warmup] = ms;
+    if (last) *last = st;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+int vshe_she_results(vshe_ctx *ctx, int64_t h, double *x_full, double *density, double *currents) {
+  if (!ctx) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  SheProblem *S = find_she(ctx, h);
+  if (!S) return ctx->fail(VSHE_E_NOT_FOUND, "");
+  cudaError_t e = cudaSuccess;
+  if (x_full) e = cudaMemcpyAsync(x_full, S->d_xf, sizeof(double) * size_t(S->n_full), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && density) e = cudaMemcpyAsync(density, S->d_dens, sizeof(double) * size_t(S->H.nc), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && currents && S->ncontacts > 0) e = cudaMemcpyAsync(currents, S->d_cur, sizeof(double) * size_t(S->ncontacts), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "download results");
+  return VSHE_OK;
+}
+
+int vshe_she_export(vshe_ctx *ctx, int64_t h, int32_t which, int64_t *rp, int32_t *ci, double *val, double *rhs) {
+  if (!ctx) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  SheProblem *S = find_she(ctx, h);
+  if (!S) return ctx->fail(VSHE_E_NOT_FOUND, "");
+  const bool full = which == 0;
+  const int64_t n = full ? S->n_full : S->n_red, nnz = full ? S->nnz_full : S->nnz_red;
+  const int64_t *drp = full ? S->d_frp : S->d_rrp;
+  const int32_t *dci = full ? S->d_fci : S->d_rci;
+  const double *dv = full ? S->d_fval : S->d_rval, *db = full ? S->d_frhs : S->d_rrhs;
+  cudaError_t e = cudaSuccess;
+  if (rp) e = cudaMemcpyAsync(rp, drp, sizeof(int64_t) * size_t(n + 1), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && ci) e = cudaMemcpyAsync(ci, dci, sizeof(int32_t) * size_t(nnz), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && val) e = cudaMemcpyAsync(val, dv, sizeof(double) * size_t(nnz), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && rhs) e = cudaMemcpyAsync(rhs, db, sizeof(double) * size_t(n), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "export");
+  return VSHE_OK;
+}
+
+int vshe_she_scaling(vshe_ctx *ctx, int64_t h, double *scaling, double *scale_factors) {
+  if (!ctx) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  SheProblem *S = find_she(ctx, h);
+  if (!S) return ctx->fail(VSHE_E_NOT_FOUND, "");
+  cudaError_t e = cudaSuccess;
+  if (scaling) e = cudaMemcpyAsync(scaling, S->d_s, sizeof(double) * size_t(S->n_red), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && scale_factors) e = cudaMemcpyAsync(scale_factors, S->d_sf, sizeof(double) * size_t(S->n_red), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "download scaling");
+  return VSHE_OK;
+}
+
+int vshe_she_free(vshe_ctx *ctx, int64_t h) {
+  if (!ctx) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  std::unique_ptr<SheProblem> dead;
+  {
+    std::lock_guard<std::mutex> lk2(g_she_mu);
+    auto it = g_she.find(ctx);
+    if (it == g_she.end() || !it->second.count(h)) return ctx->fail(VSHE_E_NOT_FOUND, "");
+    dead = std::move(it->second[h]);
+    it->second.erase(h);
+  }
+  return VSHE_OK;
+}
+
+}  // extern "C"

@@ -4,17 +4,26 @@
 // groups and fused dot products, BiCGStab vector updates fused with their
 // reductions, level-scheduled ILU(0) factorisation and triangular solves run
 // as persistent cooperative kernels with a bounded grid barrier per level,
-// and the FP64 refinement residual.  No tensor cores: nothing on this path is
-// a dense contraction.
+// and the FP64 side of the mixed-precision solve (reliable updates).  No
+// tensor cores: nothing on this path is a dense contraction.
 //
 // Batches: each kernel works on a batch of independent systems described by
 // per-system pointer tables (SysDev) and row tiles that never straddle two
 // systems; reductions are per tile and are finished by the last tile of each
 // system, in a fixed order, so a system's iterates do not depend on what else
 // is in the batch.
+//
+// BiCGStab follows van der Vorst (1992), right-preconditioned.  The shadow
+// residual r^ is a fixed dense pseudo-random vector rather than r_0: the SHE
+// right-hand side lives on the few contact rows only, and with r^ = r_0 the
+// inner products (r^, r_k) collapse to rounding noise after a few iterations.
+// Mixed precision runs the recurrences in FP32 and keeps x and the true
+// residual in FP64 (reliable updates, Sleijpen & van der Vorst 1996): whenever
+// the FP32 residual has dropped by `delta` since the last update, x64 += x32
+// and the FP32 residual is replaced by b - A x64 computed in FP64.
 
 #include <cuda_runtime.h>
-#include <cooperative_groups.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 
@@ -29,6 +38,7 @@ namespace vshe {
 #define VSHE_E_ZERO_PIVOT_DEV (-11)
 
 constexpr int kThreads = 256;
+constexpr double kReliableDelta = 0.1;
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -44,7 +54,7 @@ __device__ __forceinline__ T group_sum(T v) {
   return v;
 }
 
-// Block-wide sum of up to 3 values; result valid in thread 0.
+// Block-wide sums; results valid in thread 0.
 template <typename T, int NV>
 __device__ __forceinline__ void block_sum(T (&v)[NV]) {
   __shared__ T sh[NV][kThreads / 32];
@@ -83,7 +93,6 @@ __device__ bool tile_finish(T (&v)[NV], int tile, int sys, const Tiles &tl, T *p
   }
   __syncthreads();
   if (!is_last) return false;
-  // last block: deterministic fixed-shape reduction over the system's tiles
   __threadfence();
   const int t0 = tl.sys_tile0[sys], t1 = tl.sys_tile0[sys + 1];
   T acc[NV];
@@ -109,41 +118,50 @@ __device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
 template <>
 __device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
 
+// deterministic dense shadow residual in [0.5, 1.5): a hash of the row index
+__device__ __forceinline__ float shadow_value(int64_t i) {
+  uint32_t h = (uint32_t)((uint64_t)i * 2654435761ull) ^ (uint32_t)((uint64_t)i >> 32);
+  h ^= h >> 16; h *= 0x7feb352dU; h ^= h >> 15; h *= 0x846ca68bU; h ^= h >> 16;
+  return 0.5f + (float)(h >> 8) * (1.0f / 16777216.0f);
+}
+
 // ------------------------------------------------------------------ BiCGStab
-// init: rh = r (= b of this solve), x = p = v = 0; ||b|| -> state
+// init: r holds the right-hand side; rh = shadow; x = p = v = 0; ||b||, (rh, r) -> state
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_bicg_init(const SysDev<T> *sys, BiState<T> *st, Tiles tl, T *partials, int32_t *counters, const int32_t *active) {
   const int tile = blockIdx.x;
   const int s = tl.tile_sys[tile];
   if (!active[s]) return;
   const SysDev<T> S = sys[s];
-  T acc[1] = {T(0)};
+  T acc[2] = {T(0), T(0)};
   for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) {
-    T r = S.r[i];
-    S.rh[i] = r;
+    const T r = S.r[i];
+    const T h = (T)shadow_value(i);
+    S.rh[i] = h;
     S.x[i] = T(0); S.p[i] = T(0); S.v[i] = T(0);
     acc[0] += r * r;
+    acc[1] += h * r;
   }
-  T tot[1];
-  if (tile_finish<T, 1>(acc, tile, s, tl, partials, counters, tot)) {
+  T tot[2];
+  if (tile_finish<T, 2>(acc, tile, s, tl, partials, counters, tot)) {
     BiState<T> &b = st[s];
     b.bnorm = dsqrt(tot[0]);
-    b.rho = tot[0]; b.rho_old = T(1); b.alpha = T(1); b.omega = T(1);
-    b.res = T(1); b.iter = 0; b.s_conv = 0; b.status = 0;
+    b.rho = tot[1]; b.rho_old = T(1); b.alpha = T(1); b.omega = T(1);
+    b.res = T(1); b.iter = 0; b.s_conv = 0; b.status = 0; b.upd = 0; b.restart = 1; b.nupd = 0;
     b.done = (tot[0] == T(0)) ? 1 : 0;
     if (b.done) b.res = T(0);
   }
 }
 
-// p = r + beta (p - omega v)
+// p = r + beta (p - omega v), or p = r after a (re)start
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_update_p(const SysDev<T> *sys, const BiState<T> *st, Tiles tl, const int32_t *active) {
+__global__ void __launch_bounds__(kThreads) k_update_p(const SysDev<T> *sys, BiState<T> *st, Tiles tl, const int32_t *active) {
   const int tile = blockIdx.x;
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done) return;
   const SysDev<T> S = sys[s];
   const BiState<T> b = st[s];
-  if (b.iter == 0) {
+  if (b.restart) {
     for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) S.p[i] = S.r[i];
   } else {
     const T beta = (b.rho / b.rho_old) * (b.alpha / b.omega);
@@ -152,8 +170,8 @@ __global__ void __launch_bounds__(kThreads) k_update_p(const SysDev<T> *sys, con
   }
 }
 
-// y = A x over one tile with G lanes per row; optional dots with y.
-// which = 0: v = A ph, dot (rh, v) -> alpha.   which = 1: t = A sh, dots (t, s), (t, t) -> omega.
+// y = A x over one tile with G lanes per row, fused dots.
+// which = 0: v = A ph, (rh, v) -> alpha.   which = 1: t = A sh, (t, s), (t, t) -> omega.
 template <typename T, int G>
 __global__ void __launch_bounds__(kThreads) k_spmv_dot(const SysDev<T> *sys, BiState<T> *st, Tiles tl, T *partials, int32_t *counters, const int32_t *active, int which) {
   const int tile = blockIdx.x;
@@ -188,7 +206,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dot(const SysDev<T> *sys, BiS
   if (tile_finish<T, 2>(acc, tile, s, tl, partials, counters, tot)) {
     BiState<T> &b = st[s];
     if (which == 0) {
-      if (tot[0] == T(0)) { b.status = VSHE_E_BREAKDOWN_DEV; b.done = 1; }
+      if (tot[0] == T(0)) { b.alpha = T(0); b.s_conv = 0; b.status = VSHE_E_BREAKDOWN_DEV; }
       else b.alpha = b.rho / tot[0];
     } else {
       b.omega = tot[1] == T(0) ? T(0) : tot[0] / tot[1];
@@ -219,9 +237,11 @@ __global__ void __launch_bounds__(kThreads) k_update_s(const SysDev<T> *sys, BiS
   }
 }
 
-// x += alpha ph + omega sh; r = s - omega t; ||r||, (rh, r) -> next rho, convergence
+// x += alpha ph + omega sh; r = s - omega t; ||r||, (rh, r) -> next rho, convergence.
+// reliable = 1 (mixed): stopping is decided on the FP64 residual by k_reliable_r;
+// here only a reliable update is requested.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_update_xr(const SysDev<T> *sys, BiState<T> *st, Tiles tl, T *partials, int32_t *counters, const int32_t *active) {
+__global__ void __launch_bounds__(kThreads) k_update_xr(const SysDev<T> *sys, BiState<T> *st, Tiles tl, T *partials, int32_t *counters, const int32_t *active, int reliable) {
   const int tile = blockIdx.x;
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done) return;
@@ -229,7 +249,13 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(const SysDev<T> *sys, Bi
   const BiState<T> b0 = st[s];
   T acc[2] = {T(0), T(0)};
   if (b0.s_conv) {
-    for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) S.x[i] += b0.alpha * S.ph[i];
+    for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) {
+      S.x[i] += b0.alpha * S.ph[i];
+      T r = S.s[i];
+      S.r[i] = r;
+      acc[0] += r * r;
+      acc[1] += S.rh[i] * r;
+    }
   } else {
     for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) {
       S.x[i] += b0.alpha * S.ph[i] + b0.omega * S.sh[i];
@@ -243,13 +269,82 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(const SysDev<T> *sys, Bi
   if (tile_finish<T, 2>(acc, tile, s, tl, partials, counters, tot)) {
     BiState<T> &b = st[s];
     b.iter += 1;
-    if (b.s_conv) { b.done = 1; return; }
+    b.restart = 0;
     b.res = dsqrt(tot[0]) / b.bnorm;
     b.rho_old = b.rho;
     b.rho = tot[1];
-    if (b.res < b.tol) { b.done = 1; return; }
-    if (b.rho == T(0) || b.omega == T(0)) { b.done = 1; b.status = VSHE_E_BREAKDOWN_DEV; return; }
-    if (b.iter >= b.max_iter) { b.done = 1; b.status = VSHE_E_NOT_CONVERGED_DEV; }
+    const bool broke = (b.status == VSHE_E_BREAKDOWN_DEV) || b.rho == T(0) || (!b.s_conv && b.omega == T(0));
+    if (!reliable) {
+      if (b.s_conv || b.res < b.tol) { b.done = 1; b.status = 0; return; }
+      if (broke) { b.done = 1; b.status = VSHE_E_BREAKDOWN_DEV; return; }
+      if (b.iter >= b.max_iter) { b.done = 1; b.status = VSHE_E_NOT_CONVERGED_DEV; }
+      return;
+    }
+    // mixed: ask for the FP64 residual when the FP32 one dropped by delta, converged, broke down or ran out
+    const double rn = (double)b.res * (double)b.bnorm;
+    if (broke) { b.status = 0; b.restart = 1; b.upd = 1; }
+    if (b.s_conv || rn < kReliableDelta * b.maxr || b.res < b.tol || b.iter >= b.max_iter) b.upd = 1;
+    b.s_conv = 0;
+  }
+}
+
+// FP64 reliable update, part 1: x64 += x32, x32 = 0 (systems with upd set)
+__global__ void __launch_bounds__(kThreads) k_reliable_x(const SysDev<float> *sys, const BiState<float> *st, Tiles tl, const int32_t *active) {
+  const int tile = blockIdx.x;
+  const int s = tl.tile_sys[tile];
+  if (!active[s] || st[s].done || !st[s].upd) return;
+  const SysDev<float> S = sys[s];
+  for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) {
+    S.x64[i] += (double)S.x[i];
+    S.x[i] = 0.0f;
+  }
+}
+
+// FP64 reliable update, part 2: r64 = b - A x64, r32 = r64; ||r64||, ||b||, (rh, r32) -> state.
+// With force = 1 this is the initial residual of every active system.
+template <int G>
+__global__ void __launch_bounds__(kThreads) k_reliable_r(const SysDev<float> *sys, BiState<float> *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active, double tol64, int force) {
+  const int tile = blockIdx.x;
+  const int s = tl.tile_sys[tile];
+  if (!active[s] || st[s].done) return;
+  if (!force && !st[s].upd) return;
+  const SysDev<float> S = sys[s];
+  const int lane = threadIdx.x % G, grp = threadIdx.x / G;
+  const int wgrp = (threadIdx.x & ~31) / G;
+  constexpr int NG = kThreads / G;
+  const int64_t r0 = tl.tile_row0[tile], r1 = tl.tile_row1[tile];
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t base = r0 + wgrp; base < r1; base += NG) {
+    const int64_t row = base + (grp - wgrp);
+    const bool valid = row < r1;
+    double sum = 0.0;
+    if (valid)
+      for (int64_t k = S.rp[row] + lane; k < S.rp[row + 1]; k += G) sum += S.av64[k] * S.x64[S.ci[k]];
+    sum = group_sum<double, G>(sum);
+    if (valid && lane == 0) {
+      const double bb = S.b64[row];
+      const double r = bb - sum;
+      S.r64[row] = r;
+      const float r32 = (float)r;
+      S.r[row] = r32;
+      acc[0] += r * r;
+      acc[1] += bb * bb;
+      acc[2] += (double)S.rh[row] * (double)r32;
+    }
+  }
+  double tot[3];
+  if (tile_finish<double, 3>(acc, tile, s, tl, partials, counters, tot)) {
+    BiState<float> &b = st[s];
+    b.bnorm64 = sqrt(tot[1]);
+    const double rn = sqrt(tot[0]);
+    b.res64 = b.bnorm64 > 0 ? rn / b.bnorm64 : 0.0;
+    b.maxr = rn;
+    b.rho = (float)tot[2];
+    b.upd = 0;
+    if (!force) b.nupd += 1;
+    if (b.bnorm64 == 0.0 || b.res64 < tol64) { b.done = 1; b.status = 0; return; }
+    if (b.iter >= b.max_iter) { b.done = 1; b.status = VSHE_E_NOT_CONVERGED_DEV; return; }
+    if (force) { b.bnorm = (float)rn; b.restart = 1; }
   }
 }
 
@@ -267,9 +362,8 @@ __global__ void __launch_bounds__(kThreads) k_precond_copy(const SysDev<T> *sys,
 }
 
 // ------------------------------------------------------------ grid barrier
-// Sense-free generation barrier for a cooperative launch (all CTAs resident).
-// The spin is bounded: after `limit` polls the kernel records a timeout and
-// every CTA leaves; the host sees the error flag.
+// Generation barrier for a cooperative launch (all CTAs resident).  The spin is
+// bounded: after `limit` polls the kernel records a timeout and every CTA leaves.
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -280,7 +374,6 @@ __device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
 }
 
 __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
-  // bar[0] = arrival count, bar[1] = generation
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -304,7 +397,7 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
       while (ld_acquire_u32(&bar[1]) == gen) {
         if (++spins > limit) { atomicExch(err, VSHE_E_TIMEOUT_DEV); ok = 0; break; }
         if ((spins & 255) == 0 && *((volatile int32_t *)err) != 0) { ok = 0; break; }  // another CTA gave up
-        if (spins > 64) __nanosleep(64);
+        if (spins > 64) __nanosleep(32);
       }
     }
     if (ok && *((volatile int32_t *)err) != 0) ok = 0;
@@ -314,7 +407,7 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
 }
 
 // ------------------------------------------------- triangular solves (ILU apply)
-// out = U^{-1} L^{-1} in, level by level.  which 0: ph = M^{-1} p, 1: sh = M^{-1} s.
+// out = P^T U^{-1} L^{-1} P in over the level-ordered factors.  which 0: ph = M^{-1} p, 1: sh = M^{-1} s.
 template <typename T, int G>
 __device__ __forceinline__ void trsv_level_rows(const SysDev<T> *sys, const BiState<T> *st, const int32_t *active, const Levels lv, int k, bool lower, int which) {
   const int lane = threadIdx.x % G;
@@ -331,22 +424,30 @@ __device__ __forceinline__ void trsv_level_rows(const SysDev<T> *sys, const BiSt
       valid = active[s] && !st[s].done && !(which == 1 && st[s].s_conv);
     }
     const SysDev<T> *S = &sys[s];
-    const int64_t row = valid ? (int64_t)lv.ent_row[e] : 0;
-    T *out = which == 0 ? S->ph : S->sh;
+    const int64_t q = valid ? (lv.ent_row ? (int64_t)lv.ent_row[e] : e) : 0;
     T sum = T(0);
     if (lower) {
+      const int32_t row = valid ? S->lrow[q] : 0;
       if (valid)
-        for (int64_t q = S->lrp[row] + lane; q < S->lrp[row + 1]; q += G) sum += S->lv[q] * __ldcg(&out[S->lci[q]]);
+        for (int64_t j = S->lptr[q] + lane; j < S->lptr[q + 1]; j += G) sum += S->lval[j] * __ldcg(&S->ytmp[S->lcol[j]]);
       sum = group_sum<T, G>(sum);
       if (valid && lane == 0) {
         const T *in = which == 0 ? S->p : S->s;
-        out[row] = in[row] - sum;
+        const int32_t orow = S->perm ? S->perm[row] : row;
+        S->ytmp[row] = in[orow] - sum;
       }
     } else {
+      const int32_t row = valid ? S->urow[q] : 0;
       if (valid)
-        for (int64_t q = S->urp[row] + lane; q < S->urp[row + 1]; q += G) sum += S->uv[q] * __ldcg(&out[S->uci[q]]);
+        for (int64_t j = S->uptr[q] + lane; j < S->uptr[q + 1]; j += G) sum += S->uval[j] * __ldcg(&S->ytmp[S->ucol[j]]);
       sum = group_sum<T, G>(sum);
-      if (valid && lane == 0) out[row] = (__ldcg(&out[row]) - sum) * S->dinv[row];
+      if (valid && lane == 0) {
+        const T y = (__ldcg(&S->ytmp[row]) - sum) * S->udinv[q];
+        S->ytmp[row] = y;
+        T *out = which == 0 ? S->ph : S->sh;
+        const int32_t orow = S->perm ? S->perm[row] : row;
+        out[orow] = y;
+      }
     }
   }
 }
@@ -371,9 +472,7 @@ __global__ void __launch_bounds__(kThreads) k_trsv_level(const SysDev<T> *sys, c
 // ------------------------------------------------------ ILU(0) factorisation
 // Row-wise IKJ ILU(0) (Saad, Alg. 10.4) restricted to within-block entries,
 // one warp per row, rows of a level in parallel.  Values in FP64.
-
 __device__ __forceinline__ int64_t find_col(const int32_t *ci, int64_t a, int64_t b, int32_t j) {
-  // binary search for column j in ci[a, b)
   int64_t lo = a, hi = b - 1;
   while (lo <= hi) {
     int64_t mid = (lo + hi) >> 1;
@@ -384,6 +483,7 @@ __device__ __forceinline__ int64_t find_col(const int32_t *ci, int64_t a, int64_
   return -1;
 }
 
+// level entries here are permuted-space row ids (ent_row = row) of system ent_sys
 __device__ void ilu0_level_rows(const FactDev *fs, Levels lv, int k, int32_t *err) {
   const int lane = threadIdx.x & 31;
   const int64_t gid = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
@@ -428,26 +528,29 @@ __global__ void __launch_bounds__(kThreads) k_ilu0_level(const FactDev *fs, Leve
   ilu0_level_rows(fs, lv, k, err);
 }
 
-// Split the factor (in A's pattern, FP64) into strict L, strict U and 1/diag(U) in precision T.
-template <typename T>
-__global__ void k_split_factor(int64_t n, const int64_t *rp, const int32_t *ci, const double *lu, const int32_t *blk,
-                               const int64_t *lrp, T *lv, const int64_t *urp, T *uv, T *dinv) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t lp = lrp[i], up = urp[i];
-    const int32_t bi = blk[i];
-    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
-      const int32_t j = ci[k];
-      if (j == i) { dinv[i] = (T)(1.0 / lu[k]); continue; }
-      if (blk[j] != bi) continue;
-      if (j < i) lv[lp++] = (T)lu[k];
-      else uv[up++] = (T)lu[k];
-    }
-  }
+// permuted factor values from A: lu[kp] = av[amap[kp]]
+__global__ void k_gather_values(int64_t nnz, const int64_t *amap, const double *av, double *lu) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x)
+    lu[k] = av[amap[k]];
 }
 
-// ------------------------------------------------------- FP64 refinement
-// r = b - A x (FP64), ||r||^2 per system -> rnorm[s]; counters/partials as for the Krylov kernels.
+// Split the permuted factor (FP64, permuted CSR) into level-ordered L, U and the
+// inverse diagonal in precision T: fmap[kp] >= 0 -> L slot, <= -2 -> U slot -(fmap+2),
+// -1 -> not part of the factor; dpos[row] is the U-level position of the row.
+template <typename T>
+__global__ void k_split_factor(int64_t nnz, int64_t n, const double *lu, const int64_t *fmap, const int64_t *diag, const int64_t *dpos,
+                               T *lval, T *uval, T *udinv) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t m = fmap[k];
+    if (m >= 0) lval[m] = (T)lu[k];
+    else if (m <= -2) uval[-(m + 2)] = (T)lu[k];
+  }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    udinv[dpos[i]] = (T)(1.0 / lu[diag[i]]);
+}
 
+// ------------------------------------------------------- FP64 residual
+// r = b - A x (FP64), ||r||^2 and ||b||^2 per system -> rnorm2 / bnorm2.
 template <int G>
 __global__ void __launch_bounds__(kThreads) k_residual64(const RefDev *sys, Tiles tl, double *partials, int32_t *counters, const int32_t *active, double *rnorm2, double *bnorm2) {
   const int tile = blockIdx.x;
@@ -481,28 +584,6 @@ __global__ void __launch_bounds__(kThreads) k_residual64(const RefDev *sys, Tile
   }
 }
 
-// inner rhs: r32 = r64 / ||r64||
-__global__ void k_scale_to_f32(const RefDev *ref, const SysDev<float> *sys, Tiles tl, const int32_t *active, const double *rnorm2) {
-  const int tile = blockIdx.x;
-  const int s = tl.tile_sys[tile];
-  if (!active[s]) return;
-  const double inv = rnorm2[s] > 0.0 ? 1.0 / sqrt(rnorm2[s]) : 0.0;
-  const double *r = ref[s].r;
-  float *r32 = sys[s].r;
-  for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += blockDim.x) r32[i] = (float)(r[i] * inv);
-}
-
-// x64 += ||r64|| * x32
-__global__ void k_accumulate_x(const RefDev *ref, const SysDev<float> *sys, Tiles tl, const int32_t *active, const double *rnorm2) {
-  const int tile = blockIdx.x;
-  const int s = tl.tile_sys[tile];
-  if (!active[s]) return;
-  const double sc = sqrt(rnorm2[s]);
-  double *x = ref[s].x;
-  const float *d = sys[s].x;
-  for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += blockDim.x) x[i] += sc * (double)d[i];
-}
-
 __global__ void k_cast_f64_f32(int64_t n, const double *a, float *b) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = (float)a[i];
 }
@@ -532,8 +613,18 @@ __global__ void __launch_bounds__(kThreads) k_spmv_plain(int64_t n, const int64_
 // =====================================================================
 using namespace vshe;
 
+static inline int grid_for(int64_t n) {
+  int64_t g = (n + kThreads - 1) / kThreads;
+  if (g > 65535LL * 16) g = 65535LL * 16;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+static std::atomic<long long> g_launches{0};
+
 template <typename T, int G>
 static void launch_spmv_dot_g(int ntiles, const SysDev<T> *sys, BiState<T> *st, Tiles tl, T *part, int32_t *cnt, const int32_t *act, int which, cudaStream_t s) {
+  g_launches += 1;
   k_spmv_dot<T, G><<<ntiles, kThreads, 0, s>>>(sys, st, tl, part, cnt, act, which);
 }
 
@@ -549,61 +640,53 @@ static void launch_spmv_dot_t(int group, int ntiles, const SysDev<T> *sys, BiSta
 }
 
 template <typename T>
+static void *trsv_fn(int group) {
+  switch (group) {
+    case 1: return (void *)k_trsv_persistent<T, 1>;
+    case 2: return (void *)k_trsv_persistent<T, 2>;
+    case 4: return (void *)k_trsv_persistent<T, 4>;
+    default: return (void *)k_trsv_persistent<T, 8>;
+  }
+}
+
+template <typename T>
 static int launch_trsv_t(int mode, int group, int grid, const SysDev<T> *sys, const BiState<T> *st, const int32_t *act, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err, cudaStream_t s) {
   if (mode == 1) {
+    g_launches += 1;
     void *args[] = {(void *)&sys, (void *)&st, (void *)&act, (void *)&lL, (void *)&lU, (void *)&which, (void *)&bar, (void *)&err};
-    void *fn;
-    switch (group) {
-      case 1: fn = (void *)k_trsv_persistent<T, 1>; break;
-      case 2: fn = (void *)k_trsv_persistent<T, 2>; break;
-      case 4: fn = (void *)k_trsv_persistent<T, 4>; break;
-      default: fn = (void *)k_trsv_persistent<T, 8>; break;
-    }
-    return (int)cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, 0, s);
+    return (int)cudaLaunchCooperativeKernel(trsv_fn<T>(group), dim3(grid), dim3(kThreads), args, 0, s);
   }
-  for (int k = 0; k < lL.nlev; ++k) {
-    switch (group) {
-      case 1: k_trsv_level<T, 1><<<grid, kThreads, 0, s>>>(sys, st, act, lL, k, 1, which); break;
-      case 2: k_trsv_level<T, 2><<<grid, kThreads, 0, s>>>(sys, st, act, lL, k, 1, which); break;
-      case 4: k_trsv_level<T, 4><<<grid, kThreads, 0, s>>>(sys, st, act, lL, k, 1, which); break;
-      default: k_trsv_level<T, 8><<<grid, kThreads, 0, s>>>(sys, st, act, lL, k, 1, which); break;
-    }
-  }
-  for (int k = 0; k < lU.nlev; ++k) {
-    switch (group) {
-      case 1: k_trsv_level<T, 1><<<grid, kThreads, 0, s>>>(sys, st, act, lU, k, 0, which); break;
-      case 2: k_trsv_level<T, 2><<<grid, kThreads, 0, s>>>(sys, st, act, lU, k, 0, which); break;
-      case 4: k_trsv_level<T, 4><<<grid, kThreads, 0, s>>>(sys, st, act, lU, k, 0, which); break;
-      default: k_trsv_level<T, 8><<<grid, kThreads, 0, s>>>(sys, st, act, lU, k, 0, which); break;
+  g_launches += lL.nlev + lU.nlev;
+  for (int pass = 0; pass < 2; ++pass) {
+    const Levels &lv = pass == 0 ? lL : lU;
+    for (int k = 0; k < lv.nlev; ++k) {
+      switch (group) {
+        case 1: k_trsv_level<T, 1><<<grid, kThreads, 0, s>>>(sys, st, act, lv, k, 1 - pass, which); break;
+        case 2: k_trsv_level<T, 2><<<grid, kThreads, 0, s>>>(sys, st, act, lv, k, 1 - pass, which); break;
+        case 4: k_trsv_level<T, 4><<<grid, kThreads, 0, s>>>(sys, st, act, lv, k, 1 - pass, which); break;
+        default: k_trsv_level<T, 8><<<grid, kThreads, 0, s>>>(sys, st, act, lv, k, 1 - pass, which); break;
+      }
     }
   }
   return (int)cudaGetLastError();
 }
 
-template <typename T>
-static int occupancy_persistent_t(int group, int *blocks_per_sm) {
-  void *fn;
-  switch (group) {
-    case 1: fn = (void *)k_trsv_persistent<T, 1>; break;
-    case 2: fn = (void *)k_trsv_persistent<T, 2>; break;
-    case 4: fn = (void *)k_trsv_persistent<T, 4>; break;
-    default: fn = (void *)k_trsv_persistent<T, 8>; break;
-  }
-  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, kThreads, 0);
-}
-
 extern "C" {
 
 int vk_threads() { return kThreads; }
+void vk_count_launches(long long k) { g_launches += k; }
+long long vk_launches_total() { return g_launches.load(); }
 
 #define VK_BODY_T(T, SUF)                                                                                             \
   void vk_bicg_init_##SUF(int ntiles, const void *sys, void *st, const VkTiles *tl, T *part, int32_t *cnt,           \
                           const int32_t *act, cudaStream_t s) {                                                      \
+    g_launches += 1;                                                                                                 \
     k_bicg_init<T><<<ntiles, kThreads, 0, s>>>((const SysDev<T> *)sys, (BiState<T> *)st, *(const Tiles *)tl, part, cnt, act); \
   }                                                                                                                  \
-  void vk_update_p_##SUF(int ntiles, const void *sys, const void *st, const VkTiles *tl, const int32_t *act,        \
+  void vk_update_p_##SUF(int ntiles, const void *sys, void *st, const VkTiles *tl, const int32_t *act,              \
                          cudaStream_t s) {                                                                           \
-    k_update_p<T><<<ntiles, kThreads, 0, s>>>((const SysDev<T> *)sys, (const BiState<T> *)st, *(const Tiles *)tl, act); \
+    g_launches += 1;                                                                                                 \
+    k_update_p<T><<<ntiles, kThreads, 0, s>>>((const SysDev<T> *)sys, (BiState<T> *)st, *(const Tiles *)tl, act);    \
   }                                                                                                                  \
   void vk_spmv_dot_##SUF(int group, int ntiles, const void *sys, void *st, const VkTiles *tl, T *part, int32_t *cnt, \
                          const int32_t *act, int which, cudaStream_t s) {                                            \
@@ -611,14 +694,17 @@ int vk_threads() { return kThreads; }
   }                                                                                                                  \
   void vk_update_s_##SUF(int ntiles, const void *sys, void *st, const VkTiles *tl, T *part, int32_t *cnt,           \
                          const int32_t *act, cudaStream_t s) {                                                       \
+    g_launches += 1;                                                                                                 \
     k_update_s<T><<<ntiles, kThreads, 0, s>>>((const SysDev<T> *)sys, (BiState<T> *)st, *(const Tiles *)tl, part, cnt, act); \
   }                                                                                                                  \
   void vk_update_xr_##SUF(int ntiles, const void *sys, void *st, const VkTiles *tl, T *part, int32_t *cnt,          \
-                          const int32_t *act, cudaStream_t s) {                                                      \
-    k_update_xr<T><<<ntiles, kThreads, 0, s>>>((const SysDev<T> *)sys, (BiState<T> *)st, *(const Tiles *)tl, part, cnt, act); \
+                          const int32_t *act, int reliable, cudaStream_t s) {                                        \
+    g_launches += 1;                                                                                                 \
+    k_update_xr<T><<<ntiles, kThreads, 0, s>>>((const SysDev<T> *)sys, (BiState<T> *)st, *(const Tiles *)tl, part, cnt, act, reliable); \
   }                                                                                                                  \
   void vk_precond_copy_##SUF(int ntiles, const void *sys, const void *st, const VkTiles *tl, const int32_t *act,    \
                              int which, cudaStream_t s) {                                                            \
+    g_launches += 1;                                                                                                 \
     k_precond_copy<T><<<ntiles, kThreads, 0, s>>>((const SysDev<T> *)sys, (const BiState<T> *)st, *(const Tiles *)tl, act, which); \
   }                                                                                                                  \
   int vk_trsv_##SUF(int mode, int group, int grid, const void *sys, const void *st, const int32_t *act,             \
@@ -626,16 +712,17 @@ int vk_threads() { return kThreads; }
     return launch_trsv_t<T>(mode, group, grid, (const SysDev<T> *)sys, (const BiState<T> *)st, act, *(const Levels *)lL, \
                             *(const Levels *)lU, which, bar, err, s);                                                \
   }                                                                                                                  \
-  int vk_trsv_occupancy_##SUF(int group, int *blocks_per_sm) { return occupancy_persistent_t<T>(group, blocks_per_sm); } \
-  void vk_split_factor_##SUF(int64_t n, const int64_t *rp, const int32_t *ci, const double *lu, const int32_t *blk,  \
-                             const int64_t *lrp, T *lv, const int64_t *urp, T *uv, T *dinv, cudaStream_t s) {        \
-    int grid = (int)((n + kThreads - 1) / kThreads);                                                                 \
-    if (grid > 65535 * 16) grid = 65535 * 16;                                                                        \
-    if (grid < 1) grid = 1;                                                                                          \
-    k_split_factor<T><<<grid, kThreads, 0, s>>>(n, rp, ci, lu, blk, lrp, lv, urp, uv, dinv);                        \
+  int vk_trsv_occupancy_##SUF(int group, int *blocks_per_sm) {                                                       \
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, trsv_fn<T>(group), kThreads, 0);       \
+  }                                                                                                                  \
+  void vk_split_factor_##SUF(int64_t nnz, int64_t n, const double *lu, const int64_t *fmap, const int64_t *diag,     \
+                             const int64_t *dpos, T *lval, T *uval, T *udinv, cudaStream_t s) {                      \
+    g_launches += 1;                                                                                                 \
+    k_split_factor<T><<<grid_for(nnz > n ? nnz : n), kThreads, 0, s>>>(nnz, n, lu, fmap, diag, dpos, lval, uval, udinv); \
   }                                                                                                                  \
   void vk_spmv_plain_##SUF(int group, int grid, int64_t n, const int64_t *rp, const int32_t *ci, const T *av,       \
                            const T *x, T *y, cudaStream_t s) {                                                       \
+    g_launches += 1;                                                                                                 \
     switch (group) {                                                                                                 \
       case 2: k_spmv_plain<T, 2><<<grid, kThreads, 0, s>>>(n, rp, ci, av, x, y); break;                             \
       case 4: k_spmv_plain<T, 4><<<grid, kThreads, 0, s>>>(n, rp, ci, av, x, y); break;                             \
@@ -648,19 +735,46 @@ int vk_threads() { return kThreads; }
 VK_BODY_T(float, f32)
 VK_BODY_T(double, f64)
 
+void vk_reliable_x(int ntiles, const void *sys32, const void *st, const VkTiles *tl, const int32_t *act, cudaStream_t s) {
+  g_launches += 1;
+  k_reliable_x<<<ntiles, kThreads, 0, s>>>((const SysDev<float> *)sys32, (const BiState<float> *)st, *(const Tiles *)tl, act);
+}
+
+void vk_reliable_r(int group, int ntiles, const void *sys32, void *st, const VkTiles *tl, double *part, int32_t *cnt,
+                   const int32_t *act, double tol64, int force, cudaStream_t s) {
+  const SysDev<float> *S = (const SysDev<float> *)sys32;
+  BiState<float> *B = (BiState<float> *)st;
+  const Tiles t = *(const Tiles *)tl;
+  g_launches += 1;
+  switch (group) {
+    case 2: k_reliable_r<2><<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force); break;
+    case 4: k_reliable_r<4><<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force); break;
+    case 8: k_reliable_r<8><<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force); break;
+    case 16: k_reliable_r<16><<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force); break;
+    default: k_reliable_r<32><<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force); break;
+  }
+}
+
 int vk_ilu0(int mode, int grid, const void *fs, const VkLevels *lv, unsigned *bar, int32_t *err, cudaStream_t s) {
   const FactDev *f = (const FactDev *)fs;
   Levels L = *(const Levels *)lv;
   if (mode == 1) {
+    g_launches += 1;
     void *args[] = {(void *)&f, (void *)&L, (void *)&bar, (void *)&err};
     return (int)cudaLaunchCooperativeKernel((void *)k_ilu0_persistent, dim3(grid), dim3(kThreads), args, 0, s);
   }
+  g_launches += L.nlev;
   for (int k = 0; k < L.nlev; ++k) k_ilu0_level<<<grid, kThreads, 0, s>>>(f, L, k, err);
   return (int)cudaGetLastError();
 }
 
 int vk_ilu0_occupancy(int *blocks_per_sm) {
   return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, (void *)k_ilu0_persistent, kThreads, 0);
+}
+
+void vk_gather_values(int64_t nnz, const int64_t *amap, const double *av, double *lu, cudaStream_t s) {
+  g_launches += 1;
+  k_gather_values<<<grid_for(nnz), kThreads, 0, s>>>(nnz, amap, av, lu);
 }
 
 size_t vk_factdev_size() { return sizeof(FactDev); }
@@ -674,6 +788,7 @@ void vk_residual64(int group, int ntiles, const void *ref, const VkTiles *tl, do
                    double *rnorm2, double *bnorm2, cudaStream_t s) {
   const Tiles t = *(const Tiles *)tl;
   const RefDev *r = (const RefDev *)ref;
+  g_launches += 1;
   switch (group) {
     case 2: k_residual64<2><<<ntiles, kThreads, 0, s>>>(r, t, part, cnt, act, rnorm2, bnorm2); break;
     case 4: k_residual64<4><<<ntiles, kThreads, 0, s>>>(r, t, part, cnt, act, rnorm2, bnorm2); break;
@@ -683,19 +798,9 @@ void vk_residual64(int group, int ntiles, const void *ref, const VkTiles *tl, do
   }
 }
 
-void vk_scale_to_f32(int ntiles, const void *ref, const void *sys32, const VkTiles *tl, const int32_t *act, const double *rnorm2, cudaStream_t s) {
-  k_scale_to_f32<<<ntiles, kThreads, 0, s>>>((const RefDev *)ref, (const SysDev<float> *)sys32, *(const Tiles *)tl, act, rnorm2);
-}
-
-void vk_accumulate_x(int ntiles, const void *ref, const void *sys32, const VkTiles *tl, const int32_t *act, const double *rnorm2, cudaStream_t s) {
-  k_accumulate_x<<<ntiles, kThreads, 0, s>>>((const RefDev *)ref, (const SysDev<float> *)sys32, *(const Tiles *)tl, act, rnorm2);
-}
-
 void vk_cast_f64_f32(int64_t n, const double *a, float *b, cudaStream_t s) {
-  int grid = (int)((n + kThreads - 1) / kThreads);
-  if (grid > 65535 * 16) grid = 65535 * 16;
-  if (grid < 1) grid = 1;
-  k_cast_f64_f32<<<grid, kThreads, 0, s>>>(n, a, b);
+  g_launches += 1;
+  k_cast_f64_f32<<<grid_for(n), kThreads, 0, s>>>(n, a, b);
 }
 
 }  // extern "C"

@@ -5,35 +5,51 @@
 
 namespace vshe {
 
-// One linear system of a batch, as the kernels see it (all device pointers).
+// One linear system of a batch, as the Krylov kernels see it (all device pointers).
 // T is the arithmetic type of the Krylov iteration (float or double).
+//
+// The matrix A is kept in the caller's row order for the SpMV.  The incomplete
+// factors belong to the permuted matrix P A P^T and are stored level by level:
+// entry k of the forward solve is row lrow[k] (permuted numbering) with strict
+// lower entries [lptr[k], lptr[k+1]) of (lcol, lval); entry k of the backward
+// solve is row urow[k] with strict upper entries [uptr[k], uptr[k+1]) and the
+// inverse diagonal udinv[k].  perm[i] is the original row of permuted row i.
 template <typename T>
 struct SysDev {
   int64_t n;
-  // A in precision T (pattern shared with the FP64 copy)
   const int64_t *rp;
   const int32_t *ci;
   const T *av;
-  // incomplete factors: strict lower L (unit diagonal), strict upper U, 1 / diag(U)
-  const int64_t *lrp; const int32_t *lci; const T *lv;
-  const int64_t *urp; const int32_t *uci; const T *uv;
-  const T *dinv;
-  // Krylov vectors (length n)
+  const int32_t *perm;
+  const int32_t *lrow; const int64_t *lptr; const int32_t *lcol; const T *lval;
+  const int32_t *urow; const int64_t *uptr; const int32_t *ucol; const T *uval; const T *udinv;
+  T *ytmp;  // permuted-order work vector of the triangular solves
+  // Krylov vectors (original order)
   T *x, *r, *rh, *p, *v, *s, *t, *ph, *sh;
+  // FP64 side of the mixed-precision solve (reliable updates)
+  const double *av64;
+  const double *b64;
+  double *x64, *r64;
 };
 
 // Per-system BiCGStab state, resident on the device.
 template <typename T>
 struct BiState {
   T rho, rho_old, alpha, omega;
-  T bnorm;        // ||b|| of the current (inner) solve
-  T res;          // ||r|| / ||b||
-  T tol;          // relative tolerance of the current (inner) solve
-  int32_t iter;   // iterations done in the current solve
+  T bnorm;        // ||b|| of the Krylov solve
+  T res;          // ||r|| / ||b|| (recursive residual)
+  T tol;          // relative tolerance
+  int32_t iter;   // iterations done
   int32_t max_iter;
   int32_t done;   // 1 = converged or stopped
   int32_t s_conv; // 1 = ||s|| already below tol in this iteration
   int32_t status; // 0 ok, VSHE_E_BREAKDOWN, ...
+  int32_t upd;    // reliable update requested (mixed)
+  int32_t restart;// next iteration restarts the Krylov recurrence (p = r)
+  int32_t nupd;   // reliable updates done
+  double res64;   // true FP64 residual ||b - A x64|| / ||b|| after the last reliable update
+  double maxr;    // residual norm at the last reliable update (FP64)
+  double bnorm64; // ||b|| in FP64
 };
 
 // Tiles: contiguous row ranges inside one system.  Reductions are per tile,
@@ -46,8 +62,9 @@ struct Tiles {
   const int32_t *sys_tile0;
 };
 
-// Level schedule of a batch: entries of global level k are
-// [lvl_ptr[k], lvl_ptr[k+1]) of (ent_sys, ent_row).
+// Level schedule of a batch: entries of global level k are [lvl_ptr[k], lvl_ptr[k+1]);
+// entry e is level-ordered position ent_row[e] of system ent_sys[e] (for a single
+// system both arrays are NULL and the entry index is the position).
 struct Levels {
   int32_t nlev;
   const int64_t *lvl_ptr;
@@ -55,7 +72,9 @@ struct Levels {
   const int32_t *ent_row;
 };
 
-// ILU(0) factorisation view of one system (values in FP64, in A's pattern).
+// ILU(0) factorisation view of one system: values in FP64 in the permuted
+// matrix's CSR (prp, pci), filled from A's values through amap (permuted entry
+// -> original entry); diag[i] = position of the diagonal in row i.
 struct FactDev {
   int64_t n;
   const int64_t *rp;

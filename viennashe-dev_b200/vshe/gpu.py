@@ -21,6 +21,7 @@ ERRORS = {
 }
 PRECISION = {"fp64": 0, "mixed": 1}
 PRECOND = {"none": 0, "ilu0": 1, "block_ilu0": 2}
+ORDERING = {"natural": 0, "multicolor": 1}
 TRSV = {"auto": 0, "persistent": 1, "per_level": 2}
 
 _lib = None
@@ -61,12 +62,21 @@ def lib():
         L.vshe_system_spmv.argtypes = [vp, C.c_int64, C.c_int32, f64p, f64p]
         L.vshe_system_factor_values.argtypes = [vp, C.c_int64, f64p]
         L.vshe_system_time_spmv.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, f64p]
+        L.vshe_set_profiling.argtypes = [vp, C.c_int32]
+        L.vshe_get_profile.argtypes = [vp, f64p, i64p]
+        L.vshe_kernel_launches.restype = C.c_int64
+        L.vshe_kernel_launches.argtypes = []
         _lib = L
     return _lib
 
 
+def kernel_launches():
+    """This library's own kernel launches in the process so far."""
+    return int(lib().vshe_kernel_launches())
+
+
 def make_opts(precision="mixed", precond="ilu0", tol=1e-10, max_iters=1000, inner_tol=1e-5,
-              max_refinements=10, blocks=None, trsv="auto", check_every=8):
+              max_refinements=10, blocks=None, trsv="auto", check_every=8, ordering="natural", perm=None):
     o = SolveOptsC()
     lib().vshe_default_opts(C.byref(o))
     o.precision = PRECISION[precision]
@@ -77,11 +87,17 @@ def make_opts(precision="mixed", precond="ilu0", tol=1e-10, max_iters=1000, inne
     o.max_refinements = max_refinements
     o.trsv_mode = TRSV[trsv]
     o.check_every = check_every
-    keep = None
+    o.ordering = ORDERING[ordering]
+    keep = []
     if blocks is not None:
-        keep = np.ascontiguousarray(blocks, np.int64)
-        o.n_blocks = len(keep) - 1
-        o.block_ptr = ptr(keep, C.c_int64)
+        kb = np.ascontiguousarray(blocks, np.int64)
+        keep.append(kb)
+        o.n_blocks = len(kb) - 1
+        o.block_ptr = ptr(kb, C.c_int64)
+    if perm is not None:
+        kp = np.ascontiguousarray(perm, np.int32)
+        keep.append(kp)
+        o.perm = ptr(kp, C.c_int32)
     return o, keep
 
 
@@ -116,6 +132,17 @@ class Context:
 
     def bytes_in_use(self):
         return int(lib().vshe_bytes_in_use(self.h))
+
+    def set_profiling(self, on=True):
+        self._check(lib().vshe_set_profiling(self.h, 1 if on else 0))
+
+    def profile(self):
+        """Device ms of the last solve per kernel class and launch counts."""
+        ms = np.zeros(5)
+        cnt = np.zeros(2, np.int64)
+        self._check(lib().vshe_get_profile(self.h, ptr(ms, C.c_double), ptr(cnt, C.c_int64)))
+        return dict(spmv_ms=ms[0], trsv_ms=ms[1], vector_ms=ms[2], reliable_ms=ms[3], factor_ms=ms[4],
+                    spmv_launches=int(cnt[0]), trsv_launches=int(cnt[1]))
 
     def solve_csr(self, rp, ci, v, b, **kw):
         """The drop-in call: host CSR + rhs in, host x out (copies inside)."""
@@ -201,3 +228,136 @@ class System:
         ms = C.c_double()
         self.ctx._check(lib().vshe_system_time_spmv(self.ctx.h, self.h, PRECISION[precision], reps, C.byref(ms)))
         return ms.value
+
+
+# ---------------------------------------------------------------- SHE path
+class SheInfoC(C.Structure):
+    _fields_ = [
+        ("n_energies", C.c_int32), ("n_even", C.c_int64), ("n_odd", C.c_int64),
+        ("nnz_full", C.c_int64), ("nnz_reduced", C.c_int64),
+        ("n_cells", C.c_int32), ("n_facets", C.c_int32), ("n_contacts", C.c_int32),
+        ("hbar_omega", C.c_double), ("bytes_device", C.c_int64),
+        ("levels_L", C.c_int32), ("levels_U", C.c_int32),
+    ]
+
+
+def _she_lib():
+    L = lib()
+    if not getattr(L, "_she_ready", False):
+        i64p = C.POINTER(C.c_int64)
+        i32p = C.POINTER(C.c_int32)
+        f64p = C.POINTER(C.c_double)
+        vp = C.c_void_p
+        L.vshe_coupling_tables_compute.argtypes = [C.c_int32, f64p]
+        L.vshe_she_create.argtypes = [vp, vp, vp, vp, C.POINTER(SolveOptsC), i64p]
+        L.vshe_she_info_get.argtypes = [vp, C.c_int64, C.POINTER(SheInfoC)]
+        L.vshe_she_assemble.argtypes = [vp, C.c_int64, C.c_int32]
+        L.vshe_she_solve.argtypes = [vp, C.c_int64, C.POINTER(SolveStatsC)]
+        L.vshe_she_finish.argtypes = [vp, C.c_int64, f64p]
+        L.vshe_she_run.argtypes = [vp, C.c_int64, C.POINTER(SolveStatsC), f64p]
+        L.vshe_she_results.argtypes = [vp, C.c_int64, f64p, f64p, f64p]
+        L.vshe_she_export.argtypes = [vp, C.c_int64, C.c_int32, i64p, i32p, f64p, f64p]
+        L.vshe_she_scaling.argtypes = [vp, C.c_int64, f64p, f64p]
+        L.vshe_she_free.argtypes = [vp, C.c_int64]
+        L.vshe_she_bench.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, f64p, C.POINTER(SolveStatsC)]
+        L._she_ready = True
+    return L
+
+
+def coupling_tables(L):
+    """Coupling tables a_{x,y,z}, b_{x,y,z} of order L from the library's quadrature (no GPU needed)."""
+    from .abi import Coupling
+    D = (L + 1) ** 2
+    out = np.zeros((6, D, D))
+    rc = _she_lib().vshe_coupling_tables_compute(L, ptr(out, C.c_double))
+    if rc:
+        raise VsheError(rc, "vshe_coupling_tables_compute")
+    return Coupling(L, out)
+
+
+class SheProblem:
+    """A SHE problem assembled, eliminated, normalised and solved on the device (vshe_she_*)."""
+
+    def __init__(self, ctx: Context, dev, cfg, coupling=None, **opts):
+        from .abi import DeviceDesc, she_config_c
+        L = _she_lib()
+        self.ctx = ctx
+        self.dev = dev
+        self._desc = DeviceDesc(dev)
+        self._cfg = she_config_c(cfg)
+        self._cpl = coupling if coupling is not None else coupling_tables(cfg.max_expansion_order)
+        o, self._keep = make_opts(**opts)
+        h = C.c_int64()
+        rc = L.vshe_she_create(ctx.h, C.byref(self._desc.c), C.byref(self._cfg), C.byref(self._cpl.c), C.byref(o), C.byref(h))
+        ctx._check(rc)
+        self.h = h.value
+        self.info = self.get_info()
+
+    def get_info(self):
+        inf = SheInfoC()
+        self.ctx._check(_she_lib().vshe_she_info_get(self.ctx.h, self.h, C.byref(inf)))
+        return {k: getattr(inf, k) for k, _ in SheInfoC._fields_}
+
+    def free(self):
+        if self.h:
+            _she_lib().vshe_she_free(self.ctx.h, self.h)
+            self.h = 0
+
+    def assemble(self, upto=3):
+        self.ctx._check(_she_lib().vshe_she_assemble(self.ctx.h, self.h, upto))
+
+    def solve(self):
+        st = SolveStatsC()
+        rc = _she_lib().vshe_she_solve(self.ctx.h, self.h, C.byref(st))
+        if rc and rc != -6:
+            self.ctx._check(rc)
+        return stats_dict(st)
+
+    def finish(self):
+        r = C.c_double()
+        self.ctx._check(_she_lib().vshe_she_finish(self.ctx.h, self.h, C.byref(r)))
+        return r.value
+
+    def run(self):
+        st = SolveStatsC()
+        r = C.c_double()
+        rc = _she_lib().vshe_she_run(self.ctx.h, self.h, C.byref(st), C.byref(r))
+        if rc and rc != -6:
+            self.ctx._check(rc)
+        return stats_dict(st), r.value
+
+    def bench(self, warmup, steps):
+        """Per-run device times (ms) of assemble + solve + finish, and the last run's stats."""
+        ms = np.zeros(steps)
+        st = SolveStatsC()
+        rc = _she_lib().vshe_she_bench(self.ctx.h, self.h, warmup, steps, ptr(ms, C.c_double), C.byref(st))
+        if rc and rc != -6:
+            self.ctx._check(rc)
+        return ms, stats_dict(st)
+
+    def results(self):
+        nfull = self.info["n_even"] + self.info["n_odd"]
+        x = np.zeros(nfull)
+        dens = np.zeros(self.dev.n_cells)
+        cur = np.zeros(max(self.info["n_contacts"], 1))
+        self.ctx._check(_she_lib().vshe_she_results(self.ctx.h, self.h, ptr(x, C.c_double), ptr(dens, C.c_double), ptr(cur, C.c_double)))
+        return x, dens, cur[:self.info["n_contacts"]]
+
+    def export(self, which):
+        """which: 'full' or 'reduced' -> (row_ptr, col, val, rhs) of the current device state."""
+        w = 0 if which == "full" else 1
+        n = self.info["n_even"] + self.info["n_odd"] if w == 0 else self.info["n_even"]
+        nnz = self.info["nnz_full"] if w == 0 else self.info["nnz_reduced"]
+        rp = np.zeros(n + 1, np.int64)
+        ci = np.zeros(nnz, np.int32)
+        v = np.zeros(nnz)
+        b = np.zeros(n)
+        self.ctx._check(_she_lib().vshe_she_export(self.ctx.h, self.h, w, ptr(rp, C.c_int64), ptr(ci, C.c_int32), ptr(v, C.c_double), ptr(b, C.c_double)))
+        return rp, ci, v, b
+
+    def scaling(self):
+        n = self.info["n_even"]
+        s = np.zeros(n)
+        f = np.zeros(n)
+        self.ctx._check(_she_lib().vshe_she_scaling(self.ctx.h, self.h, ptr(s, C.c_double), ptr(f, C.c_double)))
+        return s, f
