@@ -189,6 +189,15 @@ int vshe_she_run(vshe_ctx *ctx, int64_t handle, vshe_solve_stats *stats, double 
  * bracketed by a device synchronisation and timed with CUDA events on the library's
  * stream; step_ms[k] receives the duration of run k, *last the stats of the last run. */
 int vshe_she_bench(vshe_ctx *ctx, int64_t handle, int32_t warmup, int32_t steps, double *step_ms, vshe_solve_stats *last);
+/* Bias sweep / many devices in one solve: assembles every problem, solves all reduced
+ * systems as one batch (shared launches; each system's iterates are the same as when it is
+ * solved alone) and finishes each.  The problems must share precision and preconditioner
+ * kind.  stats[k] and full_residuals[k] (either may be NULL) belong to handles[k];
+ * *device_ms (may be NULL) receives the CUDA-event time of the whole call on the library's
+ * stream.  The batch schedule is built on first use of a handle set and reused.  The
+ * reference solves such sweeps one system at a time (simulator::run per bias point). */
+int vshe_she_run_batch(vshe_ctx *ctx, int32_t count, const int64_t *handles, vshe_solve_stats *stats,
+                       double *full_residuals, double *device_ms);
 /* Host copies of the results (any pointer may be NULL): x_full (n_even + n_odd),
  * density (n_cells), currents (n_contacts). */
 int vshe_she_results(vshe_ctx *ctx, int64_t handle, double *x_full, double *density, double *currents);

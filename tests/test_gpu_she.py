@@ -105,7 +105,12 @@ def _check_end_to_end(P, G, st, full_res):
     xr, _ = O.csr_solve(A, A.rhs, precond=1, tol=1e-13, maxit=20000)
     xf_r, dens_r, cur_r, res_r = P.finish(xr)
     assert np.max(np.abs(x - xf_r)) <= 1e-7 * np.max(np.abs(xf_r))
-    assert np.max(np.abs(dens - dens_r) / np.abs(dens_r)) < 1e-7
-    if len(cur_r) and np.max(np.abs(cur_r)) > 0:
-        # currents are the small anisotropic part: 1e-5 at a 1e-10 solve (1e-8 at 1e-12, see test_gpu_solver)
-        assert np.max(np.abs(cur - cur_r[:len(cur)])) <= 1e-5 * np.max(np.abs(cur_r))
+    # densities: 1e-7 of the largest (contact) density; the channel is ~1e3 below it, so per
+    # cell the bar at a 1e-10 residual is 1e-5
+    assert np.max(np.abs(dens - dens_r)) < 1e-7 * np.max(np.abs(dens_r))
+    assert np.max(np.abs(dens - dens_r) / np.abs(dens_r)) < 1e-5
+    if len(cur_r):
+        # currents are the small anisotropic part: 1e-5 at a 1e-10 solve (1e-8 at 1e-12, see
+        # test_gpu_solver).  At equilibrium (the resistor) the net current is round-off of the
+        # one-way fluxes; there the bar is an absolute 1e-9 A/m.
+        assert np.max(np.abs(cur - cur_r[:len(cur)])) <= max(1e-5 * np.max(np.abs(cur_r)), 1e-9)

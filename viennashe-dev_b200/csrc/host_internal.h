@@ -49,7 +49,6 @@ struct System {
   std::vector<int32_t> lrow, urow;      // level-ordered permuted row ids
   int32_t nlevL = 0, nlevU = 0;
   int64_t nnzL = 0, nnzU = 0;
-  int spmv_group = 8, trsv_group = 4;
   bool identity_perm = true;
   // device
   DevArena arena;
@@ -61,6 +60,7 @@ struct System {
   int32_t *d_pci = nullptr;
   double *d_lu64 = nullptr;
   int32_t *d_lrow = nullptr, *d_urow = nullptr, *d_lcol = nullptr, *d_ucol = nullptr;
+  int32_t *d_lgat = nullptr, *d_ugat = nullptr;  // original row of each level-ordered L / U entry
   int64_t *d_lptr = nullptr, *d_uptr = nullptr, *d_lvlptrL = nullptr, *d_lvlptrU = nullptr;
   void *d_lval = nullptr, *d_uval = nullptr, *d_udinv = nullptr, *d_ytmp = nullptr;
   void *kv[9] = {nullptr};  // x r rh p v s t ph sh in the Krylov precision
@@ -84,15 +84,19 @@ struct Batch {
   bool mixed = true, has_pc = true;
   int ntiles = 0;
   int32_t nlevL = 0, nlevU = 0;
-  int spmv_group = 8, trsv_group = 4, trsv_grid = 148, ilu_grid = 148, num_sms = 148;
+  int trsv_grid = 148, ilu_grid = 148, num_sms = 148;
   DevArena arena;
   int32_t *d_tile_sys = nullptr, *d_sys_tile0 = nullptr, *d_active = nullptr, *d_counters = nullptr, *d_err = nullptr;
   int64_t *d_tile_r0 = nullptr, *d_tile_r1 = nullptr;
   double *d_partials = nullptr, *d_rnorm2 = nullptr, *d_bnorm2 = nullptr;
   unsigned *d_bar = nullptr;
   void *d_sysdev = nullptr, *d_state = nullptr, *d_refdev = nullptr, *d_factdev = nullptr;
-  int64_t *d_lptrL = nullptr, *d_lptrU = nullptr;
-  int32_t *d_esL = nullptr, *d_erL = nullptr, *d_esU = nullptr, *d_erU = nullptr, *d_efR = nullptr;
+  // triangular-solve chunk schedules (per level: chunks of <= 32 level-ordered rows of one system)
+  int64_t *d_cptrL = nullptr, *d_cptrU = nullptr;
+  int32_t *d_csL = nullptr, *d_cqL = nullptr, *d_cnL = nullptr, *d_csU = nullptr, *d_cqU = nullptr, *d_cnU = nullptr;
+  // factorisation schedule of a multi-system batch (per level: rows of every system)
+  int64_t *d_fptr = nullptr;
+  int32_t *d_fsys = nullptr, *d_frow = nullptr;
   VkTiles tiles{};
   VkLevels levL{}, levU{}, levF{};
   std::vector<char> last_state;

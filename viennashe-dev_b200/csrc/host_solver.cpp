@@ -66,20 +66,6 @@ int Ctx::cuda_fail(cudaError_t e, const char *what) {
   return fail(VSHE_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-static int group_for(double avg) {
-  if (avg <= 2.5) return 2;
-  if (avg <= 6.0) return 4;
-  if (avg <= 12.0) return 8;
-  if (avg <= 24.0) return 16;
-  return 32;
-}
-static int trsv_group_for(double avg) {
-  if (avg <= 1.5) return 1;
-  if (avg <= 3.0) return 2;
-  if (avg <= 6.0) return 4;
-  return 8;
-}
-
 void *DevArena::alloc(size_t bytes, cudaError_t &e) {
   if (bytes == 0) bytes = 16;
   void *p = nullptr;
@@ -248,7 +234,7 @@ int System::setup_pattern(Ctx &ctx) {
   for (int64_t i = 0; i < n; ++i) blk[size_t(i)] = blk0[size_t(perm[size_t(i)])];
 
   std::vector<int64_t> amap, fmap, dpos, lptr, uptr;
-  std::vector<int32_t> lcol, ucol;
+  std::vector<int32_t> lcol, ucol, lgat, ugat;
   if (has_pc) {
     // permuted pattern P A P^T with the map back to A's entries
     prp.assign(size_t(n) + 1, 0);
@@ -304,6 +290,12 @@ int System::setup_pattern(Ctx &ctx) {
     };
     order(levL, nlevL, lvlptrL, lrow);
     order(levU, nlevU, lvlptrU, urow);
+    lgat.resize(size_t(n));
+    ugat.resize(size_t(n));
+    for (int64_t q = 0; q < n; ++q) {
+      lgat[size_t(q)] = perm[size_t(lrow[size_t(q)])];
+      ugat[size_t(q)] = perm[size_t(urow[size_t(q)])];
+    }
     fmap.assign(size_t(nnz), -1);
     lptr.assign(size_t(n) + 1, 0);
     uptr.assign(size_t(n) + 1, 0);
@@ -350,8 +342,6 @@ int System::setup_pattern(Ctx &ctx) {
       }
     }
   }
-  spmv_group = group_for(double(nnz) / double(n));
-  trsv_group = has_pc ? trsv_group_for(double(nnzL + nnzU) / (2.0 * double(n))) : 1;
 
   // ---- device buffers ----
   const size_t tsz = mixed ? sizeof(float) : sizeof(double);
@@ -376,6 +366,8 @@ int System::setup_pattern(Ctx &ctx) {
     ALLOC(d_lu64, double, nnz);
     ALLOC(d_lrow, int32_t, n);
     ALLOC(d_urow, int32_t, n);
+    ALLOC(d_lgat, int32_t, n);
+    ALLOC(d_ugat, int32_t, n);
     ALLOC(d_lptr, int64_t, n + 1);
     ALLOC(d_uptr, int64_t, n + 1);
     ALLOC(d_lvlptrL, int64_t, nlevL + 1);
@@ -404,6 +396,8 @@ int System::setup_pattern(Ctx &ctx) {
     H2D(d_dpos, dpos);
     H2D(d_lrow, lrow);
     H2D(d_urow, urow);
+    H2D(d_lgat, lgat);
+    H2D(d_ugat, ugat);
     H2D(d_lptr, lptr);
     H2D(d_uptr, uptr);
     H2D(d_lvlptrL, lvlptrL);
@@ -429,6 +423,7 @@ void System::fill_sysdev(void *out) const {
   d.perm = identity_perm ? nullptr : d_perm;
   d.lrow = d_lrow; d.lptr = d_lptr; d.lcol = d_lcol; d.lval = (const float *)d_lval;
   d.urow = d_urow; d.uptr = d_uptr; d.ucol = d_ucol; d.uval = (const float *)d_uval; d.udinv = (const float *)d_udinv;
+  d.lgat = d_lgat; d.ugat = d_ugat;
   d.ytmp = (float *)d_ytmp;
   d.x = (float *)kv[0]; d.r = (float *)kv[1]; d.rh = (float *)kv[2]; d.p = (float *)kv[3];
   d.v = (float *)kv[4]; d.s = (float *)kv[5]; d.t = (float *)kv[6]; d.ph = (float *)kv[7]; d.sh = (float *)kv[8];
@@ -458,39 +453,46 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   }
   st0.push_back(int32_t(tsys.size()));
   ntiles = int(tsys.size());
-  // merged level schedules: trsv entries are level-ordered positions, factorisation entries row ids
-  std::vector<int64_t> lptrL, lptrU;
-  std::vector<int32_t> esL, erL, esU, erU, efR;
-  if (has_pc && nsys > 1) {
-    auto merge = [&](bool lower, std::vector<int64_t> &lptr, std::vector<int32_t> &es, std::vector<int32_t> &er, int32_t &nl) {
-      nl = 0;
-      for (System *S : sys) nl = std::max(nl, lower ? S->nlevL : S->nlevU);
-      lptr.assign(size_t(nl) + 1, 0);
-      for (int32_t l = 0; l < nl; ++l) {
-        int64_t c = 0;
-        for (System *S : sys) {
-          const auto &vp = lower ? S->lvlptrL : S->lvlptrU;
-          if (l + 1 < int32_t(vp.size())) c += vp[size_t(l) + 1] - vp[size_t(l)];
+  // Triangular-solve schedules: merged level l lists, system by system, the level-l rows of
+  // every member cut into chunks of at most 32 consecutive level-ordered positions.
+  std::vector<int64_t> cptrL, cptrU, fptr;
+  std::vector<int32_t> csL, cqL, cnL, csU, cqU, cnU, fsys, frow;
+  auto chunks = [&](bool lower, std::vector<int64_t> &cptr, std::vector<int32_t> &cs, std::vector<int32_t> &cq,
+                    std::vector<int32_t> &cn, int32_t &nl) {
+    nl = 0;
+    for (System *S : sys) nl = std::max(nl, lower ? S->nlevL : S->nlevU);
+    cptr.assign(1, 0);
+    for (int32_t l = 0; l < nl; ++l) {
+      for (int k = 0; k < nsys; ++k) {
+        const auto &vp = lower ? sys[size_t(k)]->lvlptrL : sys[size_t(k)]->lvlptrU;
+        if (l + 1 >= int32_t(vp.size())) continue;
+        for (int64_t q = vp[size_t(l)]; q < vp[size_t(l) + 1]; q += 32) {
+          cs.push_back(k);
+          cq.push_back(int32_t(q));
+          cn.push_back(int32_t(std::min<int64_t>(32, vp[size_t(l) + 1] - q)));
         }
-        lptr[size_t(l) + 1] = lptr[size_t(l)] + c;
       }
-      es.resize(size_t(lptr.back()));
-      er.resize(size_t(lptr.back()));
-      int64_t p = 0;
-      for (int32_t l = 0; l < nl; ++l)
-        for (int s = 0; s < nsys; ++s) {
-          const auto &vp = lower ? sys[s]->lvlptrL : sys[s]->lvlptrU;
-          if (l + 1 >= int32_t(vp.size())) continue;
-          for (int64_t q = vp[size_t(l)]; q < vp[size_t(l) + 1]; ++q) { es[size_t(p)] = s; er[size_t(p)] = int32_t(q); ++p; }
+      cptr.push_back(int64_t(cs.size()));
+    }
+  };
+  if (has_pc) {
+    chunks(true, cptrL, csL, cqL, cnL, nlevL);
+    chunks(false, cptrU, csU, cqU, cnU, nlevU);
+    if (nsys > 1) {
+      // factorisation: merged level l = the forward-solve level-l rows of every member
+      fptr.assign(1, 0);
+      for (int32_t l = 0; l < nlevL; ++l) {
+        for (int k = 0; k < nsys; ++k) {
+          const System *S = sys[size_t(k)];
+          if (l + 1 >= int32_t(S->lvlptrL.size())) continue;
+          for (int64_t q = S->lvlptrL[size_t(l)]; q < S->lvlptrL[size_t(l) + 1]; ++q) {
+            fsys.push_back(k);
+            frow.push_back(S->lrow[size_t(q)]);
+          }
         }
-    };
-    merge(true, lptrL, esL, erL, nlevL);
-    merge(false, lptrU, esU, erU, nlevU);
-    efR.resize(erL.size());
-    for (size_t e = 0; e < erL.size(); ++e) efR[e] = sys[size_t(esL[e])]->lrow[size_t(erL[e])];
-  } else if (has_pc) {
-    nlevL = sys[0]->nlevL;
-    nlevU = sys[0]->nlevU;
+        fptr.push_back(int64_t(fsys.size()));
+      }
+    }
   }
   cudaError_t e;
 #define ALLOC(ptr, type, count)                                              \
@@ -515,14 +517,20 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   if (!d_refdev) return ctx.cuda_fail(e, "cudaMalloc refdev");
   d_factdev = arena.alloc(vk_factdev_size() * size_t(nsys), e);
   if (!d_factdev) return ctx.cuda_fail(e, "cudaMalloc factdev");
-  if (has_pc && nsys > 1) {
-    ALLOC(d_lptrL, int64_t, lptrL.size());
-    ALLOC(d_lptrU, int64_t, lptrU.size());
-    ALLOC(d_esL, int32_t, std::max<size_t>(esL.size(), 1));
-    ALLOC(d_erL, int32_t, std::max<size_t>(erL.size(), 1));
-    ALLOC(d_esU, int32_t, std::max<size_t>(esU.size(), 1));
-    ALLOC(d_erU, int32_t, std::max<size_t>(erU.size(), 1));
-    ALLOC(d_efR, int32_t, std::max<size_t>(efR.size(), 1));
+  if (has_pc) {
+    ALLOC(d_cptrL, int64_t, cptrL.size());
+    ALLOC(d_cptrU, int64_t, cptrU.size());
+    ALLOC(d_csL, int32_t, std::max<size_t>(csL.size(), 1));
+    ALLOC(d_cqL, int32_t, std::max<size_t>(cqL.size(), 1));
+    ALLOC(d_cnL, int32_t, std::max<size_t>(cnL.size(), 1));
+    ALLOC(d_csU, int32_t, std::max<size_t>(csU.size(), 1));
+    ALLOC(d_cqU, int32_t, std::max<size_t>(cqU.size(), 1));
+    ALLOC(d_cnU, int32_t, std::max<size_t>(cnU.size(), 1));
+    if (nsys > 1) {
+      ALLOC(d_fptr, int64_t, fptr.size());
+      ALLOC(d_fsys, int32_t, std::max<size_t>(fsys.size(), 1));
+      ALLOC(d_frow, int32_t, std::max<size_t>(frow.size(), 1));
+    }
   }
 #undef ALLOC
   cudaStream_t s = ctx.stream;
@@ -550,11 +558,26 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   H2D(d_sysdev, sd.data(), sd.size());
   H2D(d_refdev, rd.data(), rd.size());
   H2D(d_factdev, fd.data(), fd.size());
-  if (has_pc && nsys > 1) {
-    H2D(d_lptrL, lptrL.data(), sizeof(int64_t) * lptrL.size());
-    H2D(d_lptrU, lptrU.data(), sizeof(int64_t) * lptrU.size());
-    if (!esL.empty()) { H2D(d_esL, esL.data(), sizeof(int32_t) * esL.size()); H2D(d_erL, erL.data(), sizeof(int32_t) * erL.size()); H2D(d_efR, efR.data(), sizeof(int32_t) * efR.size()); }
-    if (!esU.empty()) { H2D(d_esU, esU.data(), sizeof(int32_t) * esU.size()); H2D(d_erU, erU.data(), sizeof(int32_t) * erU.size()); }
+  if (has_pc) {
+    H2D(d_cptrL, cptrL.data(), sizeof(int64_t) * cptrL.size());
+    H2D(d_cptrU, cptrU.data(), sizeof(int64_t) * cptrU.size());
+    if (!csL.empty()) {
+      H2D(d_csL, csL.data(), sizeof(int32_t) * csL.size());
+      H2D(d_cqL, cqL.data(), sizeof(int32_t) * cqL.size());
+      H2D(d_cnL, cnL.data(), sizeof(int32_t) * cnL.size());
+    }
+    if (!csU.empty()) {
+      H2D(d_csU, csU.data(), sizeof(int32_t) * csU.size());
+      H2D(d_cqU, cqU.data(), sizeof(int32_t) * cqU.size());
+      H2D(d_cnU, cnU.data(), sizeof(int32_t) * cnU.size());
+    }
+    if (nsys > 1) {
+      H2D(d_fptr, fptr.data(), sizeof(int64_t) * fptr.size());
+      if (!fsys.empty()) {
+        H2D(d_fsys, fsys.data(), sizeof(int32_t) * fsys.size());
+        H2D(d_frow, frow.data(), sizeof(int32_t) * frow.size());
+      }
+    }
   }
 #undef H2D
   if ((e = cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
@@ -562,25 +585,16 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   if ((e = cudaMemsetAsync(d_state, 0, vk_bistate_size_f64() * size_t(nsys), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   tiles = VkTiles{ntiles, d_tile_sys, d_tile_r0, d_tile_r1, d_sys_tile0};
   if (has_pc) {
-    if (nsys > 1) {
-      levL = VkLevels{nlevL, d_lptrL, d_esL, d_erL};
-      levU = VkLevels{nlevU, d_lptrU, d_esU, d_erU};
-      levF = VkLevels{nlevL, d_lptrL, d_esL, d_efR};
-    } else {
-      levL = VkLevels{nlevL, sys[0]->d_lvlptrL, nullptr, nullptr};
-      levU = VkLevels{nlevU, sys[0]->d_lvlptrU, nullptr, nullptr};
-      levF = VkLevels{nlevL, sys[0]->d_lvlptrL, nullptr, sys[0]->d_lrow};
-    }
+    levL = VkLevels{nlevL, d_cptrL, d_csL, d_cqL, d_cnL};
+    levU = VkLevels{nlevU, d_cptrU, d_csU, d_cqU, d_cnU};
+    if (nsys > 1) levF = VkLevels{nlevL, d_fptr, d_fsys, d_frow, nullptr};
+    else levF = VkLevels{nlevL, sys[0]->d_lvlptrL, nullptr, sys[0]->d_lrow, nullptr};
   }
-  int64_t tot_nnz = 0, tot_n = 0, tot_lu = 0;
-  for (System *S : sys) { tot_nnz += S->nnz; tot_n += S->n; tot_lu += S->nnzL + S->nnzU; }
-  spmv_group = group_for(double(tot_nnz) / double(tot_n));
-  trsv_group = has_pc ? trsv_group_for(double(tot_lu) / (2.0 * double(tot_n))) : 1;
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
   int bps = 0;
-  if (mixed) vk_trsv_occupancy_f32(trsv_group, &bps); else vk_trsv_occupancy_f64(trsv_group, &bps);
+  if (mixed) vk_trsv_occupancy_f32(&bps); else vk_trsv_occupancy_f64(&bps);
   trsv_grid = std::max(1, std::min(bps, 4)) * num_sms;
   int bpf = 0;
   vk_ilu0_occupancy(&bpf);
@@ -672,7 +686,9 @@ int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, int &iters_out) {
   for (int k = 0; k < nsys; ++k) {
     if (mixed) {
       BiState<float> *b = (BiState<float> *)(stbuf.data() + bsz * size_t(k));
-      b->tol = float(tol); b->max_iter = max_iter; b->done = 0; b->upd = 0; b->iter = 0;
+      // stopping is decided on the FP64 residual only; the FP32 early exit on ||s|| is off
+      b->tol = 0.0f; b->max_iter = max_iter; b->done = 0; b->upd = 0; b->iter = 0; b->bad = 0;
+      b->sigma = 1.0; b->sigma_new = 1.0;
     } else {
       BiState<double> *b = (BiState<double> *)(stbuf.data() + bsz * size_t(k));
       b->tol = tol; b->max_iter = max_iter; b->done = 0; b->upd = 0; b->iter = 0;
@@ -682,9 +698,8 @@ int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, int &iters_out) {
   EventProf &P = g_prof;
   P.on = profile; P.s = s;
   if (mixed) {
-    // r64 = b - A x64 (x64 = 0 here), r32 = r64, then the FP32 recurrences start from it
-    vk_reliable_r(spmv_group, ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, tol, 1, s);
-    vk_bicg_init_f32(ntiles, d_sysdev, d_state, &tiles, (float *)d_partials, d_counters, d_active, s);
+    // r64 = b - A x64 (x64 = 0 here), r32 = r64 / ||r64||, and the FP32 recurrences start from it
+    vk_reliable_r(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, tol, 1, s);
   } else {
     vk_bicg_init_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s);
   }
@@ -697,34 +712,34 @@ int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, int &iters_out) {
         float *pf = (float *)d_partials;
         a = P.begin(); vk_update_p_f32(ntiles, d_sysdev, d_state, &tiles, d_active, s); P.end(2, a);
         a = P.begin();
-        if (has_pc) rc = vk_trsv_f32(mode, trsv_group, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
+        if (has_pc) rc = vk_trsv_f32(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
         else vk_precond_copy_f32(ntiles, d_sysdev, d_state, &tiles, d_active, 0, s);
         P.end(1, a);
-        a = P.begin(); vk_spmv_dot_f32(spmv_group, ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 0, s); P.end(0, a);
+        a = P.begin(); vk_spmv_dot_f32(ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 0, s); P.end(0, a);
         a = P.begin(); vk_update_s_f32(ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, s); P.end(2, a);
         a = P.begin();
-        if (has_pc) rc |= vk_trsv_f32(mode, trsv_group, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 1, d_bar, d_err, s);
+        if (has_pc) rc |= vk_trsv_f32(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 1, d_bar, d_err, s);
         else vk_precond_copy_f32(ntiles, d_sysdev, d_state, &tiles, d_active, 1, s);
         P.end(1, a);
-        a = P.begin(); vk_spmv_dot_f32(spmv_group, ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 1, s); P.end(0, a);
+        a = P.begin(); vk_spmv_dot_f32(ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 1, s); P.end(0, a);
         a = P.begin(); vk_update_xr_f32(ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 1, s); P.end(2, a);
         a = P.begin();
         vk_reliable_x(ntiles, d_sysdev, d_state, &tiles, d_active, s);
-        vk_reliable_r(spmv_group, ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, tol, 0, s);
+        vk_reliable_r(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, tol, 0, s);
         P.end(3, a);
       } else {
         a = P.begin(); vk_update_p_f64(ntiles, d_sysdev, d_state, &tiles, d_active, s); P.end(2, a);
         a = P.begin();
-        if (has_pc) rc = vk_trsv_f64(mode, trsv_group, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
+        if (has_pc) rc = vk_trsv_f64(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
         else vk_precond_copy_f64(ntiles, d_sysdev, d_state, &tiles, d_active, 0, s);
         P.end(1, a);
-        a = P.begin(); vk_spmv_dot_f64(spmv_group, ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 0, s); P.end(0, a);
+        a = P.begin(); vk_spmv_dot_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 0, s); P.end(0, a);
         a = P.begin(); vk_update_s_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s); P.end(2, a);
         a = P.begin();
-        if (has_pc) rc |= vk_trsv_f64(mode, trsv_group, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 1, d_bar, d_err, s);
+        if (has_pc) rc |= vk_trsv_f64(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 1, d_bar, d_err, s);
         else vk_precond_copy_f64(ntiles, d_sysdev, d_state, &tiles, d_active, 1, s);
         P.end(1, a);
-        a = P.begin(); vk_spmv_dot_f64(spmv_group, ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 1, s); P.end(0, a);
+        a = P.begin(); vk_spmv_dot_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 1, s); P.end(0, a);
         a = P.begin(); vk_update_xr_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 0, s); P.end(2, a);
       }
       if (rc) return ctx.cuda_fail(cudaError_t(rc), "trsv launch");
@@ -772,7 +787,7 @@ int Batch::state_of(int k, int32_t &status, int32_t &iter, int32_t &nupd, double
 // FP64 residual r = b - A x64 for all members; returns per-system ||r|| / ||b||.
 int Batch::residual(Ctx &ctx, std::vector<double> &rel) {
   cudaStream_t s = ctx.stream;
-  vk_residual64(spmv_group, ntiles, d_refdev, &tiles, d_partials, d_counters, d_active, d_rnorm2, d_bnorm2, s);
+  vk_residual64(ntiles, d_refdev, &tiles, d_partials, d_counters, d_active, d_rnorm2, d_bnorm2, s);
   std::vector<double> r2((size_t)nsys), b2((size_t)nsys);
   cudaError_t e = cudaMemcpyAsync(r2.data(), d_rnorm2, sizeof(double) * size_t(nsys), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(b2.data(), d_bnorm2, sizeof(double) * size_t(nsys), cudaMemcpyDeviceToHost, s);
@@ -1057,14 +1072,14 @@ int vshe_system_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, const double *
   System *S = it->second.get();
   cudaStream_t s = ctx->stream;
   cudaError_t e;
-  const int grid = std::max(1, int(std::min<int64_t>((S->n * S->spmv_group + 255) / 256, 65535 * 8)));
+  const int grid = std::max(1, int(std::min<int64_t>((S->n + 255) / 256, 65535 * 8)));
   if (precision == 1) {
     if (!S->mixed) return ctx->fail(VSHE_E_UNSUPPORTED, "FP32 values exist only for mixed-precision systems");
     std::vector<float> xf((size_t)S->n), yf((size_t)S->n);
     for (int64_t i = 0; i < S->n; ++i) xf[size_t(i)] = float(x[i]);
     float *dx = (float *)S->kv[0], *dy = (float *)S->kv[1];
     if ((e = cudaMemcpyAsync(dx, xf.data(), sizeof(float) * xf.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx->cuda_fail(e, "x");
-    vk_spmv_plain_f32(S->spmv_group, grid, S->n, S->d_rp, S->d_ci, S->d_av32, dx, dy, s);
+    vk_spmv_plain_f32(grid, S->n, S->d_rp, S->d_ci, S->d_av32, dx, dy, s);
     if ((e = cudaMemcpyAsync(yf.data(), dy, sizeof(float) * yf.size(), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return ctx->cuda_fail(e, "y");
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx->cuda_fail(e, "spmv");
     for (int64_t i = 0; i < S->n; ++i) y[i] = double(yf[size_t(i)]);
@@ -1072,7 +1087,7 @@ int vshe_system_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, const double *
   }
   double *dx = S->d_x64, *dy = S->d_r64;
   if ((e = cudaMemcpyAsync(dx, x, sizeof(double) * size_t(S->n), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx->cuda_fail(e, "x");
-  vk_spmv_plain_f64(S->spmv_group, grid, S->n, S->d_rp, S->d_ci, S->d_av64, dx, dy, s);
+  vk_spmv_plain_f64(grid, S->n, S->d_rp, S->d_ci, S->d_av64, dx, dy, s);
   if ((e = cudaMemcpyAsync(y, dy, sizeof(double) * size_t(S->n), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return ctx->cuda_fail(e, "y");
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx->cuda_fail(e, "spmv");
   return VSHE_OK;
@@ -1087,17 +1102,17 @@ int vshe_system_time_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, int32_t r
   System *S = it->second.get();
   if (precision == 1 && !S->mixed) return ctx->fail(VSHE_E_UNSUPPORTED, "");
   cudaStream_t s = ctx->stream;
-  const int grid = std::max(1, int(std::min<int64_t>((S->n * S->spmv_group + 255) / 256, 65535 * 8)));
+  const int grid = std::max(1, int(std::min<int64_t>((S->n + 255) / 256, 65535 * 8)));
   cudaEvent_t a, b;
   cudaEventCreate(&a); cudaEventCreate(&b);
   for (int w = 0; w < 3; ++w) {
-    if (precision == 1) vk_spmv_plain_f32(S->spmv_group, grid, S->n, S->d_rp, S->d_ci, S->d_av32, (float *)S->kv[0], (float *)S->kv[1], s);
-    else vk_spmv_plain_f64(S->spmv_group, grid, S->n, S->d_rp, S->d_ci, S->d_av64, S->d_x64, S->d_r64, s);
+    if (precision == 1) vk_spmv_plain_f32(grid, S->n, S->d_rp, S->d_ci, S->d_av32, (float *)S->kv[0], (float *)S->kv[1], s);
+    else vk_spmv_plain_f64(grid, S->n, S->d_rp, S->d_ci, S->d_av64, S->d_x64, S->d_r64, s);
   }
   cudaEventRecord(a, s);
   for (int r = 0; r < reps; ++r) {
-    if (precision == 1) vk_spmv_plain_f32(S->spmv_group, grid, S->n, S->d_rp, S->d_ci, S->d_av32, (float *)S->kv[0], (float *)S->kv[1], s);
-    else vk_spmv_plain_f64(S->spmv_group, grid, S->n, S->d_rp, S->d_ci, S->d_av64, S->d_x64, S->d_r64, s);
+    if (precision == 1) vk_spmv_plain_f32(grid, S->n, S->d_rp, S->d_ci, S->d_av32, (float *)S->kv[0], (float *)S->kv[1], s);
+    else vk_spmv_plain_f64(grid, S->n, S->d_rp, S->d_ci, S->d_av64, S->d_x64, S->d_r64, s);
   }
   cudaEventRecord(b, s);
   cudaError_t e = cudaEventSynchronize(b);

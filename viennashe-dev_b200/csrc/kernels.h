@@ -21,6 +21,7 @@ typedef struct VkLevels {
   const int64_t *lvl_ptr;
   const int32_t *ent_sys;
   const int32_t *ent_row;
+  const int32_t *ent_cnt;
 } VkLevels;
 
 int vk_threads(void);
@@ -39,7 +40,7 @@ size_t vk_bistate_size_f64(void);
                           const int32_t *act, cudaStream_t s);                                                         \
   void vk_update_p_##SUF(int ntiles, const void *sys, void *st, const VkTiles *tl, const int32_t *act,                \
                          cudaStream_t s);                                                                              \
-  void vk_spmv_dot_##SUF(int group, int ntiles, const void *sys, void *st, const VkTiles *tl, T *part, int32_t *cnt,   \
+  void vk_spmv_dot_##SUF(int ntiles, const void *sys, void *st, const VkTiles *tl, T *part, int32_t *cnt,              \
                          const int32_t *act, int which, cudaStream_t s);                                               \
   void vk_update_s_##SUF(int ntiles, const void *sys, void *st, const VkTiles *tl, T *part, int32_t *cnt,             \
                          const int32_t *act, cudaStream_t s);                                                          \
@@ -47,12 +48,12 @@ size_t vk_bistate_size_f64(void);
                           const int32_t *act, int reliable, cudaStream_t s);                                           \
   void vk_precond_copy_##SUF(int ntiles, const void *sys, const void *st, const VkTiles *tl, const int32_t *act,      \
                              int which, cudaStream_t s);                                                               \
-  int vk_trsv_##SUF(int mode, int group, int grid, const void *sys, const void *st, const int32_t *act,               \
+  int vk_trsv_##SUF(int mode, int grid, const void *sys, const void *st, const int32_t *act,                          \
                     const VkLevels *lL, const VkLevels *lU, int which, unsigned *bar, int32_t *err, cudaStream_t s);    \
-  int vk_trsv_occupancy_##SUF(int group, int *blocks_per_sm);                                                          \
+  int vk_trsv_occupancy_##SUF(int *blocks_per_sm);                                                                     \
   void vk_split_factor_##SUF(int64_t nnz, int64_t n, const double *lu, const int64_t *fmap, const int64_t *diag,       \
                              const int64_t *dpos, T *lval, T *uval, T *udinv, cudaStream_t s);                         \
-  void vk_spmv_plain_##SUF(int group, int grid, int64_t n, const int64_t *rp, const int32_t *ci, const T *av,         \
+  void vk_spmv_plain_##SUF(int grid, int64_t n, const int64_t *rp, const int32_t *ci, const T *av,                    \
                            const T *x, T *y, cudaStream_t s);
 
 VK_DECL_T(float, f32)
@@ -61,10 +62,12 @@ VK_DECL_T(double, f64)
 int vk_ilu0(int mode, int grid, const void *fs, const VkLevels *lv, unsigned *bar, int32_t *err, cudaStream_t s);
 int vk_ilu0_occupancy(int *blocks_per_sm);
 
-void vk_residual64(int group, int ntiles, const void *ref, const VkTiles *tl, double *part, int32_t *cnt,
+void vk_residual64(int ntiles, const void *ref, const VkTiles *tl, double *part, int32_t *cnt,
                    const int32_t *act, double *rnorm2, double *bnorm2, cudaStream_t s);
 void vk_reliable_x(int ntiles, const void *sys32, const void *st, const VkTiles *tl, const int32_t *act, cudaStream_t s);
-void vk_reliable_r(int group, int ntiles, const void *sys32, void *st, const VkTiles *tl, double *part, int32_t *cnt,
+// r64 = b - A x64, then r32 = r64 / ||r64|| with p, v carried to the new scale (two launches);
+// force = 1 starts the mixed solve (x64 = 0) and initialises the FP32 recurrence.
+void vk_reliable_r(int ntiles, const void *sys32, void *st, const VkTiles *tl, double *part, int32_t *cnt,
                    const int32_t *act, double tol64, int force, cudaStream_t s);
 void vk_gather_values(int64_t nnz, const int64_t *amap, const double *av, double *lu, cudaStream_t s);
 void vk_cast_f64_f32(int64_t n, const double *a, float *b, cudaStream_t s);

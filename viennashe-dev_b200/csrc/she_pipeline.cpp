@@ -319,6 +319,8 @@ int SheProblem::finish(Ctx &ctx) {
 using namespace vshe;
 
 static std::map<vshe::Ctx *, std::map<int64_t, std::unique_ptr<SheProblem>>> g_she;
+// batch schedules of vshe_she_run_batch, per context and handle set
+static std::map<vshe::Ctx *, std::map<std::vector<int64_t>, std::unique_ptr<Batch>>> g_she_batches;
 static std::mutex g_she_mu;
 
 static SheProblem *find_she(vshe_ctx *ctx, int64_t h) {
@@ -332,6 +334,7 @@ static SheProblem *find_she(vshe_ctx *ctx, int64_t h) {
 namespace vshe {
 void she_release_all(Ctx *ctx) {
   std::lock_guard<std::mutex> lk(g_she_mu);
+  g_she_batches.erase(ctx);
   g_she.erase(ctx);
 }
 }  // namespace vshe
@@ -514,7 +517,76 @@ int vshe_she_free(vshe_ctx *ctx, int64_t h) {
     if (it == g_she.end() || !it->second.count(h)) return ctx->fail(VSHE_E_NOT_FOUND, "");
     dead = std::move(it->second[h]);
     it->second.erase(h);
+    // batch schedules that include this problem point at its system: drop them
+    auto bt = g_she_batches.find(ctx);
+    if (bt != g_she_batches.end())
+      for (auto b = bt->second.begin(); b != bt->second.end();) {
+        if (std::find(b->first.begin(), b->first.end(), h) != b->first.end()) b = bt->second.erase(b);
+        else ++b;
+      }
   }
+  return VSHE_OK;
+}
+
+int vshe_she_run_batch(vshe_ctx *ctx, int32_t count, const int64_t *handles, vshe_solve_stats *stats,
+                       double *full_residuals, double *device_ms) {
+  if (!ctx || count <= 0 || !handles) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  std::vector<int64_t> key(handles, handles + count);
+  std::vector<SheProblem *> probs;
+  for (int64_t h : key) {
+    SheProblem *S = find_she(ctx, h);
+    if (!S) return ctx->fail(VSHE_E_NOT_FOUND, "handle " + std::to_string(h));
+    if (std::find(probs.begin(), probs.end(), S) != probs.end()) return ctx->fail(VSHE_E_INVALID_ARGUMENT, "handle listed twice");
+    probs.push_back(S);
+  }
+  Batch *B = nullptr;
+  {
+    std::lock_guard<std::mutex> lk2(g_she_mu);
+    auto &m = g_she_batches[ctx];
+    auto it = m.find(key);
+    if (it != m.end()) B = it->second.get();
+  }
+  if (!B) {
+    std::vector<System *> mem;
+    for (SheProblem *S : probs) mem.push_back(S->sys.get());
+    std::unique_ptr<Batch> nb(new Batch);
+    int rc = nb->build(*ctx, mem);
+    if (rc) return rc;
+    B = nb.get();
+    std::lock_guard<std::mutex> lk2(g_she_mu);
+    g_she_batches[ctx][key] = std::move(nb);
+  }
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (device_ms) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, ctx->stream);
+  }
+  int rc = VSHE_OK;
+  for (SheProblem *S : probs)
+    if ((rc = S->assemble(*ctx, 3))) break;
+  std::vector<vshe_solve_stats> st;
+  if (!rc) rc = B->solve(*ctx, st);
+  for (size_t k = 0; !rc && k < probs.size(); ++k) rc = probs[k]->finish(*ctx);
+  if (device_ms) {
+    cudaEventRecord(b, ctx->stream);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    *device_ms = ms;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  if (rc) return rc;
+  int worst = VSHE_OK;
+  for (size_t k = 0; k < probs.size(); ++k) {
+    if (stats) stats[k] = st[k];
+    if (full_residuals) full_residuals[k] = probs[k]->full_residual;
+    if (st[k].status && !worst) worst = st[k].status;
+  }
+  if (worst) return ctx->fail(worst, "one or more systems of the batch");
   return VSHE_OK;
 }
 

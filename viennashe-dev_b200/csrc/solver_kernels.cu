@@ -47,13 +47,6 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
-template <typename T, int G>
-__device__ __forceinline__ T group_sum(T v) {
-#pragma unroll
-  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
 // Block-wide sums; results valid in thread 0.
 template <typename T, int NV>
 __device__ __forceinline__ void block_sum(T (&v)[NV]) {
@@ -110,6 +103,52 @@ __device__ bool tile_finish(T (&v)[NV], int tile, int sys, const Tiles &tl, T *p
   }
   return threadIdx.x == 0;
 }
+
+// ------------------------------------------------------------ CSR row chunks
+// Row sums of a chunk of nr <= 32 consecutive CSR rows starting at row q0 of (ptr, col, val):
+// lane l returns sum_k val[k] * x[col[k]] over row q0 + l (0 for l >= nr).  The chunk's entries
+// are one contiguous range; it is streamed with coalesced loads, U entries per lane in flight
+// (all column/value loads of a pass first, then all x gathers), the products are staged in the
+// warp's shared-memory slice sm[32 * U] and every lane sums its own row in index order, so the
+// result does not depend on the launch shape.  CG: read x through L2 only (x is written by
+// other CTAs of the same launch).
+template <typename T, int U, bool CG>
+__device__ __forceinline__ T chunk_rowsums(const int64_t *__restrict__ ptr, const int32_t *__restrict__ col, const T *__restrict__ val,
+                                           const T *x, int64_t q0, int nr, T *sm) {
+  const int lane = threadIdx.x & 31;
+  int64_t b = 0, e = 0;
+  if (lane < nr) { b = ptr[q0 + lane]; e = ptr[q0 + lane + 1]; }
+  const int64_t kb = __shfl_sync(0xffffffffu, b, 0);
+  const int64_t ke = __shfl_sync(0xffffffffu, e, nr - 1);
+  T sum = T(0);
+  for (int64_t pb = kb; pb < ke; pb += 32 * U) {
+    int32_t c[U];
+    T a[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t k = pb + u * 32 + lane;
+      c[u] = 0; a[u] = T(0);
+      if (k < ke) { c[u] = col[k]; a[u] = val[k]; }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t k = pb + u * 32 + lane;
+      T xv = T(0);
+      if (k < ke) xv = CG ? __ldcg(&x[c[u]]) : x[c[u]];
+      sm[u * 32 + lane] = a[u] * xv;
+    }
+    __syncwarp();
+    const int64_t lo = b > pb ? b : pb;
+    const int64_t hi = e < pb + 32 * U ? e : pb + 32 * U;
+    for (int64_t k = lo; k < hi; ++k) sum += sm[k - pb];
+    __syncwarp();
+  }
+  return sum;
+}
+
+constexpr int kWarps = kThreads / 32;
+constexpr int kSpmvU = 12;  // entries per lane in flight: ~12 nnz per row fit one pass
+constexpr int kTrsvU = 8;   // triangular factors hold about half of A's entries per row
 
 template <typename T>
 __device__ __forceinline__ T dsqrt(T x);
@@ -170,10 +209,11 @@ __global__ void __launch_bounds__(kThreads) k_update_p(const SysDev<T> *sys, BiS
   }
 }
 
-// y = A x over one tile with G lanes per row, fused dots.
+// y = A x over one tile (32-row chunks per warp), fused dots.
 // which = 0: v = A ph, (rh, v) -> alpha.   which = 1: t = A sh, (t, s), (t, t) -> omega.
-template <typename T, int G>
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_spmv_dot(const SysDev<T> *sys, BiState<T> *st, Tiles tl, T *partials, int32_t *counters, const int32_t *active, int which) {
+  __shared__ T sm[kWarps][32 * kSpmvU];
   const int tile = blockIdx.x;
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done) return;
@@ -181,25 +221,17 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dot(const SysDev<T> *sys, BiS
   const SysDev<T> S = sys[s];
   const T *xin = which == 0 ? S.ph : S.sh;
   T *yout = which == 0 ? S.v : S.t;
-  const int lane = threadIdx.x % G;
-  const int grp = threadIdx.x / G;
-  const int wgrp = (threadIdx.x & ~31) / G;  // first group of this warp (loop bound is warp-uniform)
-  constexpr int NG = kThreads / G;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t r0 = tl.tile_row0[tile], r1 = tl.tile_row1[tile];
   T acc[2] = {T(0), T(0)};
-  for (int64_t base = r0 + wgrp; base < r1; base += NG) {
-    const int64_t row = base + (grp - wgrp);
-    const bool valid = row < r1;
-    T sum = T(0);
-    if (valid) {
-      const int64_t a = S.rp[row], e = S.rp[row + 1];
-      for (int64_t k = a + lane; k < e; k += G) sum += S.av[k] * xin[S.ci[k]];
-    }
-    sum = group_sum<T, G>(sum);
-    if (valid && lane == 0) {
-      yout[row] = sum;
-      if (which == 0) acc[0] += S.rh[row] * sum;
-      else { acc[0] += sum * S.s[row]; acc[1] += sum * sum; }
+  for (int64_t q0 = r0 + 32 * w; q0 < r1; q0 += 32 * kWarps) {
+    const int nr = (int)(r1 - q0 < 32 ? r1 - q0 : 32);
+    const T y = chunk_rowsums<T, kSpmvU, false>(S.rp, S.ci, S.av, xin, q0, nr, sm[w]);
+    if (lane < nr) {
+      const int64_t row = q0 + lane;
+      yout[row] = y;
+      if (which == 0) acc[0] += S.rh[row] * y;
+      else { acc[0] += y * S.s[row]; acc[1] += y * y; }
     }
   }
   T tot[2];
@@ -280,71 +312,116 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(const SysDev<T> *sys, Bi
       if (b.iter >= b.max_iter) { b.done = 1; b.status = VSHE_E_NOT_CONVERGED_DEV; }
       return;
     }
-    // mixed: ask for the FP64 residual when the FP32 one dropped by delta, converged, broke down or ran out
-    const double rn = (double)b.res * (double)b.bnorm;
-    if (broke) { b.status = 0; b.restart = 1; b.upd = 1; }
-    if (b.s_conv || rn < kReliableDelta * b.maxr || b.res < b.tol || b.iter >= b.max_iter) b.upd = 1;
+    // mixed: ask for an FP64 reliable update when ||r32|| dropped below the threshold (delta, or
+    // the level at which the true residual would meet the tolerance), on breakdown, on a
+    // non-finite value, or when the iteration budget is spent
+    const bool bad = !isfinite(b.res) || !isfinite(b.rho) || !isfinite(b.alpha) || !isfinite(b.omega);
+    if (bad) { b.bad = 1; b.status = 0; b.restart = 1; b.upd = 1; }
+    else if (broke) { b.status = 0; b.restart = 1; b.upd = 1; }
+    if (b.res < b.thresh || b.iter >= b.max_iter) b.upd = 1;
     b.s_conv = 0;
   }
 }
 
-// FP64 reliable update, part 1: x64 += x32, x32 = 0 (systems with upd set)
+// FP64 reliable update, part 1: x64 += sigma * x32, x32 = 0 (systems with upd set).  A cycle
+// that went non-finite contributes nothing.
 __global__ void __launch_bounds__(kThreads) k_reliable_x(const SysDev<float> *sys, const BiState<float> *st, Tiles tl, const int32_t *active) {
   const int tile = blockIdx.x;
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done || !st[s].upd) return;
   const SysDev<float> S = sys[s];
+  const double sigma = st[s].sigma;
+  const bool keep = !st[s].bad;
   for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) {
-    S.x64[i] += (double)S.x[i];
+    if (keep) S.x64[i] += sigma * (double)S.x[i];
     S.x[i] = 0.0f;
   }
 }
 
-// FP64 reliable update, part 2: r64 = b - A x64, r32 = r64; ||r64||, ||b||, (rh, r32) -> state.
-// With force = 1 this is the initial residual of every active system.
-template <int G>
+// FP64 reliable update, part 2: r64 = b - A x64; ||r64|| -> sigma_new, ||b||, convergence test.
+// With force = 1 this is the initial residual of every active system (x64 = 0).
 __global__ void __launch_bounds__(kThreads) k_reliable_r(const SysDev<float> *sys, BiState<float> *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active, double tol64, int force) {
+  __shared__ double sm[kWarps][32 * kSpmvU];
   const int tile = blockIdx.x;
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done) return;
   if (!force && !st[s].upd) return;
   const SysDev<float> S = sys[s];
-  const int lane = threadIdx.x % G, grp = threadIdx.x / G;
-  const int wgrp = (threadIdx.x & ~31) / G;
-  constexpr int NG = kThreads / G;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t r0 = tl.tile_row0[tile], r1 = tl.tile_row1[tile];
-  double acc[3] = {0.0, 0.0, 0.0};
-  for (int64_t base = r0 + wgrp; base < r1; base += NG) {
-    const int64_t row = base + (grp - wgrp);
-    const bool valid = row < r1;
-    double sum = 0.0;
-    if (valid)
-      for (int64_t k = S.rp[row] + lane; k < S.rp[row + 1]; k += G) sum += S.av64[k] * S.x64[S.ci[k]];
-    sum = group_sum<double, G>(sum);
-    if (valid && lane == 0) {
+  double acc[2] = {0.0, 0.0};
+  for (int64_t q0 = r0 + 32 * w; q0 < r1; q0 += 32 * kWarps) {
+    const int nr = (int)(r1 - q0 < 32 ? r1 - q0 : 32);
+    const double ax = chunk_rowsums<double, kSpmvU, false>(S.rp, S.ci, S.av64, S.x64, q0, nr, sm[w]);
+    if (lane < nr) {
+      const int64_t row = q0 + lane;
       const double bb = S.b64[row];
-      const double r = bb - sum;
+      const double r = bb - ax;
       S.r64[row] = r;
-      const float r32 = (float)r;
-      S.r[row] = r32;
       acc[0] += r * r;
       acc[1] += bb * bb;
-      acc[2] += (double)S.rh[row] * (double)r32;
     }
   }
-  double tot[3];
-  if (tile_finish<double, 3>(acc, tile, s, tl, partials, counters, tot)) {
+  double tot[2];
+  if (tile_finish<double, 2>(acc, tile, s, tl, partials, counters, tot)) {
     BiState<float> &b = st[s];
     b.bnorm64 = sqrt(tot[1]);
     const double rn = sqrt(tot[0]);
     b.res64 = b.bnorm64 > 0 ? rn / b.bnorm64 : 0.0;
-    b.maxr = rn;
-    b.rho = (float)tot[2];
-    b.upd = 0;
+    b.sigma_new = rn;
     if (!force) b.nupd += 1;
-    if (b.bnorm64 == 0.0 || b.res64 < tol64) { b.done = 1; b.status = 0; return; }
-    if (b.iter >= b.max_iter) { b.done = 1; b.status = VSHE_E_NOT_CONVERGED_DEV; return; }
-    if (force) { b.bnorm = (float)rn; b.restart = 1; }
+    if (b.bnorm64 == 0.0 || b.res64 < tol64) { b.done = 1; b.status = 0; b.upd = 0; return; }
+    if (!isfinite(rn)) { b.done = 1; b.status = VSHE_E_BREAKDOWN_DEV; b.upd = 0; return; }
+    if (b.iter >= b.max_iter) { b.done = 1; b.status = VSHE_E_NOT_CONVERGED_DEV; b.upd = 0; return; }
+  }
+}
+
+// FP64 reliable update, part 3: r32 = r64 / sigma_new (unit norm); the search direction p and
+// v = A M^-1 p are carried over to the new scale (times sigma / sigma_new), so the Krylov
+// recurrence continues without a restart; rho = (rh, r32).  force = 1: start of the solve
+// (shadow residual, x32 = p = v = 0).
+__global__ void __launch_bounds__(kThreads) k_reliable_scale(const SysDev<float> *sys, BiState<float> *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active, double tol64, int force) {
+  const int tile = blockIdx.x;
+  const int s = tl.tile_sys[tile];
+  if (!active[s] || st[s].done) return;
+  if (!force && !st[s].upd) return;
+  const SysDev<float> S = sys[s];
+  const double inv = 1.0 / st[s].sigma_new;
+  const float ratio = force ? 0.0f : (float)(st[s].sigma * inv);
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) {
+    const float r = (float)(S.r64[i] * inv);
+    S.r[i] = r;
+    float h;
+    if (force) {
+      h = shadow_value(i);
+      S.rh[i] = h;
+      S.x[i] = 0.0f; S.p[i] = 0.0f; S.v[i] = 0.0f;
+    } else {
+      h = S.rh[i];
+      S.p[i] *= ratio;
+      S.v[i] *= ratio;
+    }
+    acc[0] += (double)h * (double)r;
+    acc[1] += (double)r * (double)r;
+  }
+  double tot[2];
+  if (tile_finish<double, 2>(acc, tile, s, tl, partials, counters, tot)) {
+    BiState<float> &b = st[s];
+    if (force) {
+      b.iter = 0; b.s_conv = 0; b.status = 0; b.nupd = 0; b.restart = 1;
+      b.rho_old = 1.0f; b.alpha = 1.0f; b.omega = 1.0f;
+    } else {
+      b.rho_old *= ratio;
+    }
+    b.rho = (float)tot[0];
+    b.sigma = b.sigma_new;
+    b.bnorm = 1.0f;
+    b.res = (float)sqrt(tot[1]);
+    // the true residual meets tol64 once ||r32|| < tol64 * ||b|| / sigma; take the update a little before
+    b.thresh = (float)fmax(kReliableDelta, 0.5 * tol64 * b.bnorm64 / b.sigma);
+    b.upd = 0;
+    b.bad = 0;
   }
 }
 
@@ -408,65 +485,61 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
 
 // ------------------------------------------------- triangular solves (ILU apply)
 // out = P^T U^{-1} L^{-1} P in over the level-ordered factors.  which 0: ph = M^{-1} p, 1: sh = M^{-1} s.
-template <typename T, int G>
-__device__ __forceinline__ void trsv_level_rows(const SysDev<T> *sys, const BiState<T> *st, const int32_t *active, const Levels lv, int k, bool lower, int which) {
-  const int lane = threadIdx.x % G;
-  const int64_t gid = ((int64_t)blockIdx.x * kThreads + threadIdx.x) / G;
-  const int64_t wgid = ((int64_t)blockIdx.x * kThreads + (threadIdx.x & ~31)) / G;  // warp-uniform loop bound
-  const int64_t ngrp = ((int64_t)gridDim.x * kThreads) / G;
-  const int64_t e0 = lv.lvl_ptr[k], e1 = lv.lvl_ptr[k + 1];
-  for (int64_t eb = e0 + wgid; eb < e1; eb += ngrp) {
-    const int64_t e = eb + (gid - wgid);
-    bool valid = e < e1;
-    int s = 0;
-    if (valid) {
-      s = lv.ent_sys ? lv.ent_sys[e] : 0;
-      valid = active[s] && !st[s].done && !(which == 1 && st[s].s_conv);
-    }
-    const SysDev<T> *S = &sys[s];
-    const int64_t q = valid ? (lv.ent_row ? (int64_t)lv.ent_row[e] : e) : 0;
-    T sum = T(0);
+// A level is a list of chunks (system, first level-ordered position, row count <= 32); the
+// warps of the grid take its chunks in turn.  ytmp (permuted order) is written by other CTAs
+// of the same launch and read through L2 only.
+template <typename T>
+__device__ __forceinline__ void trsv_level_rows(const SysDev<T> *sys, const BiState<T> *st, const int32_t *active, const Levels lv, int k,
+                                                bool lower, int which, T *sm) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
+  const int64_t c1 = lv.lvl_ptr[k + 1];
+  for (int64_t c = lv.lvl_ptr[k] + gw; c < c1; c += nw) {
+    const int s = lv.ent_sys[c];
+    if (!active[s] || st[s].done || (which == 1 && st[s].s_conv)) continue;
+    const SysDev<T> &S = sys[s];
+    const int64_t q0 = lv.ent_row[c];
+    const int nr = lv.ent_cnt[c];
     if (lower) {
-      const int32_t row = valid ? S->lrow[q] : 0;
-      if (valid)
-        for (int64_t j = S->lptr[q] + lane; j < S->lptr[q + 1]; j += G) sum += S->lval[j] * __ldcg(&S->ytmp[S->lcol[j]]);
-      sum = group_sum<T, G>(sum);
-      if (valid && lane == 0) {
-        const T *in = which == 0 ? S->p : S->s;
-        const int32_t orow = S->perm ? S->perm[row] : row;
-        S->ytmp[row] = in[orow] - sum;
+      const T sum = chunk_rowsums<T, kTrsvU, true>(S.lptr, S.lcol, S.lval, S.ytmp, q0, nr, sm);
+      if (lane < nr) {
+        const int64_t q = q0 + lane;
+        const T *in = which == 0 ? S.p : S.s;
+        S.ytmp[S.lrow[q]] = in[S.lgat[q]] - sum;
       }
     } else {
-      const int32_t row = valid ? S->urow[q] : 0;
-      if (valid)
-        for (int64_t j = S->uptr[q] + lane; j < S->uptr[q + 1]; j += G) sum += S->uval[j] * __ldcg(&S->ytmp[S->ucol[j]]);
-      sum = group_sum<T, G>(sum);
-      if (valid && lane == 0) {
-        const T y = (__ldcg(&S->ytmp[row]) - sum) * S->udinv[q];
-        S->ytmp[row] = y;
-        T *out = which == 0 ? S->ph : S->sh;
-        const int32_t orow = S->perm ? S->perm[row] : row;
-        out[orow] = y;
+      const T sum = chunk_rowsums<T, kTrsvU, true>(S.uptr, S.ucol, S.uval, S.ytmp, q0, nr, sm);
+      if (lane < nr) {
+        const int64_t q = q0 + lane;
+        const int32_t row = S.urow[q];
+        const T y = (__ldcg(&S.ytmp[row]) - sum) * S.udinv[q];
+        S.ytmp[row] = y;
+        T *out = which == 0 ? S.ph : S.sh;
+        out[S.ugat[q]] = y;
       }
     }
   }
 }
 
-template <typename T, int G>
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_trsv_persistent(const SysDev<T> *sys, const BiState<T> *st, const int32_t *active, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err) {
+  __shared__ T sm[kWarps][32 * kTrsvU];
+  T *my = sm[threadIdx.x >> 5];
   for (int k = 0; k < lL.nlev; ++k) {
-    trsv_level_rows<T, G>(sys, st, active, lL, k, true, which);
+    trsv_level_rows<T>(sys, st, active, lL, k, true, which, my);
     if (!grid_barrier(bar, err)) return;
   }
   for (int k = 0; k < lU.nlev; ++k) {
-    trsv_level_rows<T, G>(sys, st, active, lU, k, false, which);
+    trsv_level_rows<T>(sys, st, active, lU, k, false, which, my);
     if (k + 1 < lU.nlev && !grid_barrier(bar, err)) return;
   }
 }
 
-template <typename T, int G>
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_trsv_level(const SysDev<T> *sys, const BiState<T> *st, const int32_t *active, Levels lv, int k, int lower, int which) {
-  trsv_level_rows<T, G>(sys, st, active, lv, k, lower != 0, which);
+  __shared__ T sm[kWarps][32 * kTrsvU];
+  trsv_level_rows<T>(sys, st, active, lv, k, lower != 0, which, sm[threadIdx.x >> 5]);
 }
 
 // ------------------------------------------------------ ILU(0) factorisation
@@ -551,27 +624,22 @@ __global__ void k_split_factor(int64_t nnz, int64_t n, const double *lu, const i
 
 // ------------------------------------------------------- FP64 residual
 // r = b - A x (FP64), ||r||^2 and ||b||^2 per system -> rnorm2 / bnorm2.
-template <int G>
 __global__ void __launch_bounds__(kThreads) k_residual64(const RefDev *sys, Tiles tl, double *partials, int32_t *counters, const int32_t *active, double *rnorm2, double *bnorm2) {
+  __shared__ double sm[kWarps][32 * kSpmvU];
   const int tile = blockIdx.x;
   const int s = tl.tile_sys[tile];
   if (!active[s]) return;
   const RefDev S = sys[s];
-  const int lane = threadIdx.x % G, grp = threadIdx.x / G;
-  const int wgrp = (threadIdx.x & ~31) / G;
-  constexpr int NG = kThreads / G;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t r0 = tl.tile_row0[tile], r1 = tl.tile_row1[tile];
   double acc[2] = {0.0, 0.0};
-  for (int64_t base = r0 + wgrp; base < r1; base += NG) {
-    const int64_t row = base + (grp - wgrp);
-    const bool valid = row < r1;
-    double sum = 0.0;
-    if (valid)
-      for (int64_t k = S.rp[row] + lane; k < S.rp[row + 1]; k += G) sum += S.av[k] * S.x[S.ci[k]];
-    sum = group_sum<double, G>(sum);
-    if (valid && lane == 0) {
-      double bb = S.b[row];
-      double r = bb - sum;
+  for (int64_t q0 = r0 + 32 * w; q0 < r1; q0 += 32 * kWarps) {
+    const int nr = (int)(r1 - q0 < 32 ? r1 - q0 : 32);
+    const double ax = chunk_rowsums<double, kSpmvU, false>(S.rp, S.ci, S.av, S.x, q0, nr, sm[w]);
+    if (lane < nr) {
+      const int64_t row = q0 + lane;
+      const double bb = S.b[row];
+      const double r = bb - ax;
       S.r[row] = r;
       acc[0] += r * r;
       acc[1] += bb * bb;
@@ -588,21 +656,16 @@ __global__ void k_cast_f64_f32(int64_t n, const double *a, float *b) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = (float)a[i];
 }
 
-// plain SpMV for tests / timing (y = A x), G lanes per row
-template <typename T, int G>
+// plain SpMV for tests / timing (y = A x): the warps of the grid take 32-row chunks in turn
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_spmv_plain(int64_t n, const int64_t *rp, const int32_t *ci, const T *av, const T *x, T *y) {
-  const int lane = threadIdx.x % G;
-  const int64_t grp = ((int64_t)blockIdx.x * kThreads + threadIdx.x) / G;
-  const int64_t wgrp = ((int64_t)blockIdx.x * kThreads + (threadIdx.x & ~31)) / G;
-  const int64_t ngrp = ((int64_t)gridDim.x * kThreads) / G;
-  for (int64_t base = wgrp; base < n; base += ngrp) {
-    const int64_t row = base + (grp - wgrp);
-    const bool valid = row < n;
-    T sum = T(0);
-    if (valid)
-      for (int64_t k = rp[row] + lane; k < rp[row + 1]; k += G) sum += av[k] * x[ci[k]];
-    sum = group_sum<T, G>(sum);
-    if (valid && lane == 0) y[row] = sum;
+  __shared__ T sm[kWarps][32 * kSpmvU];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t gw = (int64_t)blockIdx.x * kWarps + w, nw = (int64_t)gridDim.x * kWarps;
+  for (int64_t q0 = 32 * gw; q0 < n; q0 += 32 * nw) {
+    const int nr = (int)(n - q0 < 32 ? n - q0 : 32);
+    const T v = chunk_rowsums<T, kSpmvU, false>(rp, ci, av, x, q0, nr, sm[w]);
+    if (lane < nr) y[q0 + lane] = v;
   }
 }
 
@@ -622,51 +685,17 @@ static inline int grid_for(int64_t n) {
 
 static std::atomic<long long> g_launches{0};
 
-template <typename T, int G>
-static void launch_spmv_dot_g(int ntiles, const SysDev<T> *sys, BiState<T> *st, Tiles tl, T *part, int32_t *cnt, const int32_t *act, int which, cudaStream_t s) {
-  g_launches += 1;
-  k_spmv_dot<T, G><<<ntiles, kThreads, 0, s>>>(sys, st, tl, part, cnt, act, which);
-}
-
 template <typename T>
-static void launch_spmv_dot_t(int group, int ntiles, const SysDev<T> *sys, BiState<T> *st, Tiles tl, T *part, int32_t *cnt, const int32_t *act, int which, cudaStream_t s) {
-  switch (group) {
-    case 2: launch_spmv_dot_g<T, 2>(ntiles, sys, st, tl, part, cnt, act, which, s); break;
-    case 4: launch_spmv_dot_g<T, 4>(ntiles, sys, st, tl, part, cnt, act, which, s); break;
-    case 8: launch_spmv_dot_g<T, 8>(ntiles, sys, st, tl, part, cnt, act, which, s); break;
-    case 16: launch_spmv_dot_g<T, 16>(ntiles, sys, st, tl, part, cnt, act, which, s); break;
-    default: launch_spmv_dot_g<T, 32>(ntiles, sys, st, tl, part, cnt, act, which, s); break;
-  }
-}
-
-template <typename T>
-static void *trsv_fn(int group) {
-  switch (group) {
-    case 1: return (void *)k_trsv_persistent<T, 1>;
-    case 2: return (void *)k_trsv_persistent<T, 2>;
-    case 4: return (void *)k_trsv_persistent<T, 4>;
-    default: return (void *)k_trsv_persistent<T, 8>;
-  }
-}
-
-template <typename T>
-static int launch_trsv_t(int mode, int group, int grid, const SysDev<T> *sys, const BiState<T> *st, const int32_t *act, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err, cudaStream_t s) {
+static int launch_trsv_t(int mode, int grid, const SysDev<T> *sys, const BiState<T> *st, const int32_t *act, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err, cudaStream_t s) {
   if (mode == 1) {
     g_launches += 1;
     void *args[] = {(void *)&sys, (void *)&st, (void *)&act, (void *)&lL, (void *)&lU, (void *)&which, (void *)&bar, (void *)&err};
-    return (int)cudaLaunchCooperativeKernel(trsv_fn<T>(group), dim3(grid), dim3(kThreads), args, 0, s);
+    return (int)cudaLaunchCooperativeKernel((void *)k_trsv_persistent<T>, dim3(grid), dim3(kThreads), args, 0, s);
   }
   g_launches += lL.nlev + lU.nlev;
   for (int pass = 0; pass < 2; ++pass) {
     const Levels &lv = pass == 0 ? lL : lU;
-    for (int k = 0; k < lv.nlev; ++k) {
-      switch (group) {
-        case 1: k_trsv_level<T, 1><<<grid, kThreads, 0, s>>>(sys, st, act, lv, k, 1 - pass, which); break;
-        case 2: k_trsv_level<T, 2><<<grid, kThreads, 0, s>>>(sys, st, act, lv, k, 1 - pass, which); break;
-        case 4: k_trsv_level<T, 4><<<grid, kThreads, 0, s>>>(sys, st, act, lv, k, 1 - pass, which); break;
-        default: k_trsv_level<T, 8><<<grid, kThreads, 0, s>>>(sys, st, act, lv, k, 1 - pass, which); break;
-      }
-    }
+    for (int k = 0; k < lv.nlev; ++k) k_trsv_level<T><<<grid, kThreads, 0, s>>>(sys, st, act, lv, k, 1 - pass, which);
   }
   return (int)cudaGetLastError();
 }
@@ -688,9 +717,10 @@ long long vk_launches_total() { return g_launches.load(); }
     g_launches += 1;                                                                                                 \
     k_update_p<T><<<ntiles, kThreads, 0, s>>>((const SysDev<T> *)sys, (BiState<T> *)st, *(const Tiles *)tl, act);    \
   }                                                                                                                  \
-  void vk_spmv_dot_##SUF(int group, int ntiles, const void *sys, void *st, const VkTiles *tl, T *part, int32_t *cnt, \
+  void vk_spmv_dot_##SUF(int ntiles, const void *sys, void *st, const VkTiles *tl, T *part, int32_t *cnt,            \
                          const int32_t *act, int which, cudaStream_t s) {                                            \
-    launch_spmv_dot_t<T>(group, ntiles, (const SysDev<T> *)sys, (BiState<T> *)st, *(const Tiles *)tl, part, cnt, act, which, s); \
+    g_launches += 1;                                                                                                 \
+    k_spmv_dot<T><<<ntiles, kThreads, 0, s>>>((const SysDev<T> *)sys, (BiState<T> *)st, *(const Tiles *)tl, part, cnt, act, which); \
   }                                                                                                                  \
   void vk_update_s_##SUF(int ntiles, const void *sys, void *st, const VkTiles *tl, T *part, int32_t *cnt,           \
                          const int32_t *act, cudaStream_t s) {                                                       \
@@ -707,29 +737,23 @@ long long vk_launches_total() { return g_launches.load(); }
     g_launches += 1;                                                                                                 \
     k_precond_copy<T><<<ntiles, kThreads, 0, s>>>((const SysDev<T> *)sys, (const BiState<T> *)st, *(const Tiles *)tl, act, which); \
   }                                                                                                                  \
-  int vk_trsv_##SUF(int mode, int group, int grid, const void *sys, const void *st, const int32_t *act,             \
-                    const VkLevels *lL, const VkLevels *lU, int which, unsigned *bar, int32_t *err, cudaStream_t s) {  \
-    return launch_trsv_t<T>(mode, group, grid, (const SysDev<T> *)sys, (const BiState<T> *)st, act, *(const Levels *)lL, \
+  int vk_trsv_##SUF(int mode, int grid, const void *sys, const void *st, const int32_t *act, const VkLevels *lL,     \
+                    const VkLevels *lU, int which, unsigned *bar, int32_t *err, cudaStream_t s) {                    \
+    return launch_trsv_t<T>(mode, grid, (const SysDev<T> *)sys, (const BiState<T> *)st, act, *(const Levels *)lL,   \
                             *(const Levels *)lU, which, bar, err, s);                                                \
   }                                                                                                                  \
-  int vk_trsv_occupancy_##SUF(int group, int *blocks_per_sm) {                                                       \
-    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, trsv_fn<T>(group), kThreads, 0);       \
+  int vk_trsv_occupancy_##SUF(int *blocks_per_sm) {                                                                  \
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, (void *)k_trsv_persistent<T>, kThreads, 0); \
   }                                                                                                                  \
   void vk_split_factor_##SUF(int64_t nnz, int64_t n, const double *lu, const int64_t *fmap, const int64_t *diag,     \
                              const int64_t *dpos, T *lval, T *uval, T *udinv, cudaStream_t s) {                      \
     g_launches += 1;                                                                                                 \
     k_split_factor<T><<<grid_for(nnz > n ? nnz : n), kThreads, 0, s>>>(nnz, n, lu, fmap, diag, dpos, lval, uval, udinv); \
   }                                                                                                                  \
-  void vk_spmv_plain_##SUF(int group, int grid, int64_t n, const int64_t *rp, const int32_t *ci, const T *av,       \
-                           const T *x, T *y, cudaStream_t s) {                                                       \
+  void vk_spmv_plain_##SUF(int grid, int64_t n, const int64_t *rp, const int32_t *ci, const T *av, const T *x, T *y, \
+                           cudaStream_t s) {                                                                         \
     g_launches += 1;                                                                                                 \
-    switch (group) {                                                                                                 \
-      case 2: k_spmv_plain<T, 2><<<grid, kThreads, 0, s>>>(n, rp, ci, av, x, y); break;                             \
-      case 4: k_spmv_plain<T, 4><<<grid, kThreads, 0, s>>>(n, rp, ci, av, x, y); break;                             \
-      case 8: k_spmv_plain<T, 8><<<grid, kThreads, 0, s>>>(n, rp, ci, av, x, y); break;                             \
-      case 16: k_spmv_plain<T, 16><<<grid, kThreads, 0, s>>>(n, rp, ci, av, x, y); break;                           \
-      default: k_spmv_plain<T, 32><<<grid, kThreads, 0, s>>>(n, rp, ci, av, x, y); break;                           \
-    }                                                                                                                \
+    k_spmv_plain<T><<<grid, kThreads, 0, s>>>(n, rp, ci, av, x, y);                                                  \
   }
 
 VK_BODY_T(float, f32)
@@ -740,19 +764,14 @@ void vk_reliable_x(int ntiles, const void *sys32, const void *st, const VkTiles 
   k_reliable_x<<<ntiles, kThreads, 0, s>>>((const SysDev<float> *)sys32, (const BiState<float> *)st, *(const Tiles *)tl, act);
 }
 
-void vk_reliable_r(int group, int ntiles, const void *sys32, void *st, const VkTiles *tl, double *part, int32_t *cnt,
+void vk_reliable_r(int ntiles, const void *sys32, void *st, const VkTiles *tl, double *part, int32_t *cnt,
                    const int32_t *act, double tol64, int force, cudaStream_t s) {
   const SysDev<float> *S = (const SysDev<float> *)sys32;
   BiState<float> *B = (BiState<float> *)st;
   const Tiles t = *(const Tiles *)tl;
-  g_launches += 1;
-  switch (group) {
-    case 2: k_reliable_r<2><<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force); break;
-    case 4: k_reliable_r<4><<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force); break;
-    case 8: k_reliable_r<8><<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force); break;
-    case 16: k_reliable_r<16><<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force); break;
-    default: k_reliable_r<32><<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force); break;
-  }
+  g_launches += 2;
+  k_reliable_r<<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force);
+  k_reliable_scale<<<ntiles, kThreads, 0, s>>>(S, B, t, part, cnt, act, tol64, force);
 }
 
 int vk_ilu0(int mode, int grid, const void *fs, const VkLevels *lv, unsigned *bar, int32_t *err, cudaStream_t s) {
@@ -784,18 +803,10 @@ size_t vk_sysdev_size_f64() { return sizeof(SysDev<double>); }
 size_t vk_bistate_size_f32() { return sizeof(BiState<float>); }
 size_t vk_bistate_size_f64() { return sizeof(BiState<double>); }
 
-void vk_residual64(int group, int ntiles, const void *ref, const VkTiles *tl, double *part, int32_t *cnt, const int32_t *act,
+void vk_residual64(int ntiles, const void *ref, const VkTiles *tl, double *part, int32_t *cnt, const int32_t *act,
                    double *rnorm2, double *bnorm2, cudaStream_t s) {
-  const Tiles t = *(const Tiles *)tl;
-  const RefDev *r = (const RefDev *)ref;
   g_launches += 1;
-  switch (group) {
-    case 2: k_residual64<2><<<ntiles, kThreads, 0, s>>>(r, t, part, cnt, act, rnorm2, bnorm2); break;
-    case 4: k_residual64<4><<<ntiles, kThreads, 0, s>>>(r, t, part, cnt, act, rnorm2, bnorm2); break;
-    case 8: k_residual64<8><<<ntiles, kThreads, 0, s>>>(r, t, part, cnt, act, rnorm2, bnorm2); break;
-    case 16: k_residual64<16><<<ntiles, kThreads, 0, s>>>(r, t, part, cnt, act, rnorm2, bnorm2); break;
-    default: k_residual64<32><<<ntiles, kThreads, 0, s>>>(r, t, part, cnt, act, rnorm2, bnorm2); break;
-  }
+  k_residual64<<<ntiles, kThreads, 0, s>>>((const RefDev *)ref, *(const Tiles *)tl, part, cnt, act, rnorm2, bnorm2);
 }
 
 void vk_cast_f64_f32(int64_t n, const double *a, float *b, cudaStream_t s) {

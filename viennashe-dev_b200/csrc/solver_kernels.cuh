@@ -13,7 +13,8 @@ namespace vshe {
 // entry k of the forward solve is row lrow[k] (permuted numbering) with strict
 // lower entries [lptr[k], lptr[k+1]) of (lcol, lval); entry k of the backward
 // solve is row urow[k] with strict upper entries [uptr[k], uptr[k+1]) and the
-// inverse diagonal udinv[k].  perm[i] is the original row of permuted row i.
+// inverse diagonal udinv[k].  perm[i] is the original row of permuted row i;
+// lgat[k] = perm[lrow[k]] and ugat[k] = perm[urow[k]] (original rows of the entries).
 template <typename T>
 struct SysDev {
   int64_t n;
@@ -23,6 +24,7 @@ struct SysDev {
   const int32_t *perm;
   const int32_t *lrow; const int64_t *lptr; const int32_t *lcol; const T *lval;
   const int32_t *urow; const int64_t *uptr; const int32_t *ucol; const T *uval; const T *udinv;
+  const int32_t *lgat, *ugat;
   T *ytmp;  // permuted-order work vector of the triangular solves
   // Krylov vectors (original order)
   T *x, *r, *rh, *p, *v, *s, *t, *ph, *sh;
@@ -47,8 +49,11 @@ struct BiState {
   int32_t upd;    // reliable update requested (mixed)
   int32_t restart;// next iteration restarts the Krylov recurrence (p = r)
   int32_t nupd;   // reliable updates done
+  int32_t bad;    // mixed: the FP32 cycle produced a non-finite value; its x correction is discarded
+  T thresh;       // mixed: ||r32|| below which the next reliable update is taken
   double res64;   // true FP64 residual ||b - A x64|| / ||b|| after the last reliable update
-  double maxr;    // residual norm at the last reliable update (FP64)
+  double sigma;   // mixed: scale of the FP32 cycle, r_true = sigma * r32 (||r32|| = 1 at its start)
+  double sigma_new; // mixed: ||b - A x64|| of the reliable update in progress
   double bnorm64; // ||b|| in FP64
 };
 
@@ -62,14 +67,16 @@ struct Tiles {
   const int32_t *sys_tile0;
 };
 
-// Level schedule of a batch: entries of global level k are [lvl_ptr[k], lvl_ptr[k+1]);
-// entry e is level-ordered position ent_row[e] of system ent_sys[e] (for a single
-// system both arrays are NULL and the entry index is the position).
+// Level schedule of a batch: entries of global level k are [lvl_ptr[k], lvl_ptr[k+1]).
+// Triangular solves: entry e is a chunk of ent_cnt[e] <= 32 consecutive level-ordered
+// positions of system ent_sys[e] starting at ent_row[e].  Factorisation: entry e is the
+// permuted row ent_row[e] of system ent_sys[e] (ent_sys NULL for a single system, ent_cnt NULL).
 struct Levels {
   int32_t nlev;
   const int64_t *lvl_ptr;
   const int32_t *ent_sys;
   const int32_t *ent_row;
+  const int32_t *ent_cnt;
 };
 
 // ILU(0) factorisation view of one system: values in FP64 in the permuted

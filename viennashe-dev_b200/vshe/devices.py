@@ -263,10 +263,10 @@ def config1():
     return dev, cfg
 
 
-def config2(nx=200, ny=50, n_energies=160, L=3):
+def config2(nx=200, ny=50, n_energies=160, L=3, bias=0.8):
     """2D n+/n/n+ bar 400 x 100 nm on a 200 x 50 quad mesh, contacts 1e25, channel 1e22,
     Gaussian lateral edges (sigma 5 nm, seed 7), L = 3, 160 energies, 0.8 V."""
-    dev = nin_bar_2d(nx=nx, ny=ny, bias=0.8, seed=7, name="config2_nin2d_%dx%d" % (nx, ny))
+    dev = nin_bar_2d(nx=nx, ny=ny, bias=bias, seed=7, name="config2_nin2d_%dx%d" % (nx, ny))
     sp = HBAR_OMEGA_OP / 4.0
     cfg = SheConfig(max_expansion_order=L, energy_spacing=sp, min_kinetic_energy_range=energy_range_for(dev, sp, n_energies))
     return dev, cfg

@@ -260,6 +260,7 @@ def _she_lib():
         L.vshe_she_scaling.argtypes = [vp, C.c_int64, f64p, f64p]
         L.vshe_she_free.argtypes = [vp, C.c_int64]
         L.vshe_she_bench.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, f64p, C.POINTER(SolveStatsC)]
+        L.vshe_she_run_batch.argtypes = [vp, C.c_int32, i64p, C.POINTER(SolveStatsC), f64p, f64p]
         L._she_ready = True
     return L
 
@@ -361,3 +362,16 @@ class SheProblem:
         f = np.zeros(n)
         self.ctx._check(_she_lib().vshe_she_scaling(self.ctx.h, self.h, ptr(s, C.c_double), ptr(f, C.c_double)))
         return s, f
+
+
+def she_run_batch(ctx: Context, problems):
+    """Assemble, solve (one batch) and finish several SHE problems: per-problem stats, full
+    residuals, and the device time of the whole call in ms."""
+    hs = np.array([p.h for p in problems], np.int64)
+    st = (SolveStatsC * len(problems))()
+    fr = np.zeros(len(problems))
+    ms = C.c_double()
+    rc = _she_lib().vshe_she_run_batch(ctx.h, len(problems), ptr(hs, C.c_int64), st, ptr(fr, C.c_double), C.byref(ms))
+    if rc and rc != -6:
+        ctx._check(rc)
+    return [stats_dict(s) for s in st], fr, ms.value
