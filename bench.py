@@ -1,46 +1,47 @@
 #!/usr/bin/env python
 """Benchmark of the SHE linear-solve path on B200 (one JSON line on stdout).
 
-Workload (N = 1): the 2D n+/n/n+ bar of 400 x 100 nm on a 200 x 50 quad mesh,
-contacts 1e25 m^-3, channel 1e22 m^-3, Gaussian lateral doping edges (sigma 5 nm,
-positions jittered from seed 7), SHE order L = 3, 160 energies, 0.8 V; seeded
-synthetic device, frozen analytic potential (vshe/devices.py).
+Workload (N = 1): the 2D n+/n/n+ bar of 400 x 100 nm on a 200 x 50 quad mesh, contacts
+1e25 m^-3, channel 1e22 m^-3, Gaussian lateral doping edges (sigma 5 nm, positions jittered
+from seed 7), SHE order L = 3, 160 energies, 0.8 V; seeded synthetic device, frozen analytic
+potential (vshe/devices.py).
 
-A step is one full pass of the hot path on the device: assembly of the
-streaming and scattering operators, odd elimination, scaling and normalisation,
-ILU(0) factorisation and the mixed-precision BiCGStab (FP32 recurrences, FP64
-reliable updates) to an FP64 relative residual of 1e-10, then odd recovery,
-full-system residual, density and terminal currents.  `value` is solves/s with
-the device description resident in HBM; `e2e` is solves/s through the drop-in
-C ABI (vshe_system_set_values + vshe_system_solve + download of x) with host
-buffers, the way a ViennaSHE Gummel loop calls solvers::solve for a matrix of
-unchanged pattern.  `--impl reference` times the CPU restatement of the
-reference's serial solver (ILU(0) + BiCGStab, single thread) on the same
-reduced system (bounded sample, iterations extrapolated).
+A step is one full pass of the hot path on the device: assembly of the streaming and
+scattering operators, odd elimination, scaling and normalisation, block-ILU(0) per energy slab
+(node 4-colour order) and BiCGStab to an FP64 relative residual of 1e-10, then odd recovery,
+full-system residual, density and terminal currents.  `value` is solves/s of that pass in the
+mixed-precision mode (FP64 Krylov, FP32 ILU factors and triangular solves) with the device
+description resident in HBM; `fp64_solves_per_s` is the same pass with the plain FP64 solver.
+`e2e` is solves/s through the drop-in C ABI (vshe_system_set_values + vshe_system_solve +
+download of x) with host buffers, the way a ViennaSHE Gummel loop calls solvers::solve for a
+matrix of unchanged pattern.
 
-Multi-GPU: replicas only (independent solves, no collective); launched with
-torchrun, every rank solves its own replica on its GPU, value = all ranks'
-solves / max-over-ranks time.
+`--impl reference` times the CPU restatement of the reference's serial solver (ILU(0) +
+BiCGStab with r^ = r_0, FP64, one thread, natural order: serial_linear_solver's algorithm) on
+the same reduced system: the factorisation plus a bounded number of iterations are timed on
+the host, and the iteration count to 1e-10 of that same algorithm is counted on the device
+(untimed).
+
+Multi-GPU: replicas only (independent solves, no collective); launched with torchrun, every
+rank solves its own replica on its GPU, value = all ranks' solves / max-over-ranks time.
 """
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-PKG = os.path.join(ROOT, "viennashe-dev_b200")
-sys.path.insert(0, PKG)
+sys.path.insert(0, os.path.join(ROOT, "viennashe-dev_b200"))
 
 METRIC = "solves/s & p99 latency at 1e-10 resid (mixed vs plain FP64 GPU); SpMV GB/s"
 UNIT = "solves/s"
+TOL = 1e-10
 
 
 def parse():
@@ -53,7 +54,7 @@ def parse():
     ap.add_argument("--ny", type=int, default=50)
     ap.add_argument("--ne", type=int, default=160)
     ap.add_argument("--L", type=int, default=3)
-    ap.add_argument("--cpu-seconds", type=float, default=25.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="host time of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--pass-only", action="store_true",
@@ -67,33 +68,28 @@ class Dist:
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = None
         if self.world > 1:
-            import torch.distributed as dist
             import datetime
+            import torch.distributed as dist
             os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=900))
             self.dist = dist
 
     def barrier(self):
         if self.world > 1:
             self.dist.barrier()
 
-    def max(self, v):
-        if self.world == 1:
-            return v
+    def _reduce(self, v, op):
         import torch
         t = torch.tensor([float(v)], dtype=torch.float64)
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        self.dist.all_reduce(t, op=op)
         return float(t.item())
 
+    def max(self, v):
+        return self._reduce(v, self.dist.ReduceOp.MAX) if self.world > 1 else v
+
     def sum(self, v):
-        if self.world == 1:
-            return v
-        import torch
-        t = torch.tensor([float(v)], dtype=torch.float64)
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
-        return float(t.item())
+        return self._reduce(v, self.dist.ReduceOp.SUM) if self.world > 1 else v
 
     def close(self):
         if self.world > 1:
@@ -103,6 +99,8 @@ class Dist:
 # ------------------------------------------------------------------- clocks
 class Clocks:
     """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu):
         self.gpu = gpu
@@ -119,7 +117,7 @@ class Clocks:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except Exception:
+        except OSError:
             self.proc = None
 
     def stop(self):
@@ -128,10 +126,9 @@ class Clocks:
         self.proc.terminate()
         try:
             self.proc.wait(5)
-        except Exception:
+        except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
@@ -141,7 +138,7 @@ class Clocks:
                 mx = max(mx, float(f[2]))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
+            for nm, v in zip(self.NAMES, f[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
         os.unlink(self.path)
@@ -153,85 +150,95 @@ class Clocks:
 def measured_peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
+    except (OSError, ValueError):
         return None
 
 
-# -------------------------------------------------------------- CPU baseline
-def cpu_sample(A_rp, A_ci, A_v, b, budget_s):
-    """Serial ILU(0) + BiCGStab of the oracle (the reference's serial_linear_solver, restated) on the
-    reduced system: factorisation + as many iterations as fit the budget; the solve time is
-    extrapolated to a 1e-10 residual from the observed log-linear residual decay."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_api as O
-    A = O.CSR(A_rp, A_ci, A_v)
-    probe = O.bench_serial(A, b, 2)
-    t_iter = max(probe["t_per_iter"], 1e-6)
-    iters = int(max(3, min(400, (budget_s - probe["t_factor"]) / t_iter)))
-    r = O.bench_serial(A, b, iters)
-    rate = r["relres"] ** (1.0 / max(r["iters"], 1)) if r["relres"] > 0 else 0.0
-    need = r["iters"] if r["relres"] <= 1e-10 else (math.log(1e-10) / math.log(rate) if 0 < rate < 1 else float("inf"))
-    t_solve = r["t_factor"] + need * r["t_per_iter"]
-    return {
-        "value": 1.0 / t_solve if t_solve > 0 else 0.0,
-        "unit": UNIT,
-        "cores": 1,
-        "kind": "port",
-        "sample": ("serial ILU(0) factorisation + %d BiCGStab iterations on the full reduced system "
-                   "(n=%d, nnz=%d): factor %.2f s, %.3f s/iteration, residual %.2e; iterations to 1e-10 "
-                   "extrapolated log-linearly = %.0f; CPU assembly/elimination not included"
-                   % (r["iters"], A.n, A.nnz, r["t_factor"], r["t_per_iter"], r["relres"], need)),
-        "t_factor_s": r["t_factor"], "t_per_iter_s": r["t_per_iter"], "iters_est": need,
-    }
+def workload_name(args):
+    return "nin_bar_2d_%dx%d_L%d_E%d_0.8V" % (args.nx, args.ny, args.L, args.ne)
 
 
 def build_problem(args, ctx, precision):
     from vshe import devices as D
     from vshe import gpu
     dev, cfg = D.config2(nx=args.nx, ny=args.ny, n_energies=args.ne, L=args.L)
-    ordering = "multicolor" if dev.dim == 2 else "natural"
-    return gpu.SheProblem(ctx, dev, cfg, precision=precision, precond="ilu0", ordering=ordering,
-                          tol=1e-10, max_iters=20000, check_every=16), dev
+    return gpu.SheProblem(ctx, dev, cfg, precision=precision, precond="block_ilu0", ordering="multicolor",
+                          tol=TOL, max_iters=20000, check_every=16)
 
 
-def workload_name(args):
-    return "config2_nin2d_%dx%d_L%d_E%d_0.8V" % (args.nx, args.ny, args.L, args.ne)
+# -------------------------------------------------------------- CPU baseline
+def reference_iterations(ctx, rp, ci, v, b):
+    """Iterations the reference's serial algorithm (natural-order ILU(0), BiCGStab with
+    r^ = r_0, FP64) needs for 1e-10 on this system, counted on the device (not timed)."""
+    S = ctx.system(rp, ci, v, b, precision="fp64", precond="ilu0", ordering="natural", shadow="r0",
+                   tol=TOL, max_iters=20000, check_every=32)
+    try:
+        _, st = S.solve(want_x=False)
+    finally:
+        S.free()
+    return st
+
+
+def cpu_sample(rp, ci, v, b, iters_ref, budget_s):
+    """The oracle's serial ILU(0) factorisation and BiCGStab iterations (r^ = r_0, the
+    reference's serial_linear_solver algorithm) timed on one host core; solves/s =
+    1 / (t_factor + iters_ref * t_iteration)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_api as O
+    A = O.CSR(rp, ci, v)
+    probe = O.bench_serial(A, b, 2)
+    t_iter = max(probe["t_per_iter"], 1e-6)
+    iters = int(max(3, min(500, (budget_s - probe["t_factor"]) / t_iter)))
+    r = O.bench_serial(A, b, iters)
+    t_solve = r["t_factor"] + iters_ref * r["t_per_iter"]
+    return {
+        "value": 1.0 / t_solve, "unit": UNIT, "cores": 1, "kind": "port",
+        "sample": ("oracle serial ILU(0) + BiCGStab (r^ = r_0, FP64, natural order) on the full reduced "
+                   "system (n=%d, nnz=%d), one host core: factorisation %.2f s and %d iterations timed "
+                   "(%.3f s/iteration); %d iterations to 1e-10 counted on the device for the same "
+                   "algorithm; assembly/elimination on the CPU not included"
+                   % (A.n, A.nnz, r["t_factor"], r["iters"], r["t_per_iter"], iters_ref)),
+        "t_factor_s": r["t_factor"], "t_per_iter_s": r["t_per_iter"], "iterations": iters_ref,
+    }
 
 
 def run_reference(args, D_):
     if D_.rank != 0:
         return
     from vshe import gpu
-    # the reduced system is assembled once on the device (input preparation, not timed)
     ctx = gpu.Context(D_.local)
-    P, dev = build_problem(args, ctx, "fp64")
-    rp, ci, v, b = P.export("reduced")
+    P = build_problem(args, ctx, "fp64")
+    P.assemble(3)
+    rp, ci, v, b = P.export("reduced")   # input preparation (not timed)
     P.free()
+    st = reference_iterations(ctx, rp, ci, v, b)
     ctx.close()
     vals = []
+    per_step = args.cpu_seconds / max(1, args.warmup + args.steps)
     for k in range(args.warmup + args.steps):
-        s = cpu_sample(rp, ci, v, b, args.cpu_seconds / max(1, args.warmup + args.steps))
+        s = cpu_sample(rp, ci, v, b, st["iterations"], max(per_step, 3.0))
         if k >= args.warmup:
             vals.append(s)
     val = statistics.median([s["value"] for s in vals])
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / val if val else None,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / val,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload_name(args), "n_unknowns": int(len(b)), "nnz": int(len(v))},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": 1, "kind": "port", "sample": vals[-1]["sample"]},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_solve": {"iterations": st["iterations"], "rel_residual": st["rel_residual"]},
     }
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------- our arm
 def run_ours(args, D_):
     from vshe import gpu
     ctx = gpu.Context(D_.local)
-    P, dev = build_problem(args, ctx, "mixed")
+    P = build_problem(args, ctx, "mixed")
     info = P.info
-    # warm-up (untimed)
-    P.bench(args.warmup, 1)
+    P.bench(args.warmup, 1)  # warm-up passes (untimed)
     D_.barrier()
     clk = Clocks(D_.local)
     clk.start()
@@ -244,19 +251,15 @@ def run_ours(args, D_):
     D_.barrier()
     total_s = float(np.sum(ms)) / 1000.0
     tmax = D_.max(total_s)
-    solves = D_.sum(args.steps)
-    value = solves / tmax
-    lat = sorted(ms)
-    p50 = float(np.percentile(lat, 50))
-    p99 = float(np.percentile(lat, 99))
-    res = {"iterations": st["iterations"], "reliable_updates": st["refinements"], "rel_residual": st["rel_residual"],
-           "factor_ms": st["setup_ms"], "krylov_ms": st["solve_ms"], "levels_L": st["levels_L"], "levels_U": st["levels_U"]}
-
+    value = D_.sum(args.steps) / tmax
+    solve = {"iterations": st["iterations"], "residual_replacements": st["refinements"], "rel_residual": st["rel_residual"],
+             "factor_ms": st["setup_ms"], "krylov_ms": st["solve_ms"], "levels_L": st["levels_L"], "levels_U": st["levels_U"]}
+    n, nnz, nnz_lu = int(info["n_even"]), int(info["nnz_reduced"]), int(info["nnz_factor"])
     if args.pass_only:
         if D_.rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D_.world, "steps": args.steps,
                               "warmup": args.warmup, "ms_per_step": 1000.0 * tmax / args.steps,
-                              "config": {"workload": workload_name(args)}, "solve": res, "gpu_launches": gpu_launches,
+                              "config": {"workload": workload_name(args)}, "solve": solve, "gpu_launches": gpu_launches,
                               "pass_only": True}), flush=True)
         P.free()
         ctx.close()
@@ -264,87 +267,90 @@ def run_ours(args, D_):
 
     # per-kernel-class device time of one profiled pass (CUDA events around each launch)
     ctx.set_profiling(True)
-    stp, _ = P.run()
+    P.run()
     prof = ctx.profile()
     ctx.set_profiling(False)
 
-    # FP64 GPU solver on the same problem (the comparison the target is quoted against)
-    P64, _ = build_problem(args, ctx, "fp64")
+    # plain FP64 solver on the same problem
+    P64 = build_problem(args, ctx, "fp64")
     ms64, st64 = P64.bench(1, args.fp64_steps)
     fp64_value = args.fp64_steps / (float(np.sum(ms64)) / 1000.0)
     P64.free()
 
-    # drop-in path: reduced system as host CSR, solved through the C ABI with host buffers
+    # drop-in path: the reduced system as host CSR through the C ABI with host buffers
     rp, ci, v, b = P.export("reduced")
-    n, nnz = len(b), len(v)
-    S = ctx.system(rp, ci, v, b, precision="mixed", precond="ilu0", ordering="multicolor", tol=1e-10, max_iters=20000, check_every=16)
+    S = ctx.system(rp, ci, v, b, precision="mixed", precond="ilu0", ordering="multicolor", tol=TOL,
+                   max_iters=20000, check_every=16)
     S.set_values(v, b)
     S.solve()
     t_e2e = []
-    for k in range(max(2, args.steps // 2)):
+    for _ in range(max(2, args.steps // 2)):
         t1 = time.time()
         S.set_values(v, b)
         x, st_e = S.solve(want_x=True)
         t_e2e.append(time.time() - t1)
     e2e = {"value": len(t_e2e) / sum(t_e2e), "unit": UNIT,
            "h2d_bytes_per_step": int(nnz * 8 + n * 8), "d2h_bytes_per_step": int(n * 8),
-           "path": "vshe_system_set_values + vshe_system_solve + x download (pattern analysed once, as a Gummel loop reuses it)",
+           "path": "vshe_system_set_values + vshe_system_solve + x download; generic greedy-colour ILU(0) "
+                   "(a drop-in caller passes no slab structure); pattern analysed once, as a Gummel loop reuses it",
            "rel_residual": st_e["rel_residual"], "iterations": st_e["iterations"]}
-    spmv32_ms = S.time_spmv("mixed", 20)
-    spmv64_ms = S.time_spmv("fp64", 20)
+    spmv_ms = S.time_spmv("fp64", 20)
     S.free()
+
     peaks = measured_peaks()
     hbm = peaks["hbm_gbs"] if peaks else 6650.0
     peak_src = "measured" if peaks else "fallback"
-    # algorithmic bytes (per launch): SpMV FP32 nnz*(4+4) + (n+1)*8 + n*4 (x) + n*4 (y)
-    spmv_bytes = nnz * 8 + (n + 1) * 8 + 2 * n * 4
-    # one ILU apply (L then U): nnz_LU*(4+4) + 2*(n+1)*8 + 3*n*4, nnz_LU = nnz of the factor pattern
-    trsv_bytes = nnz * 8 + 2 * (n + 1) * 8 + 3 * n * 4
+    # algorithmic bytes per launch
+    spmv_bytes = 12 * nnz + 32 * n           # A (FP64 + int32 col), row_ptr, x, y, fused-dot vector
+    trsv_bytes = 8 * nnz_lu + n * (48 + 16)  # FP32 factors + int32 cols, ptr/row/gather maps, in/out FP64, ytmp/udinv FP32
     kern = {
         "spmv": {"ms_total": prof["spmv_ms"], "launches": prof["spmv_launches"]},
         "trsv": {"ms_total": prof["trsv_ms"], "launches": prof["trsv_launches"]},
         "vector": {"ms_total": prof["vector_ms"]},
-        "reliable_fp64": {"ms_total": prof["reliable_ms"]},
         "factor": {"ms_total": prof["factor_ms"]},
     }
     dominant = "trsv" if prof["trsv_ms"] >= prof["spmv_ms"] else "spmv"
     if dominant == "trsv":
         avg_ms = prof["trsv_ms"] / max(prof["trsv_launches"], 1)
         dbytes = trsv_bytes
+        kname = "k_trsv_persistent<float> (ILU(0) apply, L then U sweeps)"
     else:
         avg_ms = prof["spmv_ms"] / max(prof["spmv_launches"], 1)
         dbytes = spmv_bytes
+        kname = "k_spmv_dot (CSR SpMV FP64 + fused dots)"
     achieved = dbytes / (avg_ms / 1000.0) / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tfile):
         try:
             tt = json.load(open(tfile))
-            if tt.get("workload") == workload_name(args) and dominant in tt:
-                traffic = tt[dominant]
-        except Exception:
+            if tt.get("workload") == workload_name(args):
+                traffic = tt.get(dominant)
+        except (OSError, ValueError):
             traffic = None
-    roofline = {"bound": "hbm", "kernel": "k_trsv_persistent (ILU(0) apply, L then U)" if dominant == "trsv" else "k_spmv_dot (CSR SpMV, FP32)",
-                "achieved": achieved, "peak": hbm, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": traffic, "algorithmic_bytes_per_launch": dbytes, "avg_launch_ms": avg_ms}
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_source": peak_src,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "algorithmic_bytes_per_launch": dbytes, "avg_launch_ms": avg_ms}
     cpu = None
     if D_.rank == 0 and not args.no_cpu:
-        cpu = cpu_sample(rp, ci, v, b, args.cpu_seconds)
+        st_ref = reference_iterations(ctx, rp, ci, v, b)
+        cpu = cpu_sample(rp, ci, v, b, st_ref["iterations"], args.cpu_seconds)
     if D_.rank == 0:
+        lat = np.asarray(ms, float)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D_.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * tmax / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 residual/assembly)", "data": "synthetic",
-            "config": {"workload": workload_name(args), "n_unknowns_reduced": n, "nnz_reduced": nnz,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 Krylov / f32 ILU apply", "data": "synthetic",
+            "config": {"workload": workload_name(args), "n_unknowns_reduced": n, "nnz_reduced": nnz, "nnz_factor": nnz_lu,
                        "n_unknowns_full": int(info["n_even"] + info["n_odd"]), "nnz_full": int(info["nnz_full"]),
-                       "n_energies": int(info["n_energies"]), "ordering": "node 4-colour ILU(0)",
-                       "l2": "inputs larger than L2 (reduced CSR %.2f GB)" % (nnz * 12 / 1e9), "parallelism": "replicas" if D_.world > 1 else "single"},
-            "latency_ms": {"p50": p50, "p99": p99},
-            "fp64_solves_per_s": fp64_value, "mixed_over_fp64": value / fp64_value / max(D_.world, 1) if fp64_value else None,
+                       "n_energies": int(info["n_energies"]), "preconditioner": "block-ILU(0) per energy slab, node 4-colour order",
+                       "l2": "inputs larger than L2 (reduced CSR %.2f GB)" % (nnz * 12 / 1e9),
+                       "parallelism": "replicas" if D_.world > 1 else "single"},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "fp64_solves_per_s": fp64_value, "mixed_over_fp64": (value / max(D_.world, 1)) / fp64_value,
             "fp64": {"iterations": st64["iterations"], "rel_residual": st64["rel_residual"], "ms": [float(x) for x in ms64]},
-            "solve": res, "kernels_ms": kern,
-            "spmv_gbs": {"fp32": spmv_bytes / (spmv32_ms / 1000) / 1e9, "fp64": (nnz * 12 + (n + 1) * 8 + 2 * n * 8) / (spmv64_ms / 1000) / 1e9,
-                         "frac_fp32": spmv_bytes / (spmv32_ms / 1000) / 1e9 / hbm},
+            "solve": solve, "kernels_ms": kern,
+            "spmv_gbs": {"fp64": spmv_bytes / (spmv_ms / 1000) / 1e9, "frac": spmv_bytes / (spmv_ms / 1000) / 1e9 / hbm, "ms": spmv_ms},
             "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline,
             "cpu_baseline": cpu, "clocks": clocks, "wall_s_timed": wall,
         }

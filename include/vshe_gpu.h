@@ -44,9 +44,9 @@ extern "C" {
 #define VSHE_E_UNSUPPORTED      -13   /* option not available in this build */
 
 /* ---- solver options ---- */
-#define VSHE_PRECISION_FP64   0   /* FP64 BiCGStab, FP64 preconditioner */
-#define VSHE_PRECISION_MIXED  1   /* FP32 BiCGStab recurrences + FP32 preconditioner; x and the
-                                     true residual kept in FP64 (reliable updates every 10x drop) */
+#define VSHE_PRECISION_FP64   0   /* FP64 BiCGStab, FP64 ILU(0) factors and triangular solves */
+#define VSHE_PRECISION_MIXED  1   /* FP64 BiCGStab (SpMV, dots, updates), ILU(0) factors stored and
+                                     applied in FP32; convergence on the true FP64 residual */
 
 #define VSHE_PRECOND_NONE        0
 #define VSHE_PRECOND_ILU0        1   /* ILU(0) on the whole system (serial_linear_solver's choice) */
@@ -54,6 +54,9 @@ extern "C" {
 
 #define VSHE_ORDER_NATURAL     0   /* the caller's row order (the reference's) */
 #define VSHE_ORDER_MULTICOLOR  1   /* greedy colouring of the matrix graph, rows grouped by colour */
+
+#define VSHE_SHADOW_DENSE     0   /* fixed dense pseudo-random r^ in [0.5, 1.5) */
+#define VSHE_SHADOW_R0        1   /* r^ = r_0 */
 
 #define VSHE_TRSV_AUTO        0
 #define VSHE_TRSV_PERSISTENT  1   /* one cooperative launch per triangular solve, grid barrier per level */
@@ -65,7 +68,7 @@ typedef struct vshe_solve_opts {
   int32_t ordering;         /* VSHE_ORDER_* */
   double  tol;              /* FP64 relative residual ||b - A x|| / ||b|| to reach (e.g. 1e-10) */
   int32_t max_iters;        /* cap on BiCGStab iterations (all refinement sweeps together) */
-  double  inner_tol;        /* reserved (mixed precision uses reliable updates, see below) */
+  double  inner_tol;        /* reserved */
   int32_t max_refinements;  /* reserved */
   int64_t n_blocks;         /* BLOCK_ILU0: number of blocks; 0 = one block per ... see block_ptr */
   const int64_t *block_ptr; /* n_blocks + 1 row offsets (block_preconditioner_boundaries) */
@@ -73,15 +76,18 @@ typedef struct vshe_solve_opts {
   int32_t check_every;      /* iterations between host-side convergence checks (0 = default 8) */
   const int32_t *perm;      /* optional symmetric permutation for the preconditioner: perm[i] is the
                                original row placed at position i (overrides ordering); NULL = none */
+  int32_t shadow;           /* BiCGStab shadow residual: VSHE_SHADOW_DENSE (default) or
+                               VSHE_SHADOW_R0 (r^ = r_0, as the reference's ViennaCL bicgstab) */
 } vshe_solve_opts;
 
 typedef struct vshe_solve_stats {
   int32_t status;           /* VSHE_OK or an error code */
   int32_t iterations;       /* BiCGStab iterations (all sweeps) */
-  int32_t refinements;      /* FP64 refinement sweeps (mixed) */
+  int32_t refinements;      /* residual replacements: restarts from r = b - A x (FP64) after the
+                               recursive residual met tol but the true one did not */
   double  rel_residual;     /* final FP64 ||b - A x|| / ||b|| */
   double  setup_ms;         /* factorisation time (device) */
-  double  solve_ms;         /* Krylov + refinement time (device) */
+  double  solve_ms;         /* Krylov time incl. residual checks (device) */
   int32_t levels_L;         /* level-schedule depth of the L and U solves */
   int32_t levels_U;
   int64_t bytes_device;     /* device memory held by the system */
@@ -103,7 +109,7 @@ const char *vshe_last_error(vshe_ctx *ctx);
 size_t vshe_bytes_in_use(vshe_ctx *ctx);
 /* Per-kernel-class device timing (CUDA events around every launch of the next
  * solves; off by default).  vshe_get_profile returns, for the last solve, ms spent
- * in [0] SpMV, [1] triangular solves, [2] vector updates, [3] FP64 reliable updates,
+ * in [0] SpMV, [1] triangular solves, [2] vector updates, [3] unused (0),
  * [4] factorisation, and counts[0] SpMV launches, counts[1] triangular-solve launches. */
 int vshe_set_profiling(vshe_ctx *ctx, int32_t on);
 int vshe_get_profile(vshe_ctx *ctx, double *ms, int64_t *counts);
@@ -138,12 +144,13 @@ int vshe_system_get_x(vshe_ctx *ctx, int64_t handle, double *x);
 int vshe_system_free(vshe_ctx *ctx, int64_t handle);
 
 /* Kernel-level entry points on a resident system (used by parity tests and
- * the bench): y = A x in FP64 (precision 0) or FP32 (1), host x/y of length n;
- * the incomplete factor values in A's pattern (FP64, host array of length nnz). */
+ * the bench): y = A x, host x/y of length n (precision must be VSHE_PRECISION_FP64: the
+ * SpMV is FP64 in every solver mode); the incomplete factor values in A's pattern (FP64,
+ * host array of length nnz). */
 int vshe_system_spmv(vshe_ctx *ctx, int64_t handle, int32_t precision, const double *x, double *y);
 int vshe_system_factor_values(vshe_ctx *ctx, int64_t handle, double *lu);
 /* Device-timed kernel throughput on a resident system: runs `reps` SpMVs in the
- * given precision and returns the mean time per SpMV (ms) from CUDA events. */
+ * given precision (FP64 only) and returns the mean time per SpMV (ms) from CUDA events. */
 int vshe_system_time_spmv(vshe_ctx *ctx, int64_t handle, int32_t precision, int32_t reps, double *ms);
 
 /* ---- SHE path on the device: she::assemble + she::solve (secondary boundary) ----
@@ -165,6 +172,7 @@ typedef struct vshe_she_info {
   double  hbar_omega;       /* optical phonon energy snapped to the grid, J */
   int64_t bytes_device;
   int32_t levels_L, levels_U;
+  int64_t nnz_factor;       /* strict lower + upper entries the ILU(0) preconditioner keeps */
 } vshe_she_info;
 
 /* 6 * ((L+1)^2)^2 doubles, layout of vshe_coupling_tables.data; no GPU needed. */

@@ -46,8 +46,14 @@ def test_spmv_parity(gpu_ctx, prob):
         y_ref = O.spmv(A, x)
         y = S.spmv(x, "fp64")
         assert np.max(np.abs(y - y_ref)) <= 1e-13 * np.max(np.abs(y_ref))
-        y32 = S.spmv(x, "mixed")
-        assert np.max(np.abs(y32 - y_ref)) <= 1e-6 * np.max(np.abs(y_ref))
+        # the SpMV is FP64 in every mode; no FP32 copy of A exists
+        with pytest.raises(gpu.VsheError):
+            S.spmv(x, "mixed")
+        # the solution vector is not used as scratch
+        S.solve()
+        x_sol = S.x()
+        S.spmv(x, "fp64")
+        assert np.array_equal(S.x(), x_sol)
     finally:
         S.free()
 

@@ -34,7 +34,7 @@ struct Ctx;
 struct System {
   int64_t n = 0, nnz = 0;
   vshe_solve_opts opts{};
-  bool mixed = true;
+  bool mixed = true;     // FP32 ILU(0) factors and triangular solves (Krylov in FP64 either way)
   bool borrowed = false;  // A and b live in the caller's device memory
   bool has_pc = true;
   double bnorm_host = 0.0;
@@ -53,8 +53,9 @@ struct System {
   // device
   DevArena arena;
   int64_t *d_rp = nullptr; int32_t *d_ci = nullptr;
-  double *d_av64 = nullptr; float *d_av32 = nullptr;
-  double *d_b64 = nullptr, *d_x64 = nullptr, *d_r64 = nullptr;
+  double *d_av64 = nullptr;
+  double *d_b64 = nullptr;
+  double *d_x64 = nullptr;  // = kv[0], the solution
   int32_t *d_perm = nullptr, *d_blk = nullptr;
   int64_t *d_prp = nullptr, *d_pdiag = nullptr, *d_amap = nullptr, *d_fmap = nullptr, *d_dpos = nullptr;
   int32_t *d_pci = nullptr;
@@ -63,7 +64,7 @@ struct System {
   int32_t *d_lgat = nullptr, *d_ugat = nullptr;  // original row of each level-ordered L / U entry
   int64_t *d_lptr = nullptr, *d_uptr = nullptr, *d_lvlptrL = nullptr, *d_lvlptrU = nullptr;
   void *d_lval = nullptr, *d_uval = nullptr, *d_udinv = nullptr, *d_ytmp = nullptr;
-  void *kv[9] = {nullptr};  // x r rh p v s t ph sh in the Krylov precision
+  void *kv[9] = {nullptr};  // x r rh p v s t ph sh (FP64)
 
   int create(Ctx &ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *v,
              const double *rhs, const vshe_solve_opts &o);
@@ -107,12 +108,12 @@ struct Batch {
 
   int build(Ctx &ctx, const std::vector<System *> &members);
   int factor(Ctx &ctx);
-  int bicgstab(Ctx &ctx, double tol, int max_iter, int &iters_out);
+  int bicgstab(Ctx &ctx, double tol, int max_iter, bool resume, int &iters_out);
   int residual(Ctx &ctx, std::vector<double> &rel);
   int set_active(Ctx &ctx, const std::vector<int32_t> &act);
   int solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats);
   int check_err(Ctx &ctx, const char *what);
-  int state_of(int k, int32_t &status, int32_t &iter, int32_t &nupd, double &res) const;
+  int state_of(int k, int32_t &status, int32_t &iter) const;
 };
 
 struct Ctx {

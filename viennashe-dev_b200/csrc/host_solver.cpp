@@ -142,10 +142,9 @@ int System::create_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *r
   return refresh_device_values(ctx);
 }
 
-int System::refresh_device_values(Ctx &ctx) {
-  if (mixed) vk_cast_f64_f32(nnz, d_av64, d_av32, ctx.stream);
-  return VSHE_OK;
-}
+// The Krylov iteration reads A's FP64 values in place; the factors are rebuilt from them by
+// the next solve, so nothing is derived here.
+int System::refresh_device_values(Ctx &) { return VSHE_OK; }
 
 int System::set_values(Ctx &ctx, const double *v, const double *rhs) {
   cudaStream_t s = ctx.stream;
@@ -351,10 +350,9 @@ int System::setup_pattern(Ctx &ctx) {
 #define ALLOCT(ptr, count)                                                   \
   ptr = arena.alloc(tsz * size_t(count), e);                                 \
   if (!ptr) return ctx.cuda_fail(e, "cudaMalloc " #ptr);
-  ALLOC(d_x64, double, n);
-  ALLOC(d_r64, double, n);
-  if (mixed) { ALLOC(d_av32, float, nnz); }
-  for (int k = 0; k < 9; ++k) { ALLOCT(kv[k], n); }
+  // Krylov vectors x r rh p v s t ph sh (FP64); the solution is x itself
+  for (int k = 0; k < 9; ++k) { ALLOC(kv[k], double, n); }
+  d_x64 = (double *)kv[0];
   if (has_pc) {
     ALLOC(d_blk, int32_t, n);
     ALLOC(d_prp, int64_t, n + 1);
@@ -414,20 +412,18 @@ int System::setup_pattern(Ctx &ctx) {
 }
 
 void System::fill_sysdev(void *out) const {
-  // SysDev<T> has the same layout for both T (pointers); fill through the float view
+  // SysDev<P> has the same layout for both factor types (pointers only); fill through the
+  // float view, whose factor pointers the FP64 solver reads as double
   SysDev<float> d;
   std::memset(&d, 0, sizeof(d));
   d.n = n;
-  d.rp = d_rp; d.ci = d_ci;
-  d.av = mixed ? d_av32 : (const float *)d_av64;
-  d.perm = identity_perm ? nullptr : d_perm;
+  d.rp = d_rp; d.ci = d_ci; d.av = d_av64; d.b = d_b64;
   d.lrow = d_lrow; d.lptr = d_lptr; d.lcol = d_lcol; d.lval = (const float *)d_lval;
   d.urow = d_urow; d.uptr = d_uptr; d.ucol = d_ucol; d.uval = (const float *)d_uval; d.udinv = (const float *)d_udinv;
   d.lgat = d_lgat; d.ugat = d_ugat;
   d.ytmp = (float *)d_ytmp;
-  d.x = (float *)kv[0]; d.r = (float *)kv[1]; d.rh = (float *)kv[2]; d.p = (float *)kv[3];
-  d.v = (float *)kv[4]; d.s = (float *)kv[5]; d.t = (float *)kv[6]; d.ph = (float *)kv[7]; d.sh = (float *)kv[8];
-  d.av64 = d_av64; d.b64 = d_b64; d.x64 = d_x64; d.r64 = d_r64;
+  d.x = (double *)kv[0]; d.r = (double *)kv[1]; d.rh = (double *)kv[2]; d.p = (double *)kv[3];
+  d.v = (double *)kv[4]; d.s = (double *)kv[5]; d.t = (double *)kv[6]; d.ph = (double *)kv[7]; d.sh = (double *)kv[8];
   std::memcpy(out, &d, sizeof(d));
 }
 
@@ -509,9 +505,9 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   ALLOC(d_err, int32_t, 1);
   ALLOC(d_rnorm2, double, nsys);
   ALLOC(d_bnorm2, double, nsys);
-  d_sysdev = arena.alloc(vk_sysdev_size_f32() * size_t(nsys), e);
+  d_sysdev = arena.alloc(vk_sysdev_size() * size_t(nsys), e);
   if (!d_sysdev) return ctx.cuda_fail(e, "cudaMalloc sysdev");
-  d_state = arena.alloc(vk_bistate_size_f64() * size_t(nsys), e);
+  d_state = arena.alloc(vk_bistate_size() * size_t(nsys), e);
   if (!d_state) return ctx.cuda_fail(e, "cudaMalloc state");
   d_refdev = arena.alloc(vk_refdev_size() * size_t(nsys), e);
   if (!d_refdev) return ctx.cuda_fail(e, "cudaMalloc refdev");
@@ -534,13 +530,14 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   }
 #undef ALLOC
   cudaStream_t s = ctx.stream;
-  std::vector<char> sd(vk_sysdev_size_f32() * size_t(nsys));
+  std::vector<char> sd(vk_sysdev_size() * size_t(nsys));
   std::vector<char> rd(vk_refdev_size() * size_t(nsys));
   std::vector<char> fd(vk_factdev_size() * size_t(nsys));
   for (int k = 0; k < nsys; ++k) {
     System *S = sys[size_t(k)];
-    S->fill_sysdev(sd.data() + vk_sysdev_size_f32() * size_t(k));
-    RefDev r{S->n, S->d_rp, S->d_ci, S->d_av64, S->d_b64, S->d_x64, S->d_r64};
+    S->fill_sysdev(sd.data() + vk_sysdev_size() * size_t(k));
+    // the final / replacement residual is written into the Krylov r
+    RefDev r{S->n, S->d_rp, S->d_ci, S->d_av64, S->d_b64, (const double *)S->kv[0], (double *)S->kv[1]};
     std::memcpy(rd.data() + vk_refdev_size() * size_t(k), &r, sizeof(r));
     FactDev f{S->n, S->d_prp, S->d_pci, S->d_lu64, S->d_pdiag, S->d_blk};
     std::memcpy(fd.data() + vk_factdev_size() * size_t(k), &f, sizeof(f));
@@ -582,7 +579,7 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
 #undef H2D
   if ((e = cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   if ((e = cudaMemsetAsync(d_err, 0, sizeof(int32_t), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
-  if ((e = cudaMemsetAsync(d_state, 0, vk_bistate_size_f64() * size_t(nsys), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+  if ((e = cudaMemsetAsync(d_state, 0, vk_bistate_size() * size_t(nsys), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   tiles = VkTiles{ntiles, d_tile_sys, d_tile_r0, d_tile_r1, d_sys_tile0};
   if (has_pc) {
     levL = VkLevels{nlevL, d_cptrL, d_csL, d_cqL, d_cnL};
@@ -670,78 +667,47 @@ struct EventProf {
 };
 static thread_local EventProf g_prof;
 
-// BiCGStab on every active system to relative tolerance `tol` (FP64), or with
-// FP32 recurrences and FP64 reliable updates (mixed).  Iteration chunks of
-// `check_every` run without host synchronisation.
-int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, int &iters_out) {
+// BiCGStab (FP64) on every active system to relative tolerance `tol`; the ILU(0) apply runs
+// in the factor precision.  resume = true continues after a residual replacement (r holds
+// b - A x).  Iteration chunks of `check_every` run without host synchronisation.
+int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, bool resume, int &iters_out) {
   cudaStream_t s = ctx.stream;
   const int every = sys[0]->opts.check_every > 0 ? sys[0]->opts.check_every : 8;
   const int mode = (sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) ? 2 : 1;
   const int lvl_grid = mode == 1 ? trsv_grid : std::max(1, num_sms * 8);
-  const size_t bsz = mixed ? vk_bistate_size_f32() : vk_bistate_size_f64();
+  const size_t bsz = vk_bistate_size();
   std::vector<char> stbuf(bsz * size_t(nsys), 0);
   cudaError_t e = cudaMemcpyAsync(stbuf.data(), d_state, stbuf.size(), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return ctx.cuda_fail(e, "read state");
   for (int k = 0; k < nsys; ++k) {
-    if (mixed) {
-      BiState<float> *b = (BiState<float> *)(stbuf.data() + bsz * size_t(k));
-      // stopping is decided on the FP64 residual only; the FP32 early exit on ||s|| is off
-      b->tol = 0.0f; b->max_iter = max_iter; b->done = 0; b->upd = 0; b->iter = 0; b->bad = 0;
-      b->sigma = 1.0; b->sigma_new = 1.0;
-    } else {
-      BiState<double> *b = (BiState<double> *)(stbuf.data() + bsz * size_t(k));
-      b->tol = tol; b->max_iter = max_iter; b->done = 0; b->upd = 0; b->iter = 0;
-    }
+    BiState *b = (BiState *)(stbuf.data() + bsz * size_t(k));
+    b->tol = tol; b->max_iter = max_iter;
+    b->shadow_r0 = sys[size_t(k)]->opts.shadow == VSHE_SHADOW_R0 ? 1 : 0;
+    if (!resume) { b->done = 0; b->iter = 0; }
   }
   if ((e = cudaMemcpyAsync(d_state, stbuf.data(), stbuf.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "write state");
   EventProf &P = g_prof;
   P.on = profile; P.s = s;
-  if (mixed) {
-    // r64 = b - A x64 (x64 = 0 here), r32 = r64 / ||r64||, and the FP32 recurrences start from it
-    vk_reliable_r(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, tol, 1, s);
-  } else {
-    vk_bicg_init_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s);
-  }
+  if (resume) vk_bicg_resume(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s);
+  else vk_bicg_init(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s);
+  auto trsv = [&](int which) -> int {
+    if (!has_pc) { vk_precond_copy(ntiles, d_sysdev, d_state, &tiles, d_active, which, s); return 0; }
+    if (mixed) return vk_trsv_f32(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, which, d_bar, d_err, s);
+    return vk_trsv_f64(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, which, d_bar, d_err, s);
+  };
   int done_iters = 0;
   while (true) {
     for (int it = 0; it < every; ++it) {
       int rc = 0;
       cudaEvent_t a;
-      if (mixed) {
-        float *pf = (float *)d_partials;
-        a = P.begin(); vk_update_p_f32(ntiles, d_sysdev, d_state, &tiles, d_active, s); P.end(2, a);
-        a = P.begin();
-        if (has_pc) rc = vk_trsv_f32(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
-        else vk_precond_copy_f32(ntiles, d_sysdev, d_state, &tiles, d_active, 0, s);
-        P.end(1, a);
-        a = P.begin(); vk_spmv_dot_f32(ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 0, s); P.end(0, a);
-        a = P.begin(); vk_update_s_f32(ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, s); P.end(2, a);
-        a = P.begin();
-        if (has_pc) rc |= vk_trsv_f32(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 1, d_bar, d_err, s);
-        else vk_precond_copy_f32(ntiles, d_sysdev, d_state, &tiles, d_active, 1, s);
-        P.end(1, a);
-        a = P.begin(); vk_spmv_dot_f32(ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 1, s); P.end(0, a);
-        a = P.begin(); vk_update_xr_f32(ntiles, d_sysdev, d_state, &tiles, pf, d_counters, d_active, 1, s); P.end(2, a);
-        a = P.begin();
-        vk_reliable_x(ntiles, d_sysdev, d_state, &tiles, d_active, s);
-        vk_reliable_r(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, tol, 0, s);
-        P.end(3, a);
-      } else {
-        a = P.begin(); vk_update_p_f64(ntiles, d_sysdev, d_state, &tiles, d_active, s); P.end(2, a);
-        a = P.begin();
-        if (has_pc) rc = vk_trsv_f64(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
-        else vk_precond_copy_f64(ntiles, d_sysdev, d_state, &tiles, d_active, 0, s);
-        P.end(1, a);
-        a = P.begin(); vk_spmv_dot_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 0, s); P.end(0, a);
-        a = P.begin(); vk_update_s_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s); P.end(2, a);
-        a = P.begin();
-        if (has_pc) rc |= vk_trsv_f64(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, 1, d_bar, d_err, s);
-        else vk_precond_copy_f64(ntiles, d_sysdev, d_state, &tiles, d_active, 1, s);
-        P.end(1, a);
-        a = P.begin(); vk_spmv_dot_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 1, s); P.end(0, a);
-        a = P.begin(); vk_update_xr_f64(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 0, s); P.end(2, a);
-      }
+      a = P.begin(); vk_update_p(ntiles, d_sysdev, d_state, &tiles, d_active, s); P.end(2, a);
+      a = P.begin(); rc |= trsv(0); P.end(1, a);
+      a = P.begin(); vk_spmv_dot(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 0, s); P.end(0, a);
+      a = P.begin(); vk_update_s(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s); P.end(2, a);
+      a = P.begin(); rc |= trsv(1); P.end(1, a);
+      a = P.begin(); vk_spmv_dot(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 1, s); P.end(0, a);
+      a = P.begin(); vk_update_xr(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s); P.end(2, a);
       if (rc) return ctx.cuda_fail(cudaError_t(rc), "trsv launch");
     }
     done_iters += every;
@@ -751,11 +717,9 @@ int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, int &iters_out) {
     bool all_done = true;
     int maxit = 0;
     for (int k = 0; k < nsys; ++k) {
-      int32_t d, it;
-      if (mixed) { auto *b = (BiState<float> *)(stbuf.data() + bsz * size_t(k)); d = b->done; it = b->iter; }
-      else { auto *b = (BiState<double> *)(stbuf.data() + bsz * size_t(k)); d = b->done; it = b->iter; }
-      if (!d) all_done = false;
-      maxit = std::max(maxit, it);
+      const BiState *b = (const BiState *)(stbuf.data() + bsz * size_t(k));
+      if (!b->done) all_done = false;
+      maxit = std::max(maxit, int(b->iter));
     }
     iters_out = maxit;
     if (all_done || done_iters >= max_iter + 2 * every) break;
@@ -765,26 +729,22 @@ int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, int &iters_out) {
     double t[5] = {0, 0, 0, 0, 0};
     int64_t c[2] = {0, 0};
     P.collect(t, c);
-    t_spmv += t[0]; t_trsv += t[1]; t_vec += t[2]; t_reliable += t[3];
+    t_spmv += t[0]; t_trsv += t[1]; t_vec += t[2];
     n_spmv += c[0]; n_trsv += c[1];
   }
   last_state.assign(stbuf.begin(), stbuf.end());
   return VSHE_OK;
 }
 
-int Batch::state_of(int k, int32_t &status, int32_t &iter, int32_t &nupd, double &res) const {
-  if (last_state.empty()) { status = 0; iter = 0; nupd = 0; res = 0; return 0; }
-  if (mixed) {
-    auto *b = (const BiState<float> *)(last_state.data() + vk_bistate_size_f32() * size_t(k));
-    status = b->status; iter = b->iter; nupd = b->nupd; res = b->res64;
-  } else {
-    auto *b = (const BiState<double> *)(last_state.data() + vk_bistate_size_f64() * size_t(k));
-    status = b->status; iter = b->iter; nupd = 0; res = b->res;
-  }
+int Batch::state_of(int k, int32_t &status, int32_t &iter) const {
+  if (last_state.empty()) { status = 0; iter = 0; return 0; }
+  const BiState *b = (const BiState *)(last_state.data() + vk_bistate_size() * size_t(k));
+  status = b->status; iter = b->iter;
   return 0;
 }
 
-// FP64 residual r = b - A x64 for all members; returns per-system ||r|| / ||b||.
+// FP64 residual r = b - A x for all active members (written into the Krylov r);
+// returns per-system ||r|| / ||b||.
 int Batch::residual(Ctx &ctx, std::vector<double> &rel) {
   cudaStream_t s = ctx.stream;
   vk_residual64(ntiles, d_refdev, &tiles, d_partials, d_counters, d_active, d_rnorm2, d_bnorm2, s);
@@ -799,14 +759,16 @@ int Batch::residual(Ctx &ctx, std::vector<double> &rel) {
 }
 
 int Batch::set_active(Ctx &ctx, const std::vector<int32_t> &act) {
-  cudaError_t e = cudaMemcpyAsync(d_active, act.data(), sizeof(int32_t) * size_t(nsys), cudaMemcpyHostToDevice, ctx.stream);
+  cudaError_t e = cudaMemcpyAsync(d_active, act.data(), sizeof(int32_t) * act.size(), cudaMemcpyHostToDevice, ctx.stream);
   if (e != cudaSuccess) return ctx.cuda_fail(e, "active flags");
   return VSHE_OK;
 }
 
-// Full solve of every member: factorisation, then FP64 BiCGStab or FP32 BiCGStab
-// with FP64 reliable updates, to each member's tolerance.
+// Factor, iterate, then check every system's true FP64 residual; a system whose recursive
+// residual met the tolerance but whose true residual does not is resumed from r = b - A x
+// (at most kMaxReplacements times, within its iteration budget).
 int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
+  constexpr int kMaxReplacements = 3;
   cudaStream_t s = ctx.stream;
   cudaError_t e;
   stats.assign(size_t(nsys), vshe_solve_stats{});
@@ -824,35 +786,46 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
   if (rc) return rc;
   cudaEventRecord(e1, s);
   const vshe_solve_opts &o = sys[0]->opts;
-  for (System *S : sys)
-    if ((e = cudaMemsetAsync(S->d_x64, 0, sizeof(double) * size_t(S->n), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset x");
-  if (!mixed)
-    for (System *S : sys)
-      if ((e = cudaMemcpyAsync(S->kv[1], S->d_b64, sizeof(double) * size_t(S->n), cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "rhs");
   int it = 0;
-  rc = bicgstab(ctx, o.tol, o.max_iters, it);
+  rc = bicgstab(ctx, o.tol, o.max_iters, false, it);
   if (rc) return rc;
-  if (!mixed)
-    for (System *S : sys)
-      if ((e = cudaMemcpyAsync(S->d_x64, S->kv[0], sizeof(double) * size_t(S->n), cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "x");
   std::vector<double> rel;
   if ((rc = residual(ctx, rel))) return rc;  // true FP64 residual of the final x
+  std::vector<int32_t> nrep((size_t)nsys, 0);
+  for (int round = 0; round < kMaxReplacements; ++round) {
+    bool any = false;
+    for (int k = 0; k < nsys; ++k) {
+      int32_t status, iters;
+      state_of(k, status, iters);
+      act[size_t(k)] = (status == 0 && rel[size_t(k)] >= o.tol && iters < o.max_iters) ? 1 : 0;
+      if (act[size_t(k)]) { any = true; nrep[size_t(k)]++; }
+    }
+    if (!any) break;
+    if ((rc = set_active(ctx, act))) return rc;
+    if ((rc = bicgstab(ctx, o.tol, o.max_iters, true, it))) return rc;
+    std::vector<double> rel2;
+    if ((rc = residual(ctx, rel2))) return rc;
+    for (int k = 0; k < nsys; ++k)
+      if (act[size_t(k)]) rel[size_t(k)] = rel2[size_t(k)];
+  }
+  std::fill(act.begin(), act.end(), 1);
+  if ((rc = set_active(ctx, act))) return rc;
   cudaEventRecord(e2, s);
   if ((e = cudaEventSynchronize(e2)) != cudaSuccess) return ctx.cuda_fail(e, "solve");
   float ms_setup = 0, ms_solve = 0;
   cudaEventElapsedTime(&ms_setup, e0, e1);
   cudaEventElapsedTime(&ms_solve, e1, e2);
   if (profile) {
-    ctx.prof[0] = t_spmv; ctx.prof[1] = t_trsv; ctx.prof[2] = t_vec; ctx.prof[3] = t_reliable; ctx.prof[4] = ms_setup;
+    ctx.prof[0] = t_spmv; ctx.prof[1] = t_trsv; ctx.prof[2] = t_vec; ctx.prof[3] = 0.0; ctx.prof[4] = ms_setup;
     ctx.prof_counts[0] = n_spmv; ctx.prof_counts[1] = n_trsv;
   }
   for (int k = 0; k < nsys; ++k) {
     vshe_solve_stats &st = stats[size_t(k)];
     System *S = sys[size_t(k)];
-    int32_t status, iters, nupd; double res;
-    state_of(k, status, iters, nupd, res);
+    int32_t status, iters;
+    state_of(k, status, iters);
     st.iterations = iters;
-    st.refinements = nupd;
+    st.refinements = nrep[size_t(k)];
     st.rel_residual = rel[size_t(k)];
     st.setup_ms = ms_setup;
     st.solve_ms = ms_solve;
@@ -1073,21 +1046,11 @@ int vshe_system_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, const double *
   cudaStream_t s = ctx->stream;
   cudaError_t e;
   const int grid = std::max(1, int(std::min<int64_t>((S->n + 255) / 256, 65535 * 8)));
-  if (precision == 1) {
-    if (!S->mixed) return ctx->fail(VSHE_E_UNSUPPORTED, "FP32 values exist only for mixed-precision systems");
-    std::vector<float> xf((size_t)S->n), yf((size_t)S->n);
-    for (int64_t i = 0; i < S->n; ++i) xf[size_t(i)] = float(x[i]);
-    float *dx = (float *)S->kv[0], *dy = (float *)S->kv[1];
-    if ((e = cudaMemcpyAsync(dx, xf.data(), sizeof(float) * xf.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx->cuda_fail(e, "x");
-    vk_spmv_plain_f32(grid, S->n, S->d_rp, S->d_ci, S->d_av32, dx, dy, s);
-    if ((e = cudaMemcpyAsync(yf.data(), dy, sizeof(float) * yf.size(), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return ctx->cuda_fail(e, "y");
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx->cuda_fail(e, "spmv");
-    for (int64_t i = 0; i < S->n; ++i) y[i] = double(yf[size_t(i)]);
-    return VSHE_OK;
-  }
-  double *dx = S->d_x64, *dy = S->d_r64;
+  if (precision != VSHE_PRECISION_FP64) return ctx->fail(VSHE_E_UNSUPPORTED, "the SpMV runs in FP64 in every solver mode");
+  // scratch: the search-direction vectors (the solution x stays untouched)
+  double *dx = (double *)S->kv[3], *dy = (double *)S->kv[4];
   if ((e = cudaMemcpyAsync(dx, x, sizeof(double) * size_t(S->n), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx->cuda_fail(e, "x");
-  vk_spmv_plain_f64(grid, S->n, S->d_rp, S->d_ci, S->d_av64, dx, dy, s);
+  vk_spmv_plain(grid, S->n, S->d_rp, S->d_ci, S->d_av64, dx, dy, s);
   if ((e = cudaMemcpyAsync(y, dy, sizeof(double) * size_t(S->n), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return ctx->cuda_fail(e, "y");
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx->cuda_fail(e, "spmv");
   return VSHE_OK;
@@ -1100,19 +1063,17 @@ int vshe_system_time_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, int32_t r
   auto it = ctx->systems.find(h);
   if (it == ctx->systems.end()) return ctx->fail(VSHE_E_NOT_FOUND, "");
   System *S = it->second.get();
-  if (precision == 1 && !S->mixed) return ctx->fail(VSHE_E_UNSUPPORTED, "");
+  if (precision != VSHE_PRECISION_FP64) return ctx->fail(VSHE_E_UNSUPPORTED, "the SpMV runs in FP64 in every solver mode");
   cudaStream_t s = ctx->stream;
   const int grid = std::max(1, int(std::min<int64_t>((S->n + 255) / 256, 65535 * 8)));
   cudaEvent_t a, b;
   cudaEventCreate(&a); cudaEventCreate(&b);
   for (int w = 0; w < 3; ++w) {
-    if (precision == 1) vk_spmv_plain_f32(grid, S->n, S->d_rp, S->d_ci, S->d_av32, (float *)S->kv[0], (float *)S->kv[1], s);
-    else vk_spmv_plain_f64(grid, S->n, S->d_rp, S->d_ci, S->d_av64, S->d_x64, S->d_r64, s);
+    vk_spmv_plain(grid, S->n, S->d_rp, S->d_ci, S->d_av64, (const double *)S->kv[3], (double *)S->kv[4], s);
   }
   cudaEventRecord(a, s);
   for (int r = 0; r < reps; ++r) {
-    if (precision == 1) vk_spmv_plain_f32(grid, S->n, S->d_rp, S->d_ci, S->d_av32, (float *)S->kv[0], (float *)S->kv[1], s);
-    else vk_spmv_plain_f64(grid, S->n, S->d_rp, S->d_ci, S->d_av64, S->d_x64, S->d_r64, s);
+    vk_spmv_plain(grid, S->n, S->d_rp, S->d_ci, S->d_av64, (const double *)S->kv[3], (double *)S->kv[4], s);
   }
   cudaEventRecord(b, s);
   cudaError_t e = cudaEventSynchronize(b);

@@ -381,6 +381,7 @@ int vshe_she_info_get(vshe_ctx *ctx, int64_t h, vshe_she_info *info) {
   info->bytes_device = int64_t(S->arena.total + (S->sys ? S->sys->arena.total : 0) + (S->batch ? S->batch->arena.total : 0));
   info->levels_L = S->sys ? S->sys->nlevL : 0;
   info->levels_U = S->sys ? S->sys->nlevU : 0;
+  info->nnz_factor = S->sys ? S->sys->nnzL + S->sys->nnzU : 0;
   return VSHE_OK;
 }
 

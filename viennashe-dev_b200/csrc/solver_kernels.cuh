@@ -5,56 +5,45 @@
 
 namespace vshe {
 
-// One linear system of a batch, as the Krylov kernels see it (all device pointers).
-// T is the arithmetic type of the Krylov iteration (float or double).
+// One linear system of a batch, as the kernels see it (all device pointers).
 //
-// The matrix A is kept in the caller's row order for the SpMV.  The incomplete
-// factors belong to the permuted matrix P A P^T and are stored level by level:
-// entry k of the forward solve is row lrow[k] (permuted numbering) with strict
-// lower entries [lptr[k], lptr[k+1]) of (lcol, lval); entry k of the backward
-// solve is row urow[k] with strict upper entries [uptr[k], uptr[k+1]) and the
-// inverse diagonal udinv[k].  perm[i] is the original row of permuted row i;
-// lgat[k] = perm[lrow[k]] and ugat[k] = perm[urow[k]] (original rows of the entries).
-template <typename T>
+// The Krylov iteration (SpMV, dot products, vector updates) runs in FP64 on A in the
+// caller's row order.  P is the storage and arithmetic type of the ILU(0) triangular
+// solves: float for the mixed-precision solver, double for the plain FP64 solver.
+//
+// The incomplete factors belong to the permuted matrix P A P^T and are stored level by
+// level: entry k of the forward solve is row lrow[k] (permuted numbering) with strict
+// lower entries [lptr[k], lptr[k+1]) of (lcol, lval); entry k of the backward solve is
+// row urow[k] with strict upper entries [uptr[k], uptr[k+1]) and the inverse diagonal
+// udinv[k].  lgat[k] / ugat[k] are the original rows of those entries.
+template <typename P>
 struct SysDev {
   int64_t n;
   const int64_t *rp;
   const int32_t *ci;
-  const T *av;
-  const int32_t *perm;
-  const int32_t *lrow; const int64_t *lptr; const int32_t *lcol; const T *lval;
-  const int32_t *urow; const int64_t *uptr; const int32_t *ucol; const T *uval; const T *udinv;
+  const double *av;
+  const double *b;
+  const int32_t *lrow; const int64_t *lptr; const int32_t *lcol; const P *lval;
+  const int32_t *urow; const int64_t *uptr; const int32_t *ucol; const P *uval; const P *udinv;
   const int32_t *lgat, *ugat;
-  T *ytmp;  // permuted-order work vector of the triangular solves
-  // Krylov vectors (original order)
-  T *x, *r, *rh, *p, *v, *s, *t, *ph, *sh;
-  // FP64 side of the mixed-precision solve (reliable updates)
-  const double *av64;
-  const double *b64;
-  double *x64, *r64;
+  P *ytmp;  // permuted-order work vector of the triangular solves
+  // Krylov vectors (original order, FP64)
+  double *x, *r, *rh, *p, *v, *s, *t, *ph, *sh;
 };
 
 // Per-system BiCGStab state, resident on the device.
-template <typename T>
 struct BiState {
-  T rho, rho_old, alpha, omega;
-  T bnorm;        // ||b|| of the Krylov solve
-  T res;          // ||r|| / ||b|| (recursive residual)
-  T tol;          // relative tolerance
-  int32_t iter;   // iterations done
+  double rho, rho_old, alpha, omega;
+  double bnorm;    // ||b||
+  double res;      // ||r|| / ||b|| (recursive residual)
+  double tol;      // relative tolerance
+  int32_t iter;    // iterations done
   int32_t max_iter;
-  int32_t done;   // 1 = converged or stopped
-  int32_t s_conv; // 1 = ||s|| already below tol in this iteration
-  int32_t status; // 0 ok, VSHE_E_BREAKDOWN, ...
-  int32_t upd;    // reliable update requested (mixed)
-  int32_t restart;// next iteration restarts the Krylov recurrence (p = r)
-  int32_t nupd;   // reliable updates done
-  int32_t bad;    // mixed: the FP32 cycle produced a non-finite value; its x correction is discarded
-  T thresh;       // mixed: ||r32|| below which the next reliable update is taken
-  double res64;   // true FP64 residual ||b - A x64|| / ||b|| after the last reliable update
-  double sigma;   // mixed: scale of the FP32 cycle, r_true = sigma * r32 (||r32|| = 1 at its start)
-  double sigma_new; // mixed: ||b - A x64|| of the reliable update in progress
-  double bnorm64; // ||b|| in FP64
+  int32_t done;    // 1 = converged or stopped
+  int32_t s_conv;  // 1 = ||s|| already below tol in this iteration
+  int32_t status;  // 0 ok, VSHE_E_BREAKDOWN, ...
+  int32_t restart; // next iteration restarts the Krylov recurrence (p = r)
+  int32_t shadow_r0; // 1: r^ = r_0 instead of the dense pseudo-random shadow
 };
 
 // Tiles: contiguous row ranges inside one system.  Reductions are per tile,
@@ -91,11 +80,11 @@ struct FactDev {
   const int32_t *blk;
 };
 
-// FP64 refinement view of one system: r = b - A x.
+// FP64 residual view of one system: r = b - A x.
 struct RefDev {
   int64_t n;
   const int64_t *rp; const int32_t *ci; const double *av;
-  const double *b; double *x; double *r;
+  const double *b; const double *x; double *r;
 };
 
 }  // namespace vshe

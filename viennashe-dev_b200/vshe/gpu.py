@@ -76,7 +76,8 @@ def kernel_launches():
 
 
 def make_opts(precision="mixed", precond="ilu0", tol=1e-10, max_iters=1000, inner_tol=1e-5,
-              max_refinements=10, blocks=None, trsv="auto", check_every=8, ordering="natural", perm=None):
+              max_refinements=10, blocks=None, trsv="auto", check_every=8, ordering="natural", perm=None,
+              shadow="dense"):
     o = SolveOptsC()
     lib().vshe_default_opts(C.byref(o))
     o.precision = PRECISION[precision]
@@ -88,6 +89,7 @@ def make_opts(precision="mixed", precond="ilu0", tol=1e-10, max_iters=1000, inne
     o.trsv_mode = TRSV[trsv]
     o.check_every = check_every
     o.ordering = ORDERING[ordering]
+    o.shadow = {"dense": 0, "r0": 1}[shadow]
     keep = []
     if blocks is not None:
         kb = np.ascontiguousarray(blocks, np.int64)
@@ -237,7 +239,7 @@ class SheInfoC(C.Structure):
         ("nnz_full", C.c_int64), ("nnz_reduced", C.c_int64),
         ("n_cells", C.c_int32), ("n_facets", C.c_int32), ("n_contacts", C.c_int32),
         ("hbar_omega", C.c_double), ("bytes_device", C.c_int64),
-        ("levels_L", C.c_int32), ("levels_U", C.c_int32),
+        ("levels_L", C.c_int32), ("levels_U", C.c_int32), ("nnz_factor", C.c_int64),
     ]
 
 
