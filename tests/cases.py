@@ -38,3 +38,11 @@ def bar_small(L=3, nx=16, ny=6, n_energies=40, bias=0.1):
 
 def oracle_problem(dev, cfg):
     return O.OracleProblem(dev, cfg, O.golden_coupling(cfg.max_expansion_order))
+
+
+def current_scale(dens_ref, cur_ref):
+    """Scale for comparing terminal currents: the larger of the largest current and the
+    one-way thermal flux q * n_max * 1e5 m/s of the densest cell.  Near equilibrium the net
+    current is a cancellation of one-way fluxes, so its error scales with the flux, not with
+    the (vanishing) net current."""
+    return max(float(np.max(np.abs(cur_ref))) if len(cur_ref) else 0.0, 1.602176634e-19 * float(np.max(dens_ref)) * 1e5)

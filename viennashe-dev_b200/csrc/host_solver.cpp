@@ -375,7 +375,7 @@ int System::setup_pattern(Ctx &ctx) {
     ALLOCT(d_lval, std::max<int64_t>(nnzL, 1));
     ALLOCT(d_uval, std::max<int64_t>(nnzU, 1));
     ALLOCT(d_udinv, n);
-    ALLOCT(d_ytmp, n);
+    ALLOC(d_ytmp, double, n);
     if (!identity_perm) { ALLOC(d_perm, int32_t, n); }
   }
 #undef ALLOC
@@ -421,7 +421,7 @@ void System::fill_sysdev(void *out) const {
   d.lrow = d_lrow; d.lptr = d_lptr; d.lcol = d_lcol; d.lval = (const float *)d_lval;
   d.urow = d_urow; d.uptr = d_uptr; d.ucol = d_ucol; d.uval = (const float *)d_uval; d.udinv = (const float *)d_udinv;
   d.lgat = d_lgat; d.ugat = d_ugat;
-  d.ytmp = (float *)d_ytmp;
+  d.ytmp = (double *)d_ytmp;
   d.x = (double *)kv[0]; d.r = (double *)kv[1]; d.rh = (double *)kv[2]; d.p = (double *)kv[3];
   d.v = (double *)kv[4]; d.s = (double *)kv[5]; d.t = (double *)kv[6]; d.ph = (double *)kv[7]; d.sh = (double *)kv[8];
   std::memcpy(out, &d, sizeof(d));

@@ -17,9 +17,12 @@
 // BiCGStab follows van der Vorst (1992), right-preconditioned, in FP64.  The shadow residual
 // r^ is a fixed dense pseudo-random vector rather than r_0: the SHE right-hand side lives on
 // the few contact rows only, and with r^ = r_0 the inner products (r^, r_k) collapse to
-// rounding noise.  Mixed precision stores the ILU(0) factors in FP32 and runs the triangular
-// solves in FP32; SpMV, dot products and vector updates stay FP64 (FP32 Krylov vectors or an
-// FP32 copy of A cost these ill-conditioned systems 1.7-2.5x the iterations or diverge).
+// rounding noise.  Mixed precision stores the ILU(0) factors in FP32 and reads them into FP64
+// triangular solves; SpMV, dot products and vector updates stay FP64.  A fixed FP32 rounding
+// of the factors is just another (linear) preconditioner of the same quality, while FP32
+// arithmetic in the solves or FP32 Krylov vectors turn the preconditioner into a noisy one
+// that BiCGStab's short recurrences do not tolerate: on the 2D bar they cost 2-6x the
+// iterations or break down.
 
 #include <cuda_runtime.h>
 #include <atomic>
@@ -113,8 +116,8 @@ __device__ bool tile_finish(double (&v)[NV], int tile, int sys, const Tiles &tl,
 // warp's shared-memory slice sm[32 * U] and every lane sums its own row in index order, so the
 // result does not depend on the launch shape.  CG: read x through L2 only (x is written by
 // other CTAs of the same launch).
-template <typename T, int U, bool CG>
-__device__ __forceinline__ T chunk_rowsums(const int64_t *__restrict__ ptr, const int32_t *__restrict__ col, const T *__restrict__ val,
+template <typename V, typename T, int U, bool CG>
+__device__ __forceinline__ T chunk_rowsums(const int64_t *__restrict__ ptr, const int32_t *__restrict__ col, const V *__restrict__ val,
                                            const T *x, int64_t q0, int nr, T *sm) {
   const int lane = threadIdx.x & 31;
   int64_t b = 0, e = 0;
@@ -129,7 +132,7 @@ __device__ __forceinline__ T chunk_rowsums(const int64_t *__restrict__ ptr, cons
     for (int u = 0; u < U; ++u) {
       const int64_t k = pb + u * 32 + lane;
       c[u] = 0; a[u] = T(0);
-      if (k < ke) { c[u] = col[k]; a[u] = val[k]; }
+      if (k < ke) { c[u] = col[k]; a[u] = (T)val[k]; }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -238,7 +241,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_spmv_dot(const SysK *sys, BiSta
   double acc[2] = {0.0, 0.0};
   for (int64_t q0 = r0 + 32 * w; q0 < r1; q0 += 32 * kWarps) {
     const int nr = (int)(r1 - q0 < 32 ? r1 - q0 : 32);
-    const double y = chunk_rowsums<double, kSpmvU, false>(S.rp, S.ci, S.av, xin, q0, nr, sm[w]);
+    const double y = chunk_rowsums<double, double, kSpmvU, false>(S.rp, S.ci, S.av, xin, q0, nr, sm[w]);
     if (lane < nr) {
       const int64_t row = q0 + lane;
       yout[row] = y;
@@ -379,14 +382,14 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
 }
 
 // ------------------------------------------------- triangular solves (ILU apply)
-// out = P^T U^{-1} L^{-1} P in over the level-ordered factors, in precision P (in and out
-// are FP64).  which 0: ph = M^{-1} p, 1: sh = M^{-1} s.  A level is a list of chunks
+// out = P^T U^{-1} L^{-1} P in over the level-ordered factors stored in precision P; the
+// arithmetic and the work vector ytmp are FP64 in both modes (in and out are FP64).  which 0: ph = M^{-1} p, 1: sh = M^{-1} s.  A level is a list of chunks
 // (system, first level-ordered position, row count <= 32); the warps of the grid take its
 // chunks in turn.  ytmp (permuted order) is written by other CTAs of the same launch and
 // read through L2 only.
 template <typename P>
 __device__ __forceinline__ void trsv_level_rows(const SysDev<P> *sys, const BiState *st, const int32_t *active, const Levels lv, int k,
-                                                bool lower, int which, P *sm) {
+                                                bool lower, int which, double *sm) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
@@ -398,21 +401,21 @@ __device__ __forceinline__ void trsv_level_rows(const SysDev<P> *sys, const BiSt
     const int64_t q0 = lv.ent_row[c];
     const int nr = lv.ent_cnt[c];
     if (lower) {
-      const P sum = chunk_rowsums<P, kTrsvU, true>(S.lptr, S.lcol, S.lval, S.ytmp, q0, nr, sm);
+      const double sum = chunk_rowsums<P, double, kTrsvU, true>(S.lptr, S.lcol, S.lval, S.ytmp, q0, nr, sm);
       if (lane < nr) {
         const int64_t q = q0 + lane;
         const double *in = which == 0 ? S.p : S.s;
-        S.ytmp[S.lrow[q]] = (P)in[S.lgat[q]] - sum;
+        S.ytmp[S.lrow[q]] = in[S.lgat[q]] - sum;
       }
     } else {
-      const P sum = chunk_rowsums<P, kTrsvU, true>(S.uptr, S.ucol, S.uval, S.ytmp, q0, nr, sm);
+      const double sum = chunk_rowsums<P, double, kTrsvU, true>(S.uptr, S.ucol, S.uval, S.ytmp, q0, nr, sm);
       if (lane < nr) {
         const int64_t q = q0 + lane;
         const int32_t row = S.urow[q];
-        const P y = (__ldcg(&S.ytmp[row]) - sum) * S.udinv[q];
+        const double y = (__ldcg(&S.ytmp[row]) - sum) * (double)S.udinv[q];
         S.ytmp[row] = y;
         double *out = which == 0 ? S.ph : S.sh;
-        out[S.ugat[q]] = (double)y;
+        out[S.ugat[q]] = y;
       }
     }
   }
@@ -420,8 +423,8 @@ __device__ __forceinline__ void trsv_level_rows(const SysDev<P> *sys, const BiSt
 
 template <typename P>
 __global__ void __launch_bounds__(kThreads) k_trsv_persistent(const SysDev<P> *sys, const BiState *st, const int32_t *active, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err) {
-  __shared__ P sm[kWarps][32 * kTrsvU];
-  P *my = sm[threadIdx.x >> 5];
+  __shared__ double sm[kWarps][32 * kTrsvU];
+  double *my = sm[threadIdx.x >> 5];
   for (int k = 0; k < lL.nlev; ++k) {
     trsv_level_rows<P>(sys, st, active, lL, k, true, which, my);
     if (!grid_barrier(bar, err)) return;
@@ -434,7 +437,7 @@ __global__ void __launch_bounds__(kThreads) k_trsv_persistent(const SysDev<P> *s
 
 template <typename P>
 __global__ void __launch_bounds__(kThreads) k_trsv_level(const SysDev<P> *sys, const BiState *st, const int32_t *active, Levels lv, int k, int lower, int which) {
-  __shared__ P sm[kWarps][32 * kTrsvU];
+  __shared__ double sm[kWarps][32 * kTrsvU];
   trsv_level_rows<P>(sys, st, active, lv, k, lower != 0, which, sm[threadIdx.x >> 5]);
 }
 
@@ -531,7 +534,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_residual64(const RefDev *sys, T
   double acc[2] = {0.0, 0.0};
   for (int64_t q0 = r0 + 32 * w; q0 < r1; q0 += 32 * kWarps) {
     const int nr = (int)(r1 - q0 < 32 ? r1 - q0 : 32);
-    const double ax = chunk_rowsums<double, kSpmvU, false>(S.rp, S.ci, S.av, S.x, q0, nr, sm[w]);
+    const double ax = chunk_rowsums<double, double, kSpmvU, false>(S.rp, S.ci, S.av, S.x, q0, nr, sm[w]);
     if (lane < nr) {
       const int64_t row = q0 + lane;
       const double bb = S.b[row];
@@ -555,7 +558,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_spmv_plain(int64_t n, const int
   const int64_t gw = (int64_t)blockIdx.x * kWarps + w, nw = (int64_t)gridDim.x * kWarps;
   for (int64_t q0 = 32 * gw; q0 < n; q0 += 32 * nw) {
     const int nr = (int)(n - q0 < 32 ? n - q0 : 32);
-    const double v = chunk_rowsums<double, kSpmvU, false>(rp, ci, av, x, q0, nr, sm[w]);
+    const double v = chunk_rowsums<double, double, kSpmvU, false>(rp, ci, av, x, q0, nr, sm[w]);
     if (lane < nr) y[q0 + lane] = v;
   }
 }

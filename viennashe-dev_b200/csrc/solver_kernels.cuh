@@ -1,5 +1,19 @@
 // solver_kernels.cuh -- device-side data layout shared by the solver kernels
 // (solver_kernels.cu) and the C++ host driver (host_solver.cpp).
+//
+// Solver order.  Every system is solved in its own row order q = 0..n-1, a symmetric
+// permutation of the caller's rows (perm[q] = caller row): the preconditioner's base
+// ordering (natural, multicolour or caller-given), then stably sorted by the level of the
+// forward (L) sweep, then, inside a level, by row length.  Rows of one forward level are
+// therefore contiguous, and because a level never holds two structurally coupled rows, the
+// ILU(0) factors in solver order are those of the base ordering, relabelled.  The Krylov
+// vectors live in solver order; b is gathered in and x scattered out once per solve.
+//
+// SELL-32.  A (in solver order) and the incomplete factors L, U are stored as slices of 32
+// rows: entry k of the slice's row `lane` is at off + 32 k + lane, for k below the slice's
+// width (the longest row of the slice; shorter rows are padded with value 0 and a column
+// that points at a finite entry).  Lane = row, so every value and column load of a warp is
+// one coalesced 128/256-byte line and each row is summed by one thread in index order.
 #pragma once
 #include <cstdint>
 
@@ -7,27 +21,24 @@ namespace vshe {
 
 // One linear system of a batch, as the kernels see it (all device pointers).
 //
-// The Krylov iteration (SpMV, dot products, vector updates) runs in FP64 on A in the
-// caller's row order.  P is the storage and arithmetic type of the ILU(0) triangular
-// solves: float for the mixed-precision solver, double for the plain FP64 solver.
+// The Krylov iteration (SpMV, dot products, vector updates) runs in FP64.  P is the storage
+// type of the ILU(0) factors: float for the mixed-precision solver, double for the plain
+// FP64 solver; the triangular solves compute in FP64 either way.
 //
-// The incomplete factors belong to the permuted matrix P A P^T and are stored level by
-// level: entry k of the forward solve is row lrow[k] (permuted numbering) with strict
-// lower entries [lptr[k], lptr[k+1]) of (lcol, lval); entry k of the backward solve is
-// row urow[k] with strict upper entries [uptr[k], uptr[k+1]) and the inverse diagonal
-// udinv[k].  lgat[k] / ugat[k] are the original rows of those entries.
+// A: slices j = rows [32 j, 32 j + 32), entries [aoff[j], aoff[j+1]).
+// L: slices in forward-level order; slice j = solver rows [lrow0[j], lrow0[j+1]),
+//    entries [loff[j], loff[j+1]) (strict lower part inside the row's block; unit diagonal).
+// U: slices in backward-level order over slots; slice j = slots [uslot0[j], uslot0[j+1]),
+//    slot t is solver row urow[t] with inverse diagonal udinv[t]; entries [uoff[j], uoff[j+1]).
 template <typename P>
 struct SysDev {
   int64_t n;
-  const int64_t *rp;
-  const int32_t *ci;
-  const double *av;
-  const double *b;
-  const int32_t *lrow; const int64_t *lptr; const int32_t *lcol; const P *lval;
-  const int32_t *urow; const int64_t *uptr; const int32_t *ucol; const P *uval; const P *udinv;
-  const int32_t *lgat, *ugat;
-  P *ytmp;  // permuted-order work vector of the triangular solves
-  // Krylov vectors (original order, FP64)
+  const int64_t *aoff; const int32_t *acol; const double *aval;
+  const double *b;   // rhs, solver order
+  const int32_t *lrow0; const int64_t *loff; const int32_t *lcol; const P *lval;
+  const int32_t *uslot0; const int64_t *uoff; const int32_t *ucol; const P *uval; const P *udinv; const int32_t *urow;
+  double *ytmp;      // forward-sweep result (FP64)
+  // Krylov vectors (solver order, FP64)
   double *x, *r, *rh, *p, *v, *s, *t, *ph, *sh;
 };
 
@@ -46,8 +57,8 @@ struct BiState {
   int32_t shadow_r0; // 1: r^ = r_0 instead of the dense pseudo-random shadow
 };
 
-// Tiles: contiguous row ranges inside one system.  Reductions are per tile,
-// finished by the last tile of the system (sys_tile0[s] .. sys_tile0[s+1]).
+// Tiles: contiguous row ranges of 2048 rows (64 A-slices) inside one system.  Reductions are
+// per tile, finished by the last tile of the system (sys_tile0[s] .. sys_tile0[s+1]).
 struct Tiles {
   int32_t ntiles;
   const int32_t *tile_sys;
@@ -57,20 +68,19 @@ struct Tiles {
 };
 
 // Level schedule of a batch: entries of global level k are [lvl_ptr[k], lvl_ptr[k+1]).
-// Triangular solves: entry e is a chunk of ent_cnt[e] <= 32 consecutive level-ordered
-// positions of system ent_sys[e] starting at ent_row[e].  Factorisation: entry e is the
-// permuted row ent_row[e] of system ent_sys[e] (ent_sys NULL for a single system, ent_cnt NULL).
+// Triangular solves: entry e is slice ent_row[e] (of L or U) of system ent_sys[e].
+// Factorisation: entry e is the solver row ent_row[e] of system ent_sys[e]; for a single
+// system both are NULL and entry e is row e (forward levels are contiguous row ranges).
 struct Levels {
   int32_t nlev;
   const int64_t *lvl_ptr;
   const int32_t *ent_sys;
   const int32_t *ent_row;
-  const int32_t *ent_cnt;
+  const int32_t *ent_cnt;  // unused (NULL)
 };
 
-// ILU(0) factorisation view of one system: values in FP64 in the permuted
-// matrix's CSR (prp, pci), filled from A's values through amap (permuted entry
-// -> original entry); diag[i] = position of the diagonal in row i.
+// ILU(0) factorisation view of one system: values in FP64 in the solver-order CSR (rp, ci),
+// diag[i] = position of the diagonal in row i; blk[i] = preconditioner block of row i.
 struct FactDev {
   int64_t n;
   const int64_t *rp;
@@ -80,10 +90,10 @@ struct FactDev {
   const int32_t *blk;
 };
 
-// FP64 residual view of one system: r = b - A x.
+// FP64 residual view of one system (solver order): r = b - A x.
 struct RefDev {
   int64_t n;
-  const int64_t *rp; const int32_t *ci; const double *av;
+  const int64_t *aoff; const int32_t *acol; const double *aval;
   const double *b; const double *x; double *r;
 };
 
