@@ -10,7 +10,7 @@ A step is one full pass of the hot path on the device: assembly of the streaming
 scattering operators, odd elimination, scaling and normalisation, block-ILU(0) per energy slab
 (node 4-colour order) and BiCGStab to an FP64 relative residual of 1e-10, then odd recovery,
 full-system residual, density and terminal currents.  `value` is solves/s of that pass in the
-mixed-precision mode (FP64 Krylov, FP32 ILU factors and triangular solves) with the device
+mixed-precision mode (FP64 Krylov, FP32-stored ILU factors read into FP64 triangular solves) with the device
 description resident in HBM; `fp64_solves_per_s` is the same pass with the plain FP64 solver.
 `e2e` is solves/s through the drop-in C ABI (vshe_system_set_values + vshe_system_solve +
 download of x) with host buffers, the way a ViennaSHE Gummel loop calls solvers::solve for a
@@ -300,9 +300,10 @@ def run_ours(args, D_):
     peaks = measured_peaks()
     hbm = peaks["hbm_gbs"] if peaks else 6650.0
     peak_src = "measured" if peaks else "fallback"
-    # algorithmic bytes per launch
-    spmv_bytes = 12 * nnz + 32 * n           # A (FP64 + int32 col), row_ptr, x, y, fused-dot vector
-    trsv_bytes = 8 * nnz_lu + n * (48 + 16)  # FP32 factors + int32 cols, ptr/row/gather maps, in/out FP64, ytmp/udinv FP32
+    # algorithmic bytes per launch (SELL-32 in solver order; padding and the gathers of x at the
+    # column indices are not counted: x is read once under ideal caching)
+    spmv_bytes = 12 * nnz + 24 * n           # A (FP64 value + int32 column), x, y, the fused-dot vector
+    trsv_bytes = 8 * nnz_lu + 40 * n         # FP32 factor value + int32 column; in, ytmp (write, read), out (FP64), urow, udinv
     kern = {
         "spmv": {"ms_total": prof["spmv_ms"], "launches": prof["spmv_launches"]},
         "trsv": {"ms_total": prof["trsv_ms"], "launches": prof["trsv_launches"]},
@@ -313,11 +314,11 @@ def run_ours(args, D_):
     if dominant == "trsv":
         avg_ms = prof["trsv_ms"] / max(prof["trsv_launches"], 1)
         dbytes = trsv_bytes
-        kname = "k_trsv_persistent<float> (ILU(0) apply, L then U sweeps)"
+        kname = "k_trsv_persistent<float> (ILU(0) apply, forward then backward SELL-32 sweeps)"
     else:
         avg_ms = prof["spmv_ms"] / max(prof["spmv_launches"], 1)
         dbytes = spmv_bytes
-        kname = "k_spmv_dot (CSR SpMV FP64 + fused dots)"
+        kname = "k_spmv_dot (SELL-32 SpMV FP64 + fused dots)"
     achieved = dbytes / (avg_ms / 1000.0) / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
@@ -340,11 +341,11 @@ def run_ours(args, D_):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D_.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * tmax / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64 Krylov / f32 ILU apply", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 Krylov / f32-stored ILU factors", "data": "synthetic",
             "config": {"workload": workload_name(args), "n_unknowns_reduced": n, "nnz_reduced": nnz, "nnz_factor": nnz_lu,
                        "n_unknowns_full": int(info["n_even"] + info["n_odd"]), "nnz_full": int(info["nnz_full"]),
                        "n_energies": int(info["n_energies"]), "preconditioner": "block-ILU(0) per energy slab, node 4-colour order",
-                       "l2": "inputs larger than L2 (reduced CSR %.2f GB)" % (nnz * 12 / 1e9),
+                       "l2": "inputs larger than L2 (reduced system %.2f GB)" % (nnz * 12 / 1e9),
                        "parallelism": "replicas" if D_.world > 1 else "single"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "fp64_solves_per_s": fp64_value, "mixed_over_fp64": (value / max(D_.world, 1)) / fp64_value,

@@ -45,8 +45,9 @@ extern "C" {
 
 /* ---- solver options ---- */
 #define VSHE_PRECISION_FP64   0   /* FP64 BiCGStab, FP64 ILU(0) factors and triangular solves */
-#define VSHE_PRECISION_MIXED  1   /* FP64 BiCGStab (SpMV, dots, updates), ILU(0) factors stored and
-                                     applied in FP32; convergence on the true FP64 residual */
+#define VSHE_PRECISION_MIXED  1   /* FP64 BiCGStab (SpMV, dots, updates), ILU(0) factors stored in
+                                     FP32 and read into FP64 triangular solves; convergence on the
+                                     true FP64 residual */
 
 #define VSHE_PRECOND_NONE        0
 #define VSHE_PRECOND_ILU0        1   /* ILU(0) on the whole system (serial_linear_solver's choice) */
@@ -152,6 +153,26 @@ int vshe_system_factor_values(vshe_ctx *ctx, int64_t handle, double *lu);
 /* Device-timed kernel throughput on a resident system: runs `reps` SpMVs in the
  * given precision (FP64 only) and returns the mean time per SpMV (ms) from CUDA events. */
 int vshe_system_time_spmv(vshe_ctx *ctx, int64_t handle, int32_t precision, int32_t reps, double *ms);
+
+/* ---- host-only layout inspection (no GPU needed) ----
+ * The solver order and the SELL-32 tables a resident system built from (A, opts) uses, for
+ * tests of the ordering and layout logic.  No reference counterpart: the reference's
+ * ViennaCL solvers keep the caller's CSR.  The solver order q = 0..n-1 lists the caller's rows
+ * (perm[q]) sorted by forward-sweep level; forward level k is rows [lvr[k], lvr[k+1]).  A
+ * SELL-32 slice j spans slots [off[j], off[j+1]) = 32 x width; entry k of the slice's row
+ * `lane` sits in slot off[j] + 32 k + lane.  Columns are solver-order rows; padding slots point
+ * at column n and map to entry -1.  vshe_layout_sizes fills sizes[0..9] = slices_A, slots_A,
+ * slices_L, slots_L, slices_U, slots_U, levels_L, levels_U, nnz_L, nnz_U.  vshe_layout_export
+ * fills caller arrays of those sizes (any pointer may be NULL): perm[n], lvr[levels_L + 1],
+ * aoff[slices_A + 1], acol / amap_a[slots_A] (caller entry index of each slot), lrow0 /
+ * loff[slices_L + 1] (first solver row / slot offset of each L slice, plus the end), lcol /
+ * lmap[slots_L], uslot0 / uoff[slices_U + 1], ucol / umap[slots_U], urow[n] (solver row of each
+ * backward-sweep slot). */
+int vshe_layout_sizes(int64_t n, int64_t nnz, const int64_t *row_ptr, const int32_t *col, const vshe_solve_opts *opts, int64_t *sizes);
+int vshe_layout_export(int64_t n, int64_t nnz, const int64_t *row_ptr, const int32_t *col, const vshe_solve_opts *opts,
+                       int32_t *perm, int64_t *lvr, int64_t *aoff, int32_t *acol, int64_t *amap_a,
+                       int32_t *lrow0, int64_t *loff, int32_t *lcol, int64_t *lmap,
+                       int32_t *uslot0, int64_t *uoff, int32_t *ucol, int64_t *umap, int32_t *urow);
 
 /* ---- SHE path on the device: she::assemble + she::solve (secondary boundary) ----
  * vshe_she_create runs the host setup of the (x, H) space (energies, expansion

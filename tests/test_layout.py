@@ -1,0 +1,172 @@
+"""Host logic of the solver layout (no GPU): the level-sorted solver order and the SELL-32
+tables of A, L and U that the CUDA kernels read (vshe_layout_export).
+
+The kernels' arithmetic is replayed here in numpy exactly as the device runs it: the SELL-32
+SpMV, and the forward / backward sweeps level by level, where every row not yet computed holds
+NaN, so a row scheduled before one it depends on shows up as NaN.  The results must match the
+oracle's CSR SpMV and ILU(0) apply (1e-13 relative, summation order differs).
+"""
+import numpy as np
+import pytest
+
+from vshe import gpu
+import oracle_api as O
+import cases
+
+
+def _problems():
+    return [("diode_L1", *cases.diode_small(L=1, boxes=40)),
+            ("diode_L3", *cases.diode_small(L=3, boxes=30)),
+            ("bar_L3", *cases.bar_small(L=3, nx=12, ny=5, n_energies=30))]
+
+
+PROBLEMS = _problems()
+
+
+@pytest.fixture(scope="module", params=PROBLEMS, ids=[p[0] for p in PROBLEMS])
+def prob(request):
+    name, dev, cfg = request.param
+    P = cases.oracle_problem(dev, cfg)
+    return name, P, P.matrix(3)
+
+
+def sell_spmv(Lt, aval, x_p):
+    """y = A x over the SELL-32 slices (x_p in solver order, with the zero entry n)."""
+    n = Lt["n"]
+    xz = np.append(x_p, 0.0)
+    y = np.zeros(n)
+    aoff = Lt["aoff"]
+    for j in range(len(aoff) - 1):
+        w = (aoff[j + 1] - aoff[j]) // 32
+        slots = aoff[j] + 32 * np.arange(w)[:, None] + np.arange(32)[None, :]
+        part = (aval[slots] * xz[Lt["acol"][slots]]).sum(axis=0)
+        rows = 32 * j + np.arange(32)
+        m = rows < n
+        y[rows[m]] = part[m]
+    return y
+
+
+def sell_ilu_apply(Lt, lval, uval, udinv, b_p):
+    """U^{-1} L^{-1} b over the SELL-32 factor slices, forward then backward levels; rows
+    not computed yet hold NaN."""
+    n = Lt["n"]
+    y = np.full(n + 1, np.nan)
+    y[n] = 0.0
+    lrow0, loff = Lt["lrow0"], Lt["loff"]
+    for j in range(len(loff) - 1):  # slices are stored level by level
+        w = (loff[j + 1] - loff[j]) // 32
+        slots = loff[j] + 32 * np.arange(w)[:, None] + np.arange(32)[None, :]
+        cols = Lt["lcol"][slots]
+        nr = lrow0[j + 1] - lrow0[j]
+        v = lval[slots][:, :nr]
+        c = cols[:, :nr]
+        s = (v * np.where(v != 0.0, y[c], 0.0)).sum(axis=0) if w else np.zeros(nr)
+        # padded slots carry value 0 and point at the zero entry n
+        assert np.all(c[v == 0.0] == n) or np.all(v[c == n] == 0.0)
+        y[lrow0[j]:lrow0[j] + nr] = b_p[lrow0[j]:lrow0[j] + nr] - s
+    out = np.full(n + 1, np.nan)
+    out[n] = 0.0
+    us, uoff, urow = Lt["uslot0"], Lt["uoff"], Lt["urow"]
+    for j in range(len(uoff) - 1):
+        w = (uoff[j + 1] - uoff[j]) // 32
+        slots = uoff[j] + 32 * np.arange(w)[:, None] + np.arange(32)[None, :]
+        nr = us[j + 1] - us[j]
+        v = uval[slots][:, :nr]
+        c = Lt["ucol"][slots][:, :nr]
+        s = (v * np.where(v != 0.0, out[c], 0.0)).sum(axis=0) if w else np.zeros(nr)
+        t = np.arange(us[j], us[j] + nr)
+        rows = urow[t]
+        out[rows] = (y[rows] - s) * udinv[t]
+    return out[:n]
+
+
+def _diag_entries(A):
+    d = np.zeros(A.n, np.int64)
+    for i in range(A.n):
+        k = np.searchsorted(A.ci[A.rp[i]:A.rp[i + 1]], i)
+        d[i] = A.rp[i] + k
+    return d
+
+
+def _factor_slots(Lt, lu, A):
+    lval = np.where(Lt["lmap"] >= 0, lu[np.maximum(Lt["lmap"], 0)], 0.0)
+    uval = np.where(Lt["umap"] >= 0, lu[np.maximum(Lt["umap"], 0)], 0.0)
+    diag = _diag_entries(A)
+    udinv = 1.0 / lu[diag[Lt["perm"][Lt["urow"]]]]
+    return lval, uval, udinv
+
+
+def test_solver_order_is_a_level_sorted_permutation(prob):
+    name, P, A = prob
+    Lt = gpu.layout(A.rp, A.ci, precond="ilu0")
+    perm = Lt["perm"]
+    assert np.array_equal(np.sort(perm), np.arange(A.n))
+    assert Lt["lvr"][0] == 0 and Lt["lvr"][-1] == A.n and np.all(np.diff(Lt["lvr"]) > 0)
+    # every stored slot maps to a distinct entry of A; together they cover A exactly once
+    amap = Lt["amap"][Lt["amap"] >= 0]
+    assert np.array_equal(np.sort(amap), np.arange(A.nnz))
+    # widths: SELL slices hold whole 32-lane columns
+    assert np.all(np.diff(Lt["aoff"]) % 32 == 0)
+
+
+@pytest.mark.parametrize("ordering", ["natural", "multicolor"])
+def test_sell_spmv_matches_csr(prob, ordering):
+    name, P, A = prob
+    Lt = gpu.layout(A.rp, A.ci, precond="ilu0", ordering=ordering)
+    perm = Lt["perm"]
+    aval = np.where(Lt["amap"] >= 0, A.v[np.maximum(Lt["amap"], 0)], 0.0)
+    x = np.random.default_rng(3).standard_normal(A.n)
+    y_p = sell_spmv(Lt, aval, x[perm])
+    y = np.empty(A.n)
+    y[perm] = y_p
+    y_ref = O.spmv(A, x)
+    assert np.max(np.abs(y - y_ref)) <= 1e-13 * np.max(np.abs(y_ref))
+
+
+@pytest.mark.parametrize("block", [False, True])
+def test_sell_ilu0_apply_matches_oracle(prob, block):
+    """Natural base order: the level-sorted factors are the reference order's ILU(0), relabelled."""
+    name, P, A = prob
+    bl = P.blocks() if block else None
+    Lt = gpu.layout(A.rp, A.ci, precond="block_ilu0" if block else "ilu0", blocks=bl)
+    lu = O.ilu0_values(A, blocks=bl)
+    lval, uval, udinv = _factor_slots(Lt, lu, A)
+    b = np.random.default_rng(5).standard_normal(A.n)
+    perm = Lt["perm"]
+    z_p = sell_ilu_apply(Lt, lval, uval, udinv, b[perm])
+    assert np.all(np.isfinite(z_p)), "a row was scheduled before a row it depends on"
+    z = np.empty(A.n)
+    z[perm] = z_p
+    z_ref = O.ilu0_apply(A, lu, b, blocks=bl)
+    assert np.max(np.abs(z - z_ref)) <= 1e-11 * np.max(np.abs(z_ref))
+
+
+def test_sell_ilu0_apply_multicolour(prob):
+    """Multicolour base order: the sweeps over the SELL tables reproduce the oracle's ILU(0) of
+    the solver-order matrix."""
+    name, P, A = prob
+    Lt = gpu.layout(A.rp, A.ci, precond="ilu0", ordering="multicolor")
+    perm = Lt["perm"]
+    inv = np.empty(A.n, np.int64)
+    inv[perm] = np.arange(A.n)
+    # solver-order CSR and the map of its entries back to A's
+    rows, cols, src = [], [], []
+    for q in range(A.n):
+        o = perm[q]
+        ks = np.arange(A.rp[o], A.rp[o + 1])
+        c = inv[A.ci[ks]]
+        order = np.argsort(c)
+        rows.append(np.full(len(ks), q)); cols.append(c[order]); src.append(ks[order])
+    cols = np.concatenate(cols); src = np.concatenate(src)
+    rp = np.zeros(A.n + 1, np.int64)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    Ap = O.CSR(rp, cols.astype(np.int32), A.v[src])
+    lup = O.ilu0_values(Ap)
+    lu = np.empty(A.nnz)
+    lu[src] = lup
+    lval, uval, udinv = _factor_slots(Lt, lu, A)
+    b = np.random.default_rng(7).standard_normal(A.n)
+    z_p = sell_ilu_apply(Lt, lval, uval, udinv, b[perm])
+    assert np.all(np.isfinite(z_p)), "a row was scheduled before a row it depends on"
+    z_ref = O.ilu0_apply(Ap, lup, b[perm])
+    assert np.max(np.abs(z_p - z_ref)) <= 1e-11 * np.max(np.abs(z_ref))

@@ -28,43 +28,63 @@ struct DevArena {
 
 struct Ctx;
 
-// One resident linear system.  A stays in the caller's order for the SpMV; the
-// incomplete factors belong to P A P^T (P from opts.perm or the ordering) and
-// are stored level by level for the triangular solves.
+// Host-side solver layout of one system (no CUDA): the solver order, the solver-order CSR used
+// by the factorisation, and the SELL-32 tables of A, L and U (solver_kernels.cuh).
+struct Layout {
+  std::vector<int32_t> perm, blk;
+  std::vector<int64_t> lvr, lvsL, lvsU;
+  int32_t nlevL = 0, nlevU = 0;
+  int64_t nslA = 0, nslL = 0, nslU = 0, padA = 0, padL = 0, padU = 0, nnzL = 0, nnzU = 0;
+  std::vector<int64_t> prp, pdiag, amap;
+  std::vector<int32_t> pci;
+  std::vector<int64_t> aoff, astart, amapS;
+  std::vector<int32_t> acol;
+  std::vector<int64_t> fmap, dpos, loff, uoff, lstart, ustart;
+  std::vector<int32_t> lcol, ucol, urow;
+  int build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci,
+            const vshe_solve_opts &opts, std::string &err);
+};
+
+// One resident linear system.  The caller's CSR (and rhs) stay in the caller's order; the
+// solver works in a level-sorted solver order (perm[q] = caller row of solver row q) on
+// SELL-32 copies of A and of the incomplete factors (solver_kernels.cuh).
 struct System {
   int64_t n = 0, nnz = 0;
   vshe_solve_opts opts{};
-  bool mixed = true;     // FP32 ILU(0) factors and triangular solves (Krylov in FP64 either way)
+  bool mixed = true;     // FP32-stored ILU(0) factors (Krylov and triangular-solve arithmetic in FP64 either way)
   bool borrowed = false;  // A and b live in the caller's device memory
   bool has_pc = true;
   double bnorm_host = 0.0;
-  // host: pattern, permutation and schedules
+  // host: pattern and schedules
   std::vector<int64_t> rp;
   std::vector<int32_t> ci;
-  std::vector<int32_t> perm, blk;       // perm[i] = original row of permuted row i; blk in permuted order
-  std::vector<int64_t> prp, pdiag;      // permuted pattern
-  std::vector<int32_t> pci;
-  std::vector<int32_t> levL, levU;      // level of each permuted row
-  std::vector<int64_t> lvlptrL, lvlptrU;// per level, positions in the level-ordered arrays
-  std::vector<int32_t> lrow, urow;      // level-ordered permuted row ids
+  std::vector<int32_t> perm, blk;       // perm[q] = caller row of solver row q; blk in solver order
+  std::vector<int64_t> lvr;             // forward level k = solver rows [lvr[k], lvr[k+1])
+  std::vector<int64_t> lvsL, lvsU;      // forward / backward level k = L / U slices [lvs[k], lvs[k+1])
   int32_t nlevL = 0, nlevU = 0;
-  int64_t nnzL = 0, nnzU = 0;
-  bool identity_perm = true;
+  int64_t nslA = 0, nslL = 0, nslU = 0;     // SELL slices
+  int64_t padA = 0, padL = 0, padU = 0;     // SELL slots (incl. padding)
+  int64_t nnzL = 0, nnzU = 0;               // factor entries (excl. padding)
   // device
   DevArena arena;
   int64_t *d_rp = nullptr; int32_t *d_ci = nullptr;
-  double *d_av64 = nullptr;
-  double *d_b64 = nullptr;
-  double *d_x64 = nullptr;  // = kv[0], the solution
+  double *d_av64 = nullptr;   // caller-order values
+  double *d_b64 = nullptr;    // caller-order rhs
+  double *d_x64 = nullptr;    // caller-order solution
+  double *d_bp = nullptr;     // solver-order rhs
   int32_t *d_perm = nullptr, *d_blk = nullptr;
-  int64_t *d_prp = nullptr, *d_pdiag = nullptr, *d_amap = nullptr, *d_fmap = nullptr, *d_dpos = nullptr;
+  // SELL A (solver order)
+  int64_t *d_aoff = nullptr, *d_amapS = nullptr; int32_t *d_acol = nullptr; double *d_aval = nullptr;
+  // solver-order CSR for the factorisation
+  int64_t *d_prp = nullptr, *d_pdiag = nullptr, *d_amap = nullptr, *d_fmap = nullptr, *d_dpos = nullptr, *d_lvr = nullptr;
   int32_t *d_pci = nullptr;
   double *d_lu64 = nullptr;
-  int32_t *d_lrow = nullptr, *d_urow = nullptr, *d_lcol = nullptr, *d_ucol = nullptr;
-  int32_t *d_lgat = nullptr, *d_ugat = nullptr;  // original row of each level-ordered L / U entry
-  int64_t *d_lptr = nullptr, *d_uptr = nullptr, *d_lvlptrL = nullptr, *d_lvlptrU = nullptr;
-  void *d_lval = nullptr, *d_uval = nullptr, *d_udinv = nullptr, *d_ytmp = nullptr;
-  void *kv[9] = {nullptr};  // x r rh p v s t ph sh (FP64)
+  // SELL factors
+  int32_t *d_lrow0 = nullptr, *d_uslot0 = nullptr, *d_urow = nullptr, *d_lcol = nullptr, *d_ucol = nullptr;
+  int64_t *d_loff = nullptr, *d_uoff = nullptr;
+  void *d_lval = nullptr, *d_uval = nullptr, *d_udinv = nullptr;
+  double *d_ytmp = nullptr;
+  void *kv[9] = {nullptr};  // x r rh p v s t ph sh (FP64, solver order, n + 1 entries; entry n stays 0)
 
   int create(Ctx &ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *v,
              const double *rhs, const vshe_solve_opts &o);
@@ -72,9 +92,11 @@ struct System {
   // pattern is used for the schedules, values are read from the device at solve time.
   int create_borrowed(Ctx &ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, int64_t *d_rp_,
                       int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o);
-  int refresh_device_values(Ctx &ctx);  // after the borrowed values changed
   int set_values(Ctx &ctx, const double *v, const double *rhs);
   int setup_pattern(Ctx &ctx);          // ordering, schedules, device buffers
+  // gathers the caller-order values and rhs into the solver-order SELL A, the factorisation
+  // CSR and b_p (on the context's stream)
+  void prepare(Ctx &ctx);
   void fill_sysdev(void *out) const;
 };
 
@@ -92,9 +114,9 @@ struct Batch {
   double *d_partials = nullptr, *d_rnorm2 = nullptr, *d_bnorm2 = nullptr;
   unsigned *d_bar = nullptr;
   void *d_sysdev = nullptr, *d_state = nullptr, *d_refdev = nullptr, *d_factdev = nullptr;
-  // triangular-solve chunk schedules (per level: chunks of <= 32 level-ordered rows of one system)
+  // triangular-solve schedules (per level: the (system, slice) entries of every member)
   int64_t *d_cptrL = nullptr, *d_cptrU = nullptr;
-  int32_t *d_csL = nullptr, *d_cqL = nullptr, *d_cnL = nullptr, *d_csU = nullptr, *d_cqU = nullptr, *d_cnU = nullptr;
+  int32_t *d_csL = nullptr, *d_cqL = nullptr, *d_csU = nullptr, *d_cqU = nullptr;
   // factorisation schedule of a multi-system batch (per level: rows of every system)
   int64_t *d_fptr = nullptr;
   int32_t *d_fsys = nullptr, *d_frow = nullptr;

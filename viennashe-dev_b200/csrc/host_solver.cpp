@@ -86,7 +86,7 @@ int System::create(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_, const
                    const double *rhs, const vshe_solve_opts &o) {
   n = n_; nnz = nnz_; opts = o;
   if (n <= 0 || nnz <= 0 || !rp_ || !ci_ || !v || !rhs) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "empty system or null pointer");
-  if (n >= (int64_t(1) << 31)) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "more than 2^31 rows");
+  if (n >= (int64_t(1) << 31) - 64) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "more than 2^31 - 64 rows");
   if (rp_[0] != 0 || rp_[n] != nnz) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "row_ptr does not span nnz");
   rp.assign(rp_, rp_ + n + 1);
   ci.assign(ci_, ci_ + nnz);
@@ -131,20 +131,15 @@ int System::create_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *r
                             int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o) {
   n = n_; nnz = nnz_; opts = o; borrowed = true;
   if (n <= 0 || nnz <= 0) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "empty system");
+  if (n >= (int64_t(1) << 31) - 64) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "more than 2^31 - 64 rows");
   rp.assign(rp_, rp_ + n + 1);
   ci.assign(ci_, ci_ + nnz);
   for (int64_t i = 0; i < n; ++i)
     if (rp[i + 1] == rp[i]) return ctx.fail(VSHE_E_EMPTY_ROW, "row " + std::to_string(i));
   d_rp = d_rp_; d_ci = d_ci_; d_av64 = d_val; d_b64 = d_rhs;
-  int rc = setup_pattern(ctx);
-  if (rc) return rc;
   bnorm_host = 1.0;  // the trivial-rhs test uses the device-side norm
-  return refresh_device_values(ctx);
+  return setup_pattern(ctx);
 }
-
-// The Krylov iteration reads A's FP64 values in place; the factors are rebuilt from them by
-// the next solve, so nothing is derived here.
-int System::refresh_device_values(Ctx &) { return VSHE_OK; }
 
 int System::set_values(Ctx &ctx, const double *v, const double *rhs) {
   cudaStream_t s = ctx.stream;
@@ -159,7 +154,14 @@ int System::set_values(Ctx &ctx, const double *v, const double *rhs) {
   bnorm_host = std::sqrt(bnorm_host);
   if ((e = cudaMemcpyAsync(d_av64, v, sizeof(double) * size_t(nnz), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "upload values");
   if ((e = cudaMemcpyAsync(d_b64, rhs, sizeof(double) * size_t(n), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "upload rhs");
-  return refresh_device_values(ctx);
+  return VSHE_OK;
+}
+
+void System::prepare(Ctx &ctx) {
+  cudaStream_t s = ctx.stream;
+  vk_gather_values(padA, d_amapS, d_av64, d_aval, s);
+  if (has_pc) vk_gather_values(nnz, d_amap, d_av64, d_lu64, s);
+  vk_permute(n, d_perm, d_b64, d_bp, 1, s);
 }
 
 // greedy colouring of the symmetrised pattern, rows grouped by block
@@ -190,61 +192,118 @@ static void greedy_colours(int64_t n, const std::vector<int64_t> &rp, const std:
   }
 }
 
-int System::setup_pattern(Ctx &ctx) {
-  has_pc = opts.precond != VSHE_PRECOND_NONE;
-  mixed = opts.precision == VSHE_PRECISION_MIXED;
-  cudaError_t e;
-  // block ids in the original order
+// SELL-32 layout of a row sequence: rows[t] (t = 0..m-1) cut into slices of 32 that never
+// straddle a level boundary (lvs = level starts in t); width of a slice = its longest row.
+// Returns the slot offsets (one per slice + 1) and the slice starts in t.
+static void sell_layout(const std::vector<int64_t> &len_of_t, const std::vector<int64_t> &lvl_t, std::vector<int64_t> &off,
+                        std::vector<int64_t> &start, std::vector<int64_t> &lvl_slices) {
+  off.assign(1, 0);
+  start.clear();
+  lvl_slices.assign(1, 0);
+  for (size_t k = 0; k + 1 < lvl_t.size(); ++k) {
+    for (int64_t t = lvl_t[k]; t < lvl_t[k + 1]; t += 32) {
+      const int64_t e = std::min<int64_t>(t + 32, lvl_t[k + 1]);
+      int64_t w = 0;
+      for (int64_t u = t; u < e; ++u) w = std::max(w, len_of_t[size_t(u)]);
+      start.push_back(t);
+      off.push_back(off.back() + 32 * w);
+    }
+    lvl_slices.push_back(int64_t(start.size()));
+  }
+  start.push_back(lvl_t.empty() ? 0 : lvl_t.back());
+}
+
+int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci,
+                  const vshe_solve_opts &opts, std::string &err) {
+  const bool has_pc = opts.precond != VSHE_PRECOND_NONE;
+  // block ids in the caller's order
   std::vector<int32_t> blk0((size_t)(n), 0);
   if (opts.precond == VSHE_PRECOND_BLOCK_ILU0 && opts.n_blocks > 0 && opts.block_ptr) {
     const int64_t *bp = opts.block_ptr;
-    if (bp[0] != 0 || bp[opts.n_blocks] != n) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "block_ptr must span [0, n]");
+    if (bp[0] != 0 || bp[opts.n_blocks] != n) { err = "block_ptr must span [0, n]"; return VSHE_E_INVALID_ARGUMENT; }
     for (int64_t b = 0; b < opts.n_blocks; ++b) {
-      if (bp[b + 1] < bp[b]) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "block_ptr not monotone");
+      if (bp[b + 1] < bp[b]) { err = "block_ptr not monotone"; return VSHE_E_INVALID_ARGUMENT; }
       for (int64_t i = bp[b]; i < bp[b + 1]; ++i) blk0[size_t(i)] = int32_t(b);
     }
   }
-  // ordering
-  perm.resize(size_t(n));
+  // base ordering of the preconditioner: base[i] = caller row at base position i
+  std::vector<int32_t> base((size_t)n);
   if (opts.perm) {
     std::vector<char> seen((size_t)(n), 0);
     for (int64_t i = 0; i < n; ++i) {
       int32_t o = opts.perm[i];
-      if (o < 0 || o >= n || seen[size_t(o)]) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "perm is not a permutation");
+      if (o < 0 || o >= n || seen[size_t(o)]) { err = "perm is not a permutation"; return VSHE_E_INVALID_ARGUMENT; }
       seen[size_t(o)] = 1;
-      perm[size_t(i)] = o;
+      base[size_t(i)] = o;
     }
   } else if (has_pc && opts.ordering == VSHE_ORDER_MULTICOLOR) {
     std::vector<int32_t> col;
     greedy_colours(n, rp, ci, blk0, col);
-    std::iota(perm.begin(), perm.end(), 0);
-    std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) {
+    std::iota(base.begin(), base.end(), 0);
+    std::stable_sort(base.begin(), base.end(), [&](int32_t a, int32_t b) {
       if (blk0[size_t(a)] != blk0[size_t(b)]) return blk0[size_t(a)] < blk0[size_t(b)];
       return col[size_t(a)] < col[size_t(b)];
     });
   } else {
-    std::iota(perm.begin(), perm.end(), 0);
+    std::iota(base.begin(), base.end(), 0);
   }
-  identity_perm = true;
-  for (int64_t i = 0; i < n; ++i) if (perm[size_t(i)] != i) { identity_perm = false; break; }
+  std::vector<int32_t> binv((size_t)n);
+  for (int64_t i = 0; i < n; ++i) binv[size_t(base[size_t(i)])] = int32_t(i);
+
+  // Forward levels over the symmetrised, block-restricted graph in base order: a row's level is
+  // one more than the highest level of any coupled (A_ij or A_ji != 0) earlier row of its block.
+  // Sorting by these levels keeps the relative order of every coupled pair, so ILU(0) in the
+  // sorted order is ILU(0) in the base order, relabelled.
+  std::vector<int32_t> lev((size_t)n, 0);
+  nlevL = 1;
+  if (has_pc) {
+    std::vector<int64_t> tp((size_t)n + 1, 0);
+    for (int64_t k = 0; k < nnz; ++k) tp[size_t(ci[size_t(k)]) + 1]++;
+    for (int64_t i = 0; i < n; ++i) tp[size_t(i) + 1] += tp[size_t(i)];
+    std::vector<int32_t> tr((size_t)nnz);
+    {
+      std::vector<int64_t> pos(tp.begin(), tp.end() - 1);
+      for (int64_t i = 0; i < n; ++i)
+        for (int64_t k = rp[size_t(i)]; k < rp[size_t(i) + 1]; ++k) tr[size_t(pos[size_t(ci[size_t(k)])]++)] = int32_t(i);
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      const int32_t o = base[size_t(i)];
+      int32_t m = -1;
+      for (int64_t k = rp[size_t(o)]; k < rp[size_t(o) + 1]; ++k) {
+        const int32_t j = ci[size_t(k)];
+        if (binv[size_t(j)] < i && blk0[size_t(j)] == blk0[size_t(o)]) m = std::max(m, lev[size_t(j)]);
+      }
+      for (int64_t k = tp[size_t(o)]; k < tp[size_t(o) + 1]; ++k) {
+        const int32_t j = tr[size_t(k)];
+        if (binv[size_t(j)] < i && blk0[size_t(j)] == blk0[size_t(o)]) m = std::max(m, lev[size_t(j)]);
+      }
+      lev[size_t(o)] = m + 1;
+      nlevL = std::max(nlevL, m + 2);
+    }
+  }
+  // solver order: by level, then longest rows first (less SELL padding), then base position
+  perm = base;
+  std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) {
+    if (lev[size_t(a)] != lev[size_t(b)]) return lev[size_t(a)] < lev[size_t(b)];
+    return rp[size_t(a) + 1] - rp[size_t(a)] > rp[size_t(b) + 1] - rp[size_t(b)];
+  });
   std::vector<int32_t> inv((size_t)(n));
   for (int64_t i = 0; i < n; ++i) inv[size_t(perm[size_t(i)])] = int32_t(i);
   blk.resize(size_t(n));
   for (int64_t i = 0; i < n; ++i) blk[size_t(i)] = blk0[size_t(perm[size_t(i)])];
+  lvr.assign(size_t(nlevL) + 1, 0);
+  for (int64_t i = 0; i < n; ++i) lvr[size_t(lev[size_t(i)]) + 1]++;
+  for (size_t k = 1; k < lvr.size(); ++k) lvr[k] += lvr[k - 1];
 
-  std::vector<int64_t> amap, fmap, dpos, lptr, uptr;
-  std::vector<int32_t> lcol, ucol, lgat, ugat;
-  if (has_pc) {
-    // permuted pattern P A P^T with the map back to A's entries
-    prp.assign(size_t(n) + 1, 0);
-    pci.resize(size_t(nnz));
-    amap.resize(size_t(nnz));
-    pdiag.assign(size_t(n), -1);
+  // solver-order CSR with the map back to A's entries
+  prp.assign((size_t)n + 1, 0); pdiag.assign((size_t)n, -1); amap.assign((size_t)nnz, 0);
+  pci.assign((size_t)nnz, 0);
+  {
     std::vector<std::pair<int32_t, int64_t>> row;
     for (int64_t i = 0; i < n; ++i) {
       const int64_t o = perm[size_t(i)];
       row.clear();
-      for (int64_t k = rp[o]; k < rp[o + 1]; ++k) row.push_back({inv[size_t(ci[k])], k});
+      for (int64_t k = rp[size_t(o)]; k < rp[size_t(o) + 1]; ++k) row.push_back({inv[size_t(ci[size_t(k)])], k});
       std::sort(row.begin(), row.end());
       int64_t p = prp[size_t(i)];
       for (auto &x : row) {
@@ -254,94 +313,130 @@ int System::setup_pattern(Ctx &ctx) {
         ++p;
       }
       prp[size_t(i) + 1] = p;
-      if (pdiag[size_t(i)] < 0) return ctx.fail(VSHE_E_ZERO_PIVOT, "no diagonal entry in row " + std::to_string(o));
+      if (has_pc && pdiag[size_t(i)] < 0) { err = "no diagonal entry in row " + std::to_string(o); return VSHE_E_ZERO_PIVOT; }
     }
-    // levels of the forward / backward solves (block-restricted)
-    levL.assign(size_t(n), 0);
-    levU.assign(size_t(n), 0);
-    nlevL = nlevU = 0;
-    for (int64_t i = 0; i < n; ++i) {
-      int32_t m = -1;
-      for (int64_t k = prp[size_t(i)]; k < pdiag[size_t(i)]; ++k) {
-        int32_t j = pci[size_t(k)];
-        if (blk[size_t(j)] == blk[size_t(i)] && levL[size_t(j)] > m) m = levL[size_t(j)];
-      }
-      levL[size_t(i)] = m + 1;
-      nlevL = std::max(nlevL, m + 2);
-    }
-    for (int64_t i = n - 1; i >= 0; --i) {
-      int32_t m = -1;
-      for (int64_t k = pdiag[size_t(i)] + 1; k < prp[size_t(i) + 1]; ++k) {
-        int32_t j = pci[size_t(k)];
-        if (blk[size_t(j)] == blk[size_t(i)] && levU[size_t(j)] > m) m = levU[size_t(j)];
-      }
-      levU[size_t(i)] = m + 1;
-      nlevU = std::max(nlevU, m + 2);
-    }
-    // level-ordered rows (stable: by level, then row)
-    auto order = [&](const std::vector<int32_t> &lev, int32_t nl, std::vector<int64_t> &lvp, std::vector<int32_t> &rows) {
-      lvp.assign(size_t(nl) + 1, 0);
-      for (int32_t l : lev) lvp[size_t(l) + 1]++;
-      for (size_t k = 1; k < lvp.size(); ++k) lvp[k] += lvp[k - 1];
-      rows.resize(size_t(n));
-      std::vector<int64_t> cur(lvp.begin(), lvp.end() - 1);
-      for (int64_t i = 0; i < n; ++i) rows[size_t(cur[size_t(lev[size_t(i)])]++)] = int32_t(i);
-    };
-    order(levL, nlevL, lvlptrL, lrow);
-    order(levU, nlevU, lvlptrU, urow);
-    lgat.resize(size_t(n));
-    ugat.resize(size_t(n));
-    for (int64_t q = 0; q < n; ++q) {
-      lgat[size_t(q)] = perm[size_t(lrow[size_t(q)])];
-      ugat[size_t(q)] = perm[size_t(urow[size_t(q)])];
-    }
-    fmap.assign(size_t(nnz), -1);
-    lptr.assign(size_t(n) + 1, 0);
-    uptr.assign(size_t(n) + 1, 0);
-    dpos.resize(size_t(n));
-    for (int64_t q = 0; q < n; ++q) {
-      const int32_t r = lrow[size_t(q)];
-      int64_t c = 0;
-      for (int64_t k = prp[size_t(r)]; k < pdiag[size_t(r)]; ++k)
-        if (blk[size_t(pci[size_t(k)])] == blk[size_t(r)]) ++c;
-      lptr[size_t(q) + 1] = lptr[size_t(q)] + c;
-    }
-    nnzL = lptr[size_t(n)];
-    lcol.resize(size_t(nnzL));
-    for (int64_t q = 0; q < n; ++q) {
-      const int32_t r = lrow[size_t(q)];
-      int64_t p = lptr[size_t(q)];
-      for (int64_t k = prp[size_t(r)]; k < pdiag[size_t(r)]; ++k) {
-        const int32_t j = pci[size_t(k)];
-        if (blk[size_t(j)] != blk[size_t(r)]) continue;
-        lcol[size_t(p)] = j;
-        fmap[size_t(k)] = p;
-        ++p;
-      }
-    }
-    for (int64_t q = 0; q < n; ++q) {
-      const int32_t r = urow[size_t(q)];
-      dpos[size_t(r)] = q;
-      int64_t c = 0;
-      for (int64_t k = pdiag[size_t(r)] + 1; k < prp[size_t(r) + 1]; ++k)
-        if (blk[size_t(pci[size_t(k)])] == blk[size_t(r)]) ++c;
-      uptr[size_t(q) + 1] = uptr[size_t(q)] + c;
-    }
-    nnzU = uptr[size_t(n)];
-    ucol.resize(size_t(nnzU));
-    for (int64_t q = 0; q < n; ++q) {
-      const int32_t r = urow[size_t(q)];
-      int64_t p = uptr[size_t(q)];
-      for (int64_t k = pdiag[size_t(r)] + 1; k < prp[size_t(r) + 1]; ++k) {
-        const int32_t j = pci[size_t(k)];
-        if (blk[size_t(j)] != blk[size_t(r)]) continue;
-        ucol[size_t(p)] = j;
-        fmap[size_t(k)] = -(p + 2);
-        ++p;
+  }
+  const int32_t PAD = int32_t(n);  // padding column: entry n of every vector stays 0
+
+  // SELL-32 A in solver order: slices of 32 consecutive rows
+  std::vector<int64_t> alvs;
+  {
+    std::vector<int64_t> len((size_t)n);
+    for (int64_t i = 0; i < n; ++i) len[size_t(i)] = prp[size_t(i) + 1] - prp[size_t(i)];
+    std::vector<int64_t> one{0, n};
+    sell_layout(len, one, aoff, astart, alvs);
+  }
+  nslA = int64_t(astart.size()) - 1;
+  padA = aoff.back();
+  amapS.assign((size_t)padA, -1);
+  acol.assign((size_t)padA, PAD);
+  for (int64_t j = 0; j < nslA; ++j) {
+    for (int64_t i = astart[size_t(j)]; i < astart[size_t(j) + 1]; ++i) {
+      const int lane = int(i - astart[size_t(j)]);
+      int64_t kk = 0;
+      for (int64_t p = prp[size_t(i)]; p < prp[size_t(i) + 1]; ++p, ++kk) {
+        const int64_t slot = aoff[size_t(j)] + 32 * kk + lane;
+        acol[size_t(slot)] = pci[size_t(p)];
+        amapS[size_t(slot)] = amap[size_t(p)];
       }
     }
   }
 
+  // factor layouts
+  if (has_pc) {
+    // forward sweep: rows of a level are contiguous; L entries = in-block columns left of the diagonal
+    std::vector<int64_t> llen((size_t)n), ulen((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+      int64_t cl = 0, cu = 0;
+      for (int64_t k = prp[size_t(i)]; k < prp[size_t(i) + 1]; ++k) {
+        if (blk[size_t(pci[size_t(k)])] != blk[size_t(i)]) continue;
+        if (k < pdiag[size_t(i)]) ++cl; else if (k > pdiag[size_t(i)]) ++cu;
+      }
+      llen[size_t(i)] = cl; ulen[size_t(i)] = cu;
+    }
+    sell_layout(llen, lvr, loff, lstart, lvsL);
+    nslL = int64_t(lstart.size()) - 1;
+    padL = loff.back();
+    // backward levels in solver order (real U dependencies, block-restricted)
+    std::vector<int32_t> levU((size_t)n, 0);
+    nlevU = 1;
+    for (int64_t i = n - 1; i >= 0; --i) {
+      int32_t m = -1;
+      for (int64_t k = pdiag[size_t(i)] + 1; k < prp[size_t(i) + 1]; ++k) {
+        const int32_t j = pci[size_t(k)];
+        if (blk[size_t(j)] == blk[size_t(i)]) m = std::max(m, levU[size_t(j)]);
+      }
+      levU[size_t(i)] = m + 1;
+      nlevU = std::max(nlevU, m + 2);
+    }
+    std::vector<int64_t> uvt((size_t)nlevU + 1, 0);
+    for (int64_t i = 0; i < n; ++i) uvt[size_t(levU[size_t(i)]) + 1]++;
+    for (size_t k = 1; k < uvt.size(); ++k) uvt[k] += uvt[k - 1];
+    urow.resize((size_t)n);
+    {
+      std::vector<int64_t> cur(uvt.begin(), uvt.end() - 1);
+      for (int64_t i = 0; i < n; ++i) urow[size_t(cur[size_t(levU[size_t(i)])]++)] = int32_t(i);
+    }
+    std::vector<int64_t> ulen_t((size_t)n);
+    dpos.resize((size_t)n);
+    for (int64_t t = 0; t < n; ++t) { ulen_t[size_t(t)] = ulen[size_t(urow[size_t(t)])]; dpos[size_t(urow[size_t(t)])] = t; }
+    sell_layout(ulen_t, uvt, uoff, ustart, lvsU);
+    nslU = int64_t(ustart.size()) - 1;
+    padU = uoff.back();
+    fmap.assign((size_t)nnz, -1);
+    lcol.assign((size_t)padL, PAD);
+    ucol.assign((size_t)padU, PAD);
+    nnzL = nnzU = 0;
+    for (int64_t j = 0; j < nslL; ++j) {
+      for (int64_t i = lstart[size_t(j)]; i < lstart[size_t(j) + 1]; ++i) {
+        const int lane = int(i - lstart[size_t(j)]);
+        int64_t kk = 0;
+        for (int64_t k = prp[size_t(i)]; k < pdiag[size_t(i)]; ++k) {
+          if (blk[size_t(pci[size_t(k)])] != blk[size_t(i)]) continue;
+          const int64_t slot = loff[size_t(j)] + 32 * kk + lane;
+          lcol[size_t(slot)] = pci[size_t(k)];
+          fmap[size_t(k)] = slot;
+          ++kk; ++nnzL;
+        }
+      }
+    }
+    for (int64_t j = 0; j < nslU; ++j) {
+      for (int64_t t = ustart[size_t(j)]; t < ustart[size_t(j) + 1]; ++t) {
+        const int lane = int(t - ustart[size_t(j)]);
+        const int32_t i = urow[size_t(t)];
+        int64_t kk = 0;
+        for (int64_t k = pdiag[size_t(i)] + 1; k < prp[size_t(i) + 1]; ++k) {
+          if (blk[size_t(pci[size_t(k)])] != blk[size_t(i)]) continue;
+          const int64_t slot = uoff[size_t(j)] + 32 * kk + lane;
+          ucol[size_t(slot)] = pci[size_t(k)];
+          fmap[size_t(k)] = -(slot + 2);
+          ++kk; ++nnzU;
+        }
+      }
+    }
+  } else {
+    nlevU = 1;
+  }
+
+  return VSHE_OK;
+}
+
+int System::setup_pattern(Ctx &ctx) {
+  has_pc = opts.precond != VSHE_PRECOND_NONE;
+  mixed = opts.precision == VSHE_PRECISION_MIXED;
+  cudaError_t e;
+  Layout Lt;
+  std::string err;
+  int rc = Lt.build(n, nnz, rp, ci, opts, err);
+  if (rc) return ctx.fail(rc, err);
+  perm = Lt.perm; blk = Lt.blk; lvr = Lt.lvr; lvsL = Lt.lvsL; lvsU = Lt.lvsU;
+  nlevL = Lt.nlevL; nlevU = Lt.nlevU; nslA = Lt.nslA; nslL = Lt.nslL; nslU = Lt.nslU;
+  padA = Lt.padA; padL = Lt.padL; padU = Lt.padU; nnzL = Lt.nnzL; nnzU = Lt.nnzU;
+  const auto &prp = Lt.prp; const auto &pci = Lt.pci; const auto &pdiag = Lt.pdiag; const auto &amap = Lt.amap;
+  const auto &aoff = Lt.aoff; const auto &amapS = Lt.amapS; const auto &acol = Lt.acol;
+  const auto &fmap = Lt.fmap; const auto &dpos = Lt.dpos; const auto &loff = Lt.loff; const auto &uoff = Lt.uoff;
+  const auto &lstart = Lt.lstart; const auto &ustart = Lt.ustart; const auto &lcol = Lt.lcol; const auto &ucol = Lt.ucol;
+  const auto &urow = Lt.urow;
   // ---- device buffers ----
   const size_t tsz = mixed ? sizeof(float) : sizeof(double);
 #define ALLOC(ptr, type, count)                                              \
@@ -350,9 +445,15 @@ int System::setup_pattern(Ctx &ctx) {
 #define ALLOCT(ptr, count)                                                   \
   ptr = arena.alloc(tsz * size_t(count), e);                                 \
   if (!ptr) return ctx.cuda_fail(e, "cudaMalloc " #ptr);
-  // Krylov vectors x r rh p v s t ph sh (FP64); the solution is x itself
-  for (int k = 0; k < 9; ++k) { ALLOC(kv[k], double, n); }
-  d_x64 = (double *)kv[0];
+  // Krylov vectors x r rh p v s t ph sh (FP64, solver order) with the zero entry n
+  for (int k = 0; k < 9; ++k) { ALLOC(kv[k], double, n + 1); }
+  ALLOC(d_x64, double, n);
+  ALLOC(d_bp, double, n + 1);
+  ALLOC(d_perm, int32_t, n);
+  ALLOC(d_aoff, int64_t, nslA + 1);
+  ALLOC(d_amapS, int64_t, padA);
+  ALLOC(d_acol, int32_t, padA);
+  ALLOC(d_aval, double, padA);
   if (has_pc) {
     ALLOC(d_blk, int32_t, n);
     ALLOC(d_prp, int64_t, n + 1);
@@ -361,30 +462,37 @@ int System::setup_pattern(Ctx &ctx) {
     ALLOC(d_amap, int64_t, nnz);
     ALLOC(d_fmap, int64_t, nnz);
     ALLOC(d_dpos, int64_t, n);
+    ALLOC(d_lvr, int64_t, nlevL + 1);
     ALLOC(d_lu64, double, nnz);
-    ALLOC(d_lrow, int32_t, n);
+    ALLOC(d_lrow0, int32_t, nslL + 1);
+    ALLOC(d_loff, int64_t, nslL + 1);
+    ALLOC(d_uslot0, int32_t, nslU + 1);
+    ALLOC(d_uoff, int64_t, nslU + 1);
     ALLOC(d_urow, int32_t, n);
-    ALLOC(d_lgat, int32_t, n);
-    ALLOC(d_ugat, int32_t, n);
-    ALLOC(d_lptr, int64_t, n + 1);
-    ALLOC(d_uptr, int64_t, n + 1);
-    ALLOC(d_lvlptrL, int64_t, nlevL + 1);
-    ALLOC(d_lvlptrU, int64_t, nlevU + 1);
-    ALLOC(d_lcol, int32_t, std::max<int64_t>(nnzL, 1));
-    ALLOC(d_ucol, int32_t, std::max<int64_t>(nnzU, 1));
-    ALLOCT(d_lval, std::max<int64_t>(nnzL, 1));
-    ALLOCT(d_uval, std::max<int64_t>(nnzU, 1));
+    ALLOC(d_lcol, int32_t, std::max<int64_t>(padL, 1));
+    ALLOC(d_ucol, int32_t, std::max<int64_t>(padU, 1));
+    ALLOCT(d_lval, std::max<int64_t>(padL, 1));
+    ALLOCT(d_uval, std::max<int64_t>(padU, 1));
     ALLOCT(d_udinv, n);
-    ALLOC(d_ytmp, double, n);
-    if (!identity_perm) { ALLOC(d_perm, int32_t, n); }
+    ALLOC(d_ytmp, double, n + 1);
   }
 #undef ALLOC
 #undef ALLOCT
   cudaStream_t s = ctx.stream;
+  // every vector starts at 0 (entry n is the SELL padding target and is never written)
+  for (int k = 0; k < 9; ++k)
+    if ((e = cudaMemsetAsync(kv[k], 0, sizeof(double) * size_t(n + 1), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+  if ((e = cudaMemsetAsync(d_bp, 0, sizeof(double) * size_t(n + 1), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+  if ((e = cudaMemsetAsync(d_x64, 0, sizeof(double) * size_t(n), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
 #define H2D(dst, vec)                                                                                        \
   if (!vec.empty() && (e = cudaMemcpyAsync(dst, vec.data(), sizeof(vec[0]) * vec.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess) \
     return ctx.cuda_fail(e, "upload " #dst);
+  H2D(d_perm, perm);
+  H2D(d_aoff, aoff);
+  H2D(d_amapS, amapS);
+  H2D(d_acol, acol);
   if (has_pc) {
+    std::vector<int32_t> lrow0(lstart.begin(), lstart.end()), uslot0(ustart.begin(), ustart.end());
     H2D(d_blk, blk);
     H2D(d_prp, prp);
     H2D(d_pci, pci);
@@ -392,22 +500,20 @@ int System::setup_pattern(Ctx &ctx) {
     H2D(d_amap, amap);
     H2D(d_fmap, fmap);
     H2D(d_dpos, dpos);
-    H2D(d_lrow, lrow);
+    H2D(d_lvr, lvr);
+    H2D(d_lrow0, lrow0);
+    H2D(d_loff, loff);
+    H2D(d_uslot0, uslot0);
+    H2D(d_uoff, uoff);
     H2D(d_urow, urow);
-    H2D(d_lgat, lgat);
-    H2D(d_ugat, ugat);
-    H2D(d_lptr, lptr);
-    H2D(d_uptr, uptr);
-    H2D(d_lvlptrL, lvlptrL);
-    H2D(d_lvlptrU, lvlptrU);
     H2D(d_lcol, lcol);
     H2D(d_ucol, ucol);
-    if (!identity_perm) { H2D(d_perm, perm); }
+    if ((e = cudaMemsetAsync(d_lval, 0, tsz * size_t(std::max<int64_t>(padL, 1)), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+    if ((e = cudaMemsetAsync(d_uval, 0, tsz * size_t(std::max<int64_t>(padU, 1)), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+    if ((e = cudaMemsetAsync(d_ytmp, 0, sizeof(double) * size_t(n + 1), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   }
 #undef H2D
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx.cuda_fail(e, "upload pattern");
-  // the permuted host pattern is only needed to build the device tables
-  prp.clear(); prp.shrink_to_fit(); pci.clear(); pci.shrink_to_fit();
   return VSHE_OK;
 }
 
@@ -417,11 +523,11 @@ void System::fill_sysdev(void *out) const {
   SysDev<float> d;
   std::memset(&d, 0, sizeof(d));
   d.n = n;
-  d.rp = d_rp; d.ci = d_ci; d.av = d_av64; d.b = d_b64;
-  d.lrow = d_lrow; d.lptr = d_lptr; d.lcol = d_lcol; d.lval = (const float *)d_lval;
-  d.urow = d_urow; d.uptr = d_uptr; d.ucol = d_ucol; d.uval = (const float *)d_uval; d.udinv = (const float *)d_udinv;
-  d.lgat = d_lgat; d.ugat = d_ugat;
-  d.ytmp = (double *)d_ytmp;
+  d.aoff = d_aoff; d.acol = d_acol; d.aval = d_aval; d.b = d_bp;
+  d.lrow0 = d_lrow0; d.loff = d_loff; d.lcol = d_lcol; d.lval = (const float *)d_lval;
+  d.uslot0 = d_uslot0; d.uoff = d_uoff; d.ucol = d_ucol; d.uval = (const float *)d_uval; d.udinv = (const float *)d_udinv;
+  d.urow = d_urow;
+  d.ytmp = d_ytmp;
   d.x = (double *)kv[0]; d.r = (double *)kv[1]; d.rh = (double *)kv[2]; d.p = (double *)kv[3];
   d.v = (double *)kv[4]; d.s = (double *)kv[5]; d.t = (double *)kv[6]; d.ph = (double *)kv[7]; d.sh = (double *)kv[8];
   std::memcpy(out, &d, sizeof(d));
@@ -449,41 +555,39 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   }
   st0.push_back(int32_t(tsys.size()));
   ntiles = int(tsys.size());
-  // Triangular-solve schedules: merged level l lists, system by system, the level-l rows of
-  // every member cut into chunks of at most 32 consecutive level-ordered positions.
+  // Triangular-solve schedules: merged level l lists, system by system, the level-l SELL
+  // slices of every member.
   std::vector<int64_t> cptrL, cptrU, fptr;
-  std::vector<int32_t> csL, cqL, cnL, csU, cqU, cnU, fsys, frow;
-  auto chunks = [&](bool lower, std::vector<int64_t> &cptr, std::vector<int32_t> &cs, std::vector<int32_t> &cq,
-                    std::vector<int32_t> &cn, int32_t &nl) {
+  std::vector<int32_t> csL, cqL, csU, cqU, fsys, frow;
+  auto slices = [&](bool lower, std::vector<int64_t> &cptr, std::vector<int32_t> &cs, std::vector<int32_t> &cq, int32_t &nl) {
     nl = 0;
     for (System *S : sys) nl = std::max(nl, lower ? S->nlevL : S->nlevU);
     cptr.assign(1, 0);
     for (int32_t l = 0; l < nl; ++l) {
       for (int k = 0; k < nsys; ++k) {
-        const auto &vp = lower ? sys[size_t(k)]->lvlptrL : sys[size_t(k)]->lvlptrU;
+        const auto &vp = lower ? sys[size_t(k)]->lvsL : sys[size_t(k)]->lvsU;
         if (l + 1 >= int32_t(vp.size())) continue;
-        for (int64_t q = vp[size_t(l)]; q < vp[size_t(l) + 1]; q += 32) {
+        for (int64_t j = vp[size_t(l)]; j < vp[size_t(l) + 1]; ++j) {
           cs.push_back(k);
-          cq.push_back(int32_t(q));
-          cn.push_back(int32_t(std::min<int64_t>(32, vp[size_t(l) + 1] - q)));
+          cq.push_back(int32_t(j));
         }
       }
       cptr.push_back(int64_t(cs.size()));
     }
   };
   if (has_pc) {
-    chunks(true, cptrL, csL, cqL, cnL, nlevL);
-    chunks(false, cptrU, csU, cqU, cnU, nlevU);
+    slices(true, cptrL, csL, cqL, nlevL);
+    slices(false, cptrU, csU, cqU, nlevU);
     if (nsys > 1) {
-      // factorisation: merged level l = the forward-solve level-l rows of every member
+      // factorisation: merged level l = the forward-level-l rows of every member
       fptr.assign(1, 0);
       for (int32_t l = 0; l < nlevL; ++l) {
         for (int k = 0; k < nsys; ++k) {
           const System *S = sys[size_t(k)];
-          if (l + 1 >= int32_t(S->lvlptrL.size())) continue;
-          for (int64_t q = S->lvlptrL[size_t(l)]; q < S->lvlptrL[size_t(l) + 1]; ++q) {
+          if (l + 1 >= int32_t(S->lvr.size())) continue;
+          for (int64_t q = S->lvr[size_t(l)]; q < S->lvr[size_t(l) + 1]; ++q) {
             fsys.push_back(k);
-            frow.push_back(S->lrow[size_t(q)]);
+            frow.push_back(int32_t(q));
           }
         }
         fptr.push_back(int64_t(fsys.size()));
@@ -518,10 +622,8 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
     ALLOC(d_cptrU, int64_t, cptrU.size());
     ALLOC(d_csL, int32_t, std::max<size_t>(csL.size(), 1));
     ALLOC(d_cqL, int32_t, std::max<size_t>(cqL.size(), 1));
-    ALLOC(d_cnL, int32_t, std::max<size_t>(cnL.size(), 1));
     ALLOC(d_csU, int32_t, std::max<size_t>(csU.size(), 1));
     ALLOC(d_cqU, int32_t, std::max<size_t>(cqU.size(), 1));
-    ALLOC(d_cnU, int32_t, std::max<size_t>(cnU.size(), 1));
     if (nsys > 1) {
       ALLOC(d_fptr, int64_t, fptr.size());
       ALLOC(d_fsys, int32_t, std::max<size_t>(fsys.size(), 1));
@@ -537,7 +639,7 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
     System *S = sys[size_t(k)];
     S->fill_sysdev(sd.data() + vk_sysdev_size() * size_t(k));
     // the final / replacement residual is written into the Krylov r
-    RefDev r{S->n, S->d_rp, S->d_ci, S->d_av64, S->d_b64, (const double *)S->kv[0], (double *)S->kv[1]};
+    RefDev r{S->n, S->d_aoff, S->d_acol, S->d_aval, S->d_bp, (const double *)S->kv[0], (double *)S->kv[1]};
     std::memcpy(rd.data() + vk_refdev_size() * size_t(k), &r, sizeof(r));
     FactDev f{S->n, S->d_prp, S->d_pci, S->d_lu64, S->d_pdiag, S->d_blk};
     std::memcpy(fd.data() + vk_factdev_size() * size_t(k), &f, sizeof(f));
@@ -561,12 +663,10 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
     if (!csL.empty()) {
       H2D(d_csL, csL.data(), sizeof(int32_t) * csL.size());
       H2D(d_cqL, cqL.data(), sizeof(int32_t) * cqL.size());
-      H2D(d_cnL, cnL.data(), sizeof(int32_t) * cnL.size());
     }
     if (!csU.empty()) {
       H2D(d_csU, csU.data(), sizeof(int32_t) * csU.size());
       H2D(d_cqU, cqU.data(), sizeof(int32_t) * cqU.size());
-      H2D(d_cnU, cnU.data(), sizeof(int32_t) * cnU.size());
     }
     if (nsys > 1) {
       H2D(d_fptr, fptr.data(), sizeof(int64_t) * fptr.size());
@@ -582,10 +682,10 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   if ((e = cudaMemsetAsync(d_state, 0, vk_bistate_size() * size_t(nsys), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   tiles = VkTiles{ntiles, d_tile_sys, d_tile_r0, d_tile_r1, d_sys_tile0};
   if (has_pc) {
-    levL = VkLevels{nlevL, d_cptrL, d_csL, d_cqL, d_cnL};
-    levU = VkLevels{nlevU, d_cptrU, d_csU, d_cqU, d_cnU};
+    levL = VkLevels{nlevL, d_cptrL, d_csL, d_cqL, nullptr};
+    levU = VkLevels{nlevU, d_cptrU, d_csU, d_cqU, nullptr};
     if (nsys > 1) levF = VkLevels{nlevL, d_fptr, d_fsys, d_frow, nullptr};
-    else levF = VkLevels{nlevL, sys[0]->d_lvlptrL, nullptr, sys[0]->d_lrow, nullptr};
+    else levF = VkLevels{nlevL, sys[0]->d_lvr, nullptr, nullptr, nullptr};
   }
   int dev = 0;
   cudaGetDevice(&dev);
@@ -617,7 +717,6 @@ int Batch::check_err(Ctx &ctx, const char *what) {
 int Batch::factor(Ctx &ctx) {
   if (!has_pc) return VSHE_OK;
   cudaStream_t s = ctx.stream;
-  for (System *S : sys) vk_gather_values(S->nnz, S->d_amap, S->d_av64, S->d_lu64, s);
   const int mode = (sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) ? 2 : 1;
   int rc = vk_ilu0(mode, mode == 1 ? ilu_grid : std::max(1, num_sms * 8), d_factdev, &levF, d_bar, d_err, s);
   if (rc) return ctx.cuda_fail(cudaError_t(rc), "ilu0 launch");
@@ -782,6 +881,7 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
   int rc = set_active(ctx, act);
   if (rc) return rc;
   cudaEventRecord(e0, s);
+  for (System *S : sys) S->prepare(ctx);
   rc = factor(ctx);
   if (rc) return rc;
   cudaEventRecord(e1, s);
@@ -810,6 +910,7 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
   }
   std::fill(act.begin(), act.end(), 1);
   if ((rc = set_active(ctx, act))) return rc;
+  for (System *S : sys) vk_permute(S->n, S->d_perm, (const double *)S->kv[0], S->d_x64, 0, s);  // x back to caller order
   cudaEventRecord(e2, s);
   if ((e = cudaEventSynchronize(e2)) != cudaSuccess) return ctx.cuda_fail(e, "solve");
   float ms_setup = 0, ms_solve = 0;
@@ -1045,13 +1146,17 @@ int vshe_system_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, const double *
   System *S = it->second.get();
   cudaStream_t s = ctx->stream;
   cudaError_t e;
-  const int grid = std::max(1, int(std::min<int64_t>((S->n + 255) / 256, 65535 * 8)));
   if (precision != VSHE_PRECISION_FP64) return ctx->fail(VSHE_E_UNSUPPORTED, "the SpMV runs in FP64 in every solver mode");
-  // scratch: the search-direction vectors (the solution x stays untouched)
-  double *dx = (double *)S->kv[3], *dy = (double *)S->kv[4];
-  if ((e = cudaMemcpyAsync(dx, x, sizeof(double) * size_t(S->n), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx->cuda_fail(e, "x");
-  vk_spmv_plain(grid, S->n, S->d_rp, S->d_ci, S->d_av64, dx, dy, s);
-  if ((e = cudaMemcpyAsync(y, dy, sizeof(double) * size_t(S->n), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return ctx->cuda_fail(e, "y");
+  const int grid = std::max(1, int(std::min<int64_t>(S->nslA / 8 + 1, 148 * 32)));
+  // the solver-order SELL copy of A, then y = A x through it; scratch: the search-direction
+  // vectors (the solution x stays untouched)
+  S->prepare(*ctx);
+  double *dxo = (double *)S->kv[5], *dx = (double *)S->kv[3], *dy = (double *)S->kv[4];
+  if ((e = cudaMemcpyAsync(dxo, x, sizeof(double) * size_t(S->n), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx->cuda_fail(e, "x");
+  vk_permute(S->n, S->d_perm, dxo, dx, 1, s);
+  vk_spmv_plain(grid, S->n, S->d_aoff, S->d_acol, S->d_aval, dx, dy, s);
+  vk_permute(S->n, S->d_perm, dy, dxo, 0, s);
+  if ((e = cudaMemcpyAsync(y, dxo, sizeof(double) * size_t(S->n), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return ctx->cuda_fail(e, "y");
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx->cuda_fail(e, "spmv");
   return VSHE_OK;
 }
@@ -1065,16 +1170,18 @@ int vshe_system_time_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, int32_t r
   System *S = it->second.get();
   if (precision != VSHE_PRECISION_FP64) return ctx->fail(VSHE_E_UNSUPPORTED, "the SpMV runs in FP64 in every solver mode");
   cudaStream_t s = ctx->stream;
-  const int grid = std::max(1, int(std::min<int64_t>((S->n + 255) / 256, 65535 * 8)));
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::max(1, int(std::min<int64_t>(S->nslA / 8 + 1, int64_t(sms) * 4)));
+  S->prepare(*ctx);
   cudaEvent_t a, b;
   cudaEventCreate(&a); cudaEventCreate(&b);
-  for (int w = 0; w < 3; ++w) {
-    vk_spmv_plain(grid, S->n, S->d_rp, S->d_ci, S->d_av64, (const double *)S->kv[3], (double *)S->kv[4], s);
-  }
+  for (int w = 0; w < 3; ++w)
+    vk_spmv_plain(grid, S->n, S->d_aoff, S->d_acol, S->d_aval, (const double *)S->kv[3], (double *)S->kv[4], s);
   cudaEventRecord(a, s);
-  for (int r = 0; r < reps; ++r) {
-    vk_spmv_plain(grid, S->n, S->d_rp, S->d_ci, S->d_av64, (const double *)S->kv[3], (double *)S->kv[4], s);
-  }
+  for (int r = 0; r < reps; ++r)
+    vk_spmv_plain(grid, S->n, S->d_aoff, S->d_acol, S->d_aval, (const double *)S->kv[3], (double *)S->kv[4], s);
   cudaEventRecord(b, s);
   cudaError_t e = cudaEventSynchronize(b);
   float t = 0;
@@ -1085,7 +1192,7 @@ int vshe_system_time_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, int32_t r
   return VSHE_OK;
 }
 
-// Factor values of P A P^T in A's entry order (FP64, host array of length nnz);
+// Factor values of P A P^T (solver order) in A's entry order (FP64, host array of length nnz);
 // entries coupling two blocks are not part of the factor and read 0.
 int vshe_system_factor_values(vshe_ctx *ctx, int64_t h, double *lu) {
   if (!ctx || !lu) return VSHE_E_INVALID_ARGUMENT;
@@ -1096,6 +1203,7 @@ int vshe_system_factor_values(vshe_ctx *ctx, int64_t h, double *lu) {
   Batch *B = get_batch(ctx, hs, rc);
   if (!B) return rc;
   if (!B->has_pc) return ctx->fail(VSHE_E_UNSUPPORTED, "no preconditioner");
+  B->sys[0]->prepare(*ctx);
   rc = B->factor(*ctx);
   if (rc) return rc;
   System *S = B->sys[0];
@@ -1114,6 +1222,69 @@ int vshe_system_factor_values(vshe_ctx *ctx, int64_t h, double *lu) {
       const bool in_factor = S->blk[size_t(pci[size_t(k)])] == S->blk[size_t(i)];
       lu[amap[size_t(k)]] = in_factor ? lp[size_t(k)] : 0.0;
     }
+  return VSHE_OK;
+}
+
+// Host-only view of the solver layout (no GPU): validates the inputs like vshe_system_create
+// and builds the same Layout a resident system would use.
+static int layout_for(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const vshe_solve_opts *opts, Layout &L) {
+  if (n <= 0 || nnz <= 0 || !rp || !ci) return VSHE_E_INVALID_ARGUMENT;
+  if (rp[0] != 0 || rp[n] != nnz) return VSHE_E_INVALID_ARGUMENT;
+  std::vector<int64_t> vrp(rp, rp + n + 1);
+  std::vector<int32_t> vci(ci, ci + nnz);
+  for (int64_t i = 0; i < n; ++i) {
+    if (vrp[size_t(i) + 1] < vrp[size_t(i)]) return VSHE_E_INVALID_ARGUMENT;
+    if (vrp[size_t(i) + 1] == vrp[size_t(i)]) return VSHE_E_EMPTY_ROW;
+    for (int64_t k = vrp[size_t(i)]; k < vrp[size_t(i) + 1]; ++k)
+      if (vci[size_t(k)] < 0 || vci[size_t(k)] >= n || (k > vrp[size_t(i)] && vci[size_t(k)] <= vci[size_t(k) - 1])) return VSHE_E_INVALID_ARGUMENT;
+  }
+  vshe_solve_opts o;
+  if (opts) o = *opts; else vshe_default_opts(&o);
+  std::string err;
+  return L.build(n, nnz, vrp, vci, o, err);
+}
+
+int vshe_layout_sizes(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const vshe_solve_opts *opts, int64_t *sizes) {
+  if (!sizes) return VSHE_E_INVALID_ARGUMENT;
+  Layout L;
+  int rc = layout_for(n, nnz, rp, ci, opts, L);
+  if (rc) return rc;
+  const int64_t v[10] = {L.nslA, L.padA, L.nslL, L.padL, L.nslU, L.padU, L.nlevL, L.nlevU, L.nnzL, L.nnzU};
+  for (int k = 0; k < 10; ++k) sizes[k] = v[k];
+  return VSHE_OK;
+}
+
+int vshe_layout_export(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const vshe_solve_opts *opts,
+                       int32_t *perm, int64_t *lvr, int64_t *aoff, int32_t *acol, int64_t *amap_a,
+                       int32_t *lrow0, int64_t *loff, int32_t *lcol, int64_t *lmap,
+                       int32_t *uslot0, int64_t *uoff, int32_t *ucol, int64_t *umap, int32_t *urow) {
+  Layout L;
+  int rc = layout_for(n, nnz, rp, ci, opts, L);
+  if (rc) return rc;
+  auto put = [](auto *dst, const auto &src) { if (dst) for (size_t k = 0; k < src.size(); ++k) dst[k] = src[k]; };
+  put(perm, L.perm);
+  put(lvr, L.lvr);
+  put(aoff, L.aoff);
+  put(acol, L.acol);
+  put(amap_a, L.amapS);
+  put(lrow0, L.lstart);
+  put(loff, L.loff);
+  put(lcol, L.lcol);
+  put(uslot0, L.ustart);
+  put(uoff, L.uoff);
+  put(ucol, L.ucol);
+  put(urow, L.urow);
+  // caller entry of every factor slot (-1: padding)
+  if (lmap || umap) {
+    std::vector<int64_t> lm((size_t)L.padL, -1), um((size_t)L.padU, -1);
+    for (int64_t k = 0; k < nnz; ++k) {
+      const int64_t m = L.fmap.empty() ? -1 : L.fmap[size_t(k)];
+      if (m >= 0) lm[size_t(m)] = L.amap[size_t(k)];
+      else if (m <= -2) um[size_t(-(m + 2))] = L.amap[size_t(k)];
+    }
+    put(lmap, lm);
+    put(umap, um);
+  }
   return VSHE_OK;
 }
 

@@ -54,13 +54,17 @@ void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles 
 VK_DECL_P(float, f32)
 VK_DECL_P(double, f64)
 
-void vk_spmv_plain(int grid, int64_t n, const int64_t *rp, const int32_t *ci, const double *av, const double *x, double *y, cudaStream_t s);
+// y = A x on a SELL-32 matrix (solver order)
+void vk_spmv_plain(int grid, int64_t n, const int64_t *aoff, const int32_t *acol, const double *aval, const double *x, double *y, cudaStream_t s);
+// out[q] = in[perm[q]] (gather = 1) or out[perm[q]] = in[q] (gather = 0)
+void vk_permute(int64_t n, const int32_t *perm, const double *in, double *out, int gather, cudaStream_t s);
 
 int vk_ilu0(int mode, int grid, const void *fs, const VkLevels *lv, unsigned *bar, int32_t *err, cudaStream_t s);
 int vk_ilu0_occupancy(int *blocks_per_sm);
-void vk_gather_values(int64_t nnz, const int64_t *amap, const double *av, double *lu, cudaStream_t s);
+// out[k] = av[amap[k]] (0 where amap[k] < 0)
+void vk_gather_values(int64_t nnz, const int64_t *amap, const double *av, double *out, cudaStream_t s);
 
-// r = b - A x in FP64 (written to the RefDev's r), ||r||^2 and ||b||^2 per system
+// r = b - A x in FP64 (solver order, written to the RefDev's r), ||r||^2 and ||b||^2 per system
 void vk_residual64(int ntiles, const void *ref, const VkTiles *tl, double *part, int32_t *cnt,
                    const int32_t *act, double *rnorm2, double *bnorm2, cudaStream_t s);
 

@@ -295,7 +295,6 @@ int SheProblem::assemble(Ctx &ctx, int upto) {
   if ((rc = vk_she_normalise(&P, n_red, d_rrp, d_rci, d_rval, d_rrhs, d_ins, H.cfg.scale ? 1 : 0, d_s, d_sf, d_dpos, d_cptr, d_cursor, d_cpos, d_tmp, tmp_bytes, ctx.stream)))
     return ctx.cuda_fail(cudaError_t(rc), "normalise");
   stage = 3;
-  if (sys) sys->refresh_device_values(ctx);
   return VSHE_OK;
 }
 

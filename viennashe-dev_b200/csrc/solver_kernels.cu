@@ -1,13 +1,14 @@
 // solver_kernels.cu -- sm_100a kernels of the Krylov solver (thin launchers at the end).
 //
-// Everything here is memory-bound sparse work: CSR SpMV fused with the dot products that
+// Everything here is memory-bound sparse work: SELL-32 SpMV fused with the dot products that
 // follow it, BiCGStab vector updates fused with their reductions, level-scheduled ILU(0)
 // factorisation and triangular solves run as persistent cooperative kernels with a bounded
 // grid barrier per level.  No tensor cores: nothing on this path is a dense contraction.
 //
-// Rows are processed in chunks of 32 consecutive CSR rows per warp: the chunk's entries
-// form one contiguous range that is streamed with coalesced loads, several entries per lane
-// in flight, and every lane then sums its own row in index order (chunk_rowsums).
+// Data layout (solver_kernels.cuh): every system is solved in a level-sorted "solver order"
+// and A, L, U are SELL-32 slices, one row per lane, so value and column loads are coalesced
+// lines, every row is summed by one thread in index order (deterministic, launch-shape
+// independent) and the triangular solves read and write their vectors without index maps.
 //
 // Batches: each kernel works on a batch of independent systems described by per-system
 // pointer tables (SysDev) and row tiles that never straddle two systems; reductions are per
@@ -41,8 +42,8 @@ namespace vshe {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kSpmvU = 12;  // entries per lane in flight: ~12 nnz per row fit one pass
-constexpr int kTrsvU = 8;   // triangular factors hold about half of A's entries per row
+constexpr int kSpmvU = 8;  // SELL entries per lane whose loads are issued together
+constexpr int kTrsvU = 4;  // triangular factors hold about half of A's entries per row
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -108,44 +109,39 @@ __device__ bool tile_finish(double (&v)[NV], int tile, int sys, const Tiles &tl,
   return threadIdx.x == 0;
 }
 
-// ------------------------------------------------------------ CSR row chunks
-// Row sums of a chunk of nr <= 32 consecutive CSR rows starting at row q0 of (ptr, col, val):
-// lane l returns sum_k val[k] * x[col[k]] over row q0 + l (0 for l >= nr).  The chunk's entries
-// are one contiguous range; it is streamed with coalesced loads, U entries per lane in flight
-// (all column/value loads of a pass first, then all x gathers), the products are staged in the
-// warp's shared-memory slice sm[32 * U] and every lane sums its own row in index order, so the
-// result does not depend on the launch shape.  CG: read x through L2 only (x is written by
-// other CTAs of the same launch).
-template <typename V, typename T, int U, bool CG>
-__device__ __forceinline__ T chunk_rowsums(const int64_t *__restrict__ ptr, const int32_t *__restrict__ col, const V *__restrict__ val,
-                                           const T *x, int64_t q0, int nr, T *sm) {
+// ------------------------------------------------------------ SELL-32 rows
+// Lane `lane` of a warp sums row `lane` of one SELL-32 slice: sum_k val[off + 32 k + lane] *
+// x[col[off + 32 k + lane]] for k < width, in index order with FP64 fused multiply-adds, so the
+// result does not depend on the launch shape.  All column and value loads of a group of kU
+// entries are issued before their gathers of x.  Values and columns are read once per sweep
+// (streaming loads, evict-first); CG: x is written by other CTAs of the same launch and is
+// read through L2 only.
+template <typename V, bool CG, int kU>
+__device__ __forceinline__ double sell_rowsum(int64_t off, int width, const int32_t *__restrict__ col, const V *__restrict__ val,
+                                              const double *x) {
   const int lane = threadIdx.x & 31;
-  int64_t b = 0, e = 0;
-  if (lane < nr) { b = ptr[q0 + lane]; e = ptr[q0 + lane + 1]; }
-  const int64_t kb = __shfl_sync(0xffffffffu, b, 0);
-  const int64_t ke = __shfl_sync(0xffffffffu, e, nr - 1);
-  T sum = T(0);
-  for (int64_t pb = kb; pb < ke; pb += 32 * U) {
-    int32_t c[U];
-    T a[U];
+  const int32_t *c = col + off + lane;
+  const V *a = val + off + lane;
+  double sum = 0.0;
+  for (int k = 0; k < width; k += kU) {
+    // the width is the same for all lanes of the slice: the masks below are warp-uniform
+    int32_t cc[kU];
+    V aa[kU];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t k = pb + u * 32 + lane;
-      c[u] = 0; a[u] = T(0);
-      if (k < ke) { c[u] = col[k]; a[u] = (T)val[k]; }
+    for (int u = 0; u < kU; ++u) {
+      cc[u] = 0; aa[u] = V(0);
+      if (k + u < width) { cc[u] = __ldcs(c + 32 * u); aa[u] = __ldcs(a + 32 * u); }
+    }
+    double xx[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      xx[u] = 0.0;
+      if (k + u < width) xx[u] = CG ? __ldcg(x + cc[u]) : __ldg(x + cc[u]);
     }
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t k = pb + u * 32 + lane;
-      T xv = T(0);
-      if (k < ke) xv = CG ? __ldcg(&x[c[u]]) : x[c[u]];
-      sm[u * 32 + lane] = a[u] * xv;
-    }
-    __syncwarp();
-    const int64_t lo = b > pb ? b : pb;
-    const int64_t hi = e < pb + 32 * U ? e : pb + 32 * U;
-    for (int64_t k = lo; k < hi; ++k) sum += sm[k - pb];
-    __syncwarp();
+    for (int u = 0; u < kU; ++u)
+      if (k + u < width) sum = fma((double)aa[u], xx[u], sum);
+    c += 32 * kU; a += 32 * kU;
   }
   return sum;
 }
@@ -225,10 +221,9 @@ __global__ void __launch_bounds__(kThreads) k_update_p(const SysK *sys, BiState 
   }
 }
 
-// y = A x over one tile (32-row chunks per warp), fused dots.
+// y = A x over one tile (one SELL-32 slice per warp in turn), fused dots.
 // which = 0: v = A ph, (rh, v) -> alpha.   which = 1: t = A sh, (t, s), (t, t) -> omega.
-__global__ void __launch_bounds__(kThreads, 3) k_spmv_dot(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active, int which) {
-  __shared__ double sm[kWarps][32 * kSpmvU];
+__global__ void __launch_bounds__(kThreads, 4) k_spmv_dot(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active, int which) {
   const int tile = blockIdx.x;
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done) return;
@@ -240,10 +235,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_spmv_dot(const SysK *sys, BiSta
   const int64_t r0 = tl.tile_row0[tile], r1 = tl.tile_row1[tile];
   double acc[2] = {0.0, 0.0};
   for (int64_t q0 = r0 + 32 * w; q0 < r1; q0 += 32 * kWarps) {
-    const int nr = (int)(r1 - q0 < 32 ? r1 - q0 : 32);
-    const double y = chunk_rowsums<double, double, kSpmvU, false>(S.rp, S.ci, S.av, xin, q0, nr, sm[w]);
-    if (lane < nr) {
-      const int64_t row = q0 + lane;
+    const int64_t j = q0 >> 5, off = S.aoff[j];
+    const double y = sell_rowsum<double, false, kSpmvU>(off, (int)((S.aoff[j + 1] - off) >> 5), S.acol, S.aval, xin);
+    const int64_t row = q0 + lane;
+    if (row < r1) {
       yout[row] = y;
       if (which == 0) acc[0] += S.rh[row] * y;
       else { acc[0] += y * S.s[row]; acc[1] += y * y; }
@@ -382,14 +377,15 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
 }
 
 // ------------------------------------------------- triangular solves (ILU apply)
-// out = P^T U^{-1} L^{-1} P in over the level-ordered factors stored in precision P; the
-// arithmetic and the work vector ytmp are FP64 in both modes (in and out are FP64).  which 0: ph = M^{-1} p, 1: sh = M^{-1} s.  A level is a list of chunks
-// (system, first level-ordered position, row count <= 32); the warps of the grid take its
-// chunks in turn.  ytmp (permuted order) is written by other CTAs of the same launch and
-// read through L2 only.
+// out = U^{-1} L^{-1} in (solver order) over SELL-32 factor slices stored in precision P;
+// the arithmetic and the work vector ytmp are FP64 in both modes.  which 0: ph = M^{-1} p,
+// 1: sh = M^{-1} s.  A level is a list of (system, slice) entries; the warps of the grid take
+// them in turn, one slice per warp, one row per lane.  Forward slices are runs of consecutive
+// solver rows; backward slices list their rows through urow.  ytmp and out are written by
+// other CTAs of the same launch and read through L2 only.
 template <typename P>
 __device__ __forceinline__ void trsv_level_rows(const SysDev<P> *sys, const BiState *st, const int32_t *active, const Levels lv, int k,
-                                                bool lower, int which, double *sm) {
+                                                bool lower, int which) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
@@ -398,24 +394,25 @@ __device__ __forceinline__ void trsv_level_rows(const SysDev<P> *sys, const BiSt
     const int s = lv.ent_sys[c];
     if (!active[s] || st[s].done || (which == 1 && st[s].s_conv)) continue;
     const SysDev<P> &S = sys[s];
-    const int64_t q0 = lv.ent_row[c];
-    const int nr = lv.ent_cnt[c];
+    const int j = lv.ent_row[c];
     if (lower) {
-      const double sum = chunk_rowsums<P, double, kTrsvU, true>(S.lptr, S.lcol, S.lval, S.ytmp, q0, nr, sm);
+      const int64_t off = S.loff[j];
+      const int32_t q0 = S.lrow0[j], nr = S.lrow0[j + 1] - q0;
+      const double sum = sell_rowsum<P, true, kTrsvU>(off, (int)((S.loff[j + 1] - off) >> 5), S.lcol, S.lval, S.ytmp);
       if (lane < nr) {
         const int64_t q = q0 + lane;
         const double *in = which == 0 ? S.p : S.s;
-        S.ytmp[S.lrow[q]] = in[S.lgat[q]] - sum;
+        S.ytmp[q] = in[q] - sum;
       }
     } else {
-      const double sum = chunk_rowsums<P, double, kTrsvU, true>(S.uptr, S.ucol, S.uval, S.ytmp, q0, nr, sm);
+      double *out = which == 0 ? S.ph : S.sh;
+      const int64_t off = S.uoff[j];
+      const int32_t t0 = S.uslot0[j], nr = S.uslot0[j + 1] - t0;
+      const double sum = sell_rowsum<P, true, kTrsvU>(off, (int)((S.uoff[j + 1] - off) >> 5), S.ucol, S.uval, out);
       if (lane < nr) {
-        const int64_t q = q0 + lane;
-        const int32_t row = S.urow[q];
-        const double y = (__ldcg(&S.ytmp[row]) - sum) * (double)S.udinv[q];
-        S.ytmp[row] = y;
-        double *out = which == 0 ? S.ph : S.sh;
-        out[S.ugat[q]] = y;
+        const int64_t t = t0 + lane;
+        const int32_t row = S.urow[t];
+        out[row] = (__ldcg(&S.ytmp[row]) - sum) * (double)S.udinv[t];
       }
     }
   }
@@ -423,22 +420,19 @@ __device__ __forceinline__ void trsv_level_rows(const SysDev<P> *sys, const BiSt
 
 template <typename P>
 __global__ void __launch_bounds__(kThreads) k_trsv_persistent(const SysDev<P> *sys, const BiState *st, const int32_t *active, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err) {
-  __shared__ double sm[kWarps][32 * kTrsvU];
-  double *my = sm[threadIdx.x >> 5];
   for (int k = 0; k < lL.nlev; ++k) {
-    trsv_level_rows<P>(sys, st, active, lL, k, true, which, my);
+    trsv_level_rows<P>(sys, st, active, lL, k, true, which);
     if (!grid_barrier(bar, err)) return;
   }
   for (int k = 0; k < lU.nlev; ++k) {
-    trsv_level_rows<P>(sys, st, active, lU, k, false, which, my);
+    trsv_level_rows<P>(sys, st, active, lU, k, false, which);
     if (k + 1 < lU.nlev && !grid_barrier(bar, err)) return;
   }
 }
 
 template <typename P>
 __global__ void __launch_bounds__(kThreads) k_trsv_level(const SysDev<P> *sys, const BiState *st, const int32_t *active, Levels lv, int k, int lower, int which) {
-  __shared__ double sm[kWarps][32 * kTrsvU];
-  trsv_level_rows<P>(sys, st, active, lv, k, lower != 0, which, sm[threadIdx.x >> 5]);
+  trsv_level_rows<P>(sys, st, active, lv, k, lower != 0, which);
 }
 
 // ------------------------------------------------------ ILU(0) factorisation
@@ -455,7 +449,7 @@ __device__ __forceinline__ int64_t find_col(const int32_t *ci, int64_t a, int64_
   return -1;
 }
 
-// level entries here are permuted-space row ids (ent_row = row) of system ent_sys
+// level entries are solver rows ent_row[e] of system ent_sys[e] (row e of system 0 when NULL)
 __device__ void ilu0_level_rows(const FactDev *fs, Levels lv, int k, int32_t *err) {
   const int lane = threadIdx.x & 31;
   const int64_t gid = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
@@ -464,7 +458,7 @@ __device__ void ilu0_level_rows(const FactDev *fs, Levels lv, int k, int32_t *er
   for (int64_t e = e0 + gid; e < e1; e += nw) {
     const int s = lv.ent_sys ? lv.ent_sys[e] : 0;
     const FactDev F = fs[s];
-    const int64_t i = lv.ent_row[e];
+    const int64_t i = lv.ent_row ? lv.ent_row[e] : e;
     const int64_t a = F.rp[i], b = F.rp[i + 1], d = F.diag[i];
     const int32_t bi = F.blk[i];
     for (int64_t kp = a; kp < d; ++kp) {
@@ -500,15 +494,25 @@ __global__ void __launch_bounds__(kThreads) k_ilu0_level(const FactDev *fs, Leve
   ilu0_level_rows(fs, lv, k, err);
 }
 
-// permuted factor values from A: lu[kp] = av[amap[kp]]
-__global__ void k_gather_values(int64_t nnz, const int64_t *amap, const double *av, double *lu) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x)
-    lu[k] = av[amap[k]];
+// solver-order values from A: out[k] = av[amap[k]], 0 where amap[k] < 0 (SELL padding)
+__global__ void k_gather_values(int64_t nnz, const int64_t *amap, const double *av, double *out) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t m = amap[k];
+    out[k] = m >= 0 ? av[m] : 0.0;
+  }
 }
 
-// Split the permuted factor (FP64, permuted CSR) into level-ordered L, U and the
-// inverse diagonal in precision P: fmap[kp] >= 0 -> L slot, <= -2 -> U slot -(fmap+2),
-// -1 -> not part of the factor; dpos[row] is the U-level position of the row.
+// out[q] = in[perm[q]] (gather == 1) or out[perm[q]] = in[q] (gather == 0)
+__global__ void k_permute(int64_t n, const int32_t *perm, const double *in, double *out, int gather) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    if (gather) out[q] = in[perm[q]];
+    else out[perm[q]] = in[q];
+  }
+}
+
+// Split the solver-order factor (FP64 CSR) into the SELL-32 slices of L and U and the inverse
+// diagonal, in precision P: fmap[k] >= 0 -> L slot, <= -2 -> U slot -(fmap+2), -1 -> not part
+// of the factor; dpos[row] is the backward-sweep slot of the row.  Padding slots stay 0.
 template <typename P>
 __global__ void k_split_factor(int64_t nnz, int64_t n, const double *lu, const int64_t *fmap, const int64_t *diag, const int64_t *dpos,
                                P *lval, P *uval, P *udinv) {
@@ -522,9 +526,8 @@ __global__ void k_split_factor(int64_t nnz, int64_t n, const double *lu, const i
 }
 
 // ------------------------------------------------------- FP64 residual
-// r = b - A x (FP64), ||r||^2 and ||b||^2 per system -> rnorm2 / bnorm2.
-__global__ void __launch_bounds__(kThreads, 3) k_residual64(const RefDev *sys, Tiles tl, double *partials, int32_t *counters, const int32_t *active, double *rnorm2, double *bnorm2) {
-  __shared__ double sm[kWarps][32 * kSpmvU];
+// r = b - A x (FP64, solver order), ||r||^2 and ||b||^2 per system -> rnorm2 / bnorm2.
+__global__ void __launch_bounds__(kThreads, 4) k_residual64(const RefDev *sys, Tiles tl, double *partials, int32_t *counters, const int32_t *active, double *rnorm2, double *bnorm2) {
   const int tile = blockIdx.x;
   const int s = tl.tile_sys[tile];
   if (!active[s]) return;
@@ -533,10 +536,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_residual64(const RefDev *sys, T
   const int64_t r0 = tl.tile_row0[tile], r1 = tl.tile_row1[tile];
   double acc[2] = {0.0, 0.0};
   for (int64_t q0 = r0 + 32 * w; q0 < r1; q0 += 32 * kWarps) {
-    const int nr = (int)(r1 - q0 < 32 ? r1 - q0 : 32);
-    const double ax = chunk_rowsums<double, double, kSpmvU, false>(S.rp, S.ci, S.av, S.x, q0, nr, sm[w]);
-    if (lane < nr) {
-      const int64_t row = q0 + lane;
+    const int64_t j = q0 >> 5, off = S.aoff[j];
+    const double ax = sell_rowsum<double, false, kSpmvU>(off, (int)((S.aoff[j + 1] - off) >> 5), S.acol, S.aval, S.x);
+    const int64_t row = q0 + lane;
+    if (row < r1) {
       const double bb = S.b[row];
       const double r = bb - ax;
       S.r[row] = r;
@@ -551,15 +554,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_residual64(const RefDev *sys, T
   }
 }
 
-// plain SpMV for tests / timing (y = A x): the warps of the grid take 32-row chunks in turn
-__global__ void __launch_bounds__(kThreads, 3) k_spmv_plain(int64_t n, const int64_t *rp, const int32_t *ci, const double *av, const double *x, double *y) {
-  __shared__ double sm[kWarps][32 * kSpmvU];
+// plain SELL-32 SpMV for tests / timing (y = A x, solver order): one slice per warp in turn
+__global__ void __launch_bounds__(kThreads, 4) k_spmv_plain(int64_t n, const int64_t *aoff, const int32_t *acol, const double *aval, const double *x, double *y) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t gw = (int64_t)blockIdx.x * kWarps + w, nw = (int64_t)gridDim.x * kWarps;
-  for (int64_t q0 = 32 * gw; q0 < n; q0 += 32 * nw) {
-    const int nr = (int)(n - q0 < 32 ? n - q0 : 32);
-    const double v = chunk_rowsums<double, double, kSpmvU, false>(rp, ci, av, x, q0, nr, sm[w]);
-    if (lane < nr) y[q0 + lane] = v;
+  for (int64_t j = gw; 32 * j < n; j += nw) {
+    const int64_t off = aoff[j];
+    const double v = sell_rowsum<double, false, kSpmvU>(off, (int)((aoff[j + 1] - off) >> 5), acol, aval, x);
+    if (32 * j + lane < n) y[32 * j + lane] = v;
   }
 }
 
@@ -647,9 +649,14 @@ void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles 
 VK_BODY_P(float, f32)
 VK_BODY_P(double, f64)
 
-void vk_spmv_plain(int grid, int64_t n, const int64_t *rp, const int32_t *ci, const double *av, const double *x, double *y, cudaStream_t s) {
+void vk_spmv_plain(int grid, int64_t n, const int64_t *aoff, const int32_t *acol, const double *aval, const double *x, double *y, cudaStream_t s) {
   g_launches += 1;
-  k_spmv_plain<<<grid, kThreads, 0, s>>>(n, rp, ci, av, x, y);
+  k_spmv_plain<<<grid, kThreads, 0, s>>>(n, aoff, acol, aval, x, y);
+}
+
+void vk_permute(int64_t n, const int32_t *perm, const double *in, double *out, int gather, cudaStream_t s) {
+  g_launches += 1;
+  k_permute<<<grid_for(n), kThreads, 0, s>>>(n, perm, in, out, gather);
 }
 
 int vk_ilu0(int mode, int grid, const void *fs, const VkLevels *lv, unsigned *bar, int32_t *err, cudaStream_t s) {
@@ -669,9 +676,9 @@ int vk_ilu0_occupancy(int *blocks_per_sm) {
   return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, (void *)k_ilu0_persistent, kThreads, 0);
 }
 
-void vk_gather_values(int64_t nnz, const int64_t *amap, const double *av, double *lu, cudaStream_t s) {
+void vk_gather_values(int64_t nnz, const int64_t *amap, const double *av, double *out, cudaStream_t s) {
   g_launches += 1;
-  k_gather_values<<<grid_for(nnz), kThreads, 0, s>>>(nnz, amap, av, lu);
+  k_gather_values<<<grid_for(nnz), kThreads, 0, s>>>(nnz, amap, av, out);
 }
 
 size_t vk_factdev_size() { return sizeof(FactDev); }

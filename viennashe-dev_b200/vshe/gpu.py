@@ -70,6 +70,40 @@ def lib():
     return _lib
 
 
+def layout(rp, ci, **kw):
+    """The solver order and SELL-32 tables the library builds for this pattern and these
+    options (host only, no GPU): dict of numpy arrays, see vshe_layout_export."""
+    L = lib()
+    i64p = C.POINTER(C.c_int64)
+    i32p = C.POINTER(C.c_int32)
+    rp = np.ascontiguousarray(rp, np.int64)
+    ci = np.ascontiguousarray(ci, np.int32)
+    n = len(rp) - 1
+    nnz = int(rp[-1])
+    o, keep = make_opts(**kw)
+    sz = np.zeros(10, np.int64)
+    L.vshe_layout_sizes.argtypes = [C.c_int64, C.c_int64, i64p, i32p, C.POINTER(SolveOptsC), i64p]
+    rc = L.vshe_layout_sizes(n, nnz, ptr(rp, C.c_int64), ptr(ci, C.c_int32), C.byref(o), ptr(sz, C.c_int64))
+    if rc:
+        raise VsheError(rc, "vshe_layout_sizes")
+    nslA, padA, nslL, padL, nslU, padU, nlevL, nlevU, nnzL, nnzU = [int(v) for v in sz]
+    out = dict(perm=np.zeros(n, np.int32), lvr=np.zeros(nlevL + 1, np.int64), aoff=np.zeros(nslA + 1, np.int64),
+               acol=np.zeros(padA, np.int32), amap=np.zeros(padA, np.int64), lrow0=np.zeros(nslL + 1, np.int32),
+               loff=np.zeros(nslL + 1, np.int64), lcol=np.zeros(padL, np.int32), lmap=np.zeros(padL, np.int64),
+               uslot0=np.zeros(nslU + 1, np.int32), uoff=np.zeros(nslU + 1, np.int64), ucol=np.zeros(padU, np.int32),
+               umap=np.zeros(padU, np.int64), urow=np.zeros(n, np.int32))
+    order = ["perm", "lvr", "aoff", "acol", "amap", "lrow0", "loff", "lcol", "lmap", "uslot0", "uoff", "ucol", "umap", "urow"]
+    ct = {np.dtype(np.int32): C.c_int32, np.dtype(np.int64): C.c_int64}
+    L.vshe_layout_export.argtypes = [C.c_int64, C.c_int64, i64p, i32p, C.POINTER(SolveOptsC)] + \
+        [C.POINTER(ct[out[k].dtype]) for k in order]
+    rc = L.vshe_layout_export(n, nnz, ptr(rp, C.c_int64), ptr(ci, C.c_int32), C.byref(o),
+                              *[ptr(out[k], ct[out[k].dtype]) for k in order])
+    if rc:
+        raise VsheError(rc, "vshe_layout_export")
+    out.update(n=n, nlevL=nlevL, nlevU=nlevU, nnzL=nnzL, nnzU=nnzU)
+    return out
+
+
 def kernel_launches():
     """This library's own kernel launches in the process so far."""
     return int(lib().vshe_kernel_launches())
