@@ -42,6 +42,7 @@ extern "C" {
 #define VSHE_E_ZERO_PIVOT       -11   /* zero pivot in the incomplete factorisation */
 #define VSHE_E_NOT_FOUND        -12   /* unknown handle */
 #define VSHE_E_UNSUPPORTED      -13   /* option not available in this build */
+#define VSHE_E_CAPACITY         -14   /* size beyond a fixed capacity (vshe_csr_residual_noalloc) */
 
 /* ---- solver options ---- */
 #define VSHE_PRECISION_FP64   0   /* FP64 BiCGStab, FP64 ILU(0) factors and triangular solves */
@@ -153,6 +154,24 @@ int vshe_system_factor_values(vshe_ctx *ctx, int64_t handle, double *lu);
 /* Device-timed kernel throughput on a resident system: runs `reps` SpMVs in the
  * given precision (FP64 only) and returns the mean time per SpMV (ms) from CUDA events. */
 int vshe_system_time_spmv(vshe_ctx *ctx, int64_t handle, int32_t precision, int32_t reps, double *ms);
+
+/* ---- residual without device allocation ----
+ * No counterpart in the reference: an entry point for callers that cannot call cudaMalloc,
+ * because another component (a framework's caching allocator, a fixed arena) owns all device
+ * memory, or because the call sits in a loop where cudaMalloc/cudaFree would synchronise the
+ * device.  Computes r = b - A x and norms2[0] = ||r||^2, norms2[1] = ||b||^2 for an n x n CSR
+ * matrix (int64 row offsets, int32 columns, FP64 values); every pointer is a caller-owned
+ * DEVICE buffer (d_r of n doubles, d_norms2 of 2) on the current CUDA device.  The kernel is
+ * queued on `stream` (a cudaStream_t; NULL = the default stream) and the call returns without
+ * waiting.  Its scratch (one partial-sum pair per 2048 rows) is a fixed 512 KiB array in the
+ * library's device image, so n is limited to 64 Mi rows (67,108,864): larger n returns
+ * VSHE_E_CAPACITY.  The first call on each device looks up that array and clears it, so it
+ * synchronises the device once and should come before any stream capture.  All calls share
+ * the array: calls whose kernels overlap on the GPU (other streams or threads on the same
+ * device) race on it.  Nothing is allocated or freed by this call. */
+int vshe_csr_residual_noalloc(int64_t n, int64_t nnz, const int64_t *d_row_ptr, const int32_t *d_col,
+                              const double *d_val, const double *d_x, const double *d_b, double *d_r,
+                              double *d_norms2, void *stream);
 
 /* ---- host-only layout inspection (no GPU needed) ----
  * The solver order and the SELL-32 tables a resident system built from (A, opts) uses, for

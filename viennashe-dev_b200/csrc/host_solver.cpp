@@ -52,6 +52,7 @@ const char *errstr(int code) {
     case VSHE_E_ZERO_PIVOT: return "zero pivot in incomplete factorisation";
     case VSHE_E_NOT_FOUND: return "unknown handle";
     case VSHE_E_UNSUPPORTED: return "unsupported option";
+    case VSHE_E_CAPACITY: return "size exceeds the fixed scratch capacity of the no-allocation entry point";
   }
   return "unknown error";
 }
