@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="host time of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-serving", action="store_true", help="skip the batched-sweep and served-stream measurements")
+    ap.add_argument("--served-requests", type=int, default=24)
     ap.add_argument("--pass-only", action="store_true",
                     help="time only the device pass (no FP64 comparison, drop-in e2e or CPU baseline); for launch lists")
     return ap.parse_args()
@@ -232,6 +234,67 @@ def run_reference(args, D_):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------- batched sweep and served stream
+def measure_batched_sweep(ctx, reps=3):
+    """64 1D diodes from seed 11 (length 100-500 nm, 50-400 boxes, channel 1e21-1e23 m^-3,
+    L in {1, 3}, 0-1 V) assembled, solved as one batch and post-processed in one call
+    (vshe_she_run_batch: shared launches, per-system sweeps, graph-captured iteration chunks,
+    autotuned tiles), mixed precision to 1e-10, natural-order ILU(0)."""
+    from vshe import devices as D
+    from vshe import gpu
+    items = D.config3()
+    probs = [gpu.SheProblem(ctx, dev, cfg, precision="mixed", precond="ilu0", ordering="natural", tol=TOL,
+                            max_iters=20000, check_every=8) for dev, cfg in items]
+    try:
+        st, fr, _ = gpu.she_run_batch(ctx, probs)  # schedule, tile autotuning, graph capture
+        ms = []
+        for _ in range(reps):
+            st, fr, m = gpu.she_run_batch(ctx, probs)
+            ms.append(m)
+        med = float(np.median(ms))
+        n = [int(p.info["n_even"]) for p in probs]
+        return {"workload": "64 1D n+/n/n+ diodes, seed 11, L in {1,3}, 0-1 V", "systems": len(probs),
+                "unknowns_total": int(sum(n)), "unknowns_min": int(min(n)), "unknowns_max": int(max(n)),
+                "device_ms": med, "solves_per_s": len(probs) / (med / 1000.0),
+                "iterations_max": int(max(x["iterations"] for x in st)),
+                "all_converged": bool(all(x["status"] == 0 and x["rel_residual"] < TOL for x in st)),
+                "max_full_residual": float(np.max(fr))}
+    finally:
+        for p in probs:
+            p.free()
+
+
+def measure_served_stream(ctx, count=24, rate=200.0):
+    """Served stream: `count` requests arriving as a Poisson process at `rate` req/s (seed 23),
+    70 % 1D diodes / 30 % 2D bars (vshe/devices.config4), submitted at their arrival times to a
+    continuous-batching server under a 150 GB HBM budget; latency = submission -> result."""
+    from vshe import devices as D
+    from vshe import gpu
+    items = D.config4(count, rate=rate)
+    cpl = {L: gpu.coupling_tables(L) for L in (1, 3, 5)}
+    srv = gpu.Server(ctx, hbm_budget=150 * 10 ** 9, precision="mixed", precond="ilu0", tol=TOL, max_iters=20000, check_every=8)
+    try:
+        t0 = time.perf_counter()
+        tickets = []
+        for ta, dev, cfg in items:
+            now = time.perf_counter() - t0
+            if ta > now:
+                time.sleep(ta - now)
+            kw = dict(ordering="natural") if dev.dim == 1 else dict(ordering="multicolor", precond="block_ilu0")
+            tickets.append(srv.submit(dev, cfg, coupling=cpl[cfg.max_expansion_order], **kw))
+        res = [srv.wait(t)[0] for t in tickets]
+        wall = time.perf_counter() - t0
+    finally:
+        srv.close()
+    lat = np.array([r["latency_ms"] for r in res])
+    return {"workload": "Poisson arrivals at %g req/s, seed 23: 70%% 1D diodes, 30%% 2D bars (50-200 x 20-50, L 1/3/5, 60-160 energies)" % rate,
+            "requests": count, "unknowns_total": int(sum(r["n_unknowns"] for r in res)),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "throughput_solves_per_s": count / wall, "wall_s": wall,
+            "all_converged": bool(all(r["status"] == 0 and r["rel_residual"] < TOL for r in res)),
+            "iterations_max": int(max(r["iterations"] for r in res))}
+
+
 # ----------------------------------------------------------------- our arm
 def run_ours(args, D_):
     from vshe import gpu
@@ -332,6 +395,15 @@ def run_ours(args, D_):
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_source": peak_src,
                 "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                 "algorithmic_bytes_per_launch": dbytes, "avg_launch_ms": avg_ms}
+    extra = {}
+    if D_.rank == 0 and not args.no_serving:
+        extra["batched_sweep"] = measure_batched_sweep(ctx)
+        extra["served_stream"] = measure_served_stream(ctx, count=args.served_requests)
+    try:
+        tile_rows, tile_ms = ctx.autotune_info(n)
+        extra["autotune"] = {"tile_rows": tile_rows, "spmv_ms_by_tile_rows": dict(zip(["512", "1024", "2048", "4096"], [float(x) for x in tile_ms]))}
+    except Exception:
+        pass
     cpu = None
     if D_.rank == 0 and not args.no_cpu:
         st_ref = reference_iterations(ctx, rp, ci, v, b)
@@ -355,6 +427,7 @@ def run_ours(args, D_):
             "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline,
             "cpu_baseline": cpu, "clocks": clocks, "wall_s_timed": wall,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     P.free()
     ctx.close()

@@ -63,6 +63,8 @@ extern "C" {
 #define VSHE_TRSV_AUTO        0
 #define VSHE_TRSV_PERSISTENT  1   /* one cooperative launch per triangular solve, grid barrier per level */
 #define VSHE_TRSV_PER_LEVEL   2   /* one launch per level */
+#define VSHE_TRSV_PER_SYSTEM  3   /* one CTA per system walks the system's levels (CTA barrier per level);
+                                     AUTO picks it for systems with many short levels (1D devices) */
 
 typedef struct vshe_solve_opts {
   int32_t precision;        /* VSHE_PRECISION_* */
@@ -115,6 +117,11 @@ size_t vshe_bytes_in_use(vshe_ctx *ctx);
  * [4] factorisation, and counts[0] SpMV launches, counts[1] triangular-solve launches. */
 int vshe_set_profiling(vshe_ctx *ctx, int32_t on);
 int vshe_get_profile(vshe_ctx *ctx, double *ms, int64_t *counts);
+/* Autotuner record: the rows per reduction tile chosen for systems of n's size class
+ * (floor(log2 n)) on this context, and ms[0..3] = the timed FP64 SpMV for 512, 1024, 2048 and
+ * 4096-row tiles.  VSHE_E_NOT_FOUND until a system of that class was solved.  No reference
+ * counterpart: instrumentation of the tile autotuner. */
+int vshe_autotune_info(vshe_ctx *ctx, int64_t n, int64_t *tile_rows, double *ms);
 /* Number of this library's own kernel launches in the process so far (all
  * contexts; library kernels such as CUB scans are not counted).  No reference
  * counterpart: instrumentation. */
@@ -254,6 +261,47 @@ int vshe_she_export(vshe_ctx *ctx, int64_t handle, int32_t which, int64_t *row_p
 /* Unknown scaling s and column scale factors of the reduced system (length n_even). */
 int vshe_she_scaling(vshe_ctx *ctx, int64_t handle, double *scaling, double *scale_factors);
 int vshe_she_free(vshe_ctx *ctx, int64_t handle);
+
+/* ---- served stream: continuous batching of SHE solves ----
+ * No reference counterpart: the reference solves one device at a time (simulator::run).  A
+ * server owns a worker thread that admits submitted requests in arrival order while the device
+ * memory of its resident problems stays within hbm_budget and at most max_active are resident,
+ * iterates all resident problems together (one batch, chunks of check_every iterations), and
+ * retires each one as soon as it converges, its place taken by the next request.  A served
+ * result equals the result of the same request solved alone (per-system reductions in a fixed
+ * order).  The server makes its GPU calls on ctx under ctx's lock; other calls on the same
+ * context interleave with it step by step.  Every request shares the precision and the
+ * preconditioner kind of opts->solve (and its tol, max_iters, check_every); the ordering and
+ * the preconditioner variant may differ per request. */
+typedef struct vshe_server vshe_server;
+typedef struct vshe_server_opts {
+  size_t  hbm_budget;       /* bytes the resident problems may hold (0: the context's budget) */
+  int32_t max_active;       /* resident problems at most (0: 256) */
+  vshe_solve_opts solve;    /* default solver options of a request */
+} vshe_server_opts;
+typedef struct vshe_server_result {
+  int32_t status;           /* VSHE_OK or the error of this request */
+  int32_t iterations;
+  int32_t refinements;      /* residual replacements */
+  double  rel_residual;     /* FP64 relative residual of the reduced system */
+  double  full_residual;    /* relative residual of the full (even + odd) system */
+  double  queue_ms;         /* submission -> admission (host clock) */
+  double  latency_ms;       /* submission -> result ready (host clock) */
+  int64_t n_unknowns;       /* reduced-system size */
+} vshe_server_result;
+
+int vshe_server_create(vshe_ctx *ctx, const vshe_server_opts *opts, vshe_server **server);
+/* Queues one solve: the arrays of dev, cfg and coupling are copied, so they may be released
+ * on return.  opts may be NULL (the server's defaults).  *ticket identifies the request. */
+int vshe_server_submit(vshe_server *server, const vshe_device_desc *dev, const vshe_she_config *cfg,
+                       const vshe_coupling_tables *coupling, const vshe_solve_opts *opts, int64_t *ticket);
+/* Waits for a request (timeout_ms < 0: without limit; VSHE_E_TIMEOUT if it is not done in
+ * time) and copies its result, densities (n_cells) and terminal currents (one per contact);
+ * any pointer may be NULL.  Returns the request's status and forgets the ticket. */
+int vshe_server_wait(vshe_server *server, int64_t ticket, double timeout_ms, vshe_server_result *result,
+                     double *density, double *currents);
+/* Finishes the resident requests, drops the queued ones and joins the worker. */
+int vshe_server_destroy(vshe_server *server);
 
 #ifdef __cplusplus
 }

@@ -81,10 +81,11 @@ struct System {
   double *d_lu64 = nullptr;
   // SELL factors
   int32_t *d_lrow0 = nullptr, *d_uslot0 = nullptr, *d_urow = nullptr, *d_lcol = nullptr, *d_ucol = nullptr;
-  int64_t *d_loff = nullptr, *d_uoff = nullptr;
+  int64_t *d_loff = nullptr, *d_uoff = nullptr, *d_lvsL = nullptr, *d_lvsU = nullptr;
   void *d_lval = nullptr, *d_uval = nullptr, *d_udinv = nullptr;
   double *d_ytmp = nullptr;
   void *kv[9] = {nullptr};  // x r rh p v s t ph sh (FP64, solver order, n + 1 entries; entry n stays 0)
+  int64_t tile_rows = 0;    // rows per reduction tile (0: not chosen yet; see Batch::autotune_tiles)
 
   int create(Ctx &ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *v,
              const double *rhs, const vshe_solve_opts &o);
@@ -106,8 +107,23 @@ struct Batch {
   int nsys = 0;
   bool mixed = true, has_pc = true;
   int ntiles = 0;
-  int32_t nlevL = 0, nlevU = 0;
+  int32_t nlevL = 0, nlevU = 0;   // merged levels of the grid-wide sweeps
+  int32_t nlevF = 0;              // merged levels of the factorisation (all members)
   int trsv_grid = 148, ilu_grid = 148, num_sms = 148;
+  // members whose triangular sweeps run one CTA per system (k_trsv_cta); the others share the
+  // merged level schedule of the grid-wide sweep
+  std::vector<int32_t> cta_members;
+  int32_t *d_cta_members = nullptr;
+  bool grid_group = true;
+  // the BiCGStab iteration chunk (check_every iterations) captured once as a CUDA graph and
+  // replayed; graph_failed: capture was refused (then the chunk is launched directly)
+  cudaGraphExec_t chunk_exec = nullptr;
+  int chunk_every = 0;
+  long long chunk_launches = 0;
+  bool graph_failed = false;
+  ~Batch() { if (chunk_exec) cudaGraphExecDestroy(chunk_exec); }
+  // row tiles: every member's own tile_rows rows per tile, rebuilt by set_tiles
+  DevArena tile_arena;
   DevArena arena;
   int32_t *d_tile_sys = nullptr, *d_sys_tile0 = nullptr, *d_active = nullptr, *d_counters = nullptr, *d_err = nullptr;
   int64_t *d_tile_r0 = nullptr, *d_tile_r1 = nullptr;
@@ -129,8 +145,16 @@ struct Batch {
   int64_t n_spmv = 0, n_trsv = 0;
 
   int build(Ctx &ctx, const std::vector<System *> &members);
+  // only_member >= 0: tiles of that member alone, with `rows` rows (the autotuner's trial tiles)
+  int set_tiles(Ctx &ctx, int only_member = -1, int64_t rows = 0);
+  int autotune_tiles(Ctx &ctx);
   int factor(Ctx &ctx);
   int bicgstab(Ctx &ctx, double tol, int max_iter, bool resume, int &iters_out);
+  int start(Ctx &ctx, double tol, int max_iter, bool resume);
+  int run_chunk(Ctx &ctx, int every);
+  int read_states(Ctx &ctx, std::vector<char> &out);
+  int write_states(Ctx &ctx, const std::vector<char> &in);
+  std::vector<int32_t> act_host;  // host copy of the active flags
   int residual(Ctx &ctx, std::vector<double> &rel);
   int set_active(Ctx &ctx, const std::vector<int32_t> &act);
   int solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats);
@@ -151,6 +175,11 @@ struct Ctx {
   // kernel-class timings of the last profiled solve (ms): spmv, trsv, vector, reliable, factor
   double prof[5] = {0, 0, 0, 0, 0};
   int64_t prof_counts[2] = {0, 0};
+  // autotuned rows per reduction tile, per system size class (floor(log2 n)); the first system
+  // of a class is timed, later ones reuse the choice, so a system's reduction order (and its
+  // iterates) does not depend on the batch it is solved in
+  std::map<int, int64_t> tile_choice;
+  std::map<int, std::vector<double>> tile_timings;  // ms per SpMV for 512, 1024, 2048, 4096 rows
   int fail(int code, const std::string &msg);
   int cuda_fail(cudaError_t e, const char *what);
 };

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -470,6 +471,8 @@ int System::setup_pattern(Ctx &ctx) {
     ALLOC(d_uslot0, int32_t, nslU + 1);
     ALLOC(d_uoff, int64_t, nslU + 1);
     ALLOC(d_urow, int32_t, n);
+    ALLOC(d_lvsL, int64_t, lvsL.size());
+    ALLOC(d_lvsU, int64_t, lvsU.size());
     ALLOC(d_lcol, int32_t, std::max<int64_t>(padL, 1));
     ALLOC(d_ucol, int32_t, std::max<int64_t>(padU, 1));
     ALLOCT(d_lval, std::max<int64_t>(padL, 1));
@@ -507,6 +510,8 @@ int System::setup_pattern(Ctx &ctx) {
     H2D(d_uslot0, uslot0);
     H2D(d_uoff, uoff);
     H2D(d_urow, urow);
+    H2D(d_lvsL, lvsL);
+    H2D(d_lvsU, lvsU);
     H2D(d_lcol, lcol);
     H2D(d_ucol, ucol);
     if ((e = cudaMemsetAsync(d_lval, 0, tsz * size_t(std::max<int64_t>(padL, 1)), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
@@ -529,6 +534,7 @@ void System::fill_sysdev(void *out) const {
   d.uslot0 = d_uslot0; d.uoff = d_uoff; d.ucol = d_ucol; d.uval = (const float *)d_uval; d.udinv = (const float *)d_udinv;
   d.urow = d_urow;
   d.ytmp = d_ytmp;
+  d.lvsL = d_lvsL; d.lvsU = d_lvsU; d.nlevL = nlevL; d.nlevU = nlevU;
   d.x = (double *)kv[0]; d.r = (double *)kv[1]; d.rh = (double *)kv[2]; d.p = (double *)kv[3];
   d.v = (double *)kv[4]; d.s = (double *)kv[5]; d.t = (double *)kv[6]; d.ph = (double *)kv[7]; d.sh = (double *)kv[8];
   std::memcpy(out, &d, sizeof(d));
@@ -543,29 +549,35 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   for (System *S : sys)
     if (S->mixed != mixed || S->has_pc != has_pc)
       return ctx.fail(VSHE_E_INVALID_ARGUMENT, "systems in one batch need the same precision and preconditioner kind");
-  const int64_t TILE = 2048;
-  std::vector<int32_t> tsys, st0;
-  std::vector<int64_t> tr0, tr1;
-  for (int s = 0; s < nsys; ++s) {
-    st0.push_back(int32_t(tsys.size()));
-    for (int64_t a = 0; a < sys[s]->n; a += TILE) {
-      tsys.push_back(s);
-      tr0.push_back(a);
-      tr1.push_back(std::min(a + TILE, sys[s]->n));
+  // Triangular sweeps.  A member with many short levels (fewer than kCtaRowsPerLevel rows per
+  // forward level on average, and more than kCtaMinLevels levels: 1D devices) sweeps on its own
+  // CTA with a CTA barrier per level; VSHE_TRSV_PER_SYSTEM forces that for every member.  The
+  // others share a merged schedule: merged level l lists, system by system, the level-l SELL
+  // slices of every grid-swept member.
+  constexpr int64_t kCtaRowsPerLevel = 4096;
+  constexpr int32_t kCtaMinLevels = 32;
+  std::vector<char> on_cta((size_t)nsys, 0);
+  cta_members.clear();
+  if (has_pc) {
+    for (int k = 0; k < nsys; ++k) {
+      const System *S = sys[size_t(k)];
+      const int mode = S->opts.trsv_mode;
+      const bool want = mode == VSHE_TRSV_PER_SYSTEM ||
+                        (mode == VSHE_TRSV_AUTO && S->nlevL > kCtaMinLevels && S->n / std::max(S->nlevL, 1) < kCtaRowsPerLevel);
+      if (want) { on_cta[size_t(k)] = 1; cta_members.push_back(k); }
     }
   }
-  st0.push_back(int32_t(tsys.size()));
-  ntiles = int(tsys.size());
-  // Triangular-solve schedules: merged level l lists, system by system, the level-l SELL
-  // slices of every member.
+  grid_group = int(cta_members.size()) < nsys;
   std::vector<int64_t> cptrL, cptrU, fptr;
   std::vector<int32_t> csL, cqL, csU, cqU, fsys, frow;
   auto slices = [&](bool lower, std::vector<int64_t> &cptr, std::vector<int32_t> &cs, std::vector<int32_t> &cq, int32_t &nl) {
     nl = 0;
-    for (System *S : sys) nl = std::max(nl, lower ? S->nlevL : S->nlevU);
+    for (int k = 0; k < nsys; ++k)
+      if (!on_cta[size_t(k)]) nl = std::max(nl, lower ? sys[size_t(k)]->nlevL : sys[size_t(k)]->nlevU);
     cptr.assign(1, 0);
     for (int32_t l = 0; l < nl; ++l) {
       for (int k = 0; k < nsys; ++k) {
+        if (on_cta[size_t(k)]) continue;
         const auto &vp = lower ? sys[size_t(k)]->lvsL : sys[size_t(k)]->lvsU;
         if (l + 1 >= int32_t(vp.size())) continue;
         for (int64_t j = vp[size_t(l)]; j < vp[size_t(l) + 1]; ++j) {
@@ -579,10 +591,13 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   if (has_pc) {
     slices(true, cptrL, csL, cqL, nlevL);
     slices(false, cptrU, csU, cqU, nlevU);
+    // factorisation: merged level l = the forward-level-l rows of every member (all members,
+    // whichever sweep they use)
+    nlevF = 0;
+    for (System *S : sys) nlevF = std::max(nlevF, S->nlevL);
     if (nsys > 1) {
-      // factorisation: merged level l = the forward-level-l rows of every member
       fptr.assign(1, 0);
-      for (int32_t l = 0; l < nlevL; ++l) {
+      for (int32_t l = 0; l < nlevF; ++l) {
         for (int k = 0; k < nsys; ++k) {
           const System *S = sys[size_t(k)];
           if (l + 1 >= int32_t(S->lvr.size())) continue;
@@ -599,17 +614,13 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
 #define ALLOC(ptr, type, count)                                              \
   ptr = (type *)arena.alloc(sizeof(type) * size_t(count), e);               \
   if (!ptr) return ctx.cuda_fail(e, "cudaMalloc batch " #ptr);
-  ALLOC(d_tile_sys, int32_t, ntiles);
-  ALLOC(d_tile_r0, int64_t, ntiles);
-  ALLOC(d_tile_r1, int64_t, ntiles);
-  ALLOC(d_sys_tile0, int32_t, nsys + 1);
   ALLOC(d_active, int32_t, nsys);
   ALLOC(d_counters, int32_t, nsys);
-  ALLOC(d_partials, double, size_t(ntiles) * 3);
   ALLOC(d_bar, unsigned, 2);
   ALLOC(d_err, int32_t, 1);
   ALLOC(d_rnorm2, double, nsys);
   ALLOC(d_bnorm2, double, nsys);
+  ALLOC(d_cta_members, int32_t, std::max<size_t>(cta_members.size(), 1));
   d_sysdev = arena.alloc(vk_sysdev_size() * size_t(nsys), e);
   if (!d_sysdev) return ctx.cuda_fail(e, "cudaMalloc sysdev");
   d_state = arena.alloc(vk_bistate_size() * size_t(nsys), e);
@@ -649,15 +660,12 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
 #define H2D(dst, src, bytes)                                                             \
   if ((e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) \
     return ctx.cuda_fail(e, "upload batch " #dst);
-  H2D(d_tile_sys, tsys.data(), sizeof(int32_t) * tsys.size());
-  H2D(d_tile_r0, tr0.data(), sizeof(int64_t) * tr0.size());
-  H2D(d_tile_r1, tr1.data(), sizeof(int64_t) * tr1.size());
-  H2D(d_sys_tile0, st0.data(), sizeof(int32_t) * st0.size());
   H2D(d_active, ones.data(), sizeof(int32_t) * size_t(nsys));
   H2D(d_counters, zeros.data(), sizeof(int32_t) * size_t(nsys));
   H2D(d_sysdev, sd.data(), sd.size());
   H2D(d_refdev, rd.data(), rd.size());
   H2D(d_factdev, fd.data(), fd.size());
+  if (!cta_members.empty()) { H2D(d_cta_members, cta_members.data(), sizeof(int32_t) * cta_members.size()); }
   if (has_pc) {
     H2D(d_cptrL, cptrL.data(), sizeof(int64_t) * cptrL.size());
     H2D(d_cptrU, cptrU.data(), sizeof(int64_t) * cptrU.size());
@@ -681,12 +689,11 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   if ((e = cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   if ((e = cudaMemsetAsync(d_err, 0, sizeof(int32_t), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   if ((e = cudaMemsetAsync(d_state, 0, vk_bistate_size() * size_t(nsys), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
-  tiles = VkTiles{ntiles, d_tile_sys, d_tile_r0, d_tile_r1, d_sys_tile0};
   if (has_pc) {
     levL = VkLevels{nlevL, d_cptrL, d_csL, d_cqL, nullptr};
     levU = VkLevels{nlevU, d_cptrU, d_csU, d_cqU, nullptr};
-    if (nsys > 1) levF = VkLevels{nlevL, d_fptr, d_fsys, d_frow, nullptr};
-    else levF = VkLevels{nlevL, sys[0]->d_lvr, nullptr, nullptr, nullptr};
+    if (nsys > 1) levF = VkLevels{nlevF, d_fptr, d_fsys, d_frow, nullptr};
+    else levF = VkLevels{nlevF, sys[0]->d_lvr, nullptr, nullptr, nullptr};
   }
   int dev = 0;
   cudaGetDevice(&dev);
@@ -699,7 +706,97 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   ilu_grid = std::max(1, std::min(bpf, 4)) * num_sms;
   cudaError_t es = cudaStreamSynchronize(s);
   if (es != cudaSuccess) return ctx.cuda_fail(es, "batch upload");
+  return set_tiles(ctx);
+}
+
+// Row tiles (whole SELL slices: multiples of 32 rows) that never straddle two systems; the tile
+// kernels run one CTA per tile and reduce per tile.  Member k uses its own tile_rows (2048 until
+// tuned); only_member >= 0 builds tiles of `rows` rows for that member alone (autotuner trials).
+int Batch::set_tiles(Ctx &ctx, int only_member, int64_t rows) {
+  std::vector<int32_t> tsys, st0;
+  std::vector<int64_t> tr0, tr1;
+  for (int k = 0; k < nsys; ++k) {
+    st0.push_back(int32_t(tsys.size()));
+    if (only_member >= 0 && k != only_member) continue;
+    const int64_t tr = only_member >= 0 ? rows : (sys[size_t(k)]->tile_rows > 0 ? sys[size_t(k)]->tile_rows : 2048);
+    for (int64_t a = 0; a < sys[size_t(k)]->n; a += tr) {
+      tsys.push_back(k);
+      tr0.push_back(a);
+      tr1.push_back(std::min(a + tr, sys[size_t(k)]->n));
+    }
+  }
+  st0.push_back(int32_t(tsys.size()));
+  cudaError_t e;
+  cudaStream_t s = ctx.stream;
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx.cuda_fail(e, "tiles");  // old tiles no longer in use
+  tile_arena.release();
+  ntiles = int(tsys.size());
+#define ALLOC(ptr, type, count)                                              \
+  ptr = (type *)tile_arena.alloc(sizeof(type) * size_t(count), e);          \
+  if (!ptr) return ctx.cuda_fail(e, "cudaMalloc tiles " #ptr);
+  ALLOC(d_tile_sys, int32_t, ntiles);
+  ALLOC(d_tile_r0, int64_t, ntiles);
+  ALLOC(d_tile_r1, int64_t, ntiles);
+  ALLOC(d_sys_tile0, int32_t, nsys + 1);
+  ALLOC(d_partials, double, size_t(ntiles) * 3);
+#undef ALLOC
+#define H2D(dst, src, bytes)                                                             \
+  if ((e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) \
+    return ctx.cuda_fail(e, "upload tiles " #dst);
+  H2D(d_tile_sys, tsys.data(), sizeof(int32_t) * tsys.size());
+  H2D(d_tile_r0, tr0.data(), sizeof(int64_t) * tr0.size());
+  H2D(d_tile_r1, tr1.data(), sizeof(int64_t) * tr1.size());
+  H2D(d_sys_tile0, st0.data(), sizeof(int32_t) * st0.size());
+#undef H2D
+  tiles = VkTiles{ntiles, d_tile_sys, d_tile_r0, d_tile_r1, d_sys_tile0};
+  if (chunk_exec) { cudaGraphExecDestroy(chunk_exec); chunk_exec = nullptr; }  // the graph holds the old tiles
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx.cuda_fail(e, "tiles");
   return VSHE_OK;
+}
+
+// Autotuner of the row-tile size.  For a member whose size class (floor(log2 n)) has no choice
+// in the context yet, it times the FP64 SELL SpMV with its fused tile reduction (the residual
+// kernel, the same structure as the SpMV of every BiCGStab step) on that member alone for each
+// candidate, with CUDA events, and records the fastest for the class.  Runs before a solve (the
+// residual it writes is overwritten by the solve).
+int Batch::autotune_tiles(Ctx &ctx) {
+  static const int64_t cand[] = {512, 1024, 2048, 4096};
+  bool changed = false;
+  for (int k = 0; k < nsys; ++k) {
+    System *S = sys[size_t(k)];
+    if (S->tile_rows > 0) continue;
+    int cls = 0;
+    while ((int64_t(1) << (cls + 1)) <= S->n) ++cls;
+    auto it = ctx.tile_choice.find(cls);
+    if (it == ctx.tile_choice.end()) {
+      cudaStream_t s = ctx.stream;
+      cudaEvent_t a, b;
+      cudaEventCreate(&a); cudaEventCreate(&b);
+      double best = 1e30;
+      int64_t best_rows = 2048;
+      std::vector<double> t;
+      for (int64_t rows : cand) {
+        int rc = set_tiles(ctx, k, rows);
+        if (rc) { cudaEventDestroy(a); cudaEventDestroy(b); return rc; }
+        vk_residual64(ntiles, d_refdev, &tiles, d_partials, d_counters, d_active, d_rnorm2, d_bnorm2, s);  // warm-up
+        cudaEventRecord(a, s);
+        for (int r = 0; r < 5; ++r) vk_residual64(ntiles, d_refdev, &tiles, d_partials, d_counters, d_active, d_rnorm2, d_bnorm2, s);
+        cudaEventRecord(b, s);
+        cudaError_t e = cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (e != cudaSuccess) { cudaEventDestroy(a); cudaEventDestroy(b); return ctx.cuda_fail(e, "autotune"); }
+        t.push_back(ms / 5.0);
+        if (ms < best) { best = ms; best_rows = rows; }
+      }
+      cudaEventDestroy(a); cudaEventDestroy(b);
+      it = ctx.tile_choice.emplace(cls, best_rows).first;
+      ctx.tile_timings[cls] = t;
+    }
+    S->tile_rows = it->second;
+    changed = true;
+  }
+  return changed ? set_tiles(ctx) : VSHE_OK;
 }
 
 int Batch::check_err(Ctx &ctx, const char *what) {
@@ -770,36 +867,72 @@ static thread_local EventProf g_prof;
 // BiCGStab (FP64) on every active system to relative tolerance `tol`; the ILU(0) apply runs
 // in the factor precision.  resume = true continues after a residual replacement (r holds
 // b - A x).  Iteration chunks of `check_every` run without host synchronisation.
-int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, bool resume, int &iters_out) {
+// Sets the iteration parameters of the active members and (re)starts their recurrences:
+// resume = false: x = 0, r = b (k_bicg_init); true: r already holds b - A x (k_bicg_resume).
+int Batch::start(Ctx &ctx, double tol, int max_iter, bool resume) {
   cudaStream_t s = ctx.stream;
-  const int every = sys[0]->opts.check_every > 0 ? sys[0]->opts.check_every : 8;
-  const int mode = (sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) ? 2 : 1;
-  const int lvl_grid = mode == 1 ? trsv_grid : std::max(1, num_sms * 8);
+  if (sys[0]->opts.trsv_mode < VSHE_TRSV_AUTO || sys[0]->opts.trsv_mode > VSHE_TRSV_PER_SYSTEM)
+    return ctx.fail(VSHE_E_INVALID_ARGUMENT, "trsv_mode");
   const size_t bsz = vk_bistate_size();
-  std::vector<char> stbuf(bsz * size_t(nsys), 0);
-  cudaError_t e = cudaMemcpyAsync(stbuf.data(), d_state, stbuf.size(), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return ctx.cuda_fail(e, "read state");
+  std::vector<char> stbuf;
+  int rc = read_states(ctx, stbuf);
+  if (rc) return rc;
   for (int k = 0; k < nsys; ++k) {
+    if (!act_host.empty() && !act_host[size_t(k)]) continue;
     BiState *b = (BiState *)(stbuf.data() + bsz * size_t(k));
     b->tol = tol; b->max_iter = max_iter;
     b->shadow_r0 = sys[size_t(k)]->opts.shadow == VSHE_SHADOW_R0 ? 1 : 0;
     if (!resume) { b->done = 0; b->iter = 0; }
   }
+  cudaError_t e;
   if ((e = cudaMemcpyAsync(d_state, stbuf.data(), stbuf.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess) return ctx.cuda_fail(e, "write state");
-  EventProf &P = g_prof;
-  P.on = profile; P.s = s;
   if (resume) vk_bicg_resume(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s);
   else vk_bicg_init(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s);
+  return VSHE_OK;
+}
+
+int Batch::read_states(Ctx &ctx, std::vector<char> &out) {
+  out.assign(vk_bistate_size() * size_t(nsys), 0);
+  cudaError_t e = cudaMemcpyAsync(out.data(), d_state, out.size(), cudaMemcpyDeviceToHost, ctx.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+  if (e != cudaSuccess) return ctx.cuda_fail(e, "read state");
+  return VSHE_OK;
+}
+
+int Batch::write_states(Ctx &ctx, const std::vector<char> &in) {
+  cudaError_t e = cudaMemcpyAsync(d_state, in.data(), std::min(in.size(), vk_bistate_size() * size_t(nsys)), cudaMemcpyHostToDevice, ctx.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+  if (e != cudaSuccess) return ctx.cuda_fail(e, "write state");
+  return VSHE_OK;
+}
+
+// One chunk of `every` BiCGStab iterations of every active, unfinished member: 7 launches per
+// iteration (update_p, forward/backward sweeps, SpMV + dots, update_s, sweeps, SpMV + dots,
+// update_xr), no host synchronisation.  The chunk is captured once into a CUDA graph (every
+// kernel reads its scalars from the device-resident state, so one graph serves every chunk) and
+// replayed; under profiling, or if the driver refuses the capture, it is launched directly.
+int Batch::run_chunk(Ctx &ctx, int every) {
+  cudaStream_t s = ctx.stream;
+  const int mode = (sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) ? 2 : 1;
+  const int lvl_grid = mode == 1 ? trsv_grid : std::max(1, num_sms * 8);
+  EventProf &P = g_prof;
+  P.on = profile; P.s = s;
   auto trsv = [&](int which) -> int {
     if (!has_pc) { vk_precond_copy(ntiles, d_sysdev, d_state, &tiles, d_active, which, s); return 0; }
+    int rc = 0;
+    const int ncta = int(cta_members.size());
+    if (ncta) {
+      rc = mixed ? vk_trsv_cta_f32(ncta, d_sysdev, d_state, d_active, d_cta_members, which, s)
+                 : vk_trsv_cta_f64(ncta, d_sysdev, d_state, d_active, d_cta_members, which, s);
+      if (rc) return rc;
+    }
+    if (!grid_group) return 0;
     if (mixed) return vk_trsv_f32(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, which, d_bar, d_err, s);
     return vk_trsv_f64(mode, lvl_grid, d_sysdev, d_state, d_active, &levL, &levU, which, d_bar, d_err, s);
   };
-  int done_iters = 0;
-  while (true) {
+  auto chunk = [&]() -> int {
+    int rc = 0;
     for (int it = 0; it < every; ++it) {
-      int rc = 0;
       cudaEvent_t a;
       a = P.begin(); vk_update_p(ntiles, d_sysdev, d_state, &tiles, d_active, s); P.end(2, a);
       a = P.begin(); rc |= trsv(0); P.end(1, a);
@@ -808,12 +941,54 @@ int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, bool resume, int &iters_
       a = P.begin(); rc |= trsv(1); P.end(1, a);
       a = P.begin(); vk_spmv_dot(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, 1, s); P.end(0, a);
       a = P.begin(); vk_update_xr(ntiles, d_sysdev, d_state, &tiles, d_partials, d_counters, d_active, s); P.end(2, a);
-      if (rc) return ctx.cuda_fail(cudaError_t(rc), "trsv launch");
     }
+    return rc;
+  };
+  const bool use_graph = !profile && !graph_failed && std::getenv("VSHE_NO_GRAPHS") == nullptr;
+  if (use_graph && (!chunk_exec || chunk_every != every)) {
+    if (chunk_exec) { cudaGraphExecDestroy(chunk_exec); chunk_exec = nullptr; }
+    const long long l0 = vk_launches_total();
+    cudaGraph_t g = nullptr;
+    cudaError_t eb = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    int rcap = eb == cudaSuccess ? chunk() : 1;
+    cudaError_t ee = eb == cudaSuccess ? cudaStreamEndCapture(s, &g) : eb;
+    chunk_launches = vk_launches_total() - l0;
+    vk_count_launches(-chunk_launches);  // captured, not executed
+    if (eb != cudaSuccess || rcap || ee != cudaSuccess || !g || cudaGraphInstantiate(&chunk_exec, g, 0) != cudaSuccess) {
+      chunk_exec = nullptr;
+      graph_failed = true;
+      (void)cudaGetLastError();
+    }
+    if (g) cudaGraphDestroy(g);
+    chunk_every = every;
+  }
+  cudaError_t e;
+  if (use_graph && chunk_exec) {
+    if ((e = cudaGraphLaunch(chunk_exec, s)) != cudaSuccess) return ctx.cuda_fail(e, "graph launch");
+    vk_count_launches(chunk_launches);
+    return VSHE_OK;
+  }
+  int rc = chunk();
+  if (rc) return ctx.cuda_fail(cudaError_t(rc), "trsv launch");
+  return VSHE_OK;
+}
+
+// BiCGStab on every active member to relative tolerance `tol`, chunk by chunk, until all are
+// done (converged, broken down or out of iterations).
+int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, bool resume, int &iters_out) {
+  cudaStream_t s = ctx.stream;
+  const int every = sys[0]->opts.check_every > 0 ? sys[0]->opts.check_every : 8;
+  const size_t bsz = vk_bistate_size();
+  int rc = start(ctx, tol, max_iter, resume);
+  if (rc) return rc;
+  EventProf &P = g_prof;
+  std::vector<char> stbuf;
+  int done_iters = 0;
+  while (true) {
+    if ((rc = run_chunk(ctx, every))) return rc;
     done_iters += every;
-    if ((e = cudaMemcpyAsync(stbuf.data(), d_state, stbuf.size(), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return ctx.cuda_fail(e, "read state");
-    int rc = check_err(ctx, "bicgstab");
-    if (rc) return rc;
+    if ((rc = read_states(ctx, stbuf))) return rc;
+    if ((rc = check_err(ctx, "bicgstab"))) return rc;
     bool all_done = true;
     int maxit = 0;
     for (int k = 0; k < nsys; ++k) {
@@ -825,6 +1000,7 @@ int Batch::bicgstab(Ctx &ctx, double tol, int max_iter, bool resume, int &iters_
     if (all_done || done_iters >= max_iter + 2 * every) break;
   }
   if (profile) {
+    cudaError_t e;
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx.cuda_fail(e, "profile");
     double t[5] = {0, 0, 0, 0, 0};
     int64_t c[2] = {0, 0};
@@ -859,6 +1035,7 @@ int Batch::residual(Ctx &ctx, std::vector<double> &rel) {
 }
 
 int Batch::set_active(Ctx &ctx, const std::vector<int32_t> &act) {
+  act_host = act;
   cudaError_t e = cudaMemcpyAsync(d_active, act.data(), sizeof(int32_t) * act.size(), cudaMemcpyHostToDevice, ctx.stream);
   if (e != cudaSuccess) return ctx.cuda_fail(e, "active flags");
   return VSHE_OK;
@@ -883,6 +1060,7 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
   if (rc) return rc;
   cudaEventRecord(e0, s);
   for (System *S : sys) S->prepare(ctx);
+  if ((rc = autotune_tiles(ctx))) return rc;
   rc = factor(ctx);
   if (rc) return rc;
   cudaEventRecord(e1, s);
@@ -1000,7 +1178,7 @@ size_t vshe_bytes_in_use(vshe_ctx *ctx) {
   if (!ctx) return 0;
   size_t t = 0;
   for (auto &kv : ctx->systems) t += kv.second->arena.total;
-  for (auto &kv : ctx->batches) t += kv.second->arena.total;
+  for (auto &kv : ctx->batches) t += kv.second->arena.total + kv.second->tile_arena.total;
   return t;
 }
 
@@ -1011,6 +1189,21 @@ int vshe_set_profiling(vshe_ctx *ctx, int32_t on) {
 }
 
 int64_t vshe_kernel_launches(void) { return (int64_t)vk_launches_total(); }
+
+int vshe_autotune_info(vshe_ctx *ctx, int64_t n, int64_t *tile_rows, double *ms) {
+  if (!ctx || n <= 0 || !tile_rows) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  int cls = 0;
+  while ((int64_t(1) << (cls + 1)) <= n) ++cls;
+  auto it = ctx->tile_choice.find(cls);
+  if (it == ctx->tile_choice.end()) return ctx->fail(VSHE_E_NOT_FOUND, "no system of this size class solved yet");
+  *tile_rows = it->second;
+  if (ms) {
+    const auto &t = ctx->tile_timings[cls];
+    for (size_t k = 0; k < 4; ++k) ms[k] = k < t.size() ? t[k] : 0.0;
+  }
+  return VSHE_OK;
+}
 
 int vshe_get_profile(vshe_ctx *ctx, double *ms, int64_t *counts) {
   if (!ctx || !ms) return VSHE_E_INVALID_ARGUMENT;

@@ -48,6 +48,8 @@ void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles 
   int vk_trsv_##SUF(int mode, int grid, const void *sys, const void *st, const int32_t *act,                          \
                     const VkLevels *lL, const VkLevels *lU, int which, unsigned *bar, int32_t *err, cudaStream_t s);    \
   int vk_trsv_occupancy_##SUF(int *blocks_per_sm);                                                                     \
+  int vk_trsv_cta_##SUF(int ncta, const void *sys, const void *st, const int32_t *act, const int32_t *members, int which, \
+                        cudaStream_t s);                                                                     \
   void vk_split_factor_##SUF(int64_t nnz, int64_t n, const double *lu, const int64_t *fmap, const int64_t *diag,       \
                              const int64_t *dpos, P *lval, P *uval, P *udinv, cudaStream_t s);
 

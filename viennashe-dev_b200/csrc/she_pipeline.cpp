@@ -377,7 +377,7 @@ int vshe_she_info_get(vshe_ctx *ctx, int64_t h, vshe_she_info *info) {
   info->n_facets = S->H.nf;
   info->n_contacts = S->ncontacts;
   info->hbar_omega = S->H.hbar_omega;
-  info->bytes_device = int64_t(S->arena.total + (S->sys ? S->sys->arena.total : 0) + (S->batch ? S->batch->arena.total : 0));
+  info->bytes_device = int64_t(S->arena.total + (S->sys ? S->sys->arena.total : 0) + (S->batch ? S->batch->arena.total + S->batch->tile_arena.total : 0));
   info->levels_L = S->sys ? S->sys->nlevL : 0;
   info->levels_U = S->sys ? S->sys->nlevU : 0;
   info->nnz_factor = S->sys ? S->sys->nnzL + S->sys->nnzU : 0;
@@ -587,6 +587,360 @@ int vshe_she_run_batch(vshe_ctx *ctx, int32_t count, const int64_t *handles, vsh
     if (st[k].status && !worst) worst = st[k].status;
   }
   if (worst) return ctx->fail(worst, "one or more systems of the batch");
+  return VSHE_OK;
+}
+
+}  // extern "C"
+
+// =======================================================================
+// Served stream: continuous batching of SHE solves (vshe_server_*).
+//
+// A request is a device description + SHE configuration (+ solver options).  Its arrays are
+// copied at submission.  One worker thread per server admits queued requests in arrival
+// order while the HBM the resident problems hold stays within the budget (and at most
+// max_active are resident), sets each one up on the device (host set-up of the (x, H) space,
+// device assembly, odd elimination, normalisation, ILU(0) factorisation) and then iterates all
+// resident systems together, chunk by chunk, in one batch (shared launches of the SELL SpMV,
+// the sweeps and the vector kernels).  After every chunk a converged member leaves the batch:
+// its true FP64 residual is checked (a residual replacement restarts it if needed), its
+// solution is recovered and post-processed, its results are copied to the host and its
+// device memory is released, and queued requests take its place.  Each member's iterates do
+// not depend on the batch (per-system reductions in a fixed order, per-system tiles), so a
+// result in the mix equals the same request served alone.
+// =======================================================================
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+
+namespace vshe {
+
+struct ServeRequest {
+  int64_t ticket = 0;
+  // owned copies of the caller's description
+  std::vector<int32_t> mat, contact, fcells, cfp, cfi;
+  std::vector<double> vol, cen, nd, na, phi, fvol, fn, cpl;
+  vshe_device_desc d{};
+  vshe_she_config c{};
+  vshe_coupling_tables t{};
+  vshe_solve_opts o{};
+  std::chrono::steady_clock::time_point t_submit, t_admit, t_done;
+  vshe_server_result res{};
+  std::vector<double> density, currents;
+  std::unique_ptr<SheProblem> prob;
+  std::vector<char> state;  // BiState between batch rebuilds
+  int phase = 0;            // 0 queued, 1 resident, 2 done
+  bool collected = false;   // the caller has its result: the worker may free the record
+  int replacements = 0;
+  bool needs_start = true;
+};
+
+struct Server {
+  vshe_ctx *ctx = nullptr;
+  vshe_server_opts opts{};
+  std::mutex mu;
+  std::condition_variable cv;
+  bool stop = false;
+  std::deque<ServeRequest *> pending;
+  std::map<int64_t, std::unique_ptr<ServeRequest>> all;
+  std::vector<ServeRequest *> active;
+  std::unique_ptr<Batch> batch;
+  int64_t next_ticket = 0;
+  std::thread worker;
+  std::string error;
+
+  void run();
+  int admit(std::vector<ServeRequest *> &fresh);
+  int step();
+  void complete(ServeRequest *r, int status);
+};
+
+static size_t problem_bytes(const SheProblem *S) {
+  size_t b = S->arena.total;
+  if (S->sys) b += S->sys->arena.total;
+  if (S->batch) b += S->batch->arena.total + S->batch->tile_arena.total;
+  return b;
+}
+
+void Server::complete(ServeRequest *r, int status) {
+  r->t_done = std::chrono::steady_clock::now();
+  r->res.status = status;
+  r->res.queue_ms = std::chrono::duration<double, std::milli>(r->t_admit - r->t_submit).count();
+  r->res.latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+  r->prob.reset();  // releases the problem's device memory
+  std::lock_guard<std::mutex> lk(mu);
+  r->phase = 2;
+  cv.notify_all();
+}
+
+// Admits queued requests while memory and slots allow; returns the first error of a set-up.
+int Server::admit(std::vector<ServeRequest *> &fresh) {
+  Ctx &c = *ctx;
+  size_t held = 0;
+  for (ServeRequest *r : active) held += problem_bytes(r->prob.get());
+  while (true) {
+    ServeRequest *r = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (pending.empty() || int(active.size() + fresh.size()) >= opts.max_active) break;
+      r = pending.front();
+    }
+    std::unique_ptr<SheProblem> S(new SheProblem);
+    int rc = S->create(c, r->d, r->c, r->t, r->o);
+    const size_t need = rc ? 0 : problem_bytes(S.get());
+    if (!rc && held + need > opts.hbm_budget && !(active.empty() && fresh.empty())) {
+      break;  // wait for resident problems to finish (S is released here)
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      pending.pop_front();
+    }
+    r->t_admit = std::chrono::steady_clock::now();
+    if (!rc && held + need > opts.hbm_budget) rc = c.fail(VSHE_E_BUDGET, "request alone exceeds the server's HBM budget");
+    if (!rc) rc = S->assemble(c, 3);
+    if (!rc) {
+      S->sys->prepare(c);
+      rc = S->batch->autotune_tiles(c);
+    }
+    if (!rc) rc = S->batch->factor(c);
+    if (rc) { r->res.status = rc; complete(r, rc); continue; }
+    r->res.n_unknowns = S->n_red;
+    r->prob = std::move(S);
+    r->phase = 1;
+    r->needs_start = true;
+    held += need;
+    fresh.push_back(r);
+  }
+  return VSHE_OK;
+}
+
+// One scheduling step: admission, batch rebuild, one iteration chunk, completions.
+int Server::step() {
+  Ctx &c = *ctx;
+  {
+    // free the records whose results were collected (none of them is resident)
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto it = all.begin(); it != all.end();) {
+      if (it->second->collected && it->second->phase == 2) it = all.erase(it);
+      else ++it;
+    }
+  }
+  std::lock_guard<std::mutex> lk(c.mu);
+  cudaSetDevice(c.device);
+  std::vector<ServeRequest *> fresh;
+  int rc = admit(fresh);
+  if (rc) return rc;
+  if (!fresh.empty() || !batch) {
+    for (ServeRequest *r : fresh) active.push_back(r);
+    if (active.empty()) return VSHE_OK;
+    std::vector<System *> mem;
+    for (ServeRequest *r : active) mem.push_back(r->prob->sys.get());
+    std::unique_ptr<Batch> nb(new Batch);
+    if ((rc = nb->build(c, mem))) return rc;
+    batch = std::move(nb);
+    // carry the running members' states over; start the newcomers
+    const size_t bsz = vk_bistate_size();
+    std::vector<char> st(bsz * active.size(), 0);
+    std::vector<int32_t> act(active.size(), 0);
+    for (size_t k = 0; k < active.size(); ++k) {
+      if (active[k]->needs_start) act[k] = 1;
+      else std::memcpy(st.data() + bsz * k, active[k]->state.data(), bsz);
+    }
+    if ((rc = batch->write_states(c, st))) return rc;
+    if ((rc = batch->set_active(c, act))) return rc;
+    const vshe_solve_opts &o = active.front()->o;
+    if ((rc = batch->start(c, o.tol, o.max_iters, false))) return rc;
+    for (ServeRequest *r : active) r->needs_start = false;
+    std::fill(act.begin(), act.end(), 1);
+    if ((rc = batch->set_active(c, act))) return rc;
+  }
+  const vshe_solve_opts &o = active.front()->o;
+  const int every = o.check_every > 0 ? o.check_every : 8;
+  if ((rc = batch->run_chunk(c, every))) return rc;
+  std::vector<char> st;
+  if ((rc = batch->read_states(c, st))) return rc;
+  if ((rc = batch->check_err(c, "served chunk"))) return rc;
+  const size_t bsz = vk_bistate_size();
+  std::vector<int32_t> fin(active.size(), 0);
+  bool any = false;
+  for (size_t k = 0; k < active.size(); ++k) {
+    active[k]->state.assign(st.begin() + bsz * k, st.begin() + bsz * (k + 1));
+    const BiState *b = (const BiState *)active[k]->state.data();
+    if (b->done) { fin[k] = 1; any = true; }
+  }
+  if (!any) return VSHE_OK;
+  // true FP64 residual of the members that stopped
+  if ((rc = batch->set_active(c, fin))) return rc;
+  std::vector<double> rel;
+  if ((rc = batch->residual(c, rel))) return rc;
+  std::vector<int32_t> resume(active.size(), 0);
+  bool any_resume = false;
+  std::vector<ServeRequest *> keep;
+  for (size_t k = 0; k < active.size(); ++k) {
+    ServeRequest *r = active[k];
+    if (!fin[k]) { keep.push_back(r); continue; }
+    const BiState *b = (const BiState *)r->state.data();
+    if (b->status == 0 && rel[k] >= o.tol && b->iter < o.max_iters && r->replacements < 3) {
+      r->replacements++;
+      resume[k] = 1;
+      any_resume = true;
+      keep.push_back(r);
+      continue;
+    }
+    SheProblem *S = r->prob.get();
+    vk_permute(S->sys->n, S->sys->d_perm, (const double *)S->sys->kv[0], S->sys->d_x64, 0, c.stream);
+    int status = b->status;
+    if (status == 0 && rel[k] >= o.tol) status = VSHE_E_NOT_CONVERGED;
+    if (status != 0 && rel[k] < o.tol) status = 0;
+    int frc = S->finish(c);
+    r->res.iterations = b->iter;
+    r->res.refinements = r->replacements;
+    r->res.rel_residual = rel[k];
+    r->res.full_residual = S->full_residual;
+    r->density.assign(size_t(S->H.nc), 0.0);
+    r->currents.assign(size_t(std::max(S->ncontacts, 0)), 0.0);
+    cudaError_t e = cudaMemcpyAsync(r->density.data(), S->d_dens, sizeof(double) * r->density.size(), cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess && !r->currents.empty())
+      e = cudaMemcpyAsync(r->currents.data(), S->d_cur, sizeof(double) * r->currents.size(), cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+    if (frc == 0 && e != cudaSuccess) frc = c.cuda_fail(e, "served results");
+    complete(r, frc ? frc : status);
+  }
+  if (any_resume) {
+    if ((rc = batch->set_active(c, resume))) return rc;
+    if ((rc = batch->start(c, o.tol, o.max_iters, true))) return rc;
+    std::vector<char> st2;
+    if ((rc = batch->read_states(c, st2))) return rc;
+    for (size_t k = 0; k < active.size(); ++k)
+      if (resume[k]) active[k]->state.assign(st2.begin() + bsz * k, st2.begin() + bsz * (k + 1));
+  }
+  if (keep.size() != active.size()) {
+    active = keep;
+    batch.reset();  // rebuilt over the remaining members next step
+    for (ServeRequest *r : active) r->needs_start = false;
+  } else {
+    std::vector<int32_t> act(active.size(), 1);
+    if ((rc = batch->set_active(c, act))) return rc;
+  }
+  return VSHE_OK;
+}
+
+void Server::run() {
+  while (true) {
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv.wait(lk, [&] { return stop || !pending.empty() || !active.empty(); });
+      if (stop && active.empty() && pending.empty()) return;
+      if (stop && active.empty()) {
+        // drop what is still queued
+        for (ServeRequest *r : pending) { r->res.status = VSHE_E_NOT_FOUND; r->phase = 2; }
+        pending.clear();
+        cv.notify_all();
+        return;
+      }
+    }
+    int rc = step();
+    if (rc) {
+      // a device error ends every resident request with that error
+      std::vector<ServeRequest *> act = active;
+      active.clear();
+      batch.reset();
+      for (ServeRequest *r : act)
+        if (r->phase != 2) complete(r, rc);
+      std::lock_guard<std::mutex> lk(mu);
+      error = ctx->last_error;
+    }
+  }
+}
+
+}  // namespace vshe
+
+struct vshe_server : public vshe::Server {};
+
+extern "C" {
+
+int vshe_server_create(vshe_ctx *ctx, const vshe_server_opts *opts, vshe_server **out) {
+  if (!ctx || !out) return VSHE_E_INVALID_ARGUMENT;
+  std::unique_ptr<vshe_server> s(new vshe_server);
+  s->ctx = ctx;
+  if (opts) s->opts = *opts;
+  else { std::memset(&s->opts, 0, sizeof(s->opts)); vshe_default_opts(&s->opts.solve); }
+  if (s->opts.hbm_budget == 0) s->opts.hbm_budget = ctx->budget;
+  if (s->opts.max_active <= 0) s->opts.max_active = 256;
+  vshe_server *p = s.get();
+  p->worker = std::thread([p] { p->run(); });
+  *out = s.release();
+  return VSHE_OK;
+}
+
+int vshe_server_submit(vshe_server *srv, const vshe_device_desc *d, const vshe_she_config *c, const vshe_coupling_tables *ct,
+                       const vshe_solve_opts *opts, int64_t *ticket) {
+  if (!srv || !d || !c || !ct || !ticket || d->n_cells <= 0 || d->n_facets < 0 || (d->dim != 1 && d->dim != 2) || !ct->data)
+    return VSHE_E_INVALID_ARGUMENT;
+  std::unique_ptr<vshe::ServeRequest> r(new vshe::ServeRequest);
+  const size_t nc = size_t(d->n_cells), nf = size_t(d->n_facets), dim = size_t(d->dim);
+  r->mat.assign(d->cell_material, d->cell_material + nc);
+  r->vol.assign(d->cell_volume, d->cell_volume + nc);
+  r->cen.assign(d->cell_centroid, d->cell_centroid + nc * dim);
+  r->nd.assign(d->doping_n, d->doping_n + nc);
+  r->na.assign(d->doping_p, d->doping_p + nc);
+  r->phi.assign(d->potential, d->potential + nc);
+  r->contact.assign(d->contact_id, d->contact_id + nc);
+  r->fcells.assign(d->facet_cells, d->facet_cells + 2 * nf);
+  r->fvol.assign(d->facet_volume, d->facet_volume + nf);
+  r->fn.assign(d->facet_normal, d->facet_normal + nf * dim);
+  r->cfp.assign(d->cell_facet_ptr, d->cell_facet_ptr + nc + 1);
+  r->cfi.assign(d->cell_facet_idx, d->cell_facet_idx + size_t(d->cell_facet_ptr[nc]));
+  const size_t D = size_t((ct->L + 1) * (ct->L + 1));
+  r->cpl.assign(ct->data, ct->data + 6 * D * D);
+  r->d = *d;
+  r->d.cell_material = r->mat.data(); r->d.cell_volume = r->vol.data(); r->d.cell_centroid = r->cen.data();
+  r->d.doping_n = r->nd.data(); r->d.doping_p = r->na.data(); r->d.potential = r->phi.data();
+  r->d.contact_id = r->contact.data(); r->d.facet_cells = r->fcells.data(); r->d.facet_volume = r->fvol.data();
+  r->d.facet_normal = r->fn.data(); r->d.cell_facet_ptr = r->cfp.data(); r->d.cell_facet_idx = r->cfi.data();
+  r->c = *c;
+  r->t.L = ct->L; r->t.data = r->cpl.data();
+  r->o = opts ? *opts : srv->opts.solve;
+  r->o.block_ptr = nullptr; r->o.n_blocks = 0; r->o.perm = nullptr;  // per-request arrays are not carried
+  if (r->o.precision != srv->opts.solve.precision || (r->o.precond == VSHE_PRECOND_NONE) != (srv->opts.solve.precond == VSHE_PRECOND_NONE))
+    return VSHE_E_INVALID_ARGUMENT;  // one batch: same precision and preconditioner kind
+  r->o.tol = srv->opts.solve.tol; r->o.max_iters = srv->opts.solve.max_iters; r->o.check_every = srv->opts.solve.check_every;
+  r->t_submit = std::chrono::steady_clock::now();
+  std::lock_guard<std::mutex> lk(srv->mu);
+  r->ticket = ++srv->next_ticket;
+  *ticket = r->ticket;
+  srv->pending.push_back(r.get());
+  srv->all[r->ticket] = std::move(r);
+  srv->cv.notify_all();
+  return VSHE_OK;
+}
+
+int vshe_server_wait(vshe_server *srv, int64_t ticket, double timeout_ms, vshe_server_result *res, double *density, double *currents) {
+  if (!srv) return VSHE_E_INVALID_ARGUMENT;
+  std::unique_lock<std::mutex> lk(srv->mu);
+  auto it = srv->all.find(ticket);
+  if (it == srv->all.end() || it->second->collected) return VSHE_E_NOT_FOUND;
+  vshe::ServeRequest *r = it->second.get();
+  auto ready = [&] { return r->phase == 2; };
+  if (timeout_ms < 0) srv->cv.wait(lk, ready);
+  else if (!srv->cv.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), ready)) return VSHE_E_TIMEOUT;
+  if (res) *res = r->res;
+  if (density) std::copy(r->density.begin(), r->density.end(), density);
+  if (currents) std::copy(r->currents.begin(), r->currents.end(), currents);
+  const int status = r->res.status;
+  r->collected = true;  // freed by the worker once it no longer refers to it
+  return status;
+}
+
+int vshe_server_destroy(vshe_server *srv) {
+  if (!srv) return VSHE_E_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->stop = true;
+    srv->cv.notify_all();
+  }
+  if (srv->worker.joinable()) srv->worker.join();
+  delete srv;
   return VSHE_OK;
 }
 

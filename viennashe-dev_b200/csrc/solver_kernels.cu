@@ -41,9 +41,11 @@ namespace vshe {
 #define VSHE_E_ZERO_PIVOT_DEV (-11)
 
 constexpr int kThreads = 256;
+constexpr int kCtaThreads = 512;  // the per-system sweep: 16 warps, two slices in flight each
 constexpr int kWarps = kThreads / 32;
 constexpr int kSpmvU = 8;  // SELL entries per lane whose loads are issued together
-constexpr int kTrsvU = 4;  // triangular factors hold about half of A's entries per row
+constexpr int kDotU = 6;   // the same inside the tile kernels, which also carry reduction state
+constexpr int kTrsvU = 8;  // entries of a factor row loaded at once (factor rows hold ~5 entries)
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -146,6 +148,32 @@ __device__ __forceinline__ double sell_rowsum(int64_t off, int width, const int3
   return sum;
 }
 
+// Continues a SELL-32 row sum from entry k0 (entries below k0 already summed into `sum`), kU
+// entries per round trip; CG: x is written by other CTAs of the same launch (L2 reads).  The
+// triangular sweeps use kU = 1: wider groups cost registers, and with them occupancy, which
+// measured slower on the 2D bar (0.47 vs 0.40 ms per apply).
+template <typename V, bool CG, int kU>
+__device__ __forceinline__ double sell_rowsum_from(int64_t off, int width, int k0, const int32_t *__restrict__ col, const V *__restrict__ val,
+                                                const double *x, double sum) {
+  const int lane = threadIdx.x & 31;
+  for (int k = k0; k < width; k += kU) {
+    int32_t cc[kU];
+    V aa[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      cc[u] = 0; aa[u] = V(0);
+      if (k + u < width) { const int64_t e = off + 32 * (k + u) + lane; cc[u] = __ldcs(col + e); aa[u] = __ldcs(val + e); }
+    }
+    double xx[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) xx[u] = k + u < width ? (CG ? __ldcg(x + cc[u]) : x[cc[u]]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+      if (k + u < width) sum = fma((double)aa[u], xx[u], sum);
+  }
+  return sum;
+}
+
 // deterministic dense shadow residual in [0.5, 1.5): a hash of the row index
 __device__ __forceinline__ double shadow_value(int64_t i) {
   uint32_t h = (uint32_t)((uint64_t)i * 2654435761ull) ^ (uint32_t)((uint64_t)i >> 32);
@@ -157,8 +185,7 @@ typedef SysDev<double> SysK;  // the Krylov kernels touch only the FP64 members
 
 // ------------------------------------------------------------------ BiCGStab
 // init (x0 = 0): r = b, rh = shadow (or r_0), x = p = v = 0; ||b||, (rh, r) -> state
-__global__ void __launch_bounds__(kThreads) k_bicg_init(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active) {
-  const int tile = blockIdx.x;
+__device__ __forceinline__ void k_bicg_init_tile(const SysK *sys, BiState *st, const Tiles &tl, double *partials, int32_t *counters, const int32_t *active, int tile) {
   const int s = tl.tile_sys[tile];
   if (!active[s]) return;
   const SysK S = sys[s];
@@ -183,10 +210,12 @@ __global__ void __launch_bounds__(kThreads) k_bicg_init(const SysK *sys, BiState
     if (b.done) b.res = 0.0;
   }
 }
+__global__ void __launch_bounds__(kThreads) k_bicg_init(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active) {
+  k_bicg_init_tile(sys, st, tl, partials, counters, active, blockIdx.x);
+}
 
 // resume after a residual replacement: r holds b - A x (true residual); restart the recurrence
-__global__ void __launch_bounds__(kThreads) k_bicg_resume(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active) {
-  const int tile = blockIdx.x;
+__device__ __forceinline__ void k_bicg_resume_tile(const SysK *sys, BiState *st, const Tiles &tl, double *partials, int32_t *counters, const int32_t *active, int tile) {
   const int s = tl.tile_sys[tile];
   if (!active[s]) return;
   const SysK S = sys[s];
@@ -204,10 +233,12 @@ __global__ void __launch_bounds__(kThreads) k_bicg_resume(const SysK *sys, BiSta
     b.s_conv = 0; b.status = 0; b.restart = 1; b.done = 0;
   }
 }
+__global__ void __launch_bounds__(kThreads) k_bicg_resume(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active) {
+  k_bicg_resume_tile(sys, st, tl, partials, counters, active, blockIdx.x);
+}
 
 // p = r + beta (p - omega v), or p = r after a (re)start
-__global__ void __launch_bounds__(kThreads) k_update_p(const SysK *sys, BiState *st, Tiles tl, const int32_t *active) {
-  const int tile = blockIdx.x;
+__device__ __forceinline__ void k_update_p_tile(const SysK *sys, BiState *st, const Tiles &tl, const int32_t *active, int tile) {
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done) return;
   const SysK S = sys[s];
@@ -220,28 +251,35 @@ __global__ void __launch_bounds__(kThreads) k_update_p(const SysK *sys, BiState 
       S.p[i] = S.r[i] + beta * (S.p[i] - b.omega * S.v[i]);
   }
 }
+__global__ void __launch_bounds__(kThreads) k_update_p(const SysK *sys, BiState *st, Tiles tl, const int32_t *active) {
+  k_update_p_tile(sys, st, tl, active, blockIdx.x);
+}
 
 // y = A x over one tile (one SELL-32 slice per warp in turn), fused dots.
 // which = 0: v = A ph, (rh, v) -> alpha.   which = 1: t = A sh, (t, s), (t, t) -> omega.
-__global__ void __launch_bounds__(kThreads, 4) k_spmv_dot(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active, int which) {
-  const int tile = blockIdx.x;
+__device__ __forceinline__ void k_spmv_dot_tile(const SysK *sys, BiState *st, const Tiles &tl, double *partials, int32_t *counters, const int32_t *active, int which, int tile) {
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done) return;
   if (which == 1 && st[s].s_conv) return;
-  const SysK S = sys[s];
+  const SysK &S = sys[s];
+  const int64_t *__restrict__ aoff = S.aoff;
+  const int32_t *__restrict__ acol = S.acol;
+  const double *__restrict__ aval = S.aval;
   const double *xin = which == 0 ? S.ph : S.sh;
   double *yout = which == 0 ? S.v : S.t;
+  const double *dv = which == 0 ? S.rh : S.s;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t r0 = tl.tile_row0[tile], r1 = tl.tile_row1[tile];
   double acc[2] = {0.0, 0.0};
   for (int64_t q0 = r0 + 32 * w; q0 < r1; q0 += 32 * kWarps) {
-    const int64_t j = q0 >> 5, off = S.aoff[j];
-    const double y = sell_rowsum<double, false, kSpmvU>(off, (int)((S.aoff[j + 1] - off) >> 5), S.acol, S.aval, xin);
+    const int64_t j = q0 >> 5, off = aoff[j];
+    const double y = sell_rowsum<double, false, kSpmvU>(off, (int)((aoff[j + 1] - off) >> 5), acol, aval, xin);
     const int64_t row = q0 + lane;
     if (row < r1) {
       yout[row] = y;
-      if (which == 0) acc[0] += S.rh[row] * y;
-      else { acc[0] += y * S.s[row]; acc[1] += y * y; }
+      const double d = dv[row];
+      if (which == 0) acc[0] += d * y;
+      else { acc[0] += y * d; acc[1] += y * y; }
     }
   }
   double tot[2];
@@ -255,10 +293,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmv_dot(const SysK *sys, BiSta
     }
   }
 }
+__global__ void __launch_bounds__(kThreads, 4) k_spmv_dot(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active, int which) {
+  k_spmv_dot_tile(sys, st, tl, partials, counters, active, which, blockIdx.x);
+}
 
 // s = r - alpha v, ||s|| -> s_conv
-__global__ void __launch_bounds__(kThreads) k_update_s(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active) {
-  const int tile = blockIdx.x;
+__device__ __forceinline__ void k_update_s_tile(const SysK *sys, BiState *st, const Tiles &tl, double *partials, int32_t *counters, const int32_t *active, int tile) {
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done) return;
   const SysK S = sys[s];
@@ -277,10 +317,12 @@ __global__ void __launch_bounds__(kThreads) k_update_s(const SysK *sys, BiState 
     if (b.s_conv) b.res = sres;
   }
 }
+__global__ void __launch_bounds__(kThreads) k_update_s(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active) {
+  k_update_s_tile(sys, st, tl, partials, counters, active, blockIdx.x);
+}
 
 // x += alpha ph + omega sh; r = s - omega t; ||r||, (rh, r) -> next rho, convergence.
-__global__ void __launch_bounds__(kThreads) k_update_xr(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active) {
-  const int tile = blockIdx.x;
+__device__ __forceinline__ void k_update_xr_tile(const SysK *sys, BiState *st, const Tiles &tl, double *partials, int32_t *counters, const int32_t *active, int tile) {
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done) return;
   const SysK S = sys[s];
@@ -318,10 +360,12 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(const SysK *sys, BiState
     if (b.iter >= b.max_iter) { b.done = 1; b.status = VSHE_E_NOT_CONVERGED_DEV; }
   }
 }
+__global__ void __launch_bounds__(kThreads) k_update_xr(const SysK *sys, BiState *st, Tiles tl, double *partials, int32_t *counters, const int32_t *active) {
+  k_update_xr_tile(sys, st, tl, partials, counters, active, blockIdx.x);
+}
 
 // copy (no preconditioner): which 0: ph = p, which 1: sh = s
-__global__ void __launch_bounds__(kThreads) k_precond_copy(const SysK *sys, const BiState *st, Tiles tl, const int32_t *active, int which) {
-  const int tile = blockIdx.x;
+__device__ __forceinline__ void k_precond_copy_tile(const SysK *sys, const BiState *st, const Tiles &tl, const int32_t *active, int which, int tile) {
   const int s = tl.tile_sys[tile];
   if (!active[s] || st[s].done) return;
   if (which == 1 && st[s].s_conv) return;
@@ -329,6 +373,9 @@ __global__ void __launch_bounds__(kThreads) k_precond_copy(const SysK *sys, cons
   const double *in = which == 0 ? S.p : S.s;
   double *out = which == 0 ? S.ph : S.sh;
   for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) out[i] = in[i];
+}
+__global__ void __launch_bounds__(kThreads) k_precond_copy(const SysK *sys, const BiState *st, Tiles tl, const int32_t *active, int which) {
+  k_precond_copy_tile(sys, st, tl, active, which, blockIdx.x);
 }
 
 // ------------------------------------------------------------ grid barrier
@@ -383,38 +430,102 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
 // them in turn, one slice per warp, one row per lane.  Forward slices are runs of consecutive
 // solver rows; backward slices list their rows through urow.  ytmp and out are written by
 // other CTAs of the same launch and read through L2 only.
+// One SELL-32 slice of a triangular sweep as one warp holds it: lane = row.  The phases are
+// split so that a warp can keep several slices' loads in flight: load() issues the slice's first
+// kTrsvU entry loads together with the row's own operand (in[row] forward; urow, ytmp[row] and
+// the inverse diagonal backward); finish() gathers the solved values at those columns, walks any
+// further entries and writes the row.  Rows are summed in index order (FMA), as sell_rowsum.
+template <typename P, bool CG>
+struct TrsvSlice {
+  bool on = false;
+  int width = 0, nr = 0;
+  int64_t off = 0;
+  const int32_t *col = nullptr;
+  const P *val = nullptr;
+  const double *src = nullptr;  // solved values gathered at the columns (ytmp / out)
+  double *dst = nullptr;        // where the row's result goes (ytmp / out)
+  int32_t row = 0;
+  double base = 0.0, dinv = 1.0;
+  int32_t cc[kTrsvU];
+  P aa[kTrsvU];
+
+  __device__ __forceinline__ void load(const SysDev<P> *sys, const BiState *st, const int32_t *active, const Levels &lv, int64_t c,
+                                       bool lower, int which) {
+    on = false;
+    if (c < 0) return;
+    const int s = lv.ent_sys[c];
+    if (!active[s] || st[s].done || (which == 1 && st[s].s_conv)) return;
+    load_slice(sys[s], lv.ent_row[c], lower, which);
+  }
+
+  __device__ __forceinline__ void load_slice(const SysDev<P> &S, int j, bool lower, int which) {
+    const int lane = threadIdx.x & 31;
+    on = true;
+    if (lower) {
+      off = S.loff[j];
+      width = (int)((S.loff[j + 1] - off) >> 5);
+      const int32_t q0 = S.lrow0[j];
+      nr = S.lrow0[j + 1] - q0;
+      col = S.lcol; val = S.lval; src = S.ytmp; dst = S.ytmp;
+      row = q0 + lane;
+      const double *in = which == 0 ? S.p : S.s;
+      base = lane < nr ? in[row] : 0.0;
+      dinv = 1.0;
+    } else {
+      off = S.uoff[j];
+      width = (int)((S.uoff[j + 1] - off) >> 5);
+      const int32_t t0 = S.uslot0[j];
+      nr = S.uslot0[j + 1] - t0;
+      col = S.ucol; val = S.uval;
+      double *out = which == 0 ? S.ph : S.sh;
+      src = out; dst = out;
+      row = 0; base = 0.0; dinv = 1.0;
+      if (lane < nr) {
+        row = S.urow[t0 + lane];
+        dinv = (double)S.udinv[t0 + lane];
+        base = CG ? __ldcg(&S.ytmp[row]) : S.ytmp[row];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kTrsvU; ++u) {
+      cc[u] = 0; aa[u] = P(0);
+      if (u < width) {
+        const int64_t k = off + 32 * u + lane;
+        cc[u] = __ldcs(col + k); aa[u] = __ldcs(val + k);
+      }
+    }
+  }
+
+  __device__ __forceinline__ void finish() {
+    if (!on) return;
+    const int lane = threadIdx.x & 31;
+    double xx[kTrsvU];
+#pragma unroll
+    for (int u = 0; u < kTrsvU; ++u) xx[u] = u < width ? (CG ? __ldcg(src + cc[u]) : src[cc[u]]) : 0.0;
+    double sum = 0.0;
+#pragma unroll
+    for (int u = 0; u < kTrsvU; ++u)
+      if (u < width) sum = fma((double)aa[u], xx[u], sum);
+    if (width > kTrsvU) sum = sell_rowsum_from<P, CG, 1>(off, width, kTrsvU, col, val, src, sum);
+    if (lane < nr) dst[row] = (base - sum) * dinv;
+  }
+};
+
+// out = U^{-1} L^{-1} in (solver order) over SELL-32 factor slices stored in precision P;
+// the arithmetic and the work vector ytmp are FP64 in both modes.  which 0: ph = M^{-1} p,
+// 1: sh = M^{-1} s.  A level is a list of (system, slice) entries; the warps of the grid take
+// them two at a time, one row per lane.  ytmp and out are written by other CTAs of the same
+// launch and read through L2 only.
 template <typename P>
-__device__ __forceinline__ void trsv_level_rows(const SysDev<P> *sys, const BiState *st, const int32_t *active, const Levels lv, int k,
+__device__ __forceinline__ void trsv_level_rows(const SysDev<P> *sys, const BiState *st, const int32_t *active, const Levels &lv, int k,
                                                 bool lower, int which) {
-  const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
   const int64_t c1 = lv.lvl_ptr[k + 1];
   for (int64_t c = lv.lvl_ptr[k] + gw; c < c1; c += nw) {
-    const int s = lv.ent_sys[c];
-    if (!active[s] || st[s].done || (which == 1 && st[s].s_conv)) continue;
-    const SysDev<P> &S = sys[s];
-    const int j = lv.ent_row[c];
-    if (lower) {
-      const int64_t off = S.loff[j];
-      const int32_t q0 = S.lrow0[j], nr = S.lrow0[j + 1] - q0;
-      const double sum = sell_rowsum<P, true, kTrsvU>(off, (int)((S.loff[j + 1] - off) >> 5), S.lcol, S.lval, S.ytmp);
-      if (lane < nr) {
-        const int64_t q = q0 + lane;
-        const double *in = which == 0 ? S.p : S.s;
-        S.ytmp[q] = in[q] - sum;
-      }
-    } else {
-      double *out = which == 0 ? S.ph : S.sh;
-      const int64_t off = S.uoff[j];
-      const int32_t t0 = S.uslot0[j], nr = S.uslot0[j + 1] - t0;
-      const double sum = sell_rowsum<P, true, kTrsvU>(off, (int)((S.uoff[j + 1] - off) >> 5), S.ucol, S.uval, out);
-      if (lane < nr) {
-        const int64_t t = t0 + lane;
-        const int32_t row = S.urow[t];
-        out[row] = (__ldcg(&S.ytmp[row]) - sum) * (double)S.udinv[t];
-      }
-    }
+    TrsvSlice<P, true> a;
+    a.load(sys, st, active, lv, c, lower, which);
+    a.finish();
   }
 }
 
@@ -433,6 +544,37 @@ __global__ void __launch_bounds__(kThreads) k_trsv_persistent(const SysDev<P> *s
 template <typename P>
 __global__ void __launch_bounds__(kThreads) k_trsv_level(const SysDev<P> *sys, const BiState *st, const int32_t *active, Levels lv, int k, int lower, int which) {
   trsv_level_rows<P>(sys, st, active, lv, k, lower != 0, which);
+}
+
+// One CTA per system: the CTA walks its own system's forward then backward levels, with a
+// CTA barrier between levels instead of a grid barrier.  For systems whose levels are many and
+// short (1D devices: ~1000 levels of ~100-500 rows), where a grid-wide barrier per level costs
+// more than the level's work.  The gathers still read through L2 (__ldcg): with L1-cached loads
+// the 1D diodes converged slower and non-deterministically on B200, i.e. some gathers saw
+// stale lines.
+template <typename P>
+__global__ void __launch_bounds__(kCtaThreads) k_trsv_cta(const SysDev<P> *sys, const BiState *st, const int32_t *active,
+                                                        const int32_t *members, int which) {
+  const int s = members[blockIdx.x];
+  if (!active[s] || st[s].done || (which == 1 && st[s].s_conv)) return;
+  const SysDev<P> &S = sys[s];
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int pass = 0; pass < 2; ++pass) {
+    const bool lower = pass == 0;
+    const int nlev = lower ? S.nlevL : S.nlevU;
+    const int64_t *lvs = lower ? S.lvsL : S.lvsU;
+    for (int k = 0; k < nlev; ++k) {
+      const int64_t j1 = lvs[k + 1];
+      for (int64_t j = lvs[k] + w; j < j1; j += 2 * nw) {
+        TrsvSlice<P, true> a, b;
+        a.load_slice(S, (int)j, lower, which);
+        if (j + nw < j1) b.load_slice(S, (int)(j + nw), lower, which);
+        a.finish();
+        b.finish();
+      }
+      __syncthreads();
+    }
+  }
 }
 
 // ------------------------------------------------------ ILU(0) factorisation
@@ -527,22 +669,26 @@ __global__ void k_split_factor(int64_t nnz, int64_t n, const double *lu, const i
 
 // ------------------------------------------------------- FP64 residual
 // r = b - A x (FP64, solver order), ||r||^2 and ||b||^2 per system -> rnorm2 / bnorm2.
-__global__ void __launch_bounds__(kThreads, 4) k_residual64(const RefDev *sys, Tiles tl, double *partials, int32_t *counters, const int32_t *active, double *rnorm2, double *bnorm2) {
-  const int tile = blockIdx.x;
+__device__ __forceinline__ void k_residual64_tile(const RefDev *sys, const Tiles &tl, double *partials, int32_t *counters, const int32_t *active, double *rnorm2, double *bnorm2, int tile) {
   const int s = tl.tile_sys[tile];
   if (!active[s]) return;
-  const RefDev S = sys[s];
+  const RefDev &S = sys[s];
+  const int64_t *__restrict__ aoff = S.aoff;
+  const int32_t *__restrict__ acol = S.acol;
+  const double *__restrict__ aval = S.aval;
+  const double *xv = S.x, *bv = S.b;
+  double *rv = S.r;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t r0 = tl.tile_row0[tile], r1 = tl.tile_row1[tile];
   double acc[2] = {0.0, 0.0};
   for (int64_t q0 = r0 + 32 * w; q0 < r1; q0 += 32 * kWarps) {
-    const int64_t j = q0 >> 5, off = S.aoff[j];
-    const double ax = sell_rowsum<double, false, kSpmvU>(off, (int)((S.aoff[j + 1] - off) >> 5), S.acol, S.aval, S.x);
+    const int64_t j = q0 >> 5, off = aoff[j];
+    const double ax = sell_rowsum<double, false, kDotU>(off, (int)((aoff[j + 1] - off) >> 5), acol, aval, xv);
     const int64_t row = q0 + lane;
     if (row < r1) {
-      const double bb = S.b[row];
+      const double bb = bv[row];
       const double r = bb - ax;
-      S.r[row] = r;
+      rv[row] = r;
       acc[0] += r * r;
       acc[1] += bb * bb;
     }
@@ -552,6 +698,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_residual64(const RefDev *sys, T
     rnorm2[s] = tot[0];
     bnorm2[s] = tot[1];
   }
+}
+__global__ void __launch_bounds__(kThreads, 4) k_residual64(const RefDev *sys, Tiles tl, double *partials, int32_t *counters, const int32_t *active, double *rnorm2, double *bnorm2) {
+  k_residual64_tile(sys, tl, partials, counters, active, rnorm2, bnorm2, blockIdx.x);
 }
 
 // plain SELL-32 SpMV for tests / timing (y = A x, solver order): one slice per warp in turn
@@ -581,6 +730,11 @@ static inline int grid_for(int64_t n) {
 
 static std::atomic<long long> g_launches{0};
 
+// CTAs of the tile kernels: one per tile.  (Persistent CTAs looping over the tiles measured 10%
+// slower on the 2D bar: a CTA's per-tile reduction tail then stalls its next tile, where
+// separate CTAs overlap it with other CTAs' work.)
+static int tile_grid(int ntiles) { return ntiles; }
+
 template <typename P>
 static int launch_trsv_t(int mode, int grid, const SysDev<P> *sys, const BiState *st, const int32_t *act, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err, cudaStream_t s) {
   if (mode == 1) {
@@ -604,34 +758,40 @@ long long vk_launches_total() { return g_launches.load(); }
 
 void vk_bicg_init(int ntiles, const void *sys, void *st, const VkTiles *tl, double *part, int32_t *cnt, const int32_t *act, cudaStream_t s) {
   g_launches += 1;
-  k_bicg_init<<<ntiles, kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, part, cnt, act);
+  k_bicg_init<<<tile_grid(ntiles), kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, part, cnt, act);
 }
 void vk_bicg_resume(int ntiles, const void *sys, void *st, const VkTiles *tl, double *part, int32_t *cnt, const int32_t *act, cudaStream_t s) {
   g_launches += 1;
-  k_bicg_resume<<<ntiles, kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, part, cnt, act);
+  k_bicg_resume<<<tile_grid(ntiles), kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, part, cnt, act);
 }
 void vk_update_p(int ntiles, const void *sys, void *st, const VkTiles *tl, const int32_t *act, cudaStream_t s) {
   g_launches += 1;
-  k_update_p<<<ntiles, kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, act);
+  k_update_p<<<tile_grid(ntiles), kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, act);
 }
 void vk_spmv_dot(int ntiles, const void *sys, void *st, const VkTiles *tl, double *part, int32_t *cnt, const int32_t *act, int which, cudaStream_t s) {
   g_launches += 1;
-  k_spmv_dot<<<ntiles, kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, part, cnt, act, which);
+  k_spmv_dot<<<tile_grid(ntiles), kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, part, cnt, act, which);
 }
 void vk_update_s(int ntiles, const void *sys, void *st, const VkTiles *tl, double *part, int32_t *cnt, const int32_t *act, cudaStream_t s) {
   g_launches += 1;
-  k_update_s<<<ntiles, kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, part, cnt, act);
+  k_update_s<<<tile_grid(ntiles), kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, part, cnt, act);
 }
 void vk_update_xr(int ntiles, const void *sys, void *st, const VkTiles *tl, double *part, int32_t *cnt, const int32_t *act, cudaStream_t s) {
   g_launches += 1;
-  k_update_xr<<<ntiles, kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, part, cnt, act);
+  k_update_xr<<<tile_grid(ntiles), kThreads, 0, s>>>((const SysK *)sys, (BiState *)st, *(const Tiles *)tl, part, cnt, act);
 }
 void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles *tl, const int32_t *act, int which, cudaStream_t s) {
   g_launches += 1;
-  k_precond_copy<<<ntiles, kThreads, 0, s>>>((const SysK *)sys, (const BiState *)st, *(const Tiles *)tl, act, which);
+  k_precond_copy<<<tile_grid(ntiles), kThreads, 0, s>>>((const SysK *)sys, (const BiState *)st, *(const Tiles *)tl, act, which);
 }
 
 #define VK_BODY_P(P, SUF)                                                                                             \
+  int vk_trsv_cta_##SUF(int ncta, const void *sys, const void *st, const int32_t *act, const int32_t *members, int which, \
+                        cudaStream_t s) {                                                                             \
+    g_launches += 1;                                                                                                 \
+    k_trsv_cta<P><<<ncta, kCtaThreads, 0, s>>>((const SysDev<P> *)sys, (const BiState *)st, act, members, which);    \
+    return (int)cudaGetLastError();                                                                                  \
+  }                                                                                                                  \
   int vk_trsv_##SUF(int mode, int grid, const void *sys, const void *st, const int32_t *act, const VkLevels *lL,     \
                     const VkLevels *lU, int which, unsigned *bar, int32_t *err, cudaStream_t s) {                    \
     return launch_trsv_t<P>(mode, grid, (const SysDev<P> *)sys, (const BiState *)st, act, *(const Levels *)lL,       \
@@ -689,7 +849,7 @@ size_t vk_bistate_size() { return sizeof(BiState); }
 void vk_residual64(int ntiles, const void *ref, const VkTiles *tl, double *part, int32_t *cnt, const int32_t *act,
                    double *rnorm2, double *bnorm2, cudaStream_t s) {
   g_launches += 1;
-  k_residual64<<<ntiles, kThreads, 0, s>>>((const RefDev *)ref, *(const Tiles *)tl, part, cnt, act, rnorm2, bnorm2);
+  k_residual64<<<tile_grid(ntiles), kThreads, 0, s>>>((const RefDev *)ref, *(const Tiles *)tl, part, cnt, act, rnorm2, bnorm2);
 }
 
 }  // extern "C"

@@ -38,6 +38,8 @@ struct SysDev {
   const int32_t *lrow0; const int64_t *loff; const int32_t *lcol; const P *lval;
   const int32_t *uslot0; const int64_t *uoff; const int32_t *ucol; const P *uval; const P *udinv; const int32_t *urow;
   double *ytmp;      // forward-sweep result (FP64)
+  // level -> slice ranges of this system alone (the per-system sweep of k_trsv_cta)
+  const int64_t *lvsL; const int64_t *lvsU; int32_t nlevL, nlevU;
   // Krylov vectors (solver order, FP64)
   double *x, *r, *rh, *p, *v, *s, *t, *ph, *sh;
 };

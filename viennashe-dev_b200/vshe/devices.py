@@ -288,3 +288,34 @@ def config3(count=64, seed=11):
         cfg = SheConfig(max_expansion_order=L, energy_spacing=HBAR_OMEGA_OP / 4.0, min_kinetic_energy_range=1.0 * Q)
         out.append((dev, cfg))
     return out
+
+
+def config4(count=40, seed=23, rate=200.0):
+    """Served stream: `count` requests arriving as a Poisson process at `rate` req/s (seed 23).
+    70 % are 1D n+/n/n+ diodes drawn as in config3; 30 % are 2D bars as in config2 with a mesh of
+    50-200 x 20-50 cells, L in {1, 3, 5}, 60-160 energies and the bar's 0.8 V bias (lateral
+    edge jitter from the stream's generator).  Returns [(arrival_s, dev, cfg)]."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        if rng.random() < 0.7:
+            length = rng.uniform(100e-9, 500e-9)
+            boxes = int(rng.integers(50, 401))
+            nch = float(np.exp(rng.uniform(np.log(1e21), np.log(1e23))))
+            L = int(rng.choice([1, 3]))
+            bias = float(rng.uniform(0.0, 1.0))
+            lens = (0.2 * length, 0.6 * length, 0.2 * length)
+            dev = nin_diode_1d(lengths=lens, dopings=(1e25, nch, 1e25), boxes=boxes, bias=bias, name="config4_%03d_1d" % k)
+            cfg = SheConfig(max_expansion_order=L, energy_spacing=HBAR_OMEGA_OP / 4.0, min_kinetic_energy_range=1.0 * Q)
+        else:
+            nx = int(rng.integers(50, 201))
+            ny = int(rng.integers(20, 51))
+            L = int(rng.choice([1, 3, 5]))
+            ne = int(rng.integers(60, 161))
+            dev = nin_bar_2d(nx=nx, ny=ny, bias=0.8, seed=int(rng.integers(0, 2 ** 31)), name="config4_%03d_2d" % k)
+            sp = HBAR_OMEGA_OP / 4.0
+            cfg = SheConfig(max_expansion_order=L, energy_spacing=sp, min_kinetic_energy_range=energy_range_for(dev, sp, ne))
+        out.append((t, dev, cfg))
+    return out

@@ -180,6 +180,15 @@ class Context:
         return dict(spmv_ms=ms[0], trsv_ms=ms[1], vector_ms=ms[2], reliable_ms=ms[3], factor_ms=ms[4],
                     spmv_launches=int(cnt[0]), trsv_launches=int(cnt[1]))
 
+    def autotune_info(self, n):
+        """(rows per reduction tile chosen for n's size class, ms per SpMV for 512/1024/2048/4096)."""
+        L = lib()
+        L.vshe_autotune_info.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+        rows = C.c_int64()
+        ms = np.zeros(4)
+        self._check(L.vshe_autotune_info(self.h, int(n), C.byref(rows), ptr(ms, C.c_double)))
+        return int(rows.value), ms
+
     def solve_csr(self, rp, ci, v, b, **kw):
         """The drop-in call: host CSR + rhs in, host x out (copies inside)."""
         rp = np.ascontiguousarray(rp, np.int64)
@@ -411,3 +420,67 @@ def she_run_batch(ctx: Context, problems):
     if rc and rc != -6:
         ctx._check(rc)
     return [stats_dict(s) for s in st], fr, ms.value
+
+
+# ---------------------------------------------------------------- served stream
+class ServerOptsC(C.Structure):
+    _fields_ = [("hbm_budget", C.c_size_t), ("max_active", C.c_int32), ("solve", SolveOptsC)]
+
+
+class ServerResultC(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("refinements", C.c_int32),
+                ("rel_residual", C.c_double), ("full_residual", C.c_double), ("queue_ms", C.c_double),
+                ("latency_ms", C.c_double), ("n_unknowns", C.c_int64)]
+
+
+class Server:
+    """Continuous-batching request loop on one context (vshe_server_*)."""
+
+    def __init__(self, ctx: Context, hbm_budget=0, max_active=0, **solve):
+        L = lib()
+        L.vshe_server_create.argtypes = [C.c_void_p, C.POINTER(ServerOptsC), C.POINTER(C.c_void_p)]
+        L.vshe_server_submit.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveOptsC), C.POINTER(C.c_int64)]
+        L.vshe_server_wait.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.POINTER(ServerResultC), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.vshe_server_destroy.argtypes = [C.c_void_p]
+        self.ctx = ctx
+        o = ServerOptsC()
+        o.hbm_budget = int(hbm_budget)
+        o.max_active = int(max_active)
+        so, self._keep = make_opts(**solve)
+        o.solve = so
+        h = C.c_void_p()
+        ctx._check(L.vshe_server_create(ctx.h, C.byref(o), C.byref(h)))
+        self.h = h
+        self._meta = {}
+
+    def submit(self, dev, cfg, coupling=None, **solve):
+        from .abi import DeviceDesc, she_config_c
+        desc = DeviceDesc(dev)
+        cfgc = she_config_c(cfg)
+        cpl = coupling if coupling is not None else coupling_tables(cfg.max_expansion_order)
+        o = None
+        if solve:
+            o, _ = make_opts(**solve)
+        t = C.c_int64()
+        rc = lib().vshe_server_submit(self.h, C.byref(desc.c), C.byref(cfgc), C.byref(cpl.c), C.byref(o) if o is not None else None, C.byref(t))
+        if rc:
+            raise VsheError(rc, "vshe_server_submit")
+        self._meta[t.value] = (dev.n_cells, dev.n_contacts)
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1.0):
+        """-> (result dict, densities, currents); raises on a failed request."""
+        nc, ncont = self._meta.pop(ticket)
+        r = ServerResultC()
+        dens = np.zeros(nc)
+        cur = np.zeros(max(ncont, 1))
+        rc = lib().vshe_server_wait(self.h, ticket, float(timeout_ms), C.byref(r), ptr(dens, C.c_double), ptr(cur, C.c_double))
+        res = {k: getattr(r, k) for k, _ in ServerResultC._fields_}
+        if rc and rc != -6:
+            raise VsheError(rc, "served request %d failed (%s)" % (ticket, ERRORS.get(rc, "?")))
+        return res, dens, cur[:ncont]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().vshe_server_destroy(self.h)
+            self.h = None
