@@ -53,6 +53,10 @@ extern "C" {
 #define VSHE_PRECOND_NONE        0
 #define VSHE_PRECOND_ILU0        1   /* ILU(0) on the whole system (serial_linear_solver's choice) */
 #define VSHE_PRECOND_BLOCK_ILU0  2   /* ILU(0) per block (energy slabs: block_preconditioner_boundaries) */
+#define VSHE_PRECOND_ILUT        3   /* incomplete LU on the pattern of ILUT(ilut_entries, ilut_drop) (Saad
+                                        Alg. 10.6) together with A's pattern: the pattern is found on the host
+                                        from the values at system creation, the factorisation of every solve
+                                        runs on the device on that pattern without dropping */
 
 #define VSHE_ORDER_NATURAL     0   /* the caller's row order (the reference's) */
 #define VSHE_ORDER_MULTICOLOR  1   /* greedy colouring of the matrix graph, rows grouped by colour */
@@ -82,6 +86,11 @@ typedef struct vshe_solve_opts {
                                original row placed at position i (overrides ordering); NULL = none */
   int32_t shadow;           /* BiCGStab shadow residual: VSHE_SHADOW_DENSE (default) or
                                VSHE_SHADOW_R0 (r^ = r_0, as the reference's ViennaCL bicgstab) */
+  int32_t fill_level;       /* ILU0 / BLOCK_ILU0: 0 = ILU(0); k > 0 = ILU(k), the factor keeps the fill
+                               of levels <= k (Saad Alg. 10.5), inside the row's block */
+  int32_t ilut_entries;     /* ILUT: largest entries kept per row in L and in U (linear_solver_config::
+                               ilut_entries(); 0 = its default 60, viennashe/solvers/config.hpp:63) */
+  double  ilut_drop;        /* ILUT: relative drop tolerance (ilut_drop_tolerance(); 0 = its default 1e-4) */
 } vshe_solve_opts;
 
 typedef struct vshe_solve_stats {
@@ -182,7 +191,8 @@ int vshe_csr_residual_noalloc(int64_t n, int64_t nnz, const int64_t *d_row_ptr, 
 
 /* ---- host-only layout inspection (no GPU needed) ----
  * The solver order and the SELL-32 tables a resident system built from (A, opts) uses, for
- * tests of the ordering and layout logic.  No reference counterpart: the reference's
+ * tests of the ordering and layout logic (val: the values, read for VSHE_PRECOND_ILUT only, else
+ * may be NULL).  No reference counterpart: the reference's
  * ViennaCL solvers keep the caller's CSR.  The solver order q = 0..n-1 lists the caller's rows
  * (perm[q]) sorted by forward-sweep level; forward level k is rows [lvr[k], lvr[k+1]).  A
  * SELL-32 slice j spans slots [off[j], off[j+1]) = 32 x width; entry k of the slice's row
@@ -194,8 +204,10 @@ int vshe_csr_residual_noalloc(int64_t n, int64_t nnz, const int64_t *d_row_ptr, 
  * loff[slices_L + 1] (first solver row / slot offset of each L slice, plus the end), lcol /
  * lmap[slots_L], uslot0 / uoff[slices_U + 1], ucol / umap[slots_U], urow[n] (solver row of each
  * backward-sweep slot). */
-int vshe_layout_sizes(int64_t n, int64_t nnz, const int64_t *row_ptr, const int32_t *col, const vshe_solve_opts *opts, int64_t *sizes);
-int vshe_layout_export(int64_t n, int64_t nnz, const int64_t *row_ptr, const int32_t *col, const vshe_solve_opts *opts,
+int vshe_layout_sizes(int64_t n, int64_t nnz, const int64_t *row_ptr, const int32_t *col, const double *val,
+                      const vshe_solve_opts *opts, int64_t *sizes);
+int vshe_layout_export(int64_t n, int64_t nnz, const int64_t *row_ptr, const int32_t *col, const double *val,
+                       const vshe_solve_opts *opts,
                        int32_t *perm, int64_t *lvr, int64_t *aoff, int32_t *acol, int64_t *amap_a,
                        int32_t *lrow0, int64_t *loff, int32_t *lcol, int64_t *lmap,
                        int32_t *uslot0, int64_t *uoff, int32_t *ucol, int64_t *umap, int32_t *urow);

@@ -173,6 +173,44 @@ def csr_solve(A: CSR, b, precond=1, tol=1e-10, maxit=5000, ilut_p=20, ilut_tau=1
     return x, dict(rc=rc, iters=int(it[0]), relres=float(rr[0]), t_setup=float(ts[0]), t_solve=float(tv[0]))
 
 
+def iluk_csr(A: CSR, fill_level, blocks=None):
+    """ILU(k) factor (levels of fill <= k, Saad Alg. 10.5 + IKJ) as a CSR (rp, ci, values)."""
+    bp = None if blocks is None else np.ascontiguousarray(blocks, np.int64)
+    nb = 0 if bp is None else len(bp) - 1
+    L = lib()
+    L.vsheo_iluk_csr.argtypes = [C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int32,
+                                 C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    nnz = np.zeros(1, np.int64)
+    args = (A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double), int(fill_level), nb,
+            None if bp is None else ptr(bp, C.c_int64), ptr(nnz, C.c_int64))
+    if L.vsheo_iluk_csr(*args, None, None, None):
+        raise RuntimeError("oracle iluk failed")
+    rp = np.zeros(A.n + 1, np.int64)
+    ci = np.zeros(int(nnz[0]), np.int32)
+    lu = np.zeros(int(nnz[0]))
+    if L.vsheo_iluk_csr(*args, ptr(rp, C.c_int64), ptr(ci, C.c_int32), ptr(lu, C.c_double)):
+        raise RuntimeError("oracle iluk failed")
+    return rp, ci, lu
+
+
+def ilut_csr(A: CSR, p, tau):
+    """ILUT(p, tau) factor (Saad Alg. 10.6) as one CSR (rp, ci, values), columns ascending."""
+    L = lib()
+    L.vsheo_ilut_csr.argtypes = [C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int32,
+                                 C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    nnz = np.zeros(1, np.int64)
+    args = (A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double), int(p), float(tau), ptr(nnz, C.c_int64))
+    if L.vsheo_ilut_csr(*args, None, None, None):
+        raise RuntimeError("oracle ilut failed")
+    rp = np.zeros(A.n + 1, np.int64)
+    ci = np.zeros(int(nnz[0]), np.int32)
+    lu = np.zeros(int(nnz[0]))
+    if L.vsheo_ilut_csr(*args, ptr(rp, C.c_int64), ptr(ci, C.c_int32), ptr(lu, C.c_double)):
+        raise RuntimeError("oracle ilut failed")
+    return rp, ci, lu
+
+
 def ilu0_values(A: CSR, blocks=None):
     lu = np.zeros(A.nnz)
     bp = None if blocks is None else np.ascontiguousarray(blocks, np.int64)

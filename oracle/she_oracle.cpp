@@ -31,6 +31,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <set>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -909,6 +910,63 @@ static ILU ilu0(int64_t n, const int64_t *rp, const int32_t *ci, const double *v
   return f;
 }
 
+// ILU(k) by levels of fill (Saad, Alg. 10.5): the symbolic phase gives every entry of row i a
+// level, 0 for A's entries and lev(i,k) + lev(k,j) + 1 for the fill created by eliminating
+// with row k; entries of level <= k are kept.  Fill stays inside the row's block when blocks
+// are given.  The numeric phase is the IKJ elimination of ILU(0) on the resulting pattern.
+// Returns the pattern (rp, ci, sorted columns) with A's values scattered into it (fill 0).
+static void iluk_pattern(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int lev_fill,
+                         const std::vector<int32_t> &blk, std::vector<int64_t> &erp, std::vector<int32_t> &eci,
+                         std::vector<int32_t> &elev, std::vector<double> &ev) {
+  erp.assign(size_t(n) + 1, 0);
+  eci.clear(); elev.clear(); ev.clear();
+  std::vector<int> lev(size_t(n), -1);
+  std::vector<double> val(size_t(n), 0.0);
+  for (int64_t i = 0; i < n; ++i) {
+    std::set<int32_t> cols;
+    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) { cols.insert(ci[k]); lev[size_t(ci[k])] = 0; val[size_t(ci[k])] = v[k]; }
+    for (auto it = cols.begin(); it != cols.end() && *it < i; ++it) {
+      const int32_t k = *it;
+      if (blk[size_t(k)] != blk[size_t(i)]) continue;
+      const int lik = lev[size_t(k)];
+      for (int64_t kk = erp[size_t(k)]; kk < erp[size_t(k) + 1]; ++kk) {
+        const int32_t j = eci[size_t(kk)];
+        if (j <= k || blk[size_t(j)] != blk[size_t(i)]) continue;
+        const int l = lik + elev[size_t(kk)] + 1;
+        if (l > lev_fill) continue;
+        if (lev[size_t(j)] < 0) { lev[size_t(j)] = l; val[size_t(j)] = 0.0; cols.insert(j); }
+        else if (l < lev[size_t(j)]) lev[size_t(j)] = l;
+      }
+    }
+    for (int32_t j : cols) { eci.push_back(j); elev.push_back(lev[size_t(j)]); ev.push_back(val[size_t(j)]); lev[size_t(j)] = -1; val[size_t(j)] = 0.0; }
+    erp[size_t(i) + 1] = int64_t(eci.size());
+  }
+}
+
+static ILU iluk(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int lev_fill, int64_t nb, const int64_t *bptr) {
+  std::vector<int32_t> blk = row_blocks(n, nb, bptr);
+  std::vector<int64_t> erp; std::vector<int32_t> eci, elev; std::vector<double> ev;
+  iluk_pattern(n, rp, ci, v, lev_fill, blk, erp, eci, elev, ev);
+  std::vector<double> lu; std::vector<int64_t> diag;
+  ilu0_values(n, erp.data(), eci.data(), ev.data(), blk, lu, diag);
+  ILU f; f.n = n; f.lrp.assign(1, 0); f.urp.assign(1, 0);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int64_t k = erp[size_t(i)]; k < erp[size_t(i) + 1]; ++k) {
+      int64_t j = eci[size_t(k)];
+      if (blk[size_t(j)] != blk[size_t(i)]) continue;
+      if (j < i) { f.lci.push_back(int32_t(j)); f.lv.push_back(lu[size_t(k)]); }
+    }
+    f.uci.push_back(int32_t(i)); f.uv.push_back(lu[size_t(diag[size_t(i)])]);
+    for (int64_t k = erp[size_t(i)]; k < erp[size_t(i) + 1]; ++k) {
+      int64_t j = eci[size_t(k)];
+      if (blk[size_t(j)] != blk[size_t(i)]) continue;
+      if (j > i) { f.uci.push_back(int32_t(j)); f.uv.push_back(lu[size_t(k)]); }
+    }
+    f.lrp.push_back(int64_t(f.lci.size())); f.urp.push_back(int64_t(f.uci.size()));
+  }
+  return f;
+}
+
 // ILUT(p, tau), Saad Alg. 10.6 (row-wise, dual dropping).
 static ILU ilut(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int p, double tau) {
   ILU f; f.n = n; f.lrp.assign(1, 0); f.urp.assign(1, 0);
@@ -1287,6 +1345,7 @@ int vsheo_csr_solve(int64_t n, const int64_t *rp, const int32_t *ci, const doubl
     if (precond == 1) { M = ilu0(n, rp, ci, v, 0, nullptr); pm = &M; }
     else if (precond == 2) { M = ilut(n, rp, ci, v, ilut_p, ilut_tau); pm = &M; }
     else if (precond == 3) { M = ilu0(n, rp, ci, v, nb, bptr); pm = &M; }
+    else if (precond == 4) { M = iluk(n, rp, ci, v, ilut_p, nb, bptr); pm = &M; }
     auto t1 = std::chrono::steady_clock::now();
     SolveStats st;
     std::fill(x, x + n, 0.0);
@@ -1300,6 +1359,44 @@ int vsheo_csr_solve(int64_t n, const int64_t *rp, const int32_t *ci, const doubl
   } catch (std::exception &) {
     return -2;
   }
+}
+
+// ILU(k) factor in CSR (pattern of levels of fill <= k, block-restricted when nb > 0): call with
+// erp == NULL to get the entry count in *nnz_out, then with arrays of that size.
+int vsheo_iluk_csr(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int32_t lev_fill, int64_t nb, const int64_t *bptr,
+                   int64_t *nnz_out, int64_t *erp_out, int32_t *eci_out, double *lu_out) {
+  try {
+    std::vector<int32_t> blk = row_blocks(n, nb, bptr);
+    std::vector<int64_t> erp; std::vector<int32_t> eci, elev; std::vector<double> ev;
+    iluk_pattern(n, rp, ci, v, lev_fill, blk, erp, eci, elev, ev);
+    *nnz_out = erp[size_t(n)];
+    if (!erp_out) return 0;
+    std::vector<double> lu; std::vector<int64_t> diag;
+    ilu0_values(n, erp.data(), eci.data(), ev.data(), blk, lu, diag);
+    std::copy(erp.begin(), erp.end(), erp_out);
+    std::copy(eci.begin(), eci.end(), eci_out);
+    std::copy(lu.begin(), lu.end(), lu_out);
+    return 0;
+  } catch (...) { return -1; }
+}
+
+// ILUT(p, tau) factor as one CSR (L strictly lower, then U with its diagonal, columns ascending):
+// call with rp_out == NULL for the entry count, then with arrays of that size.
+int vsheo_ilut_csr(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int32_t p, double tau,
+                   int64_t *nnz_out, int64_t *rp_out, int32_t *ci_out, double *lu_out) {
+  try {
+    ILU f = ilut(n, rp, ci, v, p, tau);
+    *nnz_out = int64_t(f.lci.size() + f.uci.size());
+    if (!rp_out) return 0;
+    int64_t q = 0;
+    rp_out[0] = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      for (int64_t k = f.lrp[size_t(i)]; k < f.lrp[size_t(i) + 1]; ++k) { ci_out[q] = f.lci[size_t(k)]; lu_out[q++] = f.lv[size_t(k)]; }
+      for (int64_t k = f.urp[size_t(i)]; k < f.urp[size_t(i) + 1]; ++k) { ci_out[q] = f.uci[size_t(k)]; lu_out[q++] = f.uv[size_t(k)]; }
+      rp_out[i + 1] = q;
+    }
+    return 0;
+  } catch (...) { return -1; }
 }
 
 // ILU0 factor values in the pattern of A (block-restricted when nb > 0).

@@ -116,6 +116,21 @@ def test_end_to_end_multicolour(gpu_ctx):
         G.free()
 
 
+def test_end_to_end_ilut_L5(gpu_ctx):
+    """A 2D bar at L = 5, where ILU(0) in any order stalls (the oracle: no convergence in 3000
+    iterations on a 25 x 10 x 60 bar), solved with the ILUT-pattern preconditioner."""
+    dev, cfg = cases.bar_small(L=5, nx=8, ny=4, n_energies=24)
+    cpl = O.golden_coupling(5)
+    P = O.OracleProblem(dev, cfg, cpl)
+    G = gpu.SheProblem(gpu_ctx, dev, cfg, coupling=cpl, precision="mixed", precond="ilut", ilut_entries=20, ilut_drop=1e-3,
+                       tol=1e-10, max_iters=4000)
+    try:
+        st, full_res = G.run()
+        _check_end_to_end(P, G, st, full_res, tol=1e-10)
+    finally:
+        G.free()
+
+
 # (x, density, current) bounds per solve tolerance, relative to the largest entry
 BOUNDS = {1e-10: (5e-6, 5e-6, 5e-4), 1e-12: (5e-8, 5e-8, 5e-6)}
 

@@ -147,3 +147,48 @@ def test_reference_error_behaviour(gpu_ctx):
     # diagonal system solves exactly
     x, st = gpu_ctx.solve_csr(rp, ci, v, np.array([1.0, 1.0]), precision="fp64")
     assert np.allclose(x, [0.5, 0.25], rtol=1e-14)
+
+
+@pytest.mark.parametrize("ordering", ["natural", "multicolor"])
+def test_iluk_factor_and_solve(gpu_ctx, prob, ordering):
+    """ILU(1) (levels of fill, Saad Alg. 10.5): the factor values at A's entries match the
+    oracle's ILU(1) (natural order), and the solve reaches 1e-10 in no more iterations than
+    ILU(0) on the same ordering."""
+    name, P, A = prob
+    if ordering == "natural":
+        S = gpu_ctx.system(A.rp, A.ci, A.v, A.rhs, precision="fp64", precond="ilu0", fill_level=1)
+        try:
+            lu = S.factor_values()
+        finally:
+            S.free()
+        rp, ci, flu = O.iluk_csr(A, 1)
+        ref = np.zeros(A.nnz)
+        for i in range(A.n):
+            cols = ci[rp[i]:rp[i + 1]]
+            pos = np.searchsorted(cols, A.ci[A.rp[i]:A.rp[i + 1]])
+            ref[A.rp[i]:A.rp[i + 1]] = flu[rp[i] + pos]
+        assert np.max(np.abs(lu - ref) / np.maximum(np.abs(ref), 1.0)) < 1e-11
+    xd = O.dense_solve(A, A.rhs) if A.n <= 4000 else O.csr_solve(A, A.rhs, tol=1e-14, maxit=20000)[0]
+    its = {}
+    for k in (0, 1):
+        x, st = gpu_ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision="mixed", precond="ilu0", ordering=ordering,
+                                  fill_level=k, tol=1e-10, max_iters=4000)
+        assert st["status"] == 0 and st["rel_residual"] < 1e-10, st
+        assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-7
+        its[k] = st["iterations"]
+    assert its[1] <= its[0], its
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ilut_pattern_solve(gpu_ctx, prob, precision):
+    """VSHE_PRECOND_ILUT: incomplete LU on the ILUT(20, 1e-3) pattern joined with A's (pattern
+    from the values at creation, factorisation on the device).  Reaches 1e-10 with x within the
+    1e-7 parity bar and in no more iterations than ILU(0)."""
+    name, P, A = prob
+    xd = O.dense_solve(A, A.rhs) if A.n <= 4000 else O.csr_solve(A, A.rhs, tol=1e-14, maxit=20000)[0]
+    x, st = gpu_ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision=precision, precond="ilut", ilut_entries=20, ilut_drop=1e-3,
+                              tol=1e-10, max_iters=4000)
+    assert st["status"] == 0 and st["rel_residual"] < 1e-10, st
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-7
+    _, st0 = gpu_ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision=precision, precond="ilu0", tol=1e-10, max_iters=4000)
+    assert st["iterations"] <= st0["iterations"], (st, st0)

@@ -170,3 +170,102 @@ def test_sell_ilu0_apply_multicolour(prob):
     assert np.all(np.isfinite(z_p)), "a row was scheduled before a row it depends on"
     z_ref = O.ilu0_apply(Ap, lup, b[perm])
     assert np.max(np.abs(z_p - z_ref)) <= 1e-11 * np.max(np.abs(z_ref))
+
+
+def _csr_lookup(rp, ci, vals):
+    """(row, col) -> value of a CSR, as a dict (small cases only)."""
+    d = {}
+    for i in range(len(rp) - 1):
+        for k in range(rp[i], rp[i + 1]):
+            d[(i, int(ci[k]))] = vals[k]
+    return d
+
+
+@pytest.mark.parametrize("ordering", ["natural", "multicolor"])
+def test_sell_iluk_apply_matches_oracle(prob, ordering):
+    """ILU(1): the symbolic fill, the levels over the filled pattern and the SELL factor tables
+    reproduce the oracle's ILU(1) (Saad Alg. 10.5) apply of the solver-order matrix."""
+    name, P, A = prob
+    Lt = gpu.layout(A.rp, A.ci, precond="ilu0", ordering=ordering, fill_level=1)
+    perm = Lt["perm"]
+    n = A.n
+    inv = np.empty(n, np.int64)
+    inv[perm] = np.arange(n)
+    # solver-order matrix (the relabelling is exact for ILU(k): no coupled pair changes order)
+    rows, cols, src = [], [], []
+    for q in range(n):
+        o = perm[q]
+        ks = np.arange(A.rp[o], A.rp[o + 1])
+        c = inv[A.ci[ks]]
+        od = np.argsort(c)
+        cols.append(c[od]); src.append(ks[od]); rows.append(len(ks))
+    rpp = np.zeros(n + 1, np.int64)
+    rpp[1:] = np.cumsum(rows)
+    Ap = O.CSR(rpp, np.concatenate(cols).astype(np.int32), A.v[np.concatenate(src)])
+    frp, fci, flu = O.iluk_csr(Ap, 1)
+    assert frp[-1] == Lt["nnzL"] + Lt["nnzU"] + n, "fill pattern differs from the oracle's"
+    look = _csr_lookup(frp, fci, flu)
+    # factor slot values from (row, column) of every slot
+    lval = np.zeros(len(Lt["lcol"]))
+    for j in range(len(Lt["loff"]) - 1):
+        w = (Lt["loff"][j + 1] - Lt["loff"][j]) // 32
+        for lane in range(Lt["lrow0"][j + 1] - Lt["lrow0"][j]):
+            row = Lt["lrow0"][j] + lane
+            for k in range(w):
+                slot = Lt["loff"][j] + 32 * k + lane
+                c = Lt["lcol"][slot]
+                if c < n:
+                    lval[slot] = look[(row, int(c))]
+    uval = np.zeros(len(Lt["ucol"]))
+    udinv = np.zeros(n)
+    for j in range(len(Lt["uoff"]) - 1):
+        w = (Lt["uoff"][j + 1] - Lt["uoff"][j]) // 32
+        for lane in range(Lt["uslot0"][j + 1] - Lt["uslot0"][j]):
+            t = Lt["uslot0"][j] + lane
+            row = Lt["urow"][t]
+            udinv[t] = 1.0 / look[(row, row)]
+            for k in range(w):
+                slot = Lt["uoff"][j] + 32 * k + lane
+                c = Lt["ucol"][slot]
+                if c < n:
+                    uval[slot] = look[(row, int(c))]
+    b = np.random.default_rng(9).standard_normal(n)
+    z_p = sell_ilu_apply(Lt, lval, uval, udinv, b[perm])
+    assert np.all(np.isfinite(z_p)), "a row was scheduled before a row it depends on"
+    z_ref = O.ilu0_apply(O.CSR(frp, fci, flu), flu, b[perm])
+    assert np.max(np.abs(z_p - z_ref)) <= 1e-11 * np.max(np.abs(z_ref))
+
+
+def _slot_pattern(Lt):
+    """(solver row, solver column) of every non-padding L and U slot, and the diagonal."""
+    n = Lt["n"]
+    pat = set((i, i) for i in range(n))
+    for off, first, colk, rowof in (("loff", "lrow0", "lcol", None), ("uoff", "uslot0", "ucol", "urow")):
+        o, f, c = Lt[off], Lt[first], Lt[colk]
+        for j in range(len(o) - 1):
+            w = (o[j + 1] - o[j]) // 32
+            for lane in range(f[j + 1] - f[j]):
+                t = f[j] + lane
+                row = Lt[rowof][t] if rowof else t
+                for k in range(w):
+                    col = c[o[j] + 32 * k + lane]
+                    if col < n:
+                        pat.add((int(row), int(col)))
+    return pat
+
+
+@pytest.mark.parametrize("p,tau", [(20, 1e-3), (5, 1e-2)])
+def test_ilut_pattern_matches_oracle(prob, p, tau):
+    """VSHE_PRECOND_ILUT: the host analysis keeps the pattern of ILUT(p, tau) (Saad Alg. 10.6)
+    joined with A's; natural order, so solver rows map to the caller's through perm."""
+    name, P, A = prob
+    Lt = gpu.layout(A.rp, A.ci, values=A.v, precond="ilut", ilut_entries=p, ilut_drop=tau)
+    perm = Lt["perm"]
+    got = set((int(perm[i]), int(perm[j])) for i, j in _slot_pattern(Lt))
+    rp, ci, _ = O.ilut_csr(A, p, tau)
+    want = set()
+    for i in range(A.n):
+        want.update((i, int(j)) for j in ci[rp[i]:rp[i + 1]])
+        want.update((i, int(j)) for j in A.ci[A.rp[i]:A.rp[i + 1]])
+        want.add((i, i))
+    assert got == want

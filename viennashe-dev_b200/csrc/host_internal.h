@@ -35,14 +35,16 @@ struct Layout {
   std::vector<int64_t> lvr, lvsL, lvsU;
   int32_t nlevL = 0, nlevU = 0;
   int64_t nslA = 0, nslL = 0, nslU = 0, padA = 0, padL = 0, padU = 0, nnzL = 0, nnzU = 0;
+  int64_t nnzF = 0;                      // entries of the factor pattern (A's + ILU(k) fill)
   std::vector<int64_t> prp, pdiag, amap;
   std::vector<int32_t> pci;
   std::vector<int64_t> aoff, astart, amapS;
   std::vector<int32_t> acol;
   std::vector<int64_t> fmap, dpos, loff, uoff, lstart, ustart;
   std::vector<int32_t> lcol, ucol, urow;
+  // values (caller order, host) are read only for the ILUT pattern and may be NULL otherwise
   int build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci,
-            const vshe_solve_opts &opts, std::string &err);
+            const vshe_solve_opts &opts, const double *values, std::string &err);
 };
 
 // One resident linear system.  The caller's CSR (and rhs) stay in the caller's order; the
@@ -65,6 +67,7 @@ struct System {
   int64_t nslA = 0, nslL = 0, nslU = 0;     // SELL slices
   int64_t padA = 0, padL = 0, padU = 0;     // SELL slots (incl. padding)
   int64_t nnzL = 0, nnzU = 0;               // factor entries (excl. padding)
+  int64_t nnzF = 0;                         // entries of the factor pattern (A's + ILU(k) fill)
   // device
   DevArena arena;
   int64_t *d_rp = nullptr; int32_t *d_ci = nullptr;
@@ -92,9 +95,9 @@ struct System {
   // A system whose CSR and rhs already live on the device (owned by the caller): the host
   // pattern is used for the schedules, values are read from the device at solve time.
   int create_borrowed(Ctx &ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, int64_t *d_rp_,
-                      int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o);
+                      int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o, const double *host_val = nullptr);
   int set_values(Ctx &ctx, const double *v, const double *rhs);
-  int setup_pattern(Ctx &ctx);          // ordering, schedules, device buffers
+  int setup_pattern(Ctx &ctx, const double *host_val);  // ordering, schedules, device buffers
   // gathers the caller-order values and rhs into the solver-order SELL A, the factorisation
   // CSR and b_p (on the context's stream)
   void prepare(Ctx &ctx);

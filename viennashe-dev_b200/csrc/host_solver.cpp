@@ -121,7 +121,7 @@ int System::create(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_, const
   if (!d_b64) return ctx.cuda_fail(e, "cudaMalloc rhs");
   if ((e = cudaMemcpyAsync(d_rp, rp.data(), sizeof(int64_t) * rp.size(), cudaMemcpyHostToDevice, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "upload rp");
   if ((e = cudaMemcpyAsync(d_ci, ci.data(), sizeof(int32_t) * ci.size(), cudaMemcpyHostToDevice, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "upload ci");
-  int rc = setup_pattern(ctx);
+  int rc = setup_pattern(ctx, v);
   if (rc) return rc;
   rc = set_values(ctx, v, rhs);
   if (rc) return rc;
@@ -130,7 +130,7 @@ int System::create(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_, const
 }
 
 int System::create_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_, const int32_t *ci_, int64_t *d_rp_,
-                            int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o) {
+                            int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o, const double *host_val) {
   n = n_; nnz = nnz_; opts = o; borrowed = true;
   if (n <= 0 || nnz <= 0) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "empty system");
   if (n >= (int64_t(1) << 31) - 64) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "more than 2^31 - 64 rows");
@@ -140,7 +140,7 @@ int System::create_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *r
     if (rp[i + 1] == rp[i]) return ctx.fail(VSHE_E_EMPTY_ROW, "row " + std::to_string(i));
   d_rp = d_rp_; d_ci = d_ci_; d_av64 = d_val; d_b64 = d_rhs;
   bnorm_host = 1.0;  // the trivial-rhs test uses the device-side norm
-  return setup_pattern(ctx);
+  return setup_pattern(ctx, host_val);
 }
 
 int System::set_values(Ctx &ctx, const double *v, const double *rhs) {
@@ -162,13 +162,14 @@ int System::set_values(Ctx &ctx, const double *v, const double *rhs) {
 void System::prepare(Ctx &ctx) {
   cudaStream_t s = ctx.stream;
   vk_gather_values(padA, d_amapS, d_av64, d_aval, s);
-  if (has_pc) vk_gather_values(nnz, d_amap, d_av64, d_lu64, s);
+  if (has_pc) vk_gather_values(nnzF, d_amap, d_av64, d_lu64, s);
   vk_permute(n, d_perm, d_b64, d_bp, 1, s);
 }
 
-// greedy colouring of the symmetrised pattern, rows grouped by block
+// Greedy colouring of the symmetrised pattern within blocks: distance 1 (coupled rows differ)
+// or distance 2 (rows with a common neighbour differ as well).
 static void greedy_colours(int64_t n, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci, const std::vector<int32_t> &blk,
-                           std::vector<int32_t> &col) {
+                           std::vector<int32_t> &col, int distance) {
   std::vector<int64_t> tcnt((size_t)(n) + 1, 0);
   for (int64_t i = 0; i < n; ++i)
     for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tcnt[size_t(ci[k]) + 1]++;
@@ -179,6 +180,10 @@ static void greedy_colours(int64_t n, const std::vector<int64_t> &rp, const std:
     for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tci[size_t(pos[size_t(ci[k])]++)] = int32_t(i);
   col.assign(size_t(n), -1);
   std::vector<int64_t> mark(64, -1);
+  auto neighbours = [&](int64_t i, auto &&fn) {
+    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) fn(ci[k]);
+    for (int64_t k = tcnt[size_t(i)]; k < tcnt[size_t(i) + 1]; ++k) fn(tci[size_t(k)]);
+  };
   for (int64_t i = 0; i < n; ++i) {
     auto visit = [&](int32_t j) {
       if (j == i || col[size_t(j)] < 0 || blk[size_t(j)] != blk[size_t(i)]) return;
@@ -186,8 +191,10 @@ static void greedy_colours(int64_t n, const std::vector<int64_t> &rp, const std:
       if (c >= int32_t(mark.size())) mark.resize(size_t(c) + 1, -1);
       mark[size_t(c)] = i;
     };
-    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) visit(ci[k]);
-    for (int64_t k = tcnt[size_t(i)]; k < tcnt[size_t(i) + 1]; ++k) visit(tci[size_t(k)]);
+    neighbours(i, [&](int32_t j) {
+      visit(j);
+      if (distance > 1 && blk[size_t(j)] == blk[size_t(i)]) neighbours(j, visit);
+    });
     int32_t c = 0;
     while (c < int32_t(mark.size()) && mark[size_t(c)] == i) ++c;
     col[size_t(i)] = c;
@@ -216,8 +223,10 @@ static void sell_layout(const std::vector<int64_t> &len_of_t, const std::vector<
 }
 
 int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci,
-                  const vshe_solve_opts &opts, std::string &err) {
+                  const vshe_solve_opts &opts, const double *values, std::string &err) {
   const bool has_pc = opts.precond != VSHE_PRECOND_NONE;
+  const bool ilut = opts.precond == VSHE_PRECOND_ILUT;
+  if (ilut && !values) { err = "the ILUT pattern needs the matrix values at creation"; return VSHE_E_INVALID_ARGUMENT; }
   // block ids in the caller's order
   std::vector<int32_t> blk0((size_t)(n), 0);
   if (opts.precond == VSHE_PRECOND_BLOCK_ILU0 && opts.n_blocks > 0 && opts.block_ptr) {
@@ -240,7 +249,9 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     }
   } else if (has_pc && opts.ordering == VSHE_ORDER_MULTICOLOR) {
     std::vector<int32_t> col;
-    greedy_colours(n, rp, ci, blk0, col);
+    // ILU(k > 0): rows two steps apart get different colours too, so that the fill (which
+    // couples such rows) does not chain rows of one colour into extra levels
+    greedy_colours(n, rp, ci, blk0, col, opts.fill_level > 0 ? 2 : 1);
     std::iota(base.begin(), base.end(), 0);
     std::stable_sort(base.begin(), base.end(), [&](int32_t a, int32_t b) {
       if (blk0[size_t(a)] != blk0[size_t(b)]) return blk0[size_t(a)] < blk0[size_t(b)];
@@ -252,27 +263,201 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   std::vector<int32_t> binv((size_t)n);
   for (int64_t i = 0; i < n; ++i) binv[size_t(base[size_t(i)])] = int32_t(i);
 
-  // Forward levels over the symmetrised, block-restricted graph in base order: a row's level is
-  // one more than the highest level of any coupled (A_ij or A_ji != 0) earlier row of its block.
-  // Sorting by these levels keeps the relative order of every coupled pair, so ILU(0) in the
-  // sorted order is ILU(0) in the base order, relabelled.
+  // Pattern of the incomplete factor F, in the caller's numbering: A's entries (fsrc = entry
+  // of A) and, for ILU(k) with k = fill_level > 0, the fill of levels <= k (fsrc = -1) from the
+  // symbolic phase of Saad's Alg. 10.5 run in base order, fill kept inside the row's block.
+  std::vector<int64_t> frp;
+  std::vector<int32_t> fci;
+  std::vector<int64_t> fsrc;
+  const int kfill = has_pc && !ilut ? std::max(0, int(opts.fill_level)) : 0;
+  if (kfill == 0 && !ilut) {
+    frp = rp; fci = ci;
+    fsrc.resize((size_t)nnz);
+    std::iota(fsrc.begin(), fsrc.end(), int64_t(0));
+  } else {
+    // base-order rows of A: (base column, entry)
+    std::vector<int64_t> brp((size_t)n + 1, 0);
+    std::vector<std::pair<int32_t, int64_t>> bent((size_t)nnz);
+    for (int64_t i = 0; i < n; ++i) {
+      const int32_t o = base[size_t(i)];
+      int64_t p = brp[size_t(i)];
+      for (int64_t k = rp[size_t(o)]; k < rp[size_t(o) + 1]; ++k) bent[size_t(p++)] = {binv[size_t(ci[size_t(k)])], k};
+      std::sort(bent.begin() + brp[size_t(i)], bent.begin() + p);
+      brp[size_t(i) + 1] = p;
+    }
+    std::vector<std::vector<std::pair<int32_t, int64_t>>> rows((size_t)n);  // base order: (base column, entry or -1)
+    if (ilut) {
+      // ILUT(p, tau), Saad Alg. 10.6, in base order: the row is eliminated with the kept rows
+      // above it in increasing column order; a multiplier or entry below tau * ||a_i|| is
+      // dropped, then the p largest of L and of U are kept (the diagonal always).  Only the
+      // pattern is kept here; the device factorises on the pattern joined with A's.
+      const int pkeep = opts.ilut_entries > 0 ? opts.ilut_entries : 60;
+      const double tau = opts.ilut_drop > 0 ? opts.ilut_drop : 1e-4;
+      std::vector<int64_t> urp((size_t)n + 1, 0);
+      std::vector<int32_t> ucol;
+      std::vector<double> uval, udiag((size_t)n, 0.0);
+      std::vector<double> w((size_t)n, 0.0);
+      std::vector<char> nz((size_t)n, 0);
+      std::vector<int32_t> cols, heap;
+      std::vector<std::pair<double, int32_t>> lo, up;
+      for (int64_t i = 0; i < n; ++i) {
+        cols.clear(); heap.clear();
+        double rn = 0.0;
+        for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) {
+          const int32_t j = bent[size_t(k)].first;
+          const double a = values[bent[size_t(k)].second];
+          w[size_t(j)] = a; nz[size_t(j)] = 1; cols.push_back(j);
+          rn += a * a;
+          if (j < i) heap.push_back(j);
+        }
+        const double ti = tau * std::sqrt(rn);
+        if (!nz[size_t(i)]) { nz[size_t(i)] = 1; w[size_t(i)] = 0.0; cols.push_back(int32_t(i)); }
+        std::make_heap(heap.begin(), heap.end(), std::greater<int32_t>());
+        int32_t last = -1;
+        while (!heap.empty()) {
+          std::pop_heap(heap.begin(), heap.end(), std::greater<int32_t>());
+          const int32_t k = heap.back(); heap.pop_back();
+          if (k == last) continue;
+          last = k;
+          if (udiag[size_t(k)] == 0.0) { w[size_t(k)] = 0.0; continue; }
+          const double wk = w[size_t(k)] / udiag[size_t(k)];
+          if (std::fabs(wk) < ti) { w[size_t(k)] = 0.0; continue; }
+          w[size_t(k)] = wk;
+          for (int64_t kk = urp[size_t(k)]; kk < urp[size_t(k) + 1]; ++kk) {
+            const int32_t j = ucol[size_t(kk)];
+            if (!nz[size_t(j)]) {
+              nz[size_t(j)] = 1; w[size_t(j)] = 0.0; cols.push_back(j);
+              if (j < i) { heap.push_back(j); std::push_heap(heap.begin(), heap.end(), std::greater<int32_t>()); }
+            }
+            w[size_t(j)] -= wk * uval[size_t(kk)];
+          }
+        }
+        lo.clear(); up.clear();
+        for (int32_t j : cols) {
+          if (j == i || w[size_t(j)] == 0.0 || std::fabs(w[size_t(j)]) < ti) continue;
+          (j < i ? lo : up).push_back({std::fabs(w[size_t(j)]), j});
+        }
+        auto keep = [&](std::vector<std::pair<double, int32_t>> &v) {
+          if (int(v.size()) > pkeep) {
+            std::nth_element(v.begin(), v.begin() + pkeep, v.end(),
+                             [](const std::pair<double, int32_t> &a, const std::pair<double, int32_t> &b) { return a.first > b.first; });
+            v.resize(size_t(pkeep));
+          }
+        };
+        keep(lo); keep(up);
+        double d = w[size_t(i)];
+        if (d == 0.0) d = ti > 0.0 ? ti : 1.0;
+        udiag[size_t(i)] = d;
+        std::sort(up.begin(), up.end(), [](const std::pair<double, int32_t> &a, const std::pair<double, int32_t> &b) { return a.second < b.second; });
+        for (auto &e : up) { ucol.push_back(e.second); uval.push_back(w[size_t(e.second)]); }
+        urp[size_t(i) + 1] = int64_t(ucol.size());
+        // the factor pattern of row i: the kept entries, the diagonal and A's own entries
+        std::vector<int32_t> pat;
+        for (auto &e : lo) pat.push_back(e.second);
+        pat.push_back(int32_t(i));
+        for (auto &e : up) pat.push_back(e.second);
+        for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) pat.push_back(bent[size_t(k)].first);
+        std::sort(pat.begin(), pat.end());
+        pat.erase(std::unique(pat.begin(), pat.end()), pat.end());
+        auto &row = rows[size_t(i)];
+        row.reserve(pat.size());
+        int64_t ka = brp[size_t(i)];
+        for (int32_t j : pat) {
+          while (ka < brp[size_t(i) + 1] && bent[size_t(ka)].first < j) ++ka;
+          const bool in_a = ka < brp[size_t(i) + 1] && bent[size_t(ka)].first == j;
+          row.push_back({j, in_a ? bent[size_t(ka)].second : int64_t(-1)});
+        }
+        for (int32_t j : cols) { nz[size_t(j)] = 0; w[size_t(j)] = 0.0; }
+      }
+    } else {
+      // symbolic ILU(k): the final rows' upper parts (column, level) feed later rows
+      std::vector<int64_t> urp((size_t)n + 1, 0);
+      std::vector<int32_t> ucolv, ulevv;
+      std::vector<int32_t> lvl((size_t)n, -1);
+      std::vector<int64_t> src((size_t)n, -1);
+      std::vector<int32_t> cols, heap;
+      for (int64_t i = 0; i < n; ++i) {
+        const int32_t bi = blk0[size_t(base[size_t(i)])];
+        cols.clear(); heap.clear();
+        for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) {
+          const int32_t j = bent[size_t(k)].first;
+          lvl[size_t(j)] = 0; src[size_t(j)] = bent[size_t(k)].second; cols.push_back(j);
+          if (j < i) heap.push_back(j);
+        }
+        std::make_heap(heap.begin(), heap.end(), std::greater<int32_t>());
+        int32_t last = -1;
+        while (!heap.empty()) {
+          std::pop_heap(heap.begin(), heap.end(), std::greater<int32_t>());
+          const int32_t k = heap.back(); heap.pop_back();
+          if (k == last) continue;
+          last = k;
+          if (blk0[size_t(base[size_t(k)])] != bi) continue;
+          const int32_t lik = lvl[size_t(k)];
+          for (int64_t kk = urp[size_t(k)]; kk < urp[size_t(k) + 1]; ++kk) {
+            const int32_t j = ucolv[size_t(kk)];
+            if (blk0[size_t(base[size_t(j)])] != bi) continue;
+            const int32_t l = lik + ulevv[size_t(kk)] + 1;
+            if (l > kfill) continue;
+            if (lvl[size_t(j)] < 0) {
+              lvl[size_t(j)] = l; src[size_t(j)] = -1; cols.push_back(j);
+              if (j < i) { heap.push_back(j); std::push_heap(heap.begin(), heap.end(), std::greater<int32_t>()); }
+            } else if (l < lvl[size_t(j)]) {
+              lvl[size_t(j)] = l;
+            }
+          }
+        }
+        std::sort(cols.begin(), cols.end());
+        auto &row = rows[size_t(i)];
+        row.reserve(cols.size());
+        for (int32_t j : cols) {
+          row.push_back({j, src[size_t(j)]});
+          if (j > i) { ucolv.push_back(j); ulevv.push_back(lvl[size_t(j)]); }
+          lvl[size_t(j)] = -1; src[size_t(j)] = -1;
+        }
+        urp[size_t(i) + 1] = int64_t(ucolv.size());
+      }
+    }
+    // back to the caller's numbering, columns ascending
+    frp.assign((size_t)n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) frp[size_t(base[size_t(i)]) + 1] = int64_t(rows[size_t(i)].size());
+    for (int64_t i = 0; i < n; ++i) frp[size_t(i) + 1] += frp[size_t(i)];
+    fci.resize(size_t(frp[size_t(n)]));
+    fsrc.resize(size_t(frp[size_t(n)]));
+    std::vector<std::pair<int32_t, int64_t>> tmp;
+    for (int64_t i = 0; i < n; ++i) {
+      const int32_t o = base[size_t(i)];
+      tmp.clear();
+      for (auto &e : rows[size_t(i)]) tmp.push_back({base[size_t(e.first)], e.second});
+      std::sort(tmp.begin(), tmp.end());
+      int64_t p = frp[size_t(o)];
+      for (auto &e : tmp) { fci[size_t(p)] = e.first; fsrc[size_t(p)] = e.second; ++p; }
+      std::vector<std::pair<int32_t, int64_t>>().swap(rows[size_t(i)]);
+    }
+  }
+  const int64_t fnnz = frp[size_t(n)];
+  nnzF = fnnz;
+
+  // Forward levels over the symmetrised, block-restricted graph of F in base order: a row's
+  // level is one more than the highest level of any coupled (F_ij or F_ji != 0) earlier row of
+  // its block.  Sorting by these levels keeps the relative order of every coupled pair, so the
+  // incomplete factorisation in the sorted order is the one in the base order, relabelled.
   std::vector<int32_t> lev((size_t)n, 0);
   nlevL = 1;
   if (has_pc) {
     std::vector<int64_t> tp((size_t)n + 1, 0);
-    for (int64_t k = 0; k < nnz; ++k) tp[size_t(ci[size_t(k)]) + 1]++;
+    for (int64_t k = 0; k < fnnz; ++k) tp[size_t(fci[size_t(k)]) + 1]++;
     for (int64_t i = 0; i < n; ++i) tp[size_t(i) + 1] += tp[size_t(i)];
-    std::vector<int32_t> tr((size_t)nnz);
+    std::vector<int32_t> tr((size_t)fnnz);
     {
       std::vector<int64_t> pos(tp.begin(), tp.end() - 1);
       for (int64_t i = 0; i < n; ++i)
-        for (int64_t k = rp[size_t(i)]; k < rp[size_t(i) + 1]; ++k) tr[size_t(pos[size_t(ci[size_t(k)])]++)] = int32_t(i);
+        for (int64_t k = frp[size_t(i)]; k < frp[size_t(i) + 1]; ++k) tr[size_t(pos[size_t(fci[size_t(k)])]++)] = int32_t(i);
     }
     for (int64_t i = 0; i < n; ++i) {
       const int32_t o = base[size_t(i)];
       int32_t m = -1;
-      for (int64_t k = rp[size_t(o)]; k < rp[size_t(o) + 1]; ++k) {
-        const int32_t j = ci[size_t(k)];
+      for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k) {
+        const int32_t j = fci[size_t(k)];
         if (binv[size_t(j)] < i && blk0[size_t(j)] == blk0[size_t(o)]) m = std::max(m, lev[size_t(j)]);
       }
       for (int64_t k = tp[size_t(o)]; k < tp[size_t(o) + 1]; ++k) {
@@ -298,14 +483,14 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   for (size_t k = 1; k < lvr.size(); ++k) lvr[k] += lvr[k - 1];
 
   // solver-order CSR with the map back to A's entries
-  prp.assign((size_t)n + 1, 0); pdiag.assign((size_t)n, -1); amap.assign((size_t)nnz, 0);
-  pci.assign((size_t)nnz, 0);
+  prp.assign((size_t)n + 1, 0); pdiag.assign((size_t)n, -1); amap.assign((size_t)fnnz, 0);
+  pci.assign((size_t)fnnz, 0);
   {
     std::vector<std::pair<int32_t, int64_t>> row;
     for (int64_t i = 0; i < n; ++i) {
       const int64_t o = perm[size_t(i)];
       row.clear();
-      for (int64_t k = rp[size_t(o)]; k < rp[size_t(o) + 1]; ++k) row.push_back({inv[size_t(ci[size_t(k)])], k});
+      for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k) row.push_back({inv[size_t(fci[size_t(k)])], fsrc[size_t(k)]});
       std::sort(row.begin(), row.end());
       int64_t p = prp[size_t(i)];
       for (auto &x : row) {
@@ -320,11 +505,13 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   }
   const int32_t PAD = int32_t(n);  // padding column: entry n of every vector stays 0
 
-  // SELL-32 A in solver order: slices of 32 consecutive rows
+  // SELL-32 A in solver order: slices of 32 consecutive rows, A's own entries only (the fill of
+  // an ILU(k) factor is not part of A)
   std::vector<int64_t> alvs;
   {
-    std::vector<int64_t> len((size_t)n);
-    for (int64_t i = 0; i < n; ++i) len[size_t(i)] = prp[size_t(i) + 1] - prp[size_t(i)];
+    std::vector<int64_t> len((size_t)n, 0);
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t p = prp[size_t(i)]; p < prp[size_t(i) + 1]; ++p) len[size_t(i)] += amap[size_t(p)] >= 0 ? 1 : 0;
     std::vector<int64_t> one{0, n};
     sell_layout(len, one, aoff, astart, alvs);
   }
@@ -336,10 +523,12 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     for (int64_t i = astart[size_t(j)]; i < astart[size_t(j) + 1]; ++i) {
       const int lane = int(i - astart[size_t(j)]);
       int64_t kk = 0;
-      for (int64_t p = prp[size_t(i)]; p < prp[size_t(i) + 1]; ++p, ++kk) {
+      for (int64_t p = prp[size_t(i)]; p < prp[size_t(i) + 1]; ++p) {
+        if (amap[size_t(p)] < 0) continue;
         const int64_t slot = aoff[size_t(j)] + 32 * kk + lane;
         acol[size_t(slot)] = pci[size_t(p)];
         amapS[size_t(slot)] = amap[size_t(p)];
+        ++kk;
       }
     }
   }
@@ -385,7 +574,7 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     sell_layout(ulen_t, uvt, uoff, ustart, lvsU);
     nslU = int64_t(ustart.size()) - 1;
     padU = uoff.back();
-    fmap.assign((size_t)nnz, -1);
+    fmap.assign((size_t)fnnz, -1);
     lcol.assign((size_t)padL, PAD);
     ucol.assign((size_t)padU, PAD);
     nnzL = nnzU = 0;
@@ -423,17 +612,17 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   return VSHE_OK;
 }
 
-int System::setup_pattern(Ctx &ctx) {
+int System::setup_pattern(Ctx &ctx, const double *host_val) {
   has_pc = opts.precond != VSHE_PRECOND_NONE;
   mixed = opts.precision == VSHE_PRECISION_MIXED;
   cudaError_t e;
   Layout Lt;
   std::string err;
-  int rc = Lt.build(n, nnz, rp, ci, opts, err);
+  int rc = Lt.build(n, nnz, rp, ci, opts, host_val, err);
   if (rc) return ctx.fail(rc, err);
   perm = Lt.perm; blk = Lt.blk; lvr = Lt.lvr; lvsL = Lt.lvsL; lvsU = Lt.lvsU;
   nlevL = Lt.nlevL; nlevU = Lt.nlevU; nslA = Lt.nslA; nslL = Lt.nslL; nslU = Lt.nslU;
-  padA = Lt.padA; padL = Lt.padL; padU = Lt.padU; nnzL = Lt.nnzL; nnzU = Lt.nnzU;
+  padA = Lt.padA; padL = Lt.padL; padU = Lt.padU; nnzL = Lt.nnzL; nnzU = Lt.nnzU; nnzF = Lt.nnzF;
   const auto &prp = Lt.prp; const auto &pci = Lt.pci; const auto &pdiag = Lt.pdiag; const auto &amap = Lt.amap;
   const auto &aoff = Lt.aoff; const auto &amapS = Lt.amapS; const auto &acol = Lt.acol;
   const auto &fmap = Lt.fmap; const auto &dpos = Lt.dpos; const auto &loff = Lt.loff; const auto &uoff = Lt.uoff;
@@ -459,13 +648,13 @@ int System::setup_pattern(Ctx &ctx) {
   if (has_pc) {
     ALLOC(d_blk, int32_t, n);
     ALLOC(d_prp, int64_t, n + 1);
-    ALLOC(d_pci, int32_t, nnz);
+    ALLOC(d_pci, int32_t, nnzF);
     ALLOC(d_pdiag, int64_t, n);
-    ALLOC(d_amap, int64_t, nnz);
-    ALLOC(d_fmap, int64_t, nnz);
+    ALLOC(d_amap, int64_t, nnzF);
+    ALLOC(d_fmap, int64_t, nnzF);
     ALLOC(d_dpos, int64_t, n);
     ALLOC(d_lvr, int64_t, nlevL + 1);
-    ALLOC(d_lu64, double, nnz);
+    ALLOC(d_lu64, double, nnzF);
     ALLOC(d_lrow0, int32_t, nslL + 1);
     ALLOC(d_loff, int64_t, nslL + 1);
     ALLOC(d_uslot0, int32_t, nslU + 1);
@@ -820,9 +1009,9 @@ int Batch::factor(Ctx &ctx) {
   if (rc) return ctx.cuda_fail(cudaError_t(rc), "ilu0 launch");
   for (System *S : sys) {
     if (mixed)
-      vk_split_factor_f32(S->nnz, S->n, S->d_lu64, S->d_fmap, S->d_pdiag, S->d_dpos, (float *)S->d_lval, (float *)S->d_uval, (float *)S->d_udinv, s);
+      vk_split_factor_f32(S->nnzF, S->n, S->d_lu64, S->d_fmap, S->d_pdiag, S->d_dpos, (float *)S->d_lval, (float *)S->d_uval, (float *)S->d_udinv, s);
     else
-      vk_split_factor_f64(S->nnz, S->n, S->d_lu64, S->d_fmap, S->d_pdiag, S->d_dpos, (double *)S->d_lval, (double *)S->d_uval, (double *)S->d_udinv, s);
+      vk_split_factor_f64(S->nnzF, S->n, S->d_lu64, S->d_fmap, S->d_pdiag, S->d_dpos, (double *)S->d_lval, (double *)S->d_uval, (double *)S->d_udinv, s);
   }
   return check_err(ctx, "ilu0 factorisation");
 }
@@ -1401,9 +1590,9 @@ int vshe_system_factor_values(vshe_ctx *ctx, int64_t h, double *lu) {
   rc = B->factor(*ctx);
   if (rc) return rc;
   System *S = B->sys[0];
-  std::vector<double> lp((size_t)S->nnz);
-  std::vector<int64_t> amap((size_t)S->nnz);
-  std::vector<int32_t> pci((size_t)S->nnz);
+  std::vector<double> lp((size_t)S->nnzF);
+  std::vector<int64_t> amap((size_t)S->nnzF);
+  std::vector<int32_t> pci((size_t)S->nnzF);
   std::vector<int64_t> prp((size_t)S->n + 1);
   cudaError_t e = cudaMemcpyAsync(lp.data(), S->d_lu64, sizeof(double) * lp.size(), cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(amap.data(), S->d_amap, sizeof(int64_t) * amap.size(), cudaMemcpyDeviceToHost, ctx->stream);
@@ -1413,6 +1602,7 @@ int vshe_system_factor_values(vshe_ctx *ctx, int64_t h, double *lu) {
   if (e != cudaSuccess) return ctx->cuda_fail(e, "download factor");
   for (int64_t i = 0; i < S->n; ++i)
     for (int64_t k = prp[size_t(i)]; k < prp[size_t(i) + 1]; ++k) {
+      if (amap[size_t(k)] < 0) continue;  // ILU(k) fill: not an entry of A
       const bool in_factor = S->blk[size_t(pci[size_t(k)])] == S->blk[size_t(i)];
       lu[amap[size_t(k)]] = in_factor ? lp[size_t(k)] : 0.0;
     }
@@ -1421,7 +1611,7 @@ int vshe_system_factor_values(vshe_ctx *ctx, int64_t h, double *lu) {
 
 // Host-only view of the solver layout (no GPU): validates the inputs like vshe_system_create
 // and builds the same Layout a resident system would use.
-static int layout_for(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const vshe_solve_opts *opts, Layout &L) {
+static int layout_for(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *val, const vshe_solve_opts *opts, Layout &L) {
   if (n <= 0 || nnz <= 0 || !rp || !ci) return VSHE_E_INVALID_ARGUMENT;
   if (rp[0] != 0 || rp[n] != nnz) return VSHE_E_INVALID_ARGUMENT;
   std::vector<int64_t> vrp(rp, rp + n + 1);
@@ -1435,25 +1625,26 @@ static int layout_for(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *
   vshe_solve_opts o;
   if (opts) o = *opts; else vshe_default_opts(&o);
   std::string err;
-  return L.build(n, nnz, vrp, vci, o, err);
+  return L.build(n, nnz, vrp, vci, o, val, err);
 }
 
-int vshe_layout_sizes(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const vshe_solve_opts *opts, int64_t *sizes) {
+int vshe_layout_sizes(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *val, const vshe_solve_opts *opts,
+                      int64_t *sizes) {
   if (!sizes) return VSHE_E_INVALID_ARGUMENT;
   Layout L;
-  int rc = layout_for(n, nnz, rp, ci, opts, L);
+  int rc = layout_for(n, nnz, rp, ci, val, opts, L);
   if (rc) return rc;
   const int64_t v[10] = {L.nslA, L.padA, L.nslL, L.padL, L.nslU, L.padU, L.nlevL, L.nlevU, L.nnzL, L.nnzU};
   for (int k = 0; k < 10; ++k) sizes[k] = v[k];
   return VSHE_OK;
 }
 
-int vshe_layout_export(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const vshe_solve_opts *opts,
+int vshe_layout_export(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *val, const vshe_solve_opts *opts,
                        int32_t *perm, int64_t *lvr, int64_t *aoff, int32_t *acol, int64_t *amap_a,
                        int32_t *lrow0, int64_t *loff, int32_t *lcol, int64_t *lmap,
                        int32_t *uslot0, int64_t *uoff, int32_t *ucol, int64_t *umap, int32_t *urow) {
   Layout L;
-  int rc = layout_for(n, nnz, rp, ci, opts, L);
+  int rc = layout_for(n, nnz, rp, ci, val, opts, L);
   if (rc) return rc;
   auto put = [](auto *dst, const auto &src) { if (dst) for (size_t k = 0; k < src.size(); ++k) dst[k] = src[k]; };
   put(perm, L.perm);

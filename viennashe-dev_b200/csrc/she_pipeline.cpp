@@ -207,25 +207,35 @@ int SheProblem::create(Ctx &ctx, const vshe_device_desc &d, const vshe_she_confi
     // greedy colouring of the mesh graph, energies by the parity of H / n_op (in-scattering
     // couples H and H +- n_op).  All harmonics of a node share its colour; rows are ordered
     // by colour, then by their original position.
+    // ILU(k > 0) colours at distance 2 (cells with a common neighbour differ, and energies in
+    // three classes of H / n_op), so that the fill does not chain nodes of one colour.
+    const bool d2 = so.fill_level > 0;
     std::vector<int32_t> ccol((size_t)H.nc, -1);
     for (int c = 0; c < H.nc; ++c) {
       uint64_t used = 0;
       for (int k = H.cf_ptr[c]; k < H.cf_ptr[c + 1]; ++k) {
         const int o = H.other_cell(H.cf_idx[k], c);
-        if (o >= 0 && ccol[(size_t)o] >= 0 && ccol[(size_t)o] < 64) used |= (uint64_t(1) << ccol[(size_t)o]);
+        if (o < 0) continue;
+        if (ccol[(size_t)o] >= 0 && ccol[(size_t)o] < 64) used |= (uint64_t(1) << ccol[(size_t)o]);
+        if (!d2) continue;
+        for (int k2 = H.cf_ptr[o]; k2 < H.cf_ptr[o + 1]; ++k2) {
+          const int o2 = H.other_cell(H.cf_idx[k2], o);
+          if (o2 >= 0 && o2 != c && ccol[(size_t)o2] >= 0 && ccol[(size_t)o2] < 64) used |= (uint64_t(1) << ccol[(size_t)o2]);
+        }
       }
       int col = 0;
       while (col < 63 && (used >> col) & 1) ++col;
       ccol[(size_t)c] = col;
     }
     const int nop = std::max(1, int(std::lround(H.hbar_omega / H.cfg.energy_spacing)));
+    const int nh_classes = d2 ? 3 : 2;
     std::vector<int32_t> rowcol((size_t)n_red);
     for (size_t k = 0; k + 1 < H.even_nodes.size(); k += 2) {
       const int c = H.even_nodes[k], h = H.even_nodes[k + 1];
       const int64_t base = H.idx_c[(size_t)c * H.NH + h];
       int ne = 0;
       for (int l = 0; l <= H.ord_c[(size_t)c * H.NH + h]; l += 2) ne += 2 * l + 1;
-      const int32_t col = ccol[(size_t)c] * 2 + ((h / nop) & 1);
+      const int32_t col = ccol[(size_t)c] * nh_classes + ((h / nop) % nh_classes);
       for (int q = 0; q < ne; ++q) rowcol[(size_t)(base + q)] = col;
     }
     node_perm.resize((size_t)n_red);
@@ -238,8 +248,15 @@ int SheProblem::create(Ctx &ctx, const vshe_device_desc &d, const vshe_she_confi
     so.n_blocks = int64_t(slab_ptr.size()) - 1;
     so.block_ptr = slab_ptr.data();
   }
+  std::vector<double> hval;
+  if (so.precond == VSHE_PRECOND_ILUT) {
+    // the ILUT pattern is found from the values of this first assembly
+    hval.resize((size_t)nnz_red);
+    if ((e = cudaMemcpyAsync(hval.data(), d_rval, sizeof(double) * hval.size(), cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "values");
+    if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "values");
+  }
   sys.reset(new System);
-  rc = sys->create_borrowed(ctx, n_red, nnz_red, hrp.data(), hci.data(), d_rrp, d_rci, d_rval, d_rrhs, so);
+  rc = sys->create_borrowed(ctx, n_red, nnz_red, hrp.data(), hci.data(), d_rrp, d_rci, d_rval, d_rrhs, so, hval.empty() ? nullptr : hval.data());
   if (rc) return rc;
   sys->opts.block_ptr = nullptr;  // the pointers above are only read during creation
   sys->opts.perm = nullptr;

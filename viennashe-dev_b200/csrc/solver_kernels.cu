@@ -559,21 +559,30 @@ __global__ void __launch_bounds__(kCtaThreads) k_trsv_cta(const SysDev<P> *sys, 
   if (!active[s] || st[s].done || (which == 1 && st[s].s_conv)) return;
   const SysDev<P> &S = sys[s];
   const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // A level's slice loads (factor entries, the row's own operand) do not depend on the level
+  // before it, so each warp issues them before the barrier that closes the previous level and
+  // only the gathers of solved values wait for it.  Levels wider than one slice per warp
+  // finish their remaining slices after the first.
   for (int pass = 0; pass < 2; ++pass) {
     const bool lower = pass == 0;
     const int nlev = lower ? S.nlevL : S.nlevU;
     const int64_t *lvs = lower ? S.lvsL : S.lvsU;
+    TrsvSlice<P, true> cur;
+    if (nlev > 0 && lvs[0] + w < lvs[1]) cur.load_slice(S, (int)(lvs[0] + w), lower, which);
     for (int k = 0; k < nlev; ++k) {
-      const int64_t j1 = lvs[k + 1];
-      for (int64_t j = lvs[k] + w; j < j1; j += 2 * nw) {
-        TrsvSlice<P, true> a, b;
-        a.load_slice(S, (int)j, lower, which);
-        if (j + nw < j1) b.load_slice(S, (int)(j + nw), lower, which);
-        a.finish();
-        b.finish();
+      const int64_t j0 = lvs[k], j1 = lvs[k + 1];
+      TrsvSlice<P, true> nxt;
+      if (k + 1 < nlev && lvs[k + 1] + w < lvs[k + 2]) nxt.load_slice(S, (int)(lvs[k + 1] + w), lower, which);
+      cur.finish();
+      for (int64_t j = j0 + w + nw; j < j1; j += nw) {
+        TrsvSlice<P, true> extra;
+        extra.load_slice(S, (int)j, lower, which);
+        extra.finish();
       }
       __syncthreads();
+      cur = nxt;
     }
+    __syncthreads();
   }
 }
 

@@ -50,7 +50,7 @@ class SolveOptsC(C.Structure):
         ("tol", C.c_double), ("max_iters", C.c_int32), ("inner_tol", C.c_double),
         ("max_refinements", C.c_int32), ("n_blocks", C.c_int64), ("block_ptr", i64p),
         ("trsv_mode", C.c_int32), ("check_every", C.c_int32), ("perm", C.POINTER(C.c_int32)),
-        ("shadow", C.c_int32),
+        ("shadow", C.c_int32), ("fill_level", C.c_int32), ("ilut_entries", C.c_int32), ("ilut_drop", C.c_double),
     ]
 
 

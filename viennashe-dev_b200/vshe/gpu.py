@@ -20,9 +20,9 @@ ERRORS = {
     -11: "ZERO_PIVOT", -12: "NOT_FOUND", -13: "UNSUPPORTED",
 }
 PRECISION = {"fp64": 0, "mixed": 1}
-PRECOND = {"none": 0, "ilu0": 1, "block_ilu0": 2}
+PRECOND = {"none": 0, "ilu0": 1, "block_ilu0": 2, "ilut": 3}
 ORDERING = {"natural": 0, "multicolor": 1}
-TRSV = {"auto": 0, "persistent": 1, "per_level": 2}
+TRSV = {"auto": 0, "persistent": 1, "per_level": 2, "per_system": 3}
 
 _lib = None
 
@@ -70,7 +70,7 @@ def lib():
     return _lib
 
 
-def layout(rp, ci, **kw):
+def layout(rp, ci, values=None, **kw):
     """The solver order and SELL-32 tables the library builds for this pattern and these
     options (host only, no GPU): dict of numpy arrays, see vshe_layout_export."""
     L = lib()
@@ -82,8 +82,10 @@ def layout(rp, ci, **kw):
     nnz = int(rp[-1])
     o, keep = make_opts(**kw)
     sz = np.zeros(10, np.int64)
-    L.vshe_layout_sizes.argtypes = [C.c_int64, C.c_int64, i64p, i32p, C.POINTER(SolveOptsC), i64p]
-    rc = L.vshe_layout_sizes(n, nnz, ptr(rp, C.c_int64), ptr(ci, C.c_int32), C.byref(o), ptr(sz, C.c_int64))
+    vals = None if values is None else np.ascontiguousarray(values, np.float64)
+    vp = None if vals is None else ptr(vals, C.c_double)
+    L.vshe_layout_sizes.argtypes = [C.c_int64, C.c_int64, i64p, i32p, C.POINTER(C.c_double), C.POINTER(SolveOptsC), i64p]
+    rc = L.vshe_layout_sizes(n, nnz, ptr(rp, C.c_int64), ptr(ci, C.c_int32), vp, C.byref(o), ptr(sz, C.c_int64))
     if rc:
         raise VsheError(rc, "vshe_layout_sizes")
     nslA, padA, nslL, padL, nslU, padU, nlevL, nlevU, nnzL, nnzU = [int(v) for v in sz]
@@ -94,9 +96,9 @@ def layout(rp, ci, **kw):
                umap=np.zeros(padU, np.int64), urow=np.zeros(n, np.int32))
     order = ["perm", "lvr", "aoff", "acol", "amap", "lrow0", "loff", "lcol", "lmap", "uslot0", "uoff", "ucol", "umap", "urow"]
     ct = {np.dtype(np.int32): C.c_int32, np.dtype(np.int64): C.c_int64}
-    L.vshe_layout_export.argtypes = [C.c_int64, C.c_int64, i64p, i32p, C.POINTER(SolveOptsC)] + \
+    L.vshe_layout_export.argtypes = [C.c_int64, C.c_int64, i64p, i32p, C.POINTER(C.c_double), C.POINTER(SolveOptsC)] + \
         [C.POINTER(ct[out[k].dtype]) for k in order]
-    rc = L.vshe_layout_export(n, nnz, ptr(rp, C.c_int64), ptr(ci, C.c_int32), C.byref(o),
+    rc = L.vshe_layout_export(n, nnz, ptr(rp, C.c_int64), ptr(ci, C.c_int32), vp, C.byref(o),
                               *[ptr(out[k], ct[out[k].dtype]) for k in order])
     if rc:
         raise VsheError(rc, "vshe_layout_export")
@@ -111,7 +113,7 @@ def kernel_launches():
 
 def make_opts(precision="mixed", precond="ilu0", tol=1e-10, max_iters=1000, inner_tol=1e-5,
               max_refinements=10, blocks=None, trsv="auto", check_every=8, ordering="natural", perm=None,
-              shadow="dense"):
+              shadow="dense", fill_level=0, ilut_entries=20, ilut_drop=1e-3):
     o = SolveOptsC()
     lib().vshe_default_opts(C.byref(o))
     o.precision = PRECISION[precision]
@@ -124,6 +126,9 @@ def make_opts(precision="mixed", precond="ilu0", tol=1e-10, max_iters=1000, inne
     o.check_every = check_every
     o.ordering = ORDERING[ordering]
     o.shadow = {"dense": 0, "r0": 1}[shadow]
+    o.fill_level = int(fill_level)
+    o.ilut_entries = int(ilut_entries)
+    o.ilut_drop = float(ilut_drop)
     keep = []
     if blocks is not None:
         kb = np.ascontiguousarray(blocks, np.int64)
