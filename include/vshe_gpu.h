@@ -53,10 +53,11 @@ extern "C" {
 #define VSHE_PRECOND_NONE        0
 #define VSHE_PRECOND_ILU0        1   /* ILU(0) on the whole system (serial_linear_solver's choice) */
 #define VSHE_PRECOND_BLOCK_ILU0  2   /* ILU(0) per block (energy slabs: block_preconditioner_boundaries) */
-#define VSHE_PRECOND_ILUT        3   /* incomplete LU on the pattern of ILUT(ilut_entries, ilut_drop) (Saad
-                                        Alg. 10.6) together with A's pattern: the pattern is found on the host
-                                        from the values at system creation, the factorisation of every solve
-                                        runs on the device on that pattern without dropping */
+#define VSHE_PRECOND_ILUT        3   /* ILUT(ilut_entries, ilut_drop) (Saad Alg. 10.6): the host finds, from the
+                                        values at system creation, every position whose entry passes the drop
+                                        tolerance; the factorisation of every solve runs on the device inside
+                                        that pattern with ILUT's two dropping rules (multipliers and entries
+                                        below tol * ||a_i||, then the ilut_entries largest of L and of U) */
 
 #define VSHE_ORDER_NATURAL     0   /* the caller's row order (the reference's) */
 #define VSHE_ORDER_MULTICOLOR  1   /* greedy colouring of the matrix graph, rows grouped by colour */

@@ -211,6 +211,23 @@ def ilut_csr(A: CSR, p, tau):
     return rp, ci, lu
 
 
+def ilut_passed(A: CSR, p, tau):
+    """Per row, the columns whose entries passed ILUT(p, tau)'s tau test before the p-largest
+    rule (CSR pattern rp, ci)."""
+    L = lib()
+    L.vsheo_ilut_passed.argtypes = [C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int32,
+                                    C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+    nnz = np.zeros(1, np.int64)
+    args = (A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double), int(p), float(tau), ptr(nnz, C.c_int64))
+    if L.vsheo_ilut_passed(*args, None, None):
+        raise RuntimeError("oracle ilut failed")
+    rp = np.zeros(A.n + 1, np.int64)
+    ci = np.zeros(int(nnz[0]), np.int32)
+    if L.vsheo_ilut_passed(*args, ptr(rp, C.c_int64), ptr(ci, C.c_int32)):
+        raise RuntimeError("oracle ilut failed")
+    return rp, ci
+
+
 def ilu0_values(A: CSR, blocks=None):
     lu = np.zeros(A.nnz)
     bp = None if blocks is None else np.ascontiguousarray(blocks, np.int64)

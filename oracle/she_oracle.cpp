@@ -968,7 +968,8 @@ static ILU iluk(int64_t n, const int64_t *rp, const int32_t *ci, const double *v
 }
 
 // ILUT(p, tau), Saad Alg. 10.6 (row-wise, dual dropping).
-static ILU ilut(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int p, double tau) {
+static ILU ilut(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int p, double tau,
+                std::vector<std::vector<int32_t>> *passed = nullptr) {
   ILU f; f.n = n; f.lrp.assign(1, 0); f.urp.assign(1, 0);
   std::vector<double> w(size_t(n), 0.0);
   std::vector<char> nz(size_t(n), 0);
@@ -1012,6 +1013,12 @@ static ILU ilut(int64_t n, const int64_t *rp, const int32_t *ci, const double *v
       }
       std::sort(s.begin(), s.end(), [](const std::pair<double, int32_t> &a, const std::pair<double, int32_t> &b) { return a.second < b.second; });
     };
+    if (passed) {  // the entries that passed the tau test, before the p-largest rule
+      auto &ps = (*passed)[size_t(i)];
+      for (auto &e : lo) ps.push_back(e.second);
+      for (auto &e : up) ps.push_back(e.second);
+      std::sort(ps.begin(), ps.end());
+    }
     keep(lo); keep(up);
     for (auto &e : lo) { f.lci.push_back(e.second); f.lv.push_back(w[e.second]); }
     if (d == 0.0) d = (ti > 0 ? ti : 1.0);  // guard a zero pivot
@@ -1393,6 +1400,27 @@ int vsheo_ilut_csr(int64_t n, const int64_t *rp, const int32_t *ci, const double
     for (int64_t i = 0; i < n; ++i) {
       for (int64_t k = f.lrp[size_t(i)]; k < f.lrp[size_t(i) + 1]; ++k) { ci_out[q] = f.lci[size_t(k)]; lu_out[q++] = f.lv[size_t(k)]; }
       for (int64_t k = f.urp[size_t(i)]; k < f.urp[size_t(i) + 1]; ++k) { ci_out[q] = f.uci[size_t(k)]; lu_out[q++] = f.uv[size_t(k)]; }
+      rp_out[i + 1] = q;
+    }
+    return 0;
+  } catch (...) { return -1; }
+}
+
+// Per row, the columns whose entries passed ILUT's tau test (before its p-largest rule), as a
+// CSR pattern: call with rp_out == NULL for the count.
+int vsheo_ilut_passed(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int32_t p, double tau,
+                      int64_t *nnz_out, int64_t *rp_out, int32_t *ci_out) {
+  try {
+    std::vector<std::vector<int32_t>> passed((size_t)n);
+    ilut(n, rp, ci, v, p, tau, &passed);
+    int64_t q = 0;
+    for (auto &r : passed) q += int64_t(r.size());
+    *nnz_out = q;
+    if (!rp_out) return 0;
+    q = 0;
+    rp_out[0] = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      for (int32_t j : passed[size_t(i)]) ci_out[q++] = j;
       rp_out[i + 1] = q;
     }
     return 0;

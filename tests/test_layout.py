@@ -256,16 +256,21 @@ def _slot_pattern(Lt):
 
 @pytest.mark.parametrize("p,tau", [(20, 1e-3), (5, 1e-2)])
 def test_ilut_pattern_matches_oracle(prob, p, tau):
-    """VSHE_PRECOND_ILUT: the host analysis keeps the pattern of ILUT(p, tau) (Saad Alg. 10.6)
-    joined with A's; natural order, so solver rows map to the caller's through perm."""
+    """VSHE_PRECOND_ILUT: the host analysis keeps, per row, every position whose entry passes
+    ILUT(p, tau)'s tau test (Saad Alg. 10.6, before its p-largest rule), the diagonal and A's
+    entries; natural order, so solver rows map to the caller's through perm.  The final ILUT
+    pattern lies inside it."""
     name, P, A = prob
     Lt = gpu.layout(A.rp, A.ci, values=A.v, precond="ilut", ilut_entries=p, ilut_drop=tau)
     perm = Lt["perm"]
     got = set((int(perm[i]), int(perm[j])) for i, j in _slot_pattern(Lt))
-    rp, ci, _ = O.ilut_csr(A, p, tau)
+    rp, ci = O.ilut_passed(A, p, tau)
     want = set()
     for i in range(A.n):
         want.update((i, int(j)) for j in ci[rp[i]:rp[i + 1]])
         want.update((i, int(j)) for j in A.ci[A.rp[i]:A.rp[i + 1]])
         want.add((i, i))
     assert got == want
+    frp, fci, _ = O.ilut_csr(A, p, tau)
+    final = set((i, int(j)) for i in range(A.n) for j in fci[frp[i]:frp[i + 1]])
+    assert final <= got

@@ -290,7 +290,9 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       // ILUT(p, tau), Saad Alg. 10.6, in base order: the row is eliminated with the kept rows
       // above it in increasing column order; a multiplier or entry below tau * ||a_i|| is
       // dropped, then the p largest of L and of U are kept (the diagonal always).  Only the
-      // pattern is kept here; the device factorises on the pattern joined with A's.
+      // pattern is kept here: every position that survives the tau test, joined with A's.  The
+      // device repeats the same elimination with the same two dropping rules inside that
+      // pattern (k_ilut), which reproduces ILUT for the values seen here.
       const int pkeep = opts.ilut_entries > 0 ? opts.ilut_entries : 60;
       const double tau = opts.ilut_drop > 0 ? opts.ilut_drop : 1e-4;
       std::vector<int64_t> urp((size_t)n + 1, 0);
@@ -344,6 +346,13 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
             v.resize(size_t(pkeep));
           }
         };
+        // the factor pattern of row i: every entry that survived the tau test (the device applies
+        // the p-largest rule itself, and multipliers beyond the p largest still take part in the
+        // elimination), the diagonal and A's own entries
+        std::vector<int32_t> pat;
+        for (auto &e : lo) pat.push_back(e.second);
+        pat.push_back(int32_t(i));
+        for (auto &e : up) pat.push_back(e.second);
         keep(lo); keep(up);
         double d = w[size_t(i)];
         if (d == 0.0) d = ti > 0.0 ? ti : 1.0;
@@ -351,11 +360,6 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
         std::sort(up.begin(), up.end(), [](const std::pair<double, int32_t> &a, const std::pair<double, int32_t> &b) { return a.second < b.second; });
         for (auto &e : up) { ucol.push_back(e.second); uval.push_back(w[size_t(e.second)]); }
         urp[size_t(i) + 1] = int64_t(ucol.size());
-        // the factor pattern of row i: the kept entries, the diagonal and A's own entries
-        std::vector<int32_t> pat;
-        for (auto &e : lo) pat.push_back(e.second);
-        pat.push_back(int32_t(i));
-        for (auto &e : up) pat.push_back(e.second);
         for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) pat.push_back(bent[size_t(k)].first);
         std::sort(pat.begin(), pat.end());
         pat.erase(std::unique(pat.begin(), pat.end()), pat.end());
@@ -436,6 +440,9 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   }
   const int64_t fnnz = frp[size_t(n)];
   nnzF = fnnz;
+  if (ilut)
+    for (int64_t i = 0; i < n; ++i)
+      if (frp[size_t(i) + 1] - frp[size_t(i)] > 1024) { err = "an ILUT row pattern longer than 1024 entries"; return VSHE_E_UNSUPPORTED; }
 
   // Forward levels over the symmetrised, block-restricted graph of F in base order: a row's
   // level is one more than the highest level of any coupled (F_ij or F_ji != 0) earlier row of
@@ -739,12 +746,14 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
     if (S->mixed != mixed || S->has_pc != has_pc)
       return ctx.fail(VSHE_E_INVALID_ARGUMENT, "systems in one batch need the same precision and preconditioner kind");
   // Triangular sweeps.  A member with many short levels (fewer than kCtaRowsPerLevel rows per
-  // forward level on average, and more than kCtaMinLevels levels: 1D devices) sweeps on its own
+  // forward level on average, more than kCtaMinLevels levels and at most kCtaMaxRows rows: 1D
+  // devices, small 2D ones in natural order) sweeps on its own
   // CTA with a CTA barrier per level; VSHE_TRSV_PER_SYSTEM forces that for every member.  The
   // others share a merged schedule: merged level l lists, system by system, the level-l SELL
   // slices of every grid-swept member.
   constexpr int64_t kCtaRowsPerLevel = 4096;
   constexpr int32_t kCtaMinLevels = 32;
+  constexpr int64_t kCtaMaxRows = int64_t(2) << 20;  // beyond, one SM's bandwidth bounds the sweep
   std::vector<char> on_cta((size_t)nsys, 0);
   cta_members.clear();
   if (has_pc) {
@@ -752,7 +761,8 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
       const System *S = sys[size_t(k)];
       const int mode = S->opts.trsv_mode;
       const bool want = mode == VSHE_TRSV_PER_SYSTEM ||
-                        (mode == VSHE_TRSV_AUTO && S->nlevL > kCtaMinLevels && S->n / std::max(S->nlevL, 1) < kCtaRowsPerLevel);
+                        (mode == VSHE_TRSV_AUTO && S->nlevL > kCtaMinLevels && S->n / std::max(S->nlevL, 1) < kCtaRowsPerLevel &&
+                         S->n <= kCtaMaxRows);
       if (want) { on_cta[size_t(k)] = 1; cta_members.push_back(k); }
     }
   }
@@ -842,7 +852,12 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
     // the final / replacement residual is written into the Krylov r
     RefDev r{S->n, S->d_aoff, S->d_acol, S->d_aval, S->d_bp, (const double *)S->kv[0], (double *)S->kv[1]};
     std::memcpy(rd.data() + vk_refdev_size() * size_t(k), &r, sizeof(r));
-    FactDev f{S->n, S->d_prp, S->d_pci, S->d_lu64, S->d_pdiag, S->d_blk};
+    FactDev f{S->n, S->d_prp, S->d_pci, S->d_lu64, S->d_pdiag, S->d_blk, 0, 0, 0.0};
+    if (S->opts.precond == VSHE_PRECOND_ILUT) {
+      f.ilut = 1;
+      f.pkeep = S->opts.ilut_entries > 0 ? S->opts.ilut_entries : 60;
+      f.tau = S->opts.ilut_drop > 0 ? S->opts.ilut_drop : 1e-4;
+    }
     std::memcpy(fd.data() + vk_factdev_size() * size_t(k), &f, sizeof(f));
   }
   std::vector<int32_t> ones((size_t)(nsys), 1), zeros(size_t(nsys), 0);

@@ -41,7 +41,7 @@ namespace vshe {
 #define VSHE_E_ZERO_PIVOT_DEV (-11)
 
 constexpr int kThreads = 256;
-constexpr int kCtaThreads = 512;  // the per-system sweep: 16 warps, two slices in flight each
+constexpr int kCtaThreads = 512;  // the per-system sweep: 16 warps, each with the current and the next level's slice in flight
 constexpr int kWarps = kThreads / 32;
 constexpr int kSpmvU = 8;  // SELL entries per lane whose loads are issued together
 constexpr int kDotU = 6;   // the same inside the tile kernels, which also carry reduction state
@@ -600,7 +600,44 @@ __device__ __forceinline__ int64_t find_col(const int32_t *ci, int64_t a, int64_
   return -1;
 }
 
-// level entries are solver rows ent_row[e] of system ent_sys[e] (row e of system 0 when NULL)
+// Keeps the pkeep largest |entries| of lu[lo, hi) (ties: the lower column wins), zeroing the
+// others; one warp, entries already zero stay zero and do not count.  Parts longer than 1024
+// entries are refused by the host (Layout::build).
+__device__ void keep_largest(double *lu, int64_t lo, int64_t hi, int pkeep) {
+  const int lane = threadIdx.x & 31;
+  int cnt = 0;
+  for (int64_t k = lo + lane; k < hi; k += 32) cnt += __ldcg(&lu[k]) != 0.0 ? 1 : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (cnt <= pkeep) return;
+  __syncwarp();
+  // rank every entry against the whole part (parts are a few dozen entries), then zero; the
+  // decisions of a lane's entries (at most 32 per lane: parts up to 1024 entries) are a bitmask
+  uint32_t drop = 0;
+  int m = 0;
+  for (int64_t k = lo + lane; k < hi && m < 32; k += 32, ++m) {
+    const double v = fabs(__ldcg(&lu[k]));
+    if (v == 0.0) continue;
+    int rank = 0;
+    for (int64_t k2 = lo; k2 < hi; ++k2) {
+      const double v2 = fabs(__ldcg(&lu[k2]));
+      if (v2 > v || (v2 == v && k2 < k)) ++rank;
+    }
+    if (rank >= pkeep) drop |= 1u << m;
+  }
+  __syncwarp();
+  m = 0;
+  for (int64_t k = lo + lane; k < hi && m < 32; k += 32, ++m)
+    if (drop & (1u << m)) lu[k] = 0.0;
+  __syncwarp();
+}
+
+// level entries are solver rows ent_row[e] of system ent_sys[e] (row e of system 0 when NULL).
+// ILU(0) / ILU(k) / ILU on a pattern: Saad's IKJ elimination inside the row's pattern.  With
+// F.ilut the two ILUT dropping rules (Saad Alg. 10.6) are applied on the way: multipliers below
+// tau ||a_i|| are dropped before they eliminate, and after the row is reduced its entries below
+// tau ||a_i|| are dropped and only the pkeep largest of L and of U stay; a zero pivot is replaced
+// by tau ||a_i|| (or 1), as ILUT does.
 __device__ void ilu0_level_rows(const FactDev *fs, Levels lv, int k, int32_t *err) {
   const int lane = threadIdx.x & 31;
   const int64_t gid = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
@@ -612,6 +649,13 @@ __device__ void ilu0_level_rows(const FactDev *fs, Levels lv, int k, int32_t *er
     const int64_t i = lv.ent_row ? lv.ent_row[e] : e;
     const int64_t a = F.rp[i], b = F.rp[i + 1], d = F.diag[i];
     const int32_t bi = F.blk[i];
+    double ti = 0.0;
+    if (F.ilut) {
+      double ss = 0.0;
+      for (int64_t kk = a + lane; kk < b; kk += 32) { const double v = __ldcg(&F.lu[kk]); ss += v * v; }
+      ss = warp_sum(ss);
+      ti = F.tau * sqrt(ss);
+    }
     for (int64_t kp = a; kp < d; ++kp) {
       const int32_t c = F.ci[kp];
       if (F.blk[c] != bi) continue;
@@ -622,6 +666,11 @@ __device__ void ilu0_level_rows(const FactDev *fs, Levels lv, int k, int32_t *er
       }
       const double l = __ldcg(&F.lu[kp]) / piv;
       __syncwarp();
+      if (F.ilut && fabs(l) < ti) {  // dropped multiplier: no elimination with row c
+        if (lane == 0) F.lu[kp] = 0.0;
+        __syncwarp();
+        continue;
+      }
       if (lane == 0) F.lu[kp] = l;
       for (int64_t kk = F.diag[c] + 1 + lane; kk < F.rp[c + 1]; kk += 32) {
         const int32_t j = F.ci[kk];
@@ -629,6 +678,15 @@ __device__ void ilu0_level_rows(const FactDev *fs, Levels lv, int k, int32_t *er
         const int64_t pos = find_col(F.ci, kp + 1, b, j);
         if (pos >= 0) F.lu[pos] = __ldcg(&F.lu[pos]) - l * __ldcg(&F.lu[kk]);
       }
+      __syncwarp();
+    }
+    if (F.ilut) {
+      for (int64_t kk = a + lane; kk < b; kk += 32)
+        if (kk != d && fabs(__ldcg(&F.lu[kk])) < ti) F.lu[kk] = 0.0;
+      __syncwarp();
+      keep_largest(F.lu, a, d, F.pkeep);
+      keep_largest(F.lu, d + 1, b, F.pkeep);
+      if (lane == 0 && __ldcg(&F.lu[d]) == 0.0) F.lu[d] = ti > 0.0 ? ti : 1.0;
       __syncwarp();
     }
   }

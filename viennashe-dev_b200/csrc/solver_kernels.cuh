@@ -90,6 +90,10 @@ struct FactDev {
   double *lu;
   const int64_t *diag;
   const int32_t *blk;
+  // ILUT dropping (ilut != 0): a multiplier or entry below tau * ||a_i||_2 is dropped, then only
+  // the pkeep largest entries of the row's L part and of its U part are kept
+  int32_t ilut, pkeep;
+  double tau;
 };
 
 // FP64 residual view of one system (solver order): r = b - A x.

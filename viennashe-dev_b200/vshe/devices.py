@@ -319,3 +319,58 @@ def config4(count=40, seed=23, rate=200.0):
             cfg = SheConfig(max_expansion_order=L, energy_spacing=sp, min_kinetic_energy_range=energy_range_for(dev, sp, ne))
         out.append((t, dev, cfg))
     return out
+
+
+def mosfet_2d(nx=240, ny=80, lx=300e-9, ly=150e-9, n_sd=1e26, n_body=1e23, v_drain=1.0, v_gate=1.0,
+              well_len=75e-9, well_depth=40e-9, sigma=5e-9, gate_decay=20e-9, T=300.0, name="mosfet2d"):
+    """Three-terminal MOSFET-like structure: a p-type body (acceptors n_body) with n+ source and
+    drain wells (donors n_sd, Gaussian edges of width sigma) under the top surface at both ends,
+    metal source / drain contact cells beside the wells (contacts 0 and 1), and a gate modelled
+    as a fixed-potential top boundary at v_gate: it enters only through the frozen potential,
+    which adds to the built-in potential the drain bias across the channel and the gate bias
+    decaying from the top surface (gate_decay), smoothed with a 5 nm Gaussian.  The gate carries
+    no SHE current (it is insulated), so the SHE sees two contacts."""
+    hx, hy = lx / nx, ly / ny
+    NX = nx + 2
+    vol, cen, fc, fvol, fn, cfp, cfi = _mesh_2d(NX, ny, hx, hy)
+    cen[:, 0] -= hx
+    x, y = cen[:, 0], cen[:, 1]
+    ii = np.tile(np.arange(NX), ny)
+    top = y > ly - well_depth
+    mat = np.full(NX * ny, SI, np.int32)
+    contact = np.full(NX * ny, -1, np.int32)
+    src = (ii == 0) & top
+    drn = (ii == NX - 1) & top
+    mat[src | drn] = METAL
+    contact[src] = 0
+    contact[drn] = 1
+    from math import erf
+    verf = np.vectorize(erf)
+    s = sigma * math.sqrt(2.0)
+    depth = 0.5 * (1 + verf((y - (ly - well_depth)) / s))
+    wl = 0.5 * (1 + verf((well_len - x) / s))
+    wr = 0.5 * (1 + verf((x - (lx - well_len)) / s))
+    frac = np.clip((wl + wr) * depth, 0.0, 1.0)
+    nd = np.maximum(np.exp(np.log(1.0) + frac * np.log(n_sd)) - 1.0, 0.0)
+    na = np.full(NX * ny, n_body)
+    phi_bi = _built_in_potential(T, nd, na)
+    ramp = np.clip((x - well_len) / (lx - 2 * well_len), 0.0, 1.0) * v_drain
+    channel = np.clip(1.0 - wl - wr, 0.0, 1.0)
+    gate = v_gate * channel * np.exp(-(ly - y) / gate_decay)
+    phi = (phi_bi + ramp + gate).reshape(ny, NX)
+    for axis, hh in ((1, hx), (0, hy)):
+        phi = np.apply_along_axis(lambda v: _gauss_smooth_1d(v, hh, 5e-9), axis, phi)
+    phi = phi.ravel()
+    cpot = np.array([0.0, v_drain])
+    phi[src] = cpot[0] + _built_in_potential(T, nd[src], na[src] * 0.0)
+    phi[drn] = cpot[1] + _built_in_potential(T, nd[drn], na[drn] * 0.0)
+    return Device(2, mat, vol, cen, nd, na, phi, contact, fc, fvol, fn, cfp, cfi, T, cpot, name)
+
+
+def config5(nx=240, ny=80, n_energies=140, L=5):
+    """MOSFET-like structure of 300 x 150 nm on a 240 x 80 mesh, source / drain wells 1e26 m^-3,
+    body 1e23 m^-3, gate (top boundary) and drain at 1.0 V, SHE order L = 5, 140 energies."""
+    dev = mosfet_2d(nx=nx, ny=ny, name="config5_mosfet_%dx%d" % (nx, ny))
+    sp = HBAR_OMEGA_OP / 4.0
+    cfg = SheConfig(max_expansion_order=L, energy_spacing=sp, min_kinetic_energy_range=energy_range_for(dev, sp, n_energies))
+    return dev, cfg
