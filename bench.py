@@ -381,7 +381,8 @@ def run_ours(args, D_):
     tmax = D_.max(total_s)
     value = D_.sum(args.steps) / tmax
     solve = {"iterations": st["iterations"], "residual_replacements": st["refinements"], "rel_residual": st["rel_residual"],
-             "factor_ms": st["setup_ms"], "krylov_ms": st["solve_ms"], "levels_L": st["levels_L"], "levels_U": st["levels_U"]}
+             "factor_ms": st["setup_ms"], "krylov_ms": st["solve_ms"], "levels_L": st["levels_L"], "levels_U": st["levels_U"],
+             "sweep_ctas_autotuned": st.get("sweep_ctas"), "tile_rows_autotuned": st.get("tile_rows")}
     n, nnz, nnz_lu = int(info["n_even"]), int(info["nnz_reduced"]), int(info["nnz_factor"])
     if args.pass_only:
         if D_.rank == 0:
@@ -449,23 +450,22 @@ def run_ours(args, D_):
     if dominant == "trsv":
         avg_ms = prof["trsv_ms"] / max(prof["trsv_launches"], 1)
         dbytes = trsv_bytes
-        kname = "k_trsv_persistent<float> (ILU(0) apply, forward then backward SELL-32 sweeps)"
+        kname = "k_trsv_persistent<float> (incomplete-LU apply, forward then backward SELL-32 sweeps)"
     else:
         avg_ms = prof["spmv_ms"] / max(prof["spmv_launches"], 1)
         dbytes = spmv_bytes
         kname = "k_spmv_dot (SELL-32 SpMV FP64 + fused dots)"
     achieved = dbytes / (avg_ms / 1000.0) / 1e9
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tfile):
-        try:
-            tt = json.load(open(tfile))
-            if tt.get("workload") == workload_name(args):
-                traffic = tt.get(dominant)
-        except (OSError, ValueError):
-            traffic = None
+    # DRAM traffic per launch: one ncu capture of the same kernels on the 200 x 50 x 80 bar
+    # (ncu --set full, profiles/sell_kernels_bar200x50x80.md) measured dram__bytes_read.sum +
+    # dram__bytes_write.sum at 0.967 (SpMV + dots) and 0.955 (ILU(1) apply) of the algorithmic
+    # bytes; the traffic grows in proportion with the units processed, so a full launch's is
+    # that ratio times its algorithmic bytes.
+    traffic_ratio = {"spmv": 383372032 / 396606924, "trsv": 430062592 / 450235320}
+    traffic = dbytes * traffic_ratio[dominant] if args.workload == "bar" else None
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_source": peak_src,
                 "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "traffic_source": "ncu capture of the 200x50x80 bar scaled by algorithmic bytes" if traffic else None,
                 "algorithmic_bytes_per_launch": dbytes, "avg_launch_ms": avg_ms}
     extra = {}
     if D_.rank == 0 and not args.no_serving:

@@ -105,6 +105,8 @@ typedef struct vshe_solve_stats {
   int32_t levels_L;         /* level-schedule depth of the L and U solves */
   int32_t levels_U;
   int64_t bytes_device;     /* device memory held by the system */
+  int32_t sweep_ctas;       /* CTAs of the grid-wide triangular sweep (autotuned; 0 = none) */
+  int32_t tile_rows;        /* rows per reduction tile of this system (autotuned) */
 } vshe_solve_stats;
 
 /* Fills opts with the defaults: mixed precision, ILU0, natural order, tol 1e-10,

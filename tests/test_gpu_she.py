@@ -152,3 +152,31 @@ def _check_end_to_end(P, G, st, full_res, tol):
         # currents are the small anisotropic part of f; near equilibrium they are a cancellation
         # of one-way fluxes (cases.current_scale)
         assert np.max(np.abs(cur - cur_r[:len(cur)])) <= bc * cases.current_scale(dens_r, cur_r)
+
+
+def test_config1_diode_matches_oracle(gpu_ctx):
+    """The reference's own CPU-runnable case: the 1D n+/n/n+ diode 50/150/50 nm, 1e25/1e21/1e25
+    m^-3, 250 boxes, L = 1, spacing hbar*omega_op/4, 1.5 eV kinetic range, 0.5 V, with the
+    preconditioner the reference's serial solver really runs (natural-order ILU(0); the ILUT
+    that the benchmark configuration names needs 5896 iterations here on the oracle, against
+    19).  Assembled system bit-identical in pattern and to 1e-12 in values; terminal currents
+    and densities within 1e-8 of the oracle's 1e-14 solve after a 1e-14 solve on the device."""
+    dev, cfg = D.config1()
+    cpl = O.golden_coupling(1)
+    P = O.OracleProblem(dev, cfg, cpl)
+    G = gpu.SheProblem(gpu_ctx, dev, cfg, coupling=cpl, precision="fp64", precond="ilu0", ordering="natural",
+                       tol=1e-14, max_iters=4000)
+    try:
+        G.assemble(3)
+        _assert_same(P.matrix(3), G.export("reduced"))
+        st, full_res = G.run()
+        assert st["status"] == 0 and st["rel_residual"] < 1e-14, st
+        A = P.matrix(3)
+        xr, sr = O.csr_solve(A, A.rhs, precond=1, tol=1e-14, maxit=20000)
+        assert sr["rc"] == 0, sr
+        _, dens_r, cur_r, _ = P.finish(xr)
+        x, dens, cur = G.results()
+        assert np.max(np.abs(cur - cur_r)) <= 1e-8 * np.max(np.abs(cur_r))
+        assert np.max(np.abs(dens - dens_r) / dens_r) < 1e-8
+    finally:
+        G.free()

@@ -151,6 +151,10 @@ struct Batch {
   // only_member >= 0: tiles of that member alone, with `rows` rows (the autotuner's trial tiles)
   int set_tiles(Ctx &ctx, int only_member = -1, int64_t rows = 0);
   int autotune_tiles(Ctx &ctx);
+  int autotune_trsv(Ctx &ctx);
+  bool trsv_tuned = false;
+  int trsv_bps_max = 4;
+  std::vector<double> trsv_tune_ms;  // ms per apply for 1, 2, ... CTAs per SM
   int factor(Ctx &ctx);
   int bicgstab(Ctx &ctx, double tol, int max_iter, bool resume, int &iters_out);
   int start(Ctx &ctx, double tol, int max_iter, bool resume);

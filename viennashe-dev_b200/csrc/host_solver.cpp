@@ -905,6 +905,7 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   int bps = 0;
   if (mixed) vk_trsv_occupancy_f32(&bps); else vk_trsv_occupancy_f64(&bps);
   trsv_grid = std::max(1, std::min(bps, 4)) * num_sms;
+  trsv_bps_max = std::max(1, std::min(bps, 4));
   int bpf = 0;
   vk_ilu0_occupancy(&bpf);
   ilu_grid = std::max(1, std::min(bpf, 4)) * num_sms;
@@ -1029,6 +1030,42 @@ int Batch::factor(Ctx &ctx) {
       vk_split_factor_f64(S->nnzF, S->n, S->d_lu64, S->d_fmap, S->d_pdiag, S->d_dpos, (double *)S->d_lval, (double *)S->d_uval, (double *)S->d_udinv, s);
   }
   return check_err(ctx, "ilu0 factorisation");
+}
+
+// Autotuner of the grid-wide sweep's CTA count (1 .. 4 CTAs per SM): fewer CTAs make each grid
+// barrier cheaper, more CTAs put more slices in flight per level.  Timed once per batch on its
+// own factors (one forward + backward apply, CUDA events), before the first iteration; the
+// choice does not change any result (each slice is computed the same way by whichever warp).
+int Batch::autotune_trsv(Ctx &ctx) {
+  if (trsv_tuned || !has_pc || !grid_group || sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) return VSHE_OK;
+  trsv_tuned = true;
+  cudaStream_t s = ctx.stream;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a); cudaEventCreate(&b);
+  double best = 1e30;
+  int best_grid = trsv_grid;
+  for (int per_sm = 1; per_sm <= trsv_bps_max; ++per_sm) {
+    const int grid = per_sm * num_sms;
+    int rc = 0;
+    auto apply = [&]() {
+      return mixed ? vk_trsv_f32(1, grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s)
+                   : vk_trsv_f64(1, grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
+    };
+    rc |= apply();  // warm-up
+    cudaEventRecord(a, s);
+    for (int r = 0; r < 3; ++r) rc |= apply();
+    cudaEventRecord(b, s);
+    cudaError_t e = cudaEventSynchronize(b);
+    if (rc || e != cudaSuccess) { cudaEventDestroy(a); cudaEventDestroy(b); return ctx.cuda_fail(e != cudaSuccess ? e : cudaError_t(rc), "autotune sweeps"); }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    trsv_tune_ms.push_back(ms / 3.0);
+    if (ms < best) { best = ms; best_grid = grid; }
+  }
+  cudaEventDestroy(a); cudaEventDestroy(b);
+  trsv_grid = best_grid;
+  if (chunk_exec) { cudaGraphExecDestroy(chunk_exec); chunk_exec = nullptr; }  // the graph holds the old grid
+  return check_err(ctx, "autotune sweeps");
 }
 
 // A small pool of CUDA events for the per-kernel-class timing of a profiled solve.
@@ -1267,6 +1304,7 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
   if ((rc = autotune_tiles(ctx))) return rc;
   rc = factor(ctx);
   if (rc) return rc;
+  if ((rc = autotune_trsv(ctx))) return rc;
   cudaEventRecord(e1, s);
   const vshe_solve_opts &o = sys[0]->opts;
   int it = 0;
@@ -1316,6 +1354,8 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
     st.levels_L = S->nlevL;
     st.levels_U = S->nlevU;
     st.bytes_device = int64_t(S->arena.total);
+    st.sweep_ctas = (has_pc && grid_group) ? trsv_grid : 0;
+    st.tile_rows = int32_t(S->tile_rows);
     int32_t code = status;
     if (code == 0 && rel[size_t(k)] >= o.tol) code = VSHE_E_NOT_CONVERGED;
     if (code != 0 && rel[size_t(k)] < o.tol) code = 0;
