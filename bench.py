@@ -42,6 +42,7 @@ sys.path.insert(0, os.path.join(ROOT, "viennashe-dev_b200"))
 METRIC = "solves/s & p99 latency at 1e-10 resid (mixed vs plain FP64 GPU); SpMV GB/s"
 UNIT = "solves/s"
 TOL = 1e-10
+SWEEP_NAMES = {1: "grid barrier per level (k_trsv_persistent)", 2: "one launch per level", 4: "barrier-free flow (k_trsv_flow)"}
 
 
 def parse():
@@ -64,6 +65,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the drop-in (host-buffer) measurement")
     ap.add_argument("--mos-shrink", type=int, default=1, help="mosfet workload: mesh divided by this factor per axis")
     ap.add_argument("--served-requests", type=int, default=24)
+    ap.add_argument("--ilut-entries", type=int, default=20, help="mosfet workload: ILUT's p (entries kept per L and U row)")
+    ap.add_argument("--ilut-drop", type=float, default=1e-3, help="mosfet workload: ILUT's drop tolerance")
     ap.add_argument("--pass-only", action="store_true",
                     help="time only the device pass (no FP64 comparison, drop-in e2e or CPU baseline); for launch lists")
     return ap.parse_args()
@@ -173,7 +176,7 @@ def solver_options(args):
     instead of 960 iterations, 7 % faster per solve than ILU(0)); the L = 5 MOSFET needs
     ILUT(20, 1e-3) in natural order (ILU(0) stalls there in every order)."""
     if args.workload == "mosfet":
-        return dict(precond="ilut", ordering="natural", ilut_entries=20, ilut_drop=1e-3)
+        return dict(precond="ilut", ordering="natural", ilut_entries=args.ilut_entries, ilut_drop=args.ilut_drop)
     return dict(precond="block_ilu0", ordering="multicolor", fill_level=args.fill_level)
 
 
@@ -184,7 +187,8 @@ def build_problem(args, ctx, precision):
         dev, cfg = D.config5(nx=240 // args.mos_shrink, ny=80 // args.mos_shrink)
     else:
         dev, cfg = D.config2(nx=args.nx, ny=args.ny, n_energies=args.ne, L=args.L)
-    return gpu.SheProblem(ctx, dev, cfg, precision=precision, tol=TOL, max_iters=20000, check_every=16, **solver_options(args))
+    return gpu.SheProblem(ctx, dev, cfg, precision=precision, tol=TOL, max_iters=3000 if args.workload == "mosfet" else 20000,
+                          check_every=16, **solver_options(args))
 
 
 # -------------------------------------------------------------- CPU baseline
@@ -382,7 +386,8 @@ def run_ours(args, D_):
     value = D_.sum(args.steps) / tmax
     solve = {"iterations": st["iterations"], "residual_replacements": st["refinements"], "rel_residual": st["rel_residual"],
              "factor_ms": st["setup_ms"], "krylov_ms": st["solve_ms"], "levels_L": st["levels_L"], "levels_U": st["levels_U"],
-             "sweep_ctas_autotuned": st.get("sweep_ctas"), "tile_rows_autotuned": st.get("tile_rows")}
+             "sweep_ctas_autotuned": st.get("sweep_ctas"), "tile_rows_autotuned": st.get("tile_rows"),
+             "sweep_autotuned": SWEEP_NAMES.get(st.get("sweep_mode"), "none")}
     n, nnz, nnz_lu = int(info["n_even"]), int(info["nnz_reduced"]), int(info["nnz_factor"])
     if args.pass_only:
         if D_.rank == 0:
@@ -450,7 +455,9 @@ def run_ours(args, D_):
     if dominant == "trsv":
         avg_ms = prof["trsv_ms"] / max(prof["trsv_launches"], 1)
         dbytes = trsv_bytes
-        kname = "k_trsv_persistent<float> (incomplete-LU apply, forward then backward SELL-32 sweeps)"
+        kname = ("k_trsv_flow<float> (incomplete-LU apply, barrier-free forward then backward SELL-32 sweeps)"
+                 if st.get("sweep_mode") == 4 else
+                 "k_trsv_persistent<float> (incomplete-LU apply, forward then backward SELL-32 sweeps)")
     else:
         avg_ms = prof["spmv_ms"] / max(prof["spmv_launches"], 1)
         dbytes = spmv_bytes
@@ -462,7 +469,7 @@ def run_ours(args, D_):
     # bytes; the traffic grows in proportion with the units processed, so a full launch's is
     # that ratio times its algorithmic bytes.
     traffic_ratio = {"spmv": 383372032 / 396606924, "trsv": 430062592 / 450235320}
-    traffic = dbytes * traffic_ratio[dominant] if args.workload == "bar" else None
+    traffic = dbytes * traffic_ratio[dominant] if args.workload == "bar" and (dominant == "spmv" or st.get("sweep_mode") == 1) else None
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_source": peak_src,
                 "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                 "traffic_source": "ncu capture of the 200x50x80 bar scaled by algorithmic bytes" if traffic else None,
@@ -491,7 +498,7 @@ def run_ours(args, D_):
                        "n_energies": int(info["n_energies"]),
                        "preconditioner": ("block-ILU(%d) per energy slab, node %s colouring" % (args.fill_level, "distance-2" if args.fill_level else "4-colour")
                                           if args.workload == "bar"
-                                          else "ILU on the ILUT(20, 1e-3) pattern joined with A's, natural order"),
+                                          else "ILUT(%d, %g), natural order" % (args.ilut_entries, args.ilut_drop)),
                        "l2": "inputs larger than L2 (reduced system %.2f GB)" % (nnz * 12 / 1e9),
                        "parallelism": "replicas" if D_.world > 1 else "single"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},

@@ -70,6 +70,9 @@ extern "C" {
 #define VSHE_TRSV_PER_LEVEL   2   /* one launch per level */
 #define VSHE_TRSV_PER_SYSTEM  3   /* one CTA per system walks the system's levels (CTA barrier per level);
                                      AUTO picks it for systems with many short levels (1D devices) */
+#define VSHE_TRSV_FLOW        4   /* one cooperative launch per triangular solve without level barriers:
+                                     each row waits only on the rows it reads; AUTO times it against
+                                     VSHE_TRSV_PERSISTENT per batch and keeps the faster (same results) */
 
 typedef struct vshe_solve_opts {
   int32_t precision;        /* VSHE_PRECISION_* */
@@ -107,6 +110,7 @@ typedef struct vshe_solve_stats {
   int64_t bytes_device;     /* device memory held by the system */
   int32_t sweep_ctas;       /* CTAs of the grid-wide triangular sweep (autotuned; 0 = none) */
   int32_t tile_rows;        /* rows per reduction tile of this system (autotuned) */
+  int32_t sweep_mode;       /* grid-wide sweep used: VSHE_TRSV_PERSISTENT, _PER_LEVEL or _FLOW (0 = none) */
 } vshe_solve_stats;
 
 /* Fills opts with the defaults: mixed precision, ILU0, natural order, tol 1e-10,

@@ -46,3 +46,29 @@ def current_scale(dens_ref, cur_ref):
     current is a cancellation of one-way fluxes, so its error scales with the flux, not with
     the (vanishing) net current."""
     return max(float(np.max(np.abs(cur_ref))) if len(cur_ref) else 0.0, 1.602176634e-19 * float(np.max(dens_ref)) * 1e5)
+
+
+def arrow_csr(n=1500, seed=5):
+    """Seeded n x n 'arrow' system with one dense first row and one dense last row, diagonally
+    dominant: the first row's U part and the last row's L part hold about n entries each, longer
+    than any SHE row, which is what ILUT's p-largest selection has to handle at any length."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for i in range(n):
+        cols = {i: 4.0}
+        if i > 0:
+            cols[i - 1] = -1.0
+        if i + 1 < n:
+            cols[i + 1] = -1.0
+        if i == 0 or i == n - 1:
+            others = np.arange(2, n) if i == 0 else np.arange(0, n - 2)
+            vals = rng.uniform(0.1, 1.0, len(others)) * rng.choice([-1.0, 1.0], len(others))
+            cols.update({int(j): float(v) for j, v in zip(others, vals)})
+            cols[i] = 1.1 * float(np.sum(np.abs(vals))) + 2.0
+        rows.append(sorted(cols.items()))
+    rp = np.zeros(n + 1, np.int64)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    ci = np.array([j for r in rows for j, _ in r], np.int32)
+    v = np.array([x for r in rows for _, x in r], np.float64)
+    rhs = rng.uniform(-1.0, 1.0, n)
+    return O.CSR(rp, ci, v, rhs)

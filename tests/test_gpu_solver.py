@@ -213,3 +213,71 @@ def test_ilut_solve(gpu_ctx, prob, precision):
     assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-7
     _, st0 = gpu_ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision=precision, precond="ilu0", tol=1e-10, max_iters=4000)
     assert st["iterations"] <= st0["iterations"], (st, st0)
+
+
+def test_ilut_long_rows_match_oracle(gpu_ctx):
+    """ILUT(20, 1e-6) on a system whose first row's U part and last row's L part hold about 1500
+    entries: the device's p-largest selection keeps what the oracle's ILUT keeps (factor values
+    at A's entries to 1e-11 of the row scale), and the solve reaches 1e-10 with x within 1e-7
+    of the direct solution."""
+    A = cases.arrow_csr()
+    p, tau = 20, 1e-6
+    S = gpu_ctx.system(A.rp, A.ci, A.v, A.rhs, precision="fp64", precond="ilut", ilut_entries=p, ilut_drop=tau)
+    try:
+        lu = S.factor_values()
+    finally:
+        S.free()
+    rp, ci, flu = O.ilut_csr(A, p, tau)
+    ref = np.zeros(A.nnz)
+    for i in range(A.n):
+        cols = ci[rp[i]:rp[i + 1]]
+        mine = A.ci[A.rp[i]:A.rp[i + 1]]
+        pos = np.minimum(np.searchsorted(cols, mine), len(cols) - 1)
+        ref[A.rp[i]:A.rp[i + 1]] = np.where(cols[pos] == mine, flu[rp[i] + pos], 0.0)
+    assert np.count_nonzero(ref[A.rp[0]:A.rp[1]]) == p + 1 and np.count_nonzero(ref[A.rp[-2]:A.rp[-1]]) == p + 1
+    scale = np.maximum(np.abs(ref), 1.0)
+    assert np.max(np.abs(lu - ref) / scale) < 1e-11
+    xd = O.dense_solve(A, A.rhs)
+    x, st = gpu_ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision="fp64", precond="ilut", ilut_entries=p, ilut_drop=tau,
+                              tol=1e-10, max_iters=2000)
+    assert st["status"] == 0 and st["rel_residual"] < 1e-10, st
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-7
+
+
+def test_sweep_modes_bitwise_equal(gpu_ctx, prob):
+    """The triangular-sweep schedules (grid barrier per level, one launch per level, one CTA per
+    system, barrier-free flow) compute every row in the same order, so the iterates, the
+    iteration count and x are bitwise the same whichever one runs."""
+    name, P, A = prob
+    out = {}
+    for mode in ("persistent", "per_level", "per_system", "flow"):
+        x, st = gpu_ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision="mixed", precond="ilu0", trsv=mode, tol=1e-10, max_iters=4000)
+        assert st["status"] == 0 and st["rel_residual"] < 1e-10, (mode, st)
+        out[mode] = (x, st)
+    assert out["flow"][1]["sweep_mode"] == 4 and out["persistent"][1]["sweep_mode"] == 1
+    x0, st0 = out["persistent"]
+    for mode, (x, st) in out.items():
+        assert st["iterations"] == st0["iterations"], (mode, st["iterations"], st0["iterations"])
+        assert np.array_equal(x, x0), (mode, np.max(np.abs(x - x0)))
+
+
+def test_flow_sweep_batch_equals_alone(gpu_ctx):
+    """A batch of systems of uneven size swept by the barrier-free kernel gives each member the
+    x it gets alone."""
+    probs = [cases.oracle_problem(*cases.diode_small(L=L, boxes=b, bias=v)) for L, b, v in ((1, 30, 0.2), (3, 24, 0.5))]
+    probs.append(cases.oracle_problem(*cases.bar_small(L=3, nx=10, ny=4, n_energies=24)))
+    mats = [P.matrix(3) for P in probs]
+    alone = []
+    for A in mats:
+        x, st = gpu_ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision="mixed", trsv="flow")
+        assert st["status"] == 0
+        alone.append(x)
+    systems = [gpu_ctx.system(A.rp, A.ci, A.v, A.rhs, precision="mixed", trsv="flow") for A in mats]
+    try:
+        stats = gpu_ctx.batch_solve(systems)
+        for S, st, xa in zip(systems, stats, alone):
+            assert st["status"] == 0 and st["rel_residual"] < 1e-10 and st["sweep_mode"] == 4
+            assert np.array_equal(S.x(), xa)
+    finally:
+        for S in systems:
+            S.free()

@@ -274,3 +274,21 @@ def test_ilut_pattern_matches_oracle(prob, p, tau):
     frp, fci, _ = O.ilut_csr(A, p, tau)
     final = set((i, int(j)) for i in range(A.n) for j in fci[frp[i]:frp[i + 1]])
     assert final <= got
+
+
+def test_ilut_pattern_long_rows():
+    """Rows whose ILUT parts hold about 1500 entries: the host analysis takes them and its pass
+    sets still match the oracle's ILUT(20, 1e-6) entry for entry."""
+    A = cases.arrow_csr()
+    p, tau = 20, 1e-6
+    Lt = gpu.layout(A.rp, A.ci, values=A.v, precond="ilut", ilut_entries=p, ilut_drop=tau)
+    perm = Lt["perm"]
+    got = set((int(perm[i]), int(perm[j])) for i, j in _slot_pattern(Lt))
+    rp, ci = O.ilut_passed(A, p, tau)
+    assert np.diff(rp)[0] > 1024 and np.diff(rp)[-1] > 1024
+    want = set()
+    for i in range(A.n):
+        want.update((i, int(j)) for j in ci[rp[i]:rp[i + 1]])
+        want.update((i, int(j)) for j in A.ci[A.rp[i]:A.rp[i + 1]])
+        want.add((i, i))
+    assert got == want

@@ -154,7 +154,8 @@ struct Batch {
   int autotune_trsv(Ctx &ctx);
   bool trsv_tuned = false;
   int trsv_bps_max = 4;
-  std::vector<double> trsv_tune_ms;  // ms per apply for 1, 2, ... CTAs per SM
+  std::vector<double> trsv_tune_ms;  // ms per apply for 1, 2, ... CTAs per SM (barrier sweeps, then flow sweeps)
+  int trsv_kernel = 1;               // grid-wide sweep launched: 1 barrier per level, 3 flow (vk_trsv modes)
   int factor(Ctx &ctx);
   int bicgstab(Ctx &ctx, double tol, int max_iter, bool resume, int &iters_out);
   int start(Ctx &ctx, double tol, int max_iter, bool resume);

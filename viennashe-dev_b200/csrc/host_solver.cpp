@@ -440,9 +440,6 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   }
   const int64_t fnnz = frp[size_t(n)];
   nnzF = fnnz;
-  if (ilut)
-    for (int64_t i = 0; i < n; ++i)
-      if (frp[size_t(i) + 1] - frp[size_t(i)] > 1024) { err = "an ILUT row pattern longer than 1024 entries"; return VSHE_E_UNSUPPORTED; }
 
   // Forward levels over the symmetrised, block-restricted graph of F in base order: a row's
   // level is one more than the highest level of any coupled (F_ij or F_ji != 0) earlier row of
@@ -1032,38 +1029,45 @@ int Batch::factor(Ctx &ctx) {
   return check_err(ctx, "ilu0 factorisation");
 }
 
-// Autotuner of the grid-wide sweep's CTA count (1 .. 4 CTAs per SM): fewer CTAs make each grid
-// barrier cheaper, more CTAs put more slices in flight per level.  Timed once per batch on its
-// own factors (one forward + backward apply, CUDA events), before the first iteration; the
-// choice does not change any result (each slice is computed the same way by whichever warp).
+// Autotuner of the grid-wide sweep: its kind (a grid barrier per level, or the barrier-free flow
+// sweep) and its CTA count (1 .. 4 CTAs per SM: fewer CTAs make each grid barrier cheaper, more
+// put more slices in flight).  Timed once per batch on its own factors (one forward + backward
+// apply, CUDA events), before the first iteration; the choice does not change any result (each
+// slice is computed the same way by whichever warp, in either kind).
 int Batch::autotune_trsv(Ctx &ctx) {
-  if (trsv_tuned || !has_pc || !grid_group || sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) return VSHE_OK;
+  const int mode = sys[0]->opts.trsv_mode;
+  if (mode == VSHE_TRSV_FLOW) trsv_kernel = 3;
+  if (trsv_tuned || !has_pc || !grid_group || mode == VSHE_TRSV_PER_LEVEL) return VSHE_OK;
   trsv_tuned = true;
   cudaStream_t s = ctx.stream;
   cudaEvent_t a, b;
   cudaEventCreate(&a); cudaEventCreate(&b);
   double best = 1e30;
-  int best_grid = trsv_grid;
-  for (int per_sm = 1; per_sm <= trsv_bps_max; ++per_sm) {
-    const int grid = per_sm * num_sms;
-    int rc = 0;
-    auto apply = [&]() {
-      return mixed ? vk_trsv_f32(1, grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s)
-                   : vk_trsv_f64(1, grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
-    };
-    rc |= apply();  // warm-up
-    cudaEventRecord(a, s);
-    for (int r = 0; r < 3; ++r) rc |= apply();
-    cudaEventRecord(b, s);
-    cudaError_t e = cudaEventSynchronize(b);
-    if (rc || e != cudaSuccess) { cudaEventDestroy(a); cudaEventDestroy(b); return ctx.cuda_fail(e != cudaSuccess ? e : cudaError_t(rc), "autotune sweeps"); }
-    float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
-    trsv_tune_ms.push_back(ms / 3.0);
-    if (ms < best) { best = ms; best_grid = grid; }
+  int best_grid = trsv_grid, best_kernel = trsv_kernel;
+  for (int kernel : {1, 3}) {
+    if ((mode == VSHE_TRSV_PERSISTENT && kernel != 1) || (mode == VSHE_TRSV_FLOW && kernel != 3)) continue;
+    for (int per_sm = 1; per_sm <= trsv_bps_max; ++per_sm) {
+      const int grid = per_sm * num_sms;
+      int rc = 0;
+      auto apply = [&]() {
+        return mixed ? vk_trsv_f32(kernel, grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s)
+                     : vk_trsv_f64(kernel, grid, d_sysdev, d_state, d_active, &levL, &levU, 0, d_bar, d_err, s);
+      };
+      rc |= apply();  // warm-up
+      cudaEventRecord(a, s);
+      for (int r = 0; r < 3; ++r) rc |= apply();
+      cudaEventRecord(b, s);
+      cudaError_t e = cudaEventSynchronize(b);
+      if (rc || e != cudaSuccess) { cudaEventDestroy(a); cudaEventDestroy(b); return ctx.cuda_fail(e != cudaSuccess ? e : cudaError_t(rc), "autotune sweeps"); }
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      trsv_tune_ms.push_back(ms / 3.0);
+      if (ms < best) { best = ms; best_grid = grid; best_kernel = kernel; }
+    }
   }
   cudaEventDestroy(a); cudaEventDestroy(b);
   trsv_grid = best_grid;
+  trsv_kernel = best_kernel;
   if (chunk_exec) { cudaGraphExecDestroy(chunk_exec); chunk_exec = nullptr; }  // the graph holds the old grid
   return check_err(ctx, "autotune sweeps");
 }
@@ -1112,7 +1116,7 @@ static thread_local EventProf g_prof;
 // resume = false: x = 0, r = b (k_bicg_init); true: r already holds b - A x (k_bicg_resume).
 int Batch::start(Ctx &ctx, double tol, int max_iter, bool resume) {
   cudaStream_t s = ctx.stream;
-  if (sys[0]->opts.trsv_mode < VSHE_TRSV_AUTO || sys[0]->opts.trsv_mode > VSHE_TRSV_PER_SYSTEM)
+  if (sys[0]->opts.trsv_mode < VSHE_TRSV_AUTO || sys[0]->opts.trsv_mode > VSHE_TRSV_FLOW)
     return ctx.fail(VSHE_E_INVALID_ARGUMENT, "trsv_mode");
   const size_t bsz = vk_bistate_size();
   std::vector<char> stbuf;
@@ -1154,8 +1158,8 @@ int Batch::write_states(Ctx &ctx, const std::vector<char> &in) {
 // replayed; under profiling, or if the driver refuses the capture, it is launched directly.
 int Batch::run_chunk(Ctx &ctx, int every) {
   cudaStream_t s = ctx.stream;
-  const int mode = (sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) ? 2 : 1;
-  const int lvl_grid = mode == 1 ? trsv_grid : std::max(1, num_sms * 8);
+  const int mode = (sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) ? 2 : trsv_kernel;
+  const int lvl_grid = mode != 2 ? trsv_grid : std::max(1, num_sms * 8);
   EventProf &P = g_prof;
   P.on = profile; P.s = s;
   auto trsv = [&](int which) -> int {
@@ -1355,6 +1359,9 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
     st.levels_U = S->nlevU;
     st.bytes_device = int64_t(S->arena.total);
     st.sweep_ctas = (has_pc && grid_group) ? trsv_grid : 0;
+    st.sweep_mode = !(has_pc && grid_group) ? 0
+                    : S->opts.trsv_mode == VSHE_TRSV_PER_LEVEL ? VSHE_TRSV_PER_LEVEL
+                    : trsv_kernel == 3 ? VSHE_TRSV_FLOW : VSHE_TRSV_PERSISTENT;
     st.tile_rows = int32_t(S->tile_rows);
     int32_t code = status;
     if (code == 0 && rel[size_t(k)] >= o.tol) code = VSHE_E_NOT_CONVERGED;

@@ -424,6 +424,40 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
 }
 
 // ------------------------------------------------- triangular solves (ILU apply)
+// Barrier-free ("flow") sweeps: every row of ytmp and of the output starts the launch holding
+// kPending, a NaN bit pattern that no arithmetic produces, and a row that reads a solved value
+// polls that word until the row that produces it has written it.  The value is its own flag
+// (one 8-byte word, written once per launch), so no fence is needed between a value and a flag.
+constexpr unsigned long long kPending = 0x7FF4DEAD7FF4DEADull;
+constexpr unsigned long long kFlowSpinLimit = 4000000ull;  // a few seconds at most; a real wait lasts microseconds
+
+__device__ __forceinline__ double ld_flow(const double *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
+  return __longlong_as_double((long long)v);
+}
+__device__ __forceinline__ void st_flow(double *p, double v) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"((unsigned long long)__double_as_longlong(v)) : "memory");
+}
+__device__ __forceinline__ bool is_pending(double v) { return (unsigned long long)__double_as_longlong(v) == kPending; }
+
+// Polls *p until it holds a solved value; v is the value already loaded.  Gives up after
+// kFlowSpinLimit polls (error word set to VSHE_E_TIMEOUT) or once another warp has set the
+// error word, returning 0.
+__device__ __noinline__ double wait_flow(const double *p, double v, int32_t *err) {
+  unsigned long long spins = 0;
+  unsigned ns = 32;
+  while (is_pending(v)) {
+    if (++spins > kFlowSpinLimit) { atomicExch(err, VSHE_E_TIMEOUT_DEV); return 0.0; }
+    if ((spins & 255) == 0 && *((volatile int32_t *)err) != 0) return 0.0;
+    __nanosleep(ns);  // polls back off so that waiting lanes leave L2 to the working ones
+    if (ns < 512) ns <<= 1;
+    v = ld_flow(p);
+  }
+  return v;
+}
+
+
 // out = U^{-1} L^{-1} in (solver order) over SELL-32 factor slices stored in precision P;
 // the arithmetic and the work vector ytmp are FP64 in both modes.  which 0: ph = M^{-1} p,
 // 1: sh = M^{-1} s.  A level is a list of (system, slice) entries; the warps of the grid take
@@ -435,7 +469,7 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
 // kTrsvU entry loads together with the row's own operand (in[row] forward; urow, ytmp[row] and
 // the inverse diagonal backward); finish() gathers the solved values at those columns, walks any
 // further entries and writes the row.  Rows are summed in index order (FMA), as sell_rowsum.
-template <typename P, bool CG>
+template <typename P, bool CG, bool FLOW = false>
 struct TrsvSlice {
   bool on = false;
   int width = 0, nr = 0;
@@ -448,6 +482,7 @@ struct TrsvSlice {
   double base = 0.0, dinv = 1.0;
   int32_t cc[kTrsvU];
   P aa[kTrsvU];
+  int32_t *err = nullptr;  // flow sweeps: the launch's error word
 
   __device__ __forceinline__ void load(const SysDev<P> *sys, const BiState *st, const int32_t *active, const Levels &lv, int64_t c,
                                        bool lower, int which) {
@@ -483,7 +518,12 @@ struct TrsvSlice {
       if (lane < nr) {
         row = S.urow[t0 + lane];
         dinv = (double)S.udinv[t0 + lane];
-        base = CG ? __ldcg(&S.ytmp[row]) : S.ytmp[row];
+        if constexpr (FLOW) {
+          base = ld_flow(&S.ytmp[row]);
+          if (is_pending(base)) base = wait_flow(&S.ytmp[row], base, err);
+        } else {
+          base = CG ? __ldcg(&S.ytmp[row]) : S.ytmp[row];
+        }
       }
     }
 #pragma unroll
@@ -500,14 +540,34 @@ struct TrsvSlice {
     if (!on) return;
     const int lane = threadIdx.x & 31;
     double xx[kTrsvU];
+    if constexpr (FLOW) {
 #pragma unroll
-    for (int u = 0; u < kTrsvU; ++u) xx[u] = u < width ? (CG ? __ldcg(src + cc[u]) : src[cc[u]]) : 0.0;
+      for (int u = 0; u < kTrsvU; ++u) xx[u] = u < width ? ld_flow(src + cc[u]) : 0.0;
+#pragma unroll
+      for (int u = 0; u < kTrsvU; ++u)
+        if (u < width && is_pending(xx[u])) xx[u] = wait_flow(src + cc[u], xx[u], err);
+    } else {
+#pragma unroll
+      for (int u = 0; u < kTrsvU; ++u) xx[u] = u < width ? (CG ? __ldcg(src + cc[u]) : src[cc[u]]) : 0.0;
+    }
     double sum = 0.0;
 #pragma unroll
     for (int u = 0; u < kTrsvU; ++u)
       if (u < width) sum = fma((double)aa[u], xx[u], sum);
-    if (width > kTrsvU) sum = sell_rowsum_from<P, CG, 1>(off, width, kTrsvU, col, val, src, sum);
-    if (lane < nr) dst[row] = (base - sum) * dinv;
+    if constexpr (FLOW) {
+      for (int k = kTrsvU; k < width; ++k) {
+        const int64_t e = off + 32 * k + lane;
+        const int32_t c = __ldcs(col + e);
+        const P a = __ldcs(val + e);
+        double x = ld_flow(src + c);
+        if (is_pending(x)) x = wait_flow(src + c, x, err);
+        sum = fma((double)a, x, sum);
+      }
+      if (lane < nr) st_flow(dst + row, (base - sum) * dinv);
+    } else {
+      if (width > kTrsvU) sum = sell_rowsum_from<P, CG, 1>(off, width, kTrsvU, col, val, src, sum);
+      if (lane < nr) dst[row] = (base - sum) * dinv;
+    }
   }
 };
 
@@ -538,6 +598,46 @@ __global__ void __launch_bounds__(kThreads) k_trsv_persistent(const SysDev<P> *s
   for (int k = 0; k < lU.nlev; ++k) {
     trsv_level_rows<P>(sys, st, active, lU, k, false, which);
     if (k + 1 < lU.nlev && !grid_barrier(bar, err)) return;
+  }
+}
+
+// Barrier-free sweeps in one cooperative launch.  Phase 1 marks every row that the launch will
+// solve (ytmp for the forward slices, the output for the backward ones) as kPending; one grid
+// barrier; phase 2 deals the forward then the backward slices of the merged level lists out to
+// the warps in turn (entry g to warp g mod W, each warp in increasing g), and a row waits only on
+// the rows it reads.  Deadlock-free because every warp is resident and takes its entries in
+// increasing order: the lowest unfinished entry reads only finished rows.  Each row is summed in
+// the same order as in k_trsv_persistent, so the results are bitwise the same.
+template <typename P>
+__global__ void __launch_bounds__(kThreads, 4) k_trsv_flow(const SysDev<P> *sys, const BiState *st, const int32_t *active, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
+  const int64_t nL = lL.lvl_ptr[lL.nlev], nU = lU.lvl_ptr[lU.nlev];
+  const double pend = __longlong_as_double((long long)kPending);
+  for (int64_t g = gw; g < nL + nU; g += nw) {
+    const bool lower = g < nL;
+    const int64_t c = lower ? g : g - nL;
+    const int s = lower ? lL.ent_sys[c] : lU.ent_sys[c];
+    if (!active[s] || st[s].done || (which == 1 && st[s].s_conv)) continue;
+    const SysDev<P> &S = sys[s];
+    const int j = lower ? lL.ent_row[c] : lU.ent_row[c];
+    if (lower) {
+      const int32_t q0 = S.lrow0[j];
+      if (lane < S.lrow0[j + 1] - q0) S.ytmp[q0 + lane] = pend;
+    } else {
+      const int32_t t0 = S.uslot0[j];
+      if (lane < S.uslot0[j + 1] - t0) (which == 0 ? S.ph : S.sh)[S.urow[t0 + lane]] = pend;
+    }
+  }
+  if (!grid_barrier(bar, err)) return;
+  for (int64_t g = gw; g < nL + nU; g += nw) {
+    if (*((volatile int32_t *)err) != 0) return;
+    const bool lower = g < nL;
+    TrsvSlice<P, true, true> a;
+    a.err = err;
+    a.load(sys, st, active, lower ? lL : lU, lower ? g : g - nL, lower, which);
+    a.finish();
   }
 }
 
@@ -601,34 +701,69 @@ __device__ __forceinline__ int64_t find_col(const int32_t *ci, int64_t a, int64_
 }
 
 // Keeps the pkeep largest |entries| of lu[lo, hi) (ties: the lower column wins), zeroing the
-// others; one warp, entries already zero stay zero and do not count.  Parts longer than 1024
-// entries are refused by the host (Layout::build).
+// others; one warp, entries already zero stay zero and do not count.  In the order "|value|
+// descending, then position ascending" the nonzero entries have the distinct ranks 0 .. cnt-1;
+// the entry of rank pkeep-1 (magnitude bits vb at position kb) is the last one kept, and every
+// entry after it in that order is zeroed.  Short parts find it by ranking every entry against
+// the part; long ones (more than kRankMax entries) bisect the bits of vb (|x| of a double orders
+// like its bit pattern with the sign cleared) and then walk the ties in position order.
+constexpr int64_t kRankMax = 256;
+__device__ __forceinline__ unsigned long long abs_bits(double v) {
+  return (unsigned long long)__double_as_longlong(v) & 0x7FFFFFFFFFFFFFFFull;
+}
 __device__ void keep_largest(double *lu, int64_t lo, int64_t hi, int pkeep) {
   const int lane = threadIdx.x & 31;
   int cnt = 0;
   for (int64_t k = lo + lane; k < hi; k += 32) cnt += __ldcg(&lu[k]) != 0.0 ? 1 : 0;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  cnt = warp_sum(cnt);
   if (cnt <= pkeep) return;
   __syncwarp();
-  // rank every entry against the whole part (parts are a few dozen entries), then zero; the
-  // decisions of a lane's entries (at most 32 per lane: parts up to 1024 entries) are a bitmask
-  uint32_t drop = 0;
-  int m = 0;
-  for (int64_t k = lo + lane; k < hi && m < 32; k += 32, ++m) {
-    const double v = fabs(__ldcg(&lu[k]));
-    if (v == 0.0) continue;
-    int rank = 0;
-    for (int64_t k2 = lo; k2 < hi; ++k2) {
-      const double v2 = fabs(__ldcg(&lu[k2]));
-      if (v2 > v || (v2 == v && k2 < k)) ++rank;
+  unsigned long long vb = 0;
+  int64_t kb = -1;
+  if (pkeep > 0 && hi - lo <= kRankMax) {
+    for (int64_t k = lo + lane; k < hi; k += 32) {
+      const unsigned long long v = abs_bits(__ldcg(&lu[k]));
+      if (v == 0) continue;
+      int rank = 0;
+      for (int64_t k2 = lo; k2 < hi && rank < pkeep; ++k2) {
+        const unsigned long long v2 = abs_bits(__ldcg(&lu[k2]));
+        if (v2 > v || (v2 == v && k2 < k)) ++rank;
+      }
+      if (rank == pkeep - 1) { vb = v; kb = k; }
     }
-    if (rank >= pkeep) drop |= 1u << m;
+    const unsigned found = __ballot_sync(0xffffffffu, kb >= 0);
+    if (!found) return;
+    const int src = __ffs(found) - 1;
+    vb = __shfl_sync(0xffffffffu, vb, src);
+    kb = __shfl_sync(0xffffffffu, kb, src);
+  } else if (pkeep > 0) {
+    // vb = the largest bit pattern t with at least pkeep entries >= t
+    for (int bit = 62; bit >= 0; --bit) {
+      const unsigned long long t = vb | (1ull << bit);
+      int c = 0;
+      for (int64_t k = lo + lane; k < hi; k += 32) c += abs_bits(__ldcg(&lu[k])) >= t ? 1 : 0;
+      if (warp_sum(c) >= pkeep) vb = t;
+    }
+    // the entries equal to vb that stay: pkeep minus those above vb, the lowest positions first
+    int above = 0;
+    for (int64_t k = lo + lane; k < hi; k += 32) above += abs_bits(__ldcg(&lu[k])) > vb ? 1 : 0;
+    int need = pkeep - warp_sum(above);
+    for (int64_t k0 = lo; k0 < hi && kb < 0; k0 += 32) {
+      const int64_t k = k0 + lane;
+      const bool tie = k < hi && abs_bits(__ldcg(&lu[k])) == vb;
+      const unsigned m = __ballot_sync(0xffffffffu, tie);
+      const int before = __popc(m & ((1u << lane) - 1u));
+      const unsigned hit = __ballot_sync(0xffffffffu, tie && before == need - 1);
+      if (hit) kb = k0 + (__ffs(hit) - 1);
+      else need -= __popc(m);
+    }
+    if (kb < 0) return;
   }
   __syncwarp();
-  m = 0;
-  for (int64_t k = lo + lane; k < hi && m < 32; k += 32, ++m)
-    if (drop & (1u << m)) lu[k] = 0.0;
+  for (int64_t k = lo + lane; k < hi; k += 32) {
+    const unsigned long long v = abs_bits(__ldcg(&lu[k]));
+    if (kb < 0 || v < vb || (v == vb && k > kb)) lu[k] = 0.0;
+  }
   __syncwarp();
 }
 
@@ -804,10 +939,11 @@ static int tile_grid(int ntiles) { return ntiles; }
 
 template <typename P>
 static int launch_trsv_t(int mode, int grid, const SysDev<P> *sys, const BiState *st, const int32_t *act, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err, cudaStream_t s) {
-  if (mode == 1) {
+  if (mode == 1 || mode == 3) {
     g_launches += 1;
     void *args[] = {(void *)&sys, (void *)&st, (void *)&act, (void *)&lL, (void *)&lU, (void *)&which, (void *)&bar, (void *)&err};
-    return (int)cudaLaunchCooperativeKernel((void *)k_trsv_persistent<P>, dim3(grid), dim3(kThreads), args, 0, s);
+    return (int)cudaLaunchCooperativeKernel(mode == 1 ? (void *)k_trsv_persistent<P> : (void *)k_trsv_flow<P>, dim3(grid), dim3(kThreads),
+                                            args, 0, s);
   }
   g_launches += lL.nlev + lU.nlev;
   for (int pass = 0; pass < 2; ++pass) {
@@ -865,7 +1001,11 @@ void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles 
                             *(const Levels *)lU, which, bar, err, s);                                                \
   }                                                                                                                  \
   int vk_trsv_occupancy_##SUF(int *blocks_per_sm) {                                                                  \
-    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, (void *)k_trsv_persistent<P>, kThreads, 0); \
+    int b1 = 0, b2 = 0;                                                                                              \
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, (void *)k_trsv_persistent<P>, kThreads, 0);   \
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, (void *)k_trsv_flow<P>, kThreads, 0); \
+    *blocks_per_sm = b1 < b2 ? b1 : b2;                                                                              \
+    return (int)e;                                                                                                   \
   }                                                                                                                  \
   void vk_split_factor_##SUF(int64_t nnz, int64_t n, const double *lu, const int64_t *fmap, const int64_t *diag,     \
                              const int64_t *dpos, P *lval, P *uval, P *udinv, cudaStream_t s) {                      \

@@ -59,7 +59,7 @@ class SolveStatsC(C.Structure):
         ("status", C.c_int32), ("iterations", C.c_int32), ("refinements", C.c_int32),
         ("rel_residual", C.c_double), ("setup_ms", C.c_double), ("solve_ms", C.c_double),
         ("levels_L", C.c_int32), ("levels_U", C.c_int32), ("bytes_device", C.c_int64),
-        ("sweep_ctas", C.c_int32), ("tile_rows", C.c_int32),
+        ("sweep_ctas", C.c_int32), ("tile_rows", C.c_int32), ("sweep_mode", C.c_int32),
     ]
 
 

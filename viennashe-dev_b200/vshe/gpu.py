@@ -22,7 +22,7 @@ ERRORS = {
 PRECISION = {"fp64": 0, "mixed": 1}
 PRECOND = {"none": 0, "ilu0": 1, "block_ilu0": 2, "ilut": 3}
 ORDERING = {"natural": 0, "multicolor": 1}
-TRSV = {"auto": 0, "persistent": 1, "per_level": 2, "per_system": 3}
+TRSV = {"auto": 0, "persistent": 1, "per_level": 2, "per_system": 3, "flow": 4}
 
 _lib = None
 
