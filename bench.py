@@ -387,7 +387,7 @@ def run_ours(args, D_):
     solve = {"iterations": st["iterations"], "residual_replacements": st["refinements"], "rel_residual": st["rel_residual"],
              "factor_ms": st["setup_ms"], "krylov_ms": st["solve_ms"], "levels_L": st["levels_L"], "levels_U": st["levels_U"],
              "sweep_ctas_autotuned": st.get("sweep_ctas"), "tile_rows_autotuned": st.get("tile_rows"),
-             "sweep_autotuned": SWEEP_NAMES.get(st.get("sweep_mode"), "none")}
+             "sweep_kind": SWEEP_NAMES.get(st.get("sweep_mode"), "none")}
     n, nnz, nnz_lu = int(info["n_even"]), int(info["nnz_reduced"]), int(info["nnz_factor"])
     if args.pass_only:
         if D_.rank == 0:

@@ -71,8 +71,8 @@ extern "C" {
 #define VSHE_TRSV_PER_SYSTEM  3   /* one CTA per system walks the system's levels (CTA barrier per level);
                                      AUTO picks it for systems with many short levels (1D devices) */
 #define VSHE_TRSV_FLOW        4   /* one cooperative launch per triangular solve without level barriers:
-                                     each row waits only on the rows it reads; AUTO times it against
-                                     VSHE_TRSV_PERSISTENT per batch and keeps the faster (same results) */
+                                     each row polls the rows it reads; same results, measured 2-3x
+                                     slower than VSHE_TRSV_PERSISTENT, so AUTO never picks it */
 
 typedef struct vshe_solve_opts {
   int32_t precision;        /* VSHE_PRECISION_* */

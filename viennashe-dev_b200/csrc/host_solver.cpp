@@ -1029,11 +1029,13 @@ int Batch::factor(Ctx &ctx) {
   return check_err(ctx, "ilu0 factorisation");
 }
 
-// Autotuner of the grid-wide sweep: its kind (a grid barrier per level, or the barrier-free flow
-// sweep) and its CTA count (1 .. 4 CTAs per SM: fewer CTAs make each grid barrier cheaper, more
-// put more slices in flight).  Timed once per batch on its own factors (one forward + backward
-// apply, CUDA events), before the first iteration; the choice does not change any result (each
-// slice is computed the same way by whichever warp, in either kind).
+// Autotuner of the grid-wide sweep's CTA count (1 .. 4 CTAs per SM: fewer CTAs make each grid
+// barrier cheaper, more put more slices in flight), for the sweep kind the options name (a grid
+// barrier per level unless VSHE_TRSV_FLOW asks for the barrier-free sweep, which measured 2-3x
+// slower on the 2D bar with 21 and with 779 levels, so AUTO does not try it).  Timed once per
+// batch on its own factors (one forward + backward apply, CUDA events), before the first
+// iteration; the choice does not change any result (each slice is computed the same way by
+// whichever warp, in either kind).
 int Batch::autotune_trsv(Ctx &ctx) {
   const int mode = sys[0]->opts.trsv_mode;
   if (mode == VSHE_TRSV_FLOW) trsv_kernel = 3;
@@ -1045,7 +1047,7 @@ int Batch::autotune_trsv(Ctx &ctx) {
   double best = 1e30;
   int best_grid = trsv_grid, best_kernel = trsv_kernel;
   for (int kernel : {1, 3}) {
-    if ((mode == VSHE_TRSV_PERSISTENT && kernel != 1) || (mode == VSHE_TRSV_FLOW && kernel != 3)) continue;
+    if ((kernel == 3) != (mode == VSHE_TRSV_FLOW)) continue;
     for (int per_sm = 1; per_sm <= trsv_bps_max; ++per_sm) {
       const int grid = per_sm * num_sms;
       int rc = 0;
