@@ -65,6 +65,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the drop-in (host-buffer) measurement")
     ap.add_argument("--mos-shrink", type=int, default=1, help="mosfet workload: mesh divided by this factor per axis")
     ap.add_argument("--served-requests", type=int, default=24)
+    ap.add_argument("--mos-precond", choices=["ilut", "block_ilu0"], default="ilut",
+                    help="mosfet workload: ILUT in natural order, or node-coloured block-ILU(0) per energy slab")
+    ap.add_argument("--max-iters", type=int, default=0, help="cap on BiCGStab iterations (0: 20000, mosfet 3000)")
+    ap.add_argument("--sweep", choices=["auto", "persistent", "per_level", "flow"], default="auto",
+                    help="triangular-sweep schedule of the grid-wide sweeps (same results; auto = grid barrier per level)")
     ap.add_argument("--ilut-entries", type=int, default=20, help="mosfet workload: ILUT's p (entries kept per L and U row)")
     ap.add_argument("--ilut-drop", type=float, default=1e-3, help="mosfet workload: ILUT's drop tolerance")
     ap.add_argument("--pass-only", action="store_true",
@@ -173,11 +178,15 @@ def workload_name(args):
 def solver_options(args):
     """Preconditioner of the workload (measured per device class): the 2D bar at L <= 3 uses
     node-coloured block-ILU per energy slab, ILU(1) with a distance-2 colouring by default (576
-    instead of 960 iterations, 7 % faster per solve than ILU(0)); the L = 5 MOSFET needs
-    ILUT(20, 1e-3) in natural order (ILU(0) stalls there in every order)."""
+    instead of 960 iterations, 7 % faster per solve than ILU(0)).  The L = 5 MOSFET takes ILUT in
+    natural order (ILU(0) stalls there in every order; ILUT(20, 1e-3) converges on the 30 x 10
+    mesh in 53 iterations, but neither it nor ILUT(60, 1e-4) converges on the 60 x 20 mesh, so
+    the full-size run measures the device pass and the iteration rate, not a converged solve)."""
+    if args.workload == "mosfet" and args.mos_precond == "ilut":
+        return dict(precond="ilut", ordering="natural", ilut_entries=args.ilut_entries, ilut_drop=args.ilut_drop, trsv=args.sweep)
     if args.workload == "mosfet":
-        return dict(precond="ilut", ordering="natural", ilut_entries=args.ilut_entries, ilut_drop=args.ilut_drop)
-    return dict(precond="block_ilu0", ordering="multicolor", fill_level=args.fill_level)
+        return dict(precond="block_ilu0", ordering="multicolor", fill_level=0, trsv=args.sweep)
+    return dict(precond="block_ilu0", ordering="multicolor", fill_level=args.fill_level, trsv=args.sweep)
 
 
 def build_problem(args, ctx, precision):
@@ -187,8 +196,8 @@ def build_problem(args, ctx, precision):
         dev, cfg = D.config5(nx=240 // args.mos_shrink, ny=80 // args.mos_shrink)
     else:
         dev, cfg = D.config2(nx=args.nx, ny=args.ny, n_energies=args.ne, L=args.L)
-    return gpu.SheProblem(ctx, dev, cfg, precision=precision, tol=TOL, max_iters=3000 if args.workload == "mosfet" else 20000,
-                          check_every=16, **solver_options(args))
+    cap = args.max_iters or (3000 if args.workload == "mosfet" else 20000)
+    return gpu.SheProblem(ctx, dev, cfg, precision=precision, tol=TOL, max_iters=cap, check_every=16, **solver_options(args))
 
 
 # -------------------------------------------------------------- CPU baseline
@@ -498,7 +507,8 @@ def run_ours(args, D_):
                        "n_energies": int(info["n_energies"]),
                        "preconditioner": ("block-ILU(%d) per energy slab, node %s colouring" % (args.fill_level, "distance-2" if args.fill_level else "4-colour")
                                           if args.workload == "bar"
-                                          else "ILUT(%d, %g), natural order" % (args.ilut_entries, args.ilut_drop)),
+                                          else "ILUT(%d, %g), natural order" % (args.ilut_entries, args.ilut_drop)
+                                          if args.mos_precond == "ilut" else "block-ILU(0) per energy slab, node 4-colour colouring"),
                        "l2": "inputs larger than L2 (reduced system %.2f GB)" % (nnz * 12 / 1e9),
                        "parallelism": "replicas" if D_.world > 1 else "single"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
