@@ -902,7 +902,7 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   int bps = 0;
   if (mixed) vk_trsv_occupancy_f32(&bps); else vk_trsv_occupancy_f64(&bps);
   trsv_grid = std::max(1, std::min(bps, 4)) * num_sms;
-  trsv_bps_max = std::max(1, std::min(bps, 4));
+  trsv_bps_max = std::max(1, std::min(bps, 8));
   int bpf = 0;
   vk_ilu0_occupancy(&bpf);
   ilu_grid = std::max(1, std::min(bpf, 4)) * num_sms;
@@ -1029,7 +1029,7 @@ int Batch::factor(Ctx &ctx) {
   return check_err(ctx, "ilu0 factorisation");
 }
 
-// Autotuner of the grid-wide sweep's CTA count (1 .. 4 CTAs per SM: fewer CTAs make each grid
+// Autotuner of the grid-wide sweep's CTA count (1 .. 6 CTAs per SM: fewer CTAs make each grid
 // barrier cheaper, more put more slices in flight), for the sweep kind the options name (a grid
 // barrier per level unless VSHE_TRSV_FLOW asks for the barrier-free sweep, which measured 2-3x
 // slower on the 2D bar with 21 and with 779 levels, so AUTO does not try it).  Timed once per

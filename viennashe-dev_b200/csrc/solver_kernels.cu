@@ -46,6 +46,9 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kSpmvU = 8;  // SELL entries per lane whose loads are issued together
 constexpr int kDotU = 6;   // the same inside the tile kernels, which also carry reduction state
 constexpr int kTrsvU = 8;  // entries of a factor row loaded at once (factor rows hold ~5 entries)
+// CTAs per SM the grid-wide sweeps are compiled for (40 registers, a few spilled): up to 6 CTAs
+// of slices in flight per SM.  The autotuner picks 1 .. 6; on the 2D bar 6 beat 4 by 3 %.
+constexpr int kTrsvCtasPerSm = 6;
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -590,7 +593,7 @@ __device__ __forceinline__ void trsv_level_rows(const SysDev<P> *sys, const BiSt
 }
 
 template <typename P>
-__global__ void __launch_bounds__(kThreads) k_trsv_persistent(const SysDev<P> *sys, const BiState *st, const int32_t *active, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err) {
+__global__ void __launch_bounds__(kThreads, kTrsvCtasPerSm) k_trsv_persistent(const SysDev<P> *sys, const BiState *st, const int32_t *active, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err) {
   for (int k = 0; k < lL.nlev; ++k) {
     trsv_level_rows<P>(sys, st, active, lL, k, true, which);
     if (!grid_barrier(bar, err)) return;
@@ -609,7 +612,7 @@ __global__ void __launch_bounds__(kThreads) k_trsv_persistent(const SysDev<P> *s
 // increasing order: the lowest unfinished entry reads only finished rows.  Each row is summed in
 // the same order as in k_trsv_persistent, so the results are bitwise the same.
 template <typename P>
-__global__ void __launch_bounds__(kThreads, 4) k_trsv_flow(const SysDev<P> *sys, const BiState *st, const int32_t *active, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err) {
+__global__ void __launch_bounds__(kThreads, kTrsvCtasPerSm) k_trsv_flow(const SysDev<P> *sys, const BiState *st, const int32_t *active, Levels lL, Levels lU, int which, unsigned *bar, int32_t *err) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
