@@ -330,10 +330,12 @@ def measure_batched_sweep(ctx, reps=3):
 
 def served_options(dev, cfg):
     """Solver options per request class (measured): 1D devices natural-order ILU(0) over the whole
-    system; 2D bars node-coloured block-ILU(0) per energy slab.  The L = 5 bars of this mix (60-160
-    energies across a 0.8 V drop) do not converge with any preconditioner measured, ILUT(20, 1e-3)
-    included (the oracle's ILUT diverges on them too), so they take the cheap one and end at the
-    iteration cap as failed requests."""
+    system; 2D bars node-coloured block-ILU(0) per energy slab.  The two L = 5 bars of this mix
+    (60-160 energies across a 0.8 V drop) stall with ILU(0) in every order.  In the oracle,
+    ILUT(20, 1e-3) diverges on both; ILUT(60, 1e-4) (the reference's default) converges on the
+    smaller one (2046 cells, 24 iterations) but diverges on the larger (6188 cells, 4.2 M unknowns,
+    31 k forward levels).  So they take the cheap preconditioner and end at the iteration cap
+    as failed requests."""
     if dev.dim == 1:
         return dict(ordering="natural", precond="ilu0")
     return dict(ordering="multicolor", precond="block_ilu0")
