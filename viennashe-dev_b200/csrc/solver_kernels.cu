@@ -393,23 +393,25 @@ __device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+__device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned *p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+// The arrival is one acquire-release atomic: its release half publishes the CTA's writes
+// (ordered before it by the CTA barrier), its acquire half gives the last arriver everyone
+// else's.  The generation is read before arriving, so the release cannot be missed.  A CTA that
+// arrives after another has given up still arrives and leaves through the error check in its spin.
 __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
-    if (*((volatile int32_t *)err) != 0) ok = 0;
-  }
-  __syncthreads();
-  if (!ok) return false;
-  if (threadIdx.x == 0) {
     const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
     const unsigned gen = ld_acquire_u32(&bar[1]);
-    __threadfence();
-    const unsigned arrived = atomicAdd(&bar[0], 1u);
-    if (arrived == nb - 1) {
+    if (atom_add_acq_rel_u32(&bar[0], 1u) == nb - 1) {
       bar[0] = 0;
-      __threadfence();
       st_release_u32(&bar[1], gen + 1u);
     } else {
       unsigned long long spins = 0;
