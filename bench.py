@@ -482,12 +482,11 @@ def run_ours(args, D_):
         dbytes = spmv_bytes
         kname = "k_spmv_dot (SELL-32 SpMV FP64 + fused dots)"
     achieved = dbytes / (avg_ms / 1000.0) / 1e9
-    # DRAM traffic per launch: ncu captures of the same kernels on the 200 x 50 x 80 bar
-    # (ncu --set full; profiles/sell_kernels_bar200x50x80.md for the SpMV + dots,
-    # profiles/trsv_6cta_bar200x50x80.md for the sweeps as now compiled) measured
-    # dram__bytes_read.sum + dram__bytes_write.sum at 0.967 (SpMV + dots) and 0.980 (ILU(1)
-    # apply) of the algorithmic bytes; the traffic grows in proportion with the units processed,
-    # so a full launch's is that ratio times its algorithmic bytes.
+    # DRAM traffic per launch: ncu --set full captures of the same kernels on the 200 x 50 x 80
+    # bar (the sweeps as now compiled: 40 registers) measured dram__bytes_read.sum +
+    # dram__bytes_write.sum at 0.967 (SpMV + dots) and 0.980 (ILU(1) apply) of the algorithmic
+    # bytes; the traffic grows in proportion with the units processed, so a full launch's is
+    # that ratio times its algorithmic bytes.
     traffic_ratio = {"spmv": 383372032 / 396606924, "trsv": (421555456 + 19777280) / 450235320}
     traffic = dbytes * traffic_ratio[dominant] if args.workload == "bar" and (dominant == "spmv" or st.get("sweep_mode") == 1) else None
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_source": peak_src,
