@@ -68,11 +68,16 @@ extern "C" {
 #define VSHE_TRSV_AUTO        0
 #define VSHE_TRSV_PERSISTENT  1   /* one cooperative launch per triangular solve, grid barrier per level */
 #define VSHE_TRSV_PER_LEVEL   2   /* one launch per level */
-#define VSHE_TRSV_PER_SYSTEM  3   /* one CTA per system walks the system's levels (CTA barrier per level);
-                                     AUTO picks it for systems with many short levels (1D devices) */
+#define VSHE_TRSV_PER_SYSTEM  3   /* one CTA per system walks the system's levels (CTA barrier per level,
+                                     factor slices staged through shared memory); AUTO picks it for
+                                     systems with many short levels (1D devices) */
 #define VSHE_TRSV_FLOW        4   /* one cooperative launch per triangular solve without level barriers:
                                      each row polls the rows it reads; same results, measured 2-3x
                                      slower than VSHE_TRSV_PERSISTENT, so AUTO never picks it */
+#define VSHE_TRSV_PER_BLOCK   5   /* one CTA per preconditioner block (energy slab of BLOCK_ILU0) walks
+                                     the block's levels with a CTA barrier per level, the factor slices
+                                     staged through shared memory by bulk copies; AUTO picks it for
+                                     block-ILU systems with at least two blocks of at most 2^18 rows */
 
 typedef struct vshe_solve_opts {
   int32_t precision;        /* VSHE_PRECISION_* */
@@ -132,6 +137,11 @@ size_t vshe_bytes_in_use(vshe_ctx *ctx);
  * in [0] SpMV, [1] triangular solves, [2] vector updates, [3] unused (0),
  * [4] factorisation, and counts[0] SpMV launches, counts[1] triangular-solve launches. */
 int vshe_set_profiling(vshe_ctx *ctx, int32_t on);
+/* Polls every bounded device-side wait of this context's solves makes (grid barriers, the flow
+ * sweep's polls, the staged sweep's copy barriers) before it gives up: the solve then returns
+ * VSHE_E_TIMEOUT and the context stays usable.  0 restores the default (20,000,000 polls, about
+ * 1-2 s).  No reference counterpart: failure handling of the device-side waits. */
+int vshe_set_spin_limit(vshe_ctx *ctx, uint64_t polls);
 int vshe_get_profile(vshe_ctx *ctx, double *ms, int64_t *counts);
 /* Autotuner record: the rows per reduction tile chosen for systems of n's size class
  * (floor(log2 n)) on this context, and ms[0..3] = the timed FP64 SpMV for 512, 1024, 2048 and

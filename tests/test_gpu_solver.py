@@ -246,11 +246,11 @@ def test_ilut_long_rows_match_oracle(gpu_ctx):
 
 def test_sweep_modes_bitwise_equal(gpu_ctx, prob):
     """The triangular-sweep schedules (grid barrier per level, one launch per level, one CTA per
-    system, barrier-free flow) compute every row in the same order, so the iterates, the
+    system, barrier-free flow, one CTA per block) compute every row in the same order, so the iterates, the
     iteration count and x are bitwise the same whichever one runs."""
     name, P, A = prob
     out = {}
-    for mode in ("persistent", "per_level", "per_system", "flow"):
+    for mode in ("persistent", "per_level", "per_system", "flow", "per_block"):
         x, st = gpu_ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision="mixed", precond="ilu0", trsv=mode, tol=1e-10, max_iters=4000)
         assert st["status"] == 0 and st["rel_residual"] < 1e-10, (mode, st)
         out[mode] = (x, st)
@@ -259,6 +259,52 @@ def test_sweep_modes_bitwise_equal(gpu_ctx, prob):
     for mode, (x, st) in out.items():
         assert st["iterations"] == st0["iterations"], (mode, st["iterations"], st0["iterations"])
         assert np.array_equal(x, x0), (mode, np.max(np.abs(x - x0)))
+
+
+def test_per_block_sweep_bitwise_equal():
+    """Block-ILU per energy slab on a 2D bar: the per-block sweep (one CTA per slab, factor
+    slices staged through shared memory) computes every row as the grid-wide sweep does, so x and
+    the iteration count are bitwise the same; AUTO picks it for a slab-blocked system; and a
+    batch of such systems gives each member the x it gets alone."""
+    ctx = gpu.Context(0)
+    try:
+        out = {}
+        P = cases.oracle_problem(*cases.bar_small(L=3, nx=12, ny=5, n_energies=30))
+        A = P.matrix(3)
+        blocks = P.blocks()
+        for mode in ("persistent", "per_block", "auto", "per_system"):
+            for precision in ("mixed", "fp64"):
+                x, st = ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision=precision, precond="block_ilu0", ordering="multicolor",
+                                      blocks=blocks, fill_level=1, trsv=mode, tol=1e-10, max_iters=4000)
+                assert st["status"] == 0 and st["rel_residual"] < 1e-10, (mode, precision, st)
+                out[(mode, precision)] = (x, st)
+        assert out[("auto", "mixed")][1]["sweep_mode"] == 5 and out[("per_block", "fp64")][1]["sweep_mode"] == 5
+        assert out[("persistent", "mixed")][1]["sweep_mode"] == 1 and out[("per_system", "mixed")][1]["sweep_mode"] == 3
+        for precision in ("mixed", "fp64"):
+            x0, st0 = out[("persistent", precision)]
+            for mode in ("per_block", "auto", "per_system"):
+                x, st = out[(mode, precision)]
+                assert st["iterations"] == st0["iterations"], (mode, precision, st["iterations"], st0["iterations"])
+                assert np.array_equal(x, x0), (mode, precision, np.max(np.abs(x - x0)))
+        # a batch of two slab-blocked bars and a 1D diode (swept as one task per system)
+        probs = [P, cases.oracle_problem(*cases.bar_small(L=1, nx=10, ny=4, n_energies=24)),
+                 cases.oracle_problem(*cases.diode_small(L=1, boxes=40))]
+        mats = [Q.matrix(3) for Q in probs]
+        opts = [dict(precond="block_ilu0", ordering="multicolor", blocks=probs[0].blocks(), fill_level=1),
+                dict(precond="block_ilu0", ordering="multicolor", blocks=probs[1].blocks(), fill_level=1),
+                dict(precond="block_ilu0", ordering="natural", blocks=np.array([0, mats[2].n], np.int64))]
+        alone = [ctx.solve_csr(M.rp, M.ci, M.v, M.rhs, precision="mixed", tol=1e-10, max_iters=4000, **o)[0] for M, o in zip(mats, opts)]
+        systems = [ctx.system(M.rp, M.ci, M.v, M.rhs, precision="mixed", tol=1e-10, max_iters=4000, **o) for M, o in zip(mats, opts)]
+        try:
+            stats = ctx.batch_solve(systems)
+            for S, st, xa in zip(systems, stats, alone):
+                assert st["status"] == 0 and st["rel_residual"] < 1e-10, st
+                assert np.array_equal(S.x(), xa)
+        finally:
+            for S in systems:
+                S.free()
+    finally:
+        ctx.close()
 
 
 def test_flow_sweep_batch_equals_alone(gpu_ctx):

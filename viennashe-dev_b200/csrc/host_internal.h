@@ -17,6 +17,9 @@ namespace vshe {
 
 const char *errstr(int code);
 
+// polls of a device-side wait before it gives up with VSHE_E_TIMEOUT (about 1-2 s with backoff)
+constexpr unsigned long long kDefaultSpinLimit = 20000000ull;
+
 // Device allocations owned by one object, freed together.
 struct DevArena {
   std::vector<void *> ptrs;
@@ -42,6 +45,10 @@ struct Layout {
   std::vector<int32_t> acol;
   std::vector<int64_t> fmap, dpos, loff, uoff, lstart, ustart;
   std::vector<int32_t> lcol, ucol, urow;
+  // (level, block) groups of the L and U slices: group g = slices [grp_s0[g], grp_s0[g+1]) of
+  // level grp_lev[g] and preconditioner block grp_blk[g], ordered by level, then block
+  std::vector<int64_t> lgrp_s0, ugrp_s0;
+  std::vector<int32_t> lgrp_lev, lgrp_blk, ugrp_lev, ugrp_blk;
   // values (caller order, host) are read only for the ILUT pattern and may be NULL otherwise
   int build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci,
             const vshe_solve_opts &opts, const double *values, std::string &err);
@@ -63,6 +70,9 @@ struct System {
   std::vector<int32_t> perm, blk;       // perm[q] = caller row of solver row q; blk in solver order
   std::vector<int64_t> lvr;             // forward level k = solver rows [lvr[k], lvr[k+1])
   std::vector<int64_t> lvsL, lvsU;      // forward / backward level k = L / U slices [lvs[k], lvs[k+1])
+  std::vector<int64_t> lgrp_s0, ugrp_s0;  // (level, block) slice groups (Layout)
+  std::vector<int32_t> lgrp_lev, lgrp_blk, ugrp_lev, ugrp_blk;
+  std::vector<int64_t> loff_h, uoff_h;    // SELL slot offsets of the L and U slices (host copies)
   int32_t nlevL = 0, nlevU = 0;
   int64_t nslA = 0, nslL = 0, nslU = 0;     // SELL slices
   int64_t padA = 0, padL = 0, padU = 0;     // SELL slots (incl. padding)
@@ -113,10 +123,12 @@ struct Batch {
   int32_t nlevL = 0, nlevU = 0;   // merged levels of the grid-wide sweeps
   int32_t nlevF = 0;              // merged levels of the factorisation (all members)
   int trsv_grid = 148, ilu_grid = 148, num_sms = 148;
-  // members whose triangular sweeps run one CTA per system (k_trsv_cta); the others share the
-  // merged level schedule of the grid-wide sweep
-  std::vector<int32_t> cta_members;
-  int32_t *d_cta_members = nullptr;
+  // sweep tasks (k_trsv_task: one CTA per preconditioner block or per system, TaskDev / ChunkDev
+  // tables, ordered by decreasing work); members not swept as tasks share the merged level
+  // schedule of the grid-wide sweep (grid_group)
+  int ntasks = 0;
+  std::vector<int32_t> task_kind;  // per member: 0 grid-wide sweep, 1 one task per system, 2 one task per block
+  void *d_tasks = nullptr, *d_chunks = nullptr;
   bool grid_group = true;
   // the BiCGStab iteration chunk (check_every iterations) captured once as a CUDA graph and
   // replayed; graph_failed: capture was refused (then the chunk is launched directly)
@@ -148,6 +160,8 @@ struct Batch {
   int64_t n_spmv = 0, n_trsv = 0;
 
   int build(Ctx &ctx, const std::vector<System *> &members);
+  unsigned long long bar_limit = 0;  // poll limit last written to d_bar[2..3]
+  int sync_spin_limit(Ctx &ctx);
   // only_member >= 0: tiles of that member alone, with `rows` rows (the autotuner's trial tiles)
   int set_tiles(Ctx &ctx, int only_member = -1, int64_t rows = 0);
   int autotune_tiles(Ctx &ctx);
@@ -178,6 +192,9 @@ struct Ctx {
   std::mutex mu;
   int64_t next_handle = 0;
   bool profile = false;
+  // polls of a device-side wait (grid barrier, flow poll, stage barrier) before it gives up
+  // with VSHE_E_TIMEOUT
+  unsigned long long spin_limit = kDefaultSpinLimit;
   std::map<int64_t, std::unique_ptr<System>> systems;
   std::map<std::vector<int64_t>, std::unique_ptr<Batch>> batches;
   // kernel-class timings of the last profiled solve (ms): spmv, trsv, vector, reliable, factor

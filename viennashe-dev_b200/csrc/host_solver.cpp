@@ -22,6 +22,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -201,25 +202,45 @@ static void greedy_colours(int64_t n, const std::vector<int64_t> &rp, const std:
   }
 }
 
-// SELL-32 layout of a row sequence: rows[t] (t = 0..m-1) cut into slices of 32 that never
-// straddle a level boundary (lvs = level starts in t); width of a slice = its longest row.
-// Returns the slot offsets (one per slice + 1) and the slice starts in t.
-static void sell_layout(const std::vector<int64_t> &len_of_t, const std::vector<int64_t> &lvl_t, std::vector<int64_t> &off,
-                        std::vector<int64_t> &start, std::vector<int64_t> &lvl_slices) {
+// SELL-32 layout of a row sequence rows[t] (t = 0..m-1) made of groups: group g is the run
+// [gstart[g], gstart[g+1]) of level glev[g] (non-decreasing) and one preconditioner block.
+// Slices of 32 rows never straddle a group; width of a slice = its longest row.  Returns the slot
+// offsets (one per slice + 1), the slice starts in t, the first slice of every level
+// (lvl_slices, nlev + 1 entries) and of every group (grp_slices, groups + 1 entries).
+static void sell_layout(const std::vector<int64_t> &len_of_t, const std::vector<int64_t> &gstart, const std::vector<int32_t> &glev,
+                        int32_t nlev, std::vector<int64_t> &off, std::vector<int64_t> &start, std::vector<int64_t> &lvl_slices,
+                        std::vector<int64_t> &grp_slices) {
   off.assign(1, 0);
   start.clear();
-  lvl_slices.assign(1, 0);
-  for (size_t k = 0; k + 1 < lvl_t.size(); ++k) {
-    for (int64_t t = lvl_t[k]; t < lvl_t[k + 1]; t += 32) {
-      const int64_t e = std::min<int64_t>(t + 32, lvl_t[k + 1]);
+  lvl_slices.assign(size_t(nlev) + 1, 0);
+  grp_slices.clear();
+  int32_t lv = 0;
+  for (size_t g = 0; g + 1 < gstart.size(); ++g) {
+    while (lv < glev[g]) lvl_slices[size_t(++lv)] = int64_t(start.size());
+    grp_slices.push_back(int64_t(start.size()));
+    for (int64_t t = gstart[g]; t < gstart[g + 1]; t += 32) {
+      const int64_t e = std::min<int64_t>(t + 32, gstart[g + 1]);
       int64_t w = 0;
       for (int64_t u = t; u < e; ++u) w = std::max(w, len_of_t[size_t(u)]);
       start.push_back(t);
       off.push_back(off.back() + 32 * w);
     }
-    lvl_slices.push_back(int64_t(start.size()));
   }
-  start.push_back(lvl_t.empty() ? 0 : lvl_t.back());
+  grp_slices.push_back(int64_t(start.size()));
+  while (lv < nlev) lvl_slices[size_t(++lv)] = int64_t(start.size());
+  start.push_back(gstart.empty() ? 0 : gstart.back());
+}
+
+// Groups of a row sequence: maximal runs of equal (level, block); the sequence is sorted by
+// level, then block.
+static void row_groups(int64_t m, const std::function<int32_t(int64_t)> &lev_of, const std::function<int32_t(int64_t)> &blk_of,
+                       std::vector<int64_t> &gstart, std::vector<int32_t> &glev, std::vector<int32_t> &gblk) {
+  gstart.clear(); glev.clear(); gblk.clear();
+  for (int64_t t = 0; t < m; ++t) {
+    const int32_t l = lev_of(t), b = blk_of(t);
+    if (t == 0 || l != glev.back() || b != gblk.back()) { gstart.push_back(t); glev.push_back(l); gblk.push_back(b); }
+  }
+  gstart.push_back(m);
 }
 
 int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci,
@@ -472,10 +493,12 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       nlevL = std::max(nlevL, m + 2);
     }
   }
-  // solver order: by level, then longest rows first (less SELL padding), then base position
+  // solver order: by level, then block (each block's rows of a level are one run, which the
+  // per-block sweeps walk), then longest rows first (less SELL padding), then base position
   perm = base;
   std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) {
     if (lev[size_t(a)] != lev[size_t(b)]) return lev[size_t(a)] < lev[size_t(b)];
+    if (blk0[size_t(a)] != blk0[size_t(b)]) return blk0[size_t(a)] < blk0[size_t(b)];
     return rp[size_t(a) + 1] - rp[size_t(a)] > rp[size_t(b) + 1] - rp[size_t(b)];
   });
   std::vector<int32_t> inv((size_t)(n));
@@ -516,8 +539,8 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     std::vector<int64_t> len((size_t)n, 0);
     for (int64_t i = 0; i < n; ++i)
       for (int64_t p = prp[size_t(i)]; p < prp[size_t(i) + 1]; ++p) len[size_t(i)] += amap[size_t(p)] >= 0 ? 1 : 0;
-    std::vector<int64_t> one{0, n};
-    sell_layout(len, one, aoff, astart, alvs);
+    std::vector<int64_t> one{0, n}, agrp;
+    sell_layout(len, one, std::vector<int32_t>{0}, 1, aoff, astart, alvs, agrp);
   }
   nslA = int64_t(astart.size()) - 1;
   padA = aoff.back();
@@ -549,7 +572,14 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       }
       llen[size_t(i)] = cl; ulen[size_t(i)] = cu;
     }
-    sell_layout(llen, lvr, loff, lstart, lvsL);
+    {
+      std::vector<int64_t> gs;
+      std::vector<int32_t> qlev((size_t)n);
+      for (int32_t k = 0; k < nlevL; ++k)
+        for (int64_t q = lvr[size_t(k)]; q < lvr[size_t(k) + 1]; ++q) qlev[size_t(q)] = k;
+      row_groups(n, [&](int64_t q) { return qlev[size_t(q)]; }, [&](int64_t q) { return blk[size_t(q)]; }, gs, lgrp_lev, lgrp_blk);
+      sell_layout(llen, gs, lgrp_lev, nlevL, loff, lstart, lvsL, lgrp_s0);
+    }
     nslL = int64_t(lstart.size()) - 1;
     padL = loff.back();
     // backward levels in solver order (real U dependencies, block-restricted)
@@ -564,18 +594,22 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       levU[size_t(i)] = m + 1;
       nlevU = std::max(nlevU, m + 2);
     }
-    std::vector<int64_t> uvt((size_t)nlevU + 1, 0);
-    for (int64_t i = 0; i < n; ++i) uvt[size_t(levU[size_t(i)]) + 1]++;
-    for (size_t k = 1; k < uvt.size(); ++k) uvt[k] += uvt[k - 1];
+    // backward-sweep slots: by backward level, then block, then solver row
     urow.resize((size_t)n);
-    {
-      std::vector<int64_t> cur(uvt.begin(), uvt.end() - 1);
-      for (int64_t i = 0; i < n; ++i) urow[size_t(cur[size_t(levU[size_t(i)])]++)] = int32_t(i);
-    }
+    std::iota(urow.begin(), urow.end(), 0);
+    std::stable_sort(urow.begin(), urow.end(), [&](int32_t a, int32_t b) {
+      if (levU[size_t(a)] != levU[size_t(b)]) return levU[size_t(a)] < levU[size_t(b)];
+      return blk[size_t(a)] < blk[size_t(b)];
+    });
     std::vector<int64_t> ulen_t((size_t)n);
     dpos.resize((size_t)n);
     for (int64_t t = 0; t < n; ++t) { ulen_t[size_t(t)] = ulen[size_t(urow[size_t(t)])]; dpos[size_t(urow[size_t(t)])] = t; }
-    sell_layout(ulen_t, uvt, uoff, ustart, lvsU);
+    {
+      std::vector<int64_t> gs;
+      row_groups(n, [&](int64_t t) { return levU[size_t(urow[size_t(t)])]; }, [&](int64_t t) { return blk[size_t(urow[size_t(t)])]; },
+                 gs, ugrp_lev, ugrp_blk);
+      sell_layout(ulen_t, gs, ugrp_lev, nlevU, uoff, ustart, lvsU, ugrp_s0);
+    }
     nslU = int64_t(ustart.size()) - 1;
     padU = uoff.back();
     fmap.assign((size_t)fnnz, -1);
@@ -625,6 +659,9 @@ int System::setup_pattern(Ctx &ctx, const double *host_val) {
   int rc = Lt.build(n, nnz, rp, ci, opts, host_val, err);
   if (rc) return ctx.fail(rc, err);
   perm = Lt.perm; blk = Lt.blk; lvr = Lt.lvr; lvsL = Lt.lvsL; lvsU = Lt.lvsU;
+  lgrp_s0 = Lt.lgrp_s0; lgrp_lev = Lt.lgrp_lev; lgrp_blk = Lt.lgrp_blk;
+  ugrp_s0 = Lt.ugrp_s0; ugrp_lev = Lt.ugrp_lev; ugrp_blk = Lt.ugrp_blk;
+  loff_h = Lt.loff; uoff_h = Lt.uoff;
   nlevL = Lt.nlevL; nlevU = Lt.nlevU; nslA = Lt.nslA; nslL = Lt.nslL; nslU = Lt.nslU;
   padA = Lt.padA; padL = Lt.padL; padU = Lt.padU; nnzL = Lt.nnzL; nnzU = Lt.nnzU; nnzF = Lt.nnzF;
   const auto &prp = Lt.prp; const auto &pci = Lt.pci; const auto &pdiag = Lt.pdiag; const auto &amap = Lt.amap;
@@ -734,7 +771,20 @@ void System::fill_sysdev(void *out) const {
 }
 
 // ------------------------------------------------------------------ Batch
+// Writes the context's poll limit into the batch's barrier words (bar[2..3]) when it changed;
+// every bounded device-side wait of the batch's kernels reads it there (outside any capture).
+int Batch::sync_spin_limit(Ctx &ctx) {
+  if (bar_limit == ctx.spin_limit) return VSHE_OK;
+  const unsigned long long v = ctx.spin_limit;
+  cudaError_t e = cudaMemcpyAsync(d_bar + 2, &v, sizeof(v), cudaMemcpyHostToDevice, ctx.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+  if (e != cudaSuccess) return ctx.cuda_fail(e, "spin limit");
+  bar_limit = v;
+  return VSHE_OK;
+}
+
 int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
+  int rc0 = 0;
   sys = members;
   nsys = int(sys.size());
   mixed = sys[0]->mixed;
@@ -742,38 +792,108 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   for (System *S : sys)
     if (S->mixed != mixed || S->has_pc != has_pc)
       return ctx.fail(VSHE_E_INVALID_ARGUMENT, "systems in one batch need the same precision and preconditioner kind");
-  // Triangular sweeps.  A member with many short levels (fewer than kCtaRowsPerLevel rows per
-  // forward level on average, more than kCtaMinLevels levels and at most kCtaMaxRows rows: 1D
-  // devices, small 2D ones in natural order) sweeps on its own
-  // CTA with a CTA barrier per level; VSHE_TRSV_PER_SYSTEM forces that for every member.  The
-  // others share a merged schedule: merged level l lists, system by system, the level-l SELL
-  // slices of every grid-swept member.
+  // Triangular sweeps.  A member sweeps either as tasks, one CTA each walking its levels with
+  // a CTA barrier per level (k_trsv_task), or in the merged level schedule of the grid-wide sweep
+  // (k_trsv_persistent).  Tasks are whole systems for members with many short levels (fewer than
+  // kCtaRowsPerLevel rows per forward level on average, more than kCtaMinLevels levels and at
+  // most kCtaMaxRows rows: 1D devices), and preconditioner blocks for block-ILU members with at
+  // least two blocks of at most kTaskMaxRows rows (energy slabs: the factor has no entry between
+  // blocks, so they sweep independently).  VSHE_TRSV_PER_SYSTEM / VSHE_TRSV_PER_BLOCK force the
+  // former / latter for every member; the grid-wide modes force the merged schedule.
   constexpr int64_t kCtaRowsPerLevel = 4096;
   constexpr int32_t kCtaMinLevels = 32;
   constexpr int64_t kCtaMaxRows = int64_t(2) << 20;  // beyond, one SM's bandwidth bounds the sweep
-  std::vector<char> on_cta((size_t)nsys, 0);
-  cta_members.clear();
+  constexpr int64_t kTaskMaxRows = int64_t(1) << 18;
+  std::vector<char> on_task((size_t)nsys, 0);  // 0 grid, 1 whole system, 2 per block
+  ntasks = 0;
   if (has_pc) {
     for (int k = 0; k < nsys; ++k) {
       const System *S = sys[size_t(k)];
       const int mode = S->opts.trsv_mode;
-      const bool want = mode == VSHE_TRSV_PER_SYSTEM ||
-                        (mode == VSHE_TRSV_AUTO && S->nlevL > kCtaMinLevels && S->n / std::max(S->nlevL, 1) < kCtaRowsPerLevel &&
-                         S->n <= kCtaMaxRows);
-      if (want) { on_cta[size_t(k)] = 1; cta_members.push_back(k); }
+      int32_t nb = 0;
+      for (int32_t b : S->blk) nb = std::max(nb, b + 1);
+      std::vector<int64_t> bsz((size_t)nb, 0);
+      for (int32_t b : S->blk) bsz[size_t(b)]++;
+      const int64_t bmax = nb ? *std::max_element(bsz.begin(), bsz.end()) : 0;
+      const bool per_sys = S->nlevL > kCtaMinLevels && S->n / std::max(S->nlevL, 1) < kCtaRowsPerLevel && S->n <= kCtaMaxRows;
+      const bool per_blk = S->opts.precond == VSHE_PRECOND_BLOCK_ILU0 && nb >= 2 && bmax <= kTaskMaxRows;
+      if (mode == VSHE_TRSV_PER_SYSTEM) on_task[size_t(k)] = 1;
+      else if (mode == VSHE_TRSV_PER_BLOCK) on_task[size_t(k)] = 2;
+      else if (mode == VSHE_TRSV_AUTO) on_task[size_t(k)] = per_blk ? 2 : per_sys ? 1 : 0;
     }
   }
-  grid_group = int(cta_members.size()) < nsys;
+  std::vector<TaskDev> tasks;
+  std::vector<ChunkDev> chunks;
+  {
+    const int64_t cap = mixed ? vk_task_stage_slots_f32() : vk_task_stage_slots_f64();
+    // chunks of the slices [a, b) of one level: runs of whole slices that fit one stage; a wider
+    // slice is its own chunk, read from global memory
+    auto add_level = [&](const std::vector<int64_t> &off, int64_t a, int64_t b) {
+      if (a >= b) return;
+      for (int64_t j = a; j < b;) {
+        const int64_t sz = off[size_t(j) + 1] - off[size_t(j)];
+        if (sz > cap) { chunks.push_back({int32_t(j), int32_t(j + 1), int32_t(a), kChunkDirect}); ++j; continue; }
+        int64_t e = j, tot = 0;
+        while (e < b && off[size_t(e) + 1] - off[size_t(e)] <= cap && tot + (off[size_t(e) + 1] - off[size_t(e)]) <= cap) {
+          tot += off[size_t(e) + 1] - off[size_t(e)];
+          ++e;
+        }
+        chunks.push_back({int32_t(j), int32_t(e), int32_t(a), 0});
+        j = e;
+      }
+      chunks.back().flags |= kChunkLevelEnd;
+    };
+    std::vector<std::pair<int64_t, TaskDev>> tw;  // (work in slots, task)
+    for (int k = 0; k < nsys; ++k) {
+      if (!on_task[size_t(k)]) continue;
+      const System *S = sys[size_t(k)];
+      auto make = [&](const std::vector<std::pair<int64_t, int64_t>> &lv_l, const std::vector<std::pair<int64_t, int64_t>> &lv_u) {
+        TaskDev t{k, int32_t(chunks.size()), 0, 0, 0, 0};
+        int64_t work = 0;
+        for (auto &r : lv_l) {
+          add_level(S->loff_h, r.first, r.second);
+          work += S->loff_h[size_t(r.second)] - S->loff_h[size_t(r.first)] + 32 * (r.second - r.first);
+        }
+        t.cL1 = int32_t(chunks.size());
+        t.cU0 = int32_t(chunks.size());
+        for (auto &r : lv_u) {
+          add_level(S->uoff_h, r.first, r.second);
+          work += S->uoff_h[size_t(r.second)] - S->uoff_h[size_t(r.first)] + 32 * (r.second - r.first);
+        }
+        t.cU1 = int32_t(chunks.size());
+        if (t.cL1 > t.cL0 || t.cU1 > t.cU0) tw.push_back({work, t});
+      };
+      if (on_task[size_t(k)] == 1) {
+        std::vector<std::pair<int64_t, int64_t>> l, u;
+        for (int32_t v = 0; v < S->nlevL; ++v) l.push_back({S->lvsL[size_t(v)], S->lvsL[size_t(v) + 1]});
+        for (int32_t v = 0; v < S->nlevU; ++v) u.push_back({S->lvsU[size_t(v)], S->lvsU[size_t(v) + 1]});
+        make(l, u);
+      } else {
+        int32_t nb = 0;
+        for (int32_t b : S->blk) nb = std::max(nb, b + 1);
+        std::vector<std::vector<std::pair<int64_t, int64_t>>> l((size_t)nb), u((size_t)nb);
+        for (size_t g = 0; g + 1 < S->lgrp_s0.size(); ++g) l[size_t(S->lgrp_blk[g])].push_back({S->lgrp_s0[g], S->lgrp_s0[g + 1]});
+        for (size_t g = 0; g + 1 < S->ugrp_s0.size(); ++g) u[size_t(S->ugrp_blk[g])].push_back({S->ugrp_s0[g], S->ugrp_s0[g + 1]});
+        for (int32_t b = 0; b < nb; ++b) make(l[size_t(b)], u[size_t(b)]);
+      }
+    }
+    std::stable_sort(tw.begin(), tw.end(), [](const std::pair<int64_t, TaskDev> &a, const std::pair<int64_t, TaskDev> &b) { return a.first > b.first; });
+    for (auto &t : tw) tasks.push_back(t.second);
+    ntasks = int(tasks.size());
+  }
+  grid_group = false;
+  for (int k = 0; k < nsys; ++k) if (!on_task[size_t(k)]) grid_group = true;
+  task_kind.assign(on_task.begin(), on_task.end());
   std::vector<int64_t> cptrL, cptrU, fptr;
   std::vector<int32_t> csL, cqL, csU, cqU, fsys, frow;
   auto slices = [&](bool lower, std::vector<int64_t> &cptr, std::vector<int32_t> &cs, std::vector<int32_t> &cq, int32_t &nl) {
     nl = 0;
     for (int k = 0; k < nsys; ++k)
-      if (!on_cta[size_t(k)]) nl = std::max(nl, lower ? sys[size_t(k)]->nlevL : sys[size_t(k)]->nlevU);
+      if (!on_task[size_t(k)]) nl = std::max(nl, lower ? sys[size_t(k)]->nlevL : sys[size_t(k)]->nlevU);
     cptr.assign(1, 0);
     for (int32_t l = 0; l < nl; ++l) {
       for (int k = 0; k < nsys; ++k) {
-        if (on_cta[size_t(k)]) continue;
+        if (on_task[size_t(k)]) continue;
         const auto &vp = lower ? sys[size_t(k)]->lvsL : sys[size_t(k)]->lvsU;
         if (l + 1 >= int32_t(vp.size())) continue;
         for (int64_t j = vp[size_t(l)]; j < vp[size_t(l) + 1]; ++j) {
@@ -812,11 +932,14 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   if (!ptr) return ctx.cuda_fail(e, "cudaMalloc batch " #ptr);
   ALLOC(d_active, int32_t, nsys);
   ALLOC(d_counters, int32_t, nsys);
-  ALLOC(d_bar, unsigned, 2);
+  ALLOC(d_bar, unsigned, 4);
   ALLOC(d_err, int32_t, 1);
   ALLOC(d_rnorm2, double, nsys);
   ALLOC(d_bnorm2, double, nsys);
-  ALLOC(d_cta_members, int32_t, std::max<size_t>(cta_members.size(), 1));
+  d_tasks = arena.alloc(sizeof(TaskDev) * std::max<size_t>(tasks.size(), 1), e);
+  if (!d_tasks) return ctx.cuda_fail(e, "cudaMalloc tasks");
+  d_chunks = arena.alloc(sizeof(ChunkDev) * std::max<size_t>(chunks.size(), 1), e);
+  if (!d_chunks) return ctx.cuda_fail(e, "cudaMalloc chunks");
   d_sysdev = arena.alloc(vk_sysdev_size() * size_t(nsys), e);
   if (!d_sysdev) return ctx.cuda_fail(e, "cudaMalloc sysdev");
   d_state = arena.alloc(vk_bistate_size() * size_t(nsys), e);
@@ -866,7 +989,8 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   H2D(d_sysdev, sd.data(), sd.size());
   H2D(d_refdev, rd.data(), rd.size());
   H2D(d_factdev, fd.data(), fd.size());
-  if (!cta_members.empty()) { H2D(d_cta_members, cta_members.data(), sizeof(int32_t) * cta_members.size()); }
+  if (!tasks.empty()) { H2D(d_tasks, tasks.data(), sizeof(TaskDev) * tasks.size()); }
+  if (!chunks.empty()) { H2D(d_chunks, chunks.data(), sizeof(ChunkDev) * chunks.size()); }
   if (has_pc) {
     H2D(d_cptrL, cptrL.data(), sizeof(int64_t) * cptrL.size());
     H2D(d_cptrU, cptrU.data(), sizeof(int64_t) * cptrU.size());
@@ -888,6 +1012,8 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   }
 #undef H2D
   if ((e = cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+  bar_limit = 0;
+  if ((rc0 = sync_spin_limit(ctx))) return rc0;
   if ((e = cudaMemsetAsync(d_err, 0, sizeof(int32_t), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   if ((e = cudaMemsetAsync(d_state, 0, vk_bistate_size() * size_t(nsys), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   if (has_pc) {
@@ -1016,6 +1142,8 @@ int Batch::check_err(Ctx &ctx, const char *what) {
 
 int Batch::factor(Ctx &ctx) {
   if (!has_pc) return VSHE_OK;
+  int rs = sync_spin_limit(ctx);
+  if (rs) return rs;
   cudaStream_t s = ctx.stream;
   const int mode = (sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) ? 2 : 1;
   int rc = vk_ilu0(mode, mode == 1 ? ilu_grid : std::max(1, num_sms * 8), d_factdev, &levF, d_bar, d_err, s);
@@ -1118,7 +1246,7 @@ static thread_local EventProf g_prof;
 // resume = false: x = 0, r = b (k_bicg_init); true: r already holds b - A x (k_bicg_resume).
 int Batch::start(Ctx &ctx, double tol, int max_iter, bool resume) {
   cudaStream_t s = ctx.stream;
-  if (sys[0]->opts.trsv_mode < VSHE_TRSV_AUTO || sys[0]->opts.trsv_mode > VSHE_TRSV_FLOW)
+  if (sys[0]->opts.trsv_mode < VSHE_TRSV_AUTO || sys[0]->opts.trsv_mode > VSHE_TRSV_PER_BLOCK)
     return ctx.fail(VSHE_E_INVALID_ARGUMENT, "trsv_mode");
   const size_t bsz = vk_bistate_size();
   std::vector<char> stbuf;
@@ -1159,6 +1287,8 @@ int Batch::write_states(Ctx &ctx, const std::vector<char> &in) {
 // kernel reads its scalars from the device-resident state, so one graph serves every chunk) and
 // replayed; under profiling, or if the driver refuses the capture, it is launched directly.
 int Batch::run_chunk(Ctx &ctx, int every) {
+  int rs = sync_spin_limit(ctx);
+  if (rs) return rs;
   cudaStream_t s = ctx.stream;
   const int mode = (sys[0]->opts.trsv_mode == VSHE_TRSV_PER_LEVEL) ? 2 : trsv_kernel;
   const int lvl_grid = mode != 2 ? trsv_grid : std::max(1, num_sms * 8);
@@ -1167,10 +1297,9 @@ int Batch::run_chunk(Ctx &ctx, int every) {
   auto trsv = [&](int which) -> int {
     if (!has_pc) { vk_precond_copy(ntiles, d_sysdev, d_state, &tiles, d_active, which, s); return 0; }
     int rc = 0;
-    const int ncta = int(cta_members.size());
-    if (ncta) {
-      rc = mixed ? vk_trsv_cta_f32(ncta, d_sysdev, d_state, d_active, d_cta_members, which, s)
-                 : vk_trsv_cta_f64(ncta, d_sysdev, d_state, d_active, d_cta_members, which, s);
+    if (ntasks) {
+      rc = mixed ? vk_trsv_task_f32(ntasks, d_sysdev, d_state, d_active, d_tasks, d_chunks, which, d_bar, d_err, s)
+                 : vk_trsv_task_f64(ntasks, d_sysdev, d_state, d_active, d_tasks, d_chunks, which, d_bar, d_err, s);
       if (rc) return rc;
     }
     if (!grid_group) return 0;
@@ -1360,8 +1489,11 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
     st.levels_L = S->nlevL;
     st.levels_U = S->nlevU;
     st.bytes_device = int64_t(S->arena.total);
-    st.sweep_ctas = (has_pc && grid_group) ? trsv_grid : 0;
-    st.sweep_mode = !(has_pc && grid_group) ? 0
+    const int tk = task_kind.empty() ? 0 : task_kind[size_t(k)];
+    st.sweep_ctas = !has_pc ? 0 : tk ? 0 : trsv_grid;
+    st.sweep_mode = !has_pc ? 0
+                    : tk == 1 ? VSHE_TRSV_PER_SYSTEM
+                    : tk == 2 ? VSHE_TRSV_PER_BLOCK
                     : S->opts.trsv_mode == VSHE_TRSV_PER_LEVEL ? VSHE_TRSV_PER_LEVEL
                     : trsv_kernel == 3 ? VSHE_TRSV_FLOW : VSHE_TRSV_PERSISTENT;
     st.tile_rows = int32_t(S->tile_rows);
@@ -1433,6 +1565,13 @@ size_t vshe_bytes_in_use(vshe_ctx *ctx) {
   for (auto &kv : ctx->systems) t += kv.second->arena.total;
   for (auto &kv : ctx->batches) t += kv.second->arena.total + kv.second->tile_arena.total;
   return t;
+}
+
+int vshe_set_spin_limit(vshe_ctx *ctx, uint64_t polls) {
+  if (!ctx) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->spin_limit = polls ? polls : kDefaultSpinLimit;
+  return VSHE_OK;
 }
 
 int vshe_set_profiling(vshe_ctx *ctx, int32_t on) {

@@ -43,13 +43,15 @@ void vk_update_xr(int ntiles, const void *sys, void *st, const VkTiles *tl, doub
 void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles *tl, const int32_t *act, int which, cudaStream_t s);
 
 // ILU(0) apply in factor precision P (f32 / f64); mode 1 = one persistent cooperative launch,
-// 2 = one launch per level
+// 2 = one launch per level.  bar: 4 words (arrival count, generation, poll limit as uint64) that
+// every bounded device-side wait of the batch reads; k_trsv_task sweeps one task per CTA.
 #define VK_DECL_P(P, SUF)                                                                                               \
   int vk_trsv_##SUF(int mode, int grid, const void *sys, const void *st, const int32_t *act,                          \
                     const VkLevels *lL, const VkLevels *lU, int which, unsigned *bar, int32_t *err, cudaStream_t s);    \
   int vk_trsv_occupancy_##SUF(int *blocks_per_sm);                                                                     \
-  int vk_trsv_cta_##SUF(int ncta, const void *sys, const void *st, const int32_t *act, const int32_t *members, int which, \
-                        cudaStream_t s);                                                                     \
+  int vk_trsv_task_##SUF(int ntasks, const void *sys, const void *st, const int32_t *act, const void *tasks,          \
+                         const void *chunks, int which, const unsigned *bar, int32_t *err, cudaStream_t s);      \
+  int vk_task_stage_slots_##SUF(void);                                                                               \
   void vk_split_factor_##SUF(int64_t nnz, int64_t n, const double *lu, const int64_t *fmap, const int64_t *diag,       \
                              const int64_t *dpos, P *lval, P *uval, P *udinv, cudaStream_t s);
 

@@ -41,7 +41,6 @@ namespace vshe {
 #define VSHE_E_ZERO_PIVOT_DEV (-11)
 
 constexpr int kThreads = 256;
-constexpr int kCtaThreads = 512;  // the per-system sweep: 16 warps, each with the current and the next level's slice in flight
 constexpr int kWarps = kThreads / 32;
 constexpr int kSpmvU = 8;  // SELL entries per lane whose loads are issued together
 constexpr int kDotU = 6;   // the same inside the tile kernels, which also carry reduction state
@@ -384,6 +383,8 @@ __global__ void __launch_bounds__(kThreads) k_precond_copy(const SysK *sys, cons
 // ------------------------------------------------------------ grid barrier
 // Generation barrier for a cooperative launch (all CTAs resident).  The spin is
 // bounded: after `limit` polls the kernel records a timeout and every CTA leaves.
+// bar[0] counts arrivals, bar[1] is the generation, bar[2..3] hold the poll limit (uint64) the
+// host sets (vshe_set_spin_limit) for every wait of the batch's kernels.
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -403,6 +404,10 @@ __device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned *p, unsigned v
 // (ordered before it by the CTA barrier), its acquire half gives the last arriver everyone
 // else's.  The generation is read before arriving, so the release cannot be missed.  A CTA that
 // arrives after another has given up still arrives and leaves through the error check in its spin.
+__device__ __forceinline__ unsigned long long spin_limit_of(const unsigned *bar) {
+  return *((const volatile unsigned long long *)(bar + 2));
+}
+
 __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
   __shared__ int ok;
   __syncthreads();
@@ -415,7 +420,7 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
       st_release_u32(&bar[1], gen + 1u);
     } else {
       unsigned long long spins = 0;
-      const unsigned long long limit = 20000000ull;  // ~ 1-2 s with the backoff below
+      const unsigned long long limit = spin_limit_of(bar);  // default 20 M: ~ 1-2 s with the backoff below
       while (ld_acquire_u32(&bar[1]) == gen) {
         if (++spins > limit) { atomicExch(err, VSHE_E_TIMEOUT_DEV); ok = 0; break; }
         if ((spins & 255) == 0 && *((volatile int32_t *)err) != 0) { ok = 0; break; }  // another CTA gave up
@@ -434,7 +439,6 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *err) {
 // polls that word until the row that produces it has written it.  The value is its own flag
 // (one 8-byte word, written once per launch), so no fence is needed between a value and a flag.
 constexpr unsigned long long kPending = 0x7FF4DEAD7FF4DEADull;
-constexpr unsigned long long kFlowSpinLimit = 4000000ull;  // a few seconds at most; a real wait lasts microseconds
 
 __device__ __forceinline__ double ld_flow(const double *p) {
   unsigned long long v;
@@ -447,13 +451,13 @@ __device__ __forceinline__ void st_flow(double *p, double v) {
 __device__ __forceinline__ bool is_pending(double v) { return (unsigned long long)__double_as_longlong(v) == kPending; }
 
 // Polls *p until it holds a solved value; v is the value already loaded.  Gives up after
-// kFlowSpinLimit polls (error word set to VSHE_E_TIMEOUT) or once another warp has set the
-// error word, returning 0.
-__device__ __noinline__ double wait_flow(const double *p, double v, int32_t *err) {
+// `limit` polls (error word set to VSHE_E_TIMEOUT) or once another warp has set the error word,
+// returning 0.
+__device__ __noinline__ double wait_flow(const double *p, double v, int32_t *err, unsigned long long limit) {
   unsigned long long spins = 0;
   unsigned ns = 32;
   while (is_pending(v)) {
-    if (++spins > kFlowSpinLimit) { atomicExch(err, VSHE_E_TIMEOUT_DEV); return 0.0; }
+    if (++spins > limit) { atomicExch(err, VSHE_E_TIMEOUT_DEV); return 0.0; }
     if ((spins & 255) == 0 && *((volatile int32_t *)err) != 0) return 0.0;
     __nanosleep(ns);  // polls back off so that waiting lanes leave L2 to the working ones
     if (ns < 512) ns <<= 1;
@@ -487,7 +491,8 @@ struct TrsvSlice {
   double base = 0.0, dinv = 1.0;
   int32_t cc[kTrsvU];
   P aa[kTrsvU];
-  int32_t *err = nullptr;  // flow sweeps: the launch's error word
+  int32_t *err = nullptr;  // flow sweeps: the launch's error word and poll limit
+  unsigned long long limit = 0;
 
   __device__ __forceinline__ void load(const SysDev<P> *sys, const BiState *st, const int32_t *active, const Levels &lv, int64_t c,
                                        bool lower, int which) {
@@ -525,7 +530,7 @@ struct TrsvSlice {
         dinv = (double)S.udinv[t0 + lane];
         if constexpr (FLOW) {
           base = ld_flow(&S.ytmp[row]);
-          if (is_pending(base)) base = wait_flow(&S.ytmp[row], base, err);
+          if (is_pending(base)) base = wait_flow(&S.ytmp[row], base, err, limit);
         } else {
           base = CG ? __ldcg(&S.ytmp[row]) : S.ytmp[row];
         }
@@ -550,7 +555,7 @@ struct TrsvSlice {
       for (int u = 0; u < kTrsvU; ++u) xx[u] = u < width ? ld_flow(src + cc[u]) : 0.0;
 #pragma unroll
       for (int u = 0; u < kTrsvU; ++u)
-        if (u < width && is_pending(xx[u])) xx[u] = wait_flow(src + cc[u], xx[u], err);
+        if (u < width && is_pending(xx[u])) xx[u] = wait_flow(src + cc[u], xx[u], err, limit);
     } else {
 #pragma unroll
       for (int u = 0; u < kTrsvU; ++u) xx[u] = u < width ? (CG ? __ldcg(src + cc[u]) : src[cc[u]]) : 0.0;
@@ -565,7 +570,7 @@ struct TrsvSlice {
         const int32_t c = __ldcs(col + e);
         const P a = __ldcs(val + e);
         double x = ld_flow(src + c);
-        if (is_pending(x)) x = wait_flow(src + c, x, err);
+        if (is_pending(x)) x = wait_flow(src + c, x, err, limit);
         sum = fma((double)a, x, sum);
       }
       if (lane < nr) st_flow(dst + row, (base - sum) * dinv);
@@ -620,6 +625,7 @@ __global__ void __launch_bounds__(kThreads, kTrsvCtasPerSm) k_trsv_flow(const Sy
   const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
   const int64_t nL = lL.lvl_ptr[lL.nlev], nU = lU.lvl_ptr[lU.nlev];
   const double pend = __longlong_as_double((long long)kPending);
+  const unsigned long long limit = spin_limit_of(bar);
   for (int64_t g = gw; g < nL + nU; g += nw) {
     const bool lower = g < nL;
     const int64_t c = lower ? g : g - nL;
@@ -641,6 +647,7 @@ __global__ void __launch_bounds__(kThreads, kTrsvCtasPerSm) k_trsv_flow(const Sy
     const bool lower = g < nL;
     TrsvSlice<P, true, true> a;
     a.err = err;
+    a.limit = limit;
     a.load(sys, st, active, lower ? lL : lU, lower ? g : g - nL, lower, which);
     a.finish();
   }
@@ -651,43 +658,197 @@ __global__ void __launch_bounds__(kThreads) k_trsv_level(const SysDev<P> *sys, c
   trsv_level_rows<P>(sys, st, active, lv, k, lower != 0, which);
 }
 
-// One CTA per system: the CTA walks its own system's forward then backward levels, with a
-// CTA barrier between levels instead of a grid barrier.  For systems whose levels are many and
-// short (1D devices: ~1000 levels of ~100-500 rows), where a grid-wide barrier per level costs
-// more than the level's work.  The gathers still read through L2 (__ldcg): with L1-cached loads
-// the 1D diodes converged slower and non-deterministically on B200, i.e. some gathers saw
-// stale lines.
+// ------------------------------------------- per-task sweeps staged through shared memory
+// mbarrier and bulk-copy primitives (PTX ISA 8.x; sm_90 and later).
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for the phase of the given parity to complete; gives up after `limit` polls (the error
+// word is then set to VSHE_E_TIMEOUT) or once the error word is set by another thread.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned long long limit, int32_t *err) {
+  unsigned long long spins = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    if (++spins > limit) { atomicExch(err, VSHE_E_TIMEOUT_DEV); return false; }
+    if ((spins & 63) == 0 && *((volatile int32_t *)err) != 0) return false;
+    if (spins > 16) __nanosleep(64);
+  }
+  return true;
+}
+// Waits for a phase regardless of the error word, at most kDrainPolls polls: copies in flight
+// complete within microseconds, and shared memory must not be released under them.
+constexpr unsigned long long kDrainPolls = 1ull << 24;
+__device__ __forceinline__ void mbar_drain(uint64_t *bar, unsigned parity) {
+  for (unsigned long long spins = 0; !mbar_try_wait(bar, parity) && spins < kDrainPolls; ++spins)
+    if (spins > 16) __nanosleep(64);
+}
+// Bulk copy (the untiled TMA form) of `bytes` from global memory into this CTA's shared memory;
+// completion is counted on the mbarrier.  Source, destination and size are multiples of 16 bytes.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// Barrier of the consumer warps only (named barrier 1; the producer warp does not take part).
+__device__ __forceinline__ void consumers_sync(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
+
+// One slice of a sweep read straight from global memory (a slice wider than a stage).
 template <typename P>
-__global__ void __launch_bounds__(kCtaThreads) k_trsv_cta(const SysDev<P> *sys, const BiState *st, const int32_t *active,
-                                                        const int32_t *members, int which) {
-  const int s = members[blockIdx.x];
+__device__ __noinline__ void trsv_slice_direct(const SysDev<P> &S, int j, bool lower, int which) {
+  TrsvSlice<P, true> a;
+  a.load_slice(S, j, lower, which);
+  a.finish();
+}
+
+constexpr int kTaskConsumers = 16;                          // warps that sum rows
+constexpr int kTaskThreads = 32 * (kTaskConsumers + 1);     // + one warp that issues the bulk copies
+constexpr int kStageBytes = 32768;                          // one chunk: its columns, then its values
+constexpr int kStages = 3;                                  // chunks in flight per CTA
+constexpr int kTaskSmem = kStages * kStageBytes;
+template <typename P>
+__host__ __device__ constexpr int stage_slots() { return (kStageBytes / int(4 + sizeof(P))) & ~31; }
+
+// The incomplete-LU apply of one task (a preconditioner block, or a whole system) on one CTA:
+// out = U^{-1} L^{-1} in over the task's SELL-32 slices, level after level, a CTA barrier
+// between levels instead of a grid barrier.  The factor columns and values of a level do not
+// depend on the sweep, so one producer thread streams them chunk by chunk into a ring of
+// kStages shared-memory stages with bulk copies (chunks of later levels are in flight while
+// the consumer warps work on the current one), and the consumer warps read them from there.
+// Slice j of a level is summed by consumer warp (j - level's first slice) mod kTaskConsumers,
+// one row per lane, in index order with FP64 FMAs: the same arithmetic as k_trsv_persistent,
+// so both give bitwise the same results.  The gathers of solved values (written by other warps
+// of this CTA before the last CTA barrier) read through L2.  Grid = one CTA per task, tasks
+// ordered by decreasing work, so the CTAs that start late take the smallest tasks.  Every wait
+// is bounded (bar[2..3] polls); after a failed wait a consumer stops reading the stages but keeps
+// arriving on the barriers, and the producer stops issuing and drains its copies in flight.
+template <typename P>
+__global__ void __launch_bounds__(kTaskThreads, 2) k_trsv_task(const SysDev<P> *sys, const BiState *st, const int32_t *active,
+                                                                const TaskDev *tasks, const ChunkDev *chunks, int which,
+                                                                const unsigned *bar, int32_t *err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
+  constexpr int CAP = stage_slots<P>();
+  const TaskDev T = tasks[blockIdx.x];
+  const int s = T.sys;
   if (!active[s] || st[s].done || (which == 1 && st[s].s_conv)) return;
   const SysDev<P> &S = sys[s];
-  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  // A level's slice loads (factor entries, the row's own operand) do not depend on the level
-  // before it, so each warp issues them before the barrier that closes the previous level and
-  // only the gathers of solved values wait for it.  Levels wider than one slice per warp
-  // finish their remaining slices after the first.
-  for (int pass = 0; pass < 2; ++pass) {
-    const bool lower = pass == 0;
-    const int nlev = lower ? S.nlevL : S.nlevU;
-    const int64_t *lvs = lower ? S.lvsL : S.lvsU;
-    TrsvSlice<P, true> cur;
-    if (nlev > 0 && lvs[0] + w < lvs[1]) cur.load_slice(S, (int)(lvs[0] + w), lower, which);
-    for (int k = 0; k < nlev; ++k) {
-      const int64_t j0 = lvs[k], j1 = lvs[k + 1];
-      TrsvSlice<P, true> nxt;
-      if (k + 1 < nlev && lvs[k + 1] + w < lvs[k + 2]) nxt.load_slice(S, (int)(lvs[k + 1] + w), lower, which);
-      cur.finish();
-      for (int64_t j = j0 + w + nw; j < j1; j += nw) {
-        TrsvSlice<P, true> extra;
-        extra.load_slice(S, (int)j, lower, which);
-        extra.finish();
-      }
-      __syncthreads();
-      cur = nxt;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kStages; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], kTaskConsumers); }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const int nL = T.cL1 - T.cL0, nch = nL + (T.cU1 - T.cU0);
+  const unsigned long long spin_limit = spin_limit_of(bar);
+
+  if (warp == kTaskConsumers) {
+    // producer: one thread issues the chunks in sweep order, each into the stage its
+    // predecessor kStages chunks back has released
+    if (lane != 0) return;
+    int issued = 0;
+    for (int g = 0; g < nch; ++g) {
+      const bool lower = g < nL;
+      const ChunkDev c = chunks[lower ? T.cL0 + g : T.cU0 + (g - nL)];
+      const int stg = g % kStages, round = g / kStages;
+      if (round > 0 && !mbar_wait(&empty[stg], (round - 1) & 1, spin_limit, err)) break;
+      if (*((volatile int32_t *)err) != 0) break;  // after a failed wait the stages may hold copies in flight
+      const int64_t *off = lower ? S.loff : S.uoff;
+      const int64_t o0 = off[c.s0];
+      const unsigned nslot = (unsigned)(off[c.s1] - o0);
+      if ((c.flags & kChunkDirect) || nslot == 0) { mbar_arrive(&full[stg]); issued = g + 1; continue; }
+      unsigned char *base = smem + stg * kStageBytes;
+      mbar_arrive_expect_tx(&full[stg], nslot * (4u + (unsigned)sizeof(P)));
+      bulk_g2s(base, (lower ? S.lcol : S.ucol) + o0, nslot * 4u, &full[stg]);
+      bulk_g2s(base + CAP * 4, (lower ? S.lval : S.uval) + o0, nslot * (unsigned)sizeof(P), &full[stg]);
+      issued = g + 1;
     }
-    __syncthreads();
+    // leave only once this thread's copies have landed: every chunk before the last kStages
+    // issued had its stage released before the next copy into it, so only these can be in
+    // flight (a fixed bound, independent of the error word and of the caller's poll limit)
+    for (int g = issued > kStages ? issued - kStages : 0; g < issued; ++g) mbar_drain(&full[g % kStages], (g / kStages) & 1);
+    return;
+  }
+
+  // consumers
+  const double *in = which == 0 ? S.p : S.s;
+  double *out = which == 0 ? S.ph : S.sh;
+  double *ytmp = S.ytmp;
+  bool ok = true;
+  for (int g = 0; g < nch; ++g) {
+    const bool lower = g < nL;
+    const ChunkDev c = chunks[lower ? T.cL0 + g : T.cU0 + (g - nL)];
+    const int stg = g % kStages;
+    if (ok && !mbar_wait(&full[stg], (g / kStages) & 1, spin_limit, err)) ok = false;
+    if (ok) {
+      const int64_t *off = lower ? S.loff : S.uoff;
+      const int64_t o0 = off[c.s0];
+      const int32_t *scol = (const int32_t *)(smem + stg * kStageBytes);
+      const P *sval = (const P *)(smem + stg * kStageBytes + CAP * 4);
+      int j = c.s0 + ((warp - (c.s0 - c.lvl_s0) % kTaskConsumers) + kTaskConsumers) % kTaskConsumers;
+      for (; j < c.s1; j += kTaskConsumers) {
+        if (c.flags & kChunkDirect) { trsv_slice_direct<P>(S, j, lower, which); continue; }
+        const int64_t oj = off[j];
+        const int width = (int)((off[j + 1] - oj) >> 5);
+        const double *src;
+        double *dst;
+        int32_t row = 0;
+        int nr;
+        double base = 0.0, dinv = 1.0;
+        if (lower) {
+          const int32_t q0 = S.lrow0[j];
+          nr = S.lrow0[j + 1] - q0;
+          row = q0 + lane;
+          if (lane < nr) base = __ldcs(in + row);
+          src = ytmp; dst = ytmp;
+        } else {
+          const int32_t t0 = S.uslot0[j];
+          nr = S.uslot0[j + 1] - t0;
+          if (lane < nr) {
+            row = __ldcs(S.urow + t0 + lane);
+            dinv = (double)__ldcs(S.udinv + t0 + lane);
+            base = __ldcg(ytmp + row);
+          }
+          src = out; dst = out;
+        }
+        const int32_t *cj = scol + (oj - o0) + lane;
+        const P *vj = sval + (oj - o0) + lane;
+        double sum = 0.0;
+        for (int k = 0; k < width; k += kTrsvU) {
+          int32_t cc[kTrsvU];
+          P aa[kTrsvU];
+          double xx[kTrsvU];
+#pragma unroll
+          for (int u = 0; u < kTrsvU; ++u) {
+            cc[u] = 0; aa[u] = P(0);
+            if (k + u < width) { cc[u] = cj[32 * (k + u)]; aa[u] = vj[32 * (k + u)]; }
+          }
+#pragma unroll
+          for (int u = 0; u < kTrsvU; ++u) xx[u] = k + u < width ? __ldcg(src + cc[u]) : 0.0;
+#pragma unroll
+          for (int u = 0; u < kTrsvU; ++u)
+            if (k + u < width) sum = fma((double)aa[u], xx[u], sum);
+        }
+        if (lane < nr) dst[row] = (base - sum) * dinv;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[stg]);
+    if (c.flags & kChunkLevelEnd) consumers_sync(32 * kTaskConsumers);
   }
 }
 
@@ -994,12 +1155,22 @@ void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles 
 }
 
 #define VK_BODY_P(P, SUF)                                                                                             \
-  int vk_trsv_cta_##SUF(int ncta, const void *sys, const void *st, const int32_t *act, const int32_t *members, int which, \
-                        cudaStream_t s) {                                                                             \
+  int vk_trsv_task_##SUF(int ntasks, const void *sys, const void *st, const int32_t *act, const void *tasks,          \
+                         const void *chunks, int which, const unsigned *bar, int32_t *err, cudaStream_t s) {      \
+    static bool attr = false;                                                                                        \
+    if (!attr) {                                                                                                     \
+      cudaError_t e = cudaFuncSetAttribute((const void *)k_trsv_task<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                           kTaskSmem);                                                               \
+      if (e != cudaSuccess) return (int)e;                                                                           \
+      attr = true;                                                                                                   \
+    }                                                                                                                \
     g_launches += 1;                                                                                                 \
-    k_trsv_cta<P><<<ncta, kCtaThreads, 0, s>>>((const SysDev<P> *)sys, (const BiState *)st, act, members, which);    \
+    k_trsv_task<P><<<ntasks, kTaskThreads, kTaskSmem, s>>>((const SysDev<P> *)sys, (const BiState *)st, act,         \
+                                                           (const TaskDev *)tasks, (const ChunkDev *)chunks, which,   \
+                                                           bar, err);                                                 \
     return (int)cudaGetLastError();                                                                                  \
   }                                                                                                                  \
+  int vk_task_stage_slots_##SUF(void) { return stage_slots<P>(); }                                                  \
   int vk_trsv_##SUF(int mode, int grid, const void *sys, const void *st, const int32_t *act, const VkLevels *lL,     \
                     const VkLevels *lU, int which, unsigned *bar, int32_t *err, cudaStream_t s) {                    \
     return launch_trsv_t<P>(mode, grid, (const SysDev<P> *)sys, (const BiState *)st, act, *(const Levels *)lL,       \

@@ -4,7 +4,7 @@
 // Solver order.  Every system is solved in its own row order q = 0..n-1, a symmetric
 // permutation of the caller's rows (perm[q] = caller row): the preconditioner's base
 // ordering (natural, multicolour or caller-given), then stably sorted by the level of the
-// forward (L) sweep, then, inside a level, by row length.  Rows of one forward level are
+// forward (L) sweep, then, inside a level, by preconditioner block and by row length.  Rows of one forward level are
 // therefore contiguous, and because a level never holds two structurally coupled rows, the
 // ILU(0) factors in solver order are those of the base ordering, relabelled.  The Krylov
 // vectors live in solver order; b is gathered in and x scattered out once per solve.
@@ -38,7 +38,7 @@ struct SysDev {
   const int32_t *lrow0; const int64_t *loff; const int32_t *lcol; const P *lval;
   const int32_t *uslot0; const int64_t *uoff; const int32_t *ucol; const P *uval; const P *udinv; const int32_t *urow;
   double *ytmp;      // forward-sweep result (FP64)
-  // level -> slice ranges of this system alone (the per-system sweep of k_trsv_cta)
+  // level -> slice ranges of this system alone
   const int64_t *lvsL; const int64_t *lvsU; int32_t nlevL, nlevU;
   // Krylov vectors (solver order, FP64)
   double *x, *r, *rh, *p, *v, *s, *t, *ph, *sh;
@@ -94,6 +94,23 @@ struct FactDev {
   // the pkeep largest entries of the row's L part and of its U part are kept
   int32_t ilut, pkeep;
   double tau;
+};
+
+// Sweep tasks.  A task is one independent unit of the incomplete-LU apply that one CTA walks
+// alone: a preconditioner block of one system (an energy slab of block-ILU: its factor has no
+// entry outside the block, so blocks sweep independently), or a whole system.  Its forward
+// (L) and backward (U) sweeps are lists of chunks [cL0, cL1) and [cU0, cU1): a chunk is a run of
+// consecutive SELL slices [s0, s1) of one level (lvl_s0 = the level's first slice in the task)
+// whose factor slots fit one shared-memory stage and are staged there by bulk copies, or one
+// slice wider than a stage (kChunkDirect: read from global memory).  kChunkLevelEnd marks the
+// last chunk of a level: the CTA synchronises before the next level.
+constexpr int32_t kChunkLevelEnd = 1;
+constexpr int32_t kChunkDirect = 2;
+struct TaskDev {
+  int32_t sys, cL0, cL1, cU0, cU1, pad;
+};
+struct ChunkDev {
+  int32_t s0, s1, lvl_s0, flags;
 };
 
 // FP64 residual view of one system (solver order): r = b - A x.

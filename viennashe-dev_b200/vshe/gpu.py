@@ -17,12 +17,12 @@ VSHE_OK = 0
 ERRORS = {
     -1: "INVALID_ARGUMENT", -2: "EMPTY_ROW", -3: "NAN", -4: "ODD_DIAGONAL", -5: "BREAKDOWN",
     -6: "NOT_CONVERGED", -7: "OUT_OF_MEMORY", -8: "BUDGET", -9: "CUDA", -10: "TIMEOUT",
-    -11: "ZERO_PIVOT", -12: "NOT_FOUND", -13: "UNSUPPORTED",
+    -11: "ZERO_PIVOT", -12: "NOT_FOUND", -13: "UNSUPPORTED", -14: "CAPACITY",
 }
 PRECISION = {"fp64": 0, "mixed": 1}
 PRECOND = {"none": 0, "ilu0": 1, "block_ilu0": 2, "ilut": 3}
 ORDERING = {"natural": 0, "multicolor": 1}
-TRSV = {"auto": 0, "persistent": 1, "per_level": 2, "per_system": 3, "flow": 4}
+TRSV = {"auto": 0, "persistent": 1, "per_level": 2, "per_system": 3, "flow": 4, "per_block": 5}
 
 _lib = None
 
@@ -63,6 +63,7 @@ def lib():
         L.vshe_system_factor_values.argtypes = [vp, C.c_int64, f64p]
         L.vshe_system_time_spmv.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, f64p]
         L.vshe_set_profiling.argtypes = [vp, C.c_int32]
+        L.vshe_set_spin_limit.argtypes = [vp, C.c_uint64]
         L.vshe_get_profile.argtypes = [vp, f64p, i64p]
         L.vshe_kernel_launches.restype = C.c_int64
         L.vshe_kernel_launches.argtypes = []
@@ -176,6 +177,10 @@ class Context:
 
     def set_profiling(self, on=True):
         self._check(lib().vshe_set_profiling(self.h, 1 if on else 0))
+
+    def set_spin_limit(self, polls=0):
+        """Polls of every bounded device-side wait before VSHE_E_TIMEOUT (0: the default)."""
+        self._check(lib().vshe_set_spin_limit(self.h, int(polls)))
 
     def profile(self):
         """Device ms of the last solve per kernel class and launch counts."""
