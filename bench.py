@@ -16,11 +16,11 @@ description resident in HBM; `fp64_solves_per_s` is the same pass with the plain
 download of x) with host buffers, the way a ViennaSHE Gummel loop calls solvers::solve for a
 matrix of unchanged pattern.
 
-`--impl reference` times the CPU restatement of the reference's serial solver (ILU(0) +
-BiCGStab with r^ = r_0, FP64, one thread, natural order: serial_linear_solver's algorithm) on
-the same reduced system: the factorisation plus a bounded number of iterations are timed on
-the host, and the iteration count to 1e-10 of that same algorithm is counted on the device
-(untimed).
+`--impl reference` runs the reference's path on the host only (no GPU library is loaded): the
+oracle builds the same reduced system (setup, assembly, odd elimination, scaling and
+normalisation, untimed), then one complete solve by the reference's serial solver algorithm
+(natural-order ILU(0) + BiCGStab with r^ = r_0, FP64: serial_linear_solver's) on all host
+threads to 1e-10 is timed, its iterations counted on the CPU.
 
 Multi-GPU: replicas only (independent solves, no collective); launched with torchrun, every
 rank solves its own replica on its GPU, value = all ranks' solves / max-over-ranks time.
@@ -42,7 +42,8 @@ sys.path.insert(0, os.path.join(ROOT, "viennashe-dev_b200"))
 METRIC = "solves/s & p99 latency at 1e-10 resid (mixed vs plain FP64 GPU); SpMV GB/s"
 UNIT = "solves/s"
 TOL = 1e-10
-SWEEP_NAMES = {1: "grid barrier per level (k_trsv_persistent)", 2: "one launch per level", 4: "barrier-free flow (k_trsv_flow)"}
+SWEEP_NAMES = {1: "grid barrier per level (k_trsv_persistent)", 2: "one launch per level", 3: "one CTA per system (k_trsv_task)",
+               4: "barrier-free flow (k_trsv_flow)", 5: "one CTA per energy slab (k_trsv_task)"}
 
 
 def parse():
@@ -57,7 +58,6 @@ def parse():
     ap.add_argument("--ny", type=int, default=50)
     ap.add_argument("--ne", type=int, default=160)
     ap.add_argument("--L", type=int, default=3)
-    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="host time of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-serving", action="store_true", help="skip the batched-sweep and served-stream measurements")
@@ -207,99 +207,87 @@ def build_problem(args, ctx, precision):
 
 
 # -------------------------------------------------------------- CPU baseline
-def reference_iterations(ctx, rp, ci, v, b):
-    """Iterations the reference's serial algorithm (natural-order ILU(0), BiCGStab with
-    r^ = r_0, FP64) needs for 1e-10 on this system, counted on the device (not timed)."""
-    S = ctx.system(rp, ci, v, b, precision="fp64", precond="ilu0", ordering="natural", shadow="r0",
-                   tol=TOL, max_iters=20000, check_every=32)
-    try:
-        _, st = S.solve(want_x=False)
-    finally:
-        S.free()
-    return st
-
-
-def cpu_sample(rp, ci, v, b, iters_ref, budget_s):
-    """The oracle's serial ILU(0) factorisation and BiCGStab iterations (r^ = r_0, the
-    reference's serial_linear_solver algorithm) timed on one host core; solves/s =
-    1 / (t_factor + iters_ref * t_iteration)."""
+def cpu_solve(rp, ci, v, b, threads=0):
+    """One complete solve by the reference's serial solver algorithm (natural-order ILU(0) +
+    BiCGStab with r^ = r_0, FP64; serial_linear_solver.hpp:112-136) on `threads` host threads
+    (0: all), to 1e-10 from x0 = 0, iterations counted on the CPU (oracle/serial_solver_mt.cpp:
+    level-scheduled, every row's arithmetic as in the serial oracle)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_api as O
     A = O.CSR(rp, ci, v)
-    probe = O.bench_serial(A, b, 2)
-    t_iter = max(probe["t_per_iter"], 1e-6)
-    iters = int(max(3, min(500, (budget_s - probe["t_factor"]) / t_iter)))
-    r = O.bench_serial(A, b, iters)
-    t_solve = r["t_factor"] + iters_ref * r["t_per_iter"]
+    t0 = time.perf_counter()
+    x, st = O.serial_solve_mt(A, b, tol=TOL, maxit=20000, threads=threads, trace=True)
+    st["wall_s"] = time.perf_counter() - t0
+    st["x"] = x
+    return st
+
+
+def cpu_baseline_line(st, n, nnz, source):
     return {
-        "value": 1.0 / t_solve, "unit": UNIT, "cores": 1, "kind": "port",
-        "sample": ("oracle serial ILU(0) + BiCGStab (r^ = r_0, FP64, natural order) on the full reduced "
-                   "system (n=%d, nnz=%d), one host core: factorisation %.2f s and %d iterations timed "
-                   "(%.3f s/iteration); %d iterations to 1e-10 counted on the device for the same "
-                   "algorithm; assembly/elimination on the CPU not included"
-                   % (A.n, A.nnz, r["t_factor"], r["iters"], r["t_per_iter"], iters_ref)),
-        "t_factor_s": r["t_factor"], "t_per_iter_s": r["t_per_iter"], "iterations": iters_ref,
+        "value": 1.0 / st["wall_s"], "unit": UNIT, "cores": st["threads"], "kind": "port",
+        "sample": ("one complete solve of the full reduced system (n=%d, nnz=%d, %s) by the oracle's restatement of "
+                   "the reference's serial_linear_solver (natural-order ILU(0) + BiCGStab, r^ = r_0, FP64) on %d host "
+                   "threads (level-scheduled triangular solves, each row's arithmetic as in the serial solver): "
+                   "factorisation %.2f s + %d iterations %.2f s to a relative residual of %.2e (rc %d)"
+                   % (n, nnz, source, st["threads"], st["t_factor"], st["iters"], st["t_iter"], st["relres"], st["rc"])),
+        "iterations": st["iters"], "t_factor_s": st["t_factor"], "t_iterations_s": st["t_iter"], "rel_residual": st["relres"],
     }
 
 
-def _cpu_worker(path, iters_ref, budget_s):
-    """One host process of the reference arm: loads the reduced system and times the serial
-    solver on it (spawned, so it holds no CUDA state)."""
-    d = np.load(path)
-    return cpu_sample(d["rp"], d["ci"], d["v"], d["b"], iters_ref, budget_s)
-
-
-def host_workers():
-    """Host processes the reference arm runs concurrently: one per core, as far as host memory
-    allows about 4 GB per process (the 2D bar's reduced system and its factor)."""
-    cores = os.cpu_count() or 1
-    try:
-        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
-    except (ValueError, OSError):
-        avail = 16 << 30
-    return max(1, min(cores, int(avail // (4 << 30))))
+def config_dict(args, info):
+    """The workload as both arms report it (same keys and values)."""
+    return {"workload": workload_name(args), "n_unknowns_reduced": int(info["n_even"]), "nnz_reduced": int(info["nnz_reduced"]),
+            "n_unknowns_full": int(info["n_even"] + info["n_odd"]), "nnz_full": int(info["nnz_full"]),
+            "n_energies": int(info["n_energies"]),
+            "l2": "inputs larger than L2 (reduced system %.2f GB)" % (int(info["nnz_reduced"]) * 12 / 1e9),
+            "parallelism": "replicas" if args.gpus > 1 else "single"}
 
 
 def run_reference(args, D_):
+    """Reference arm: the reduced system built on the host by the oracle (the reference's
+    setup, assembly, odd elimination, scaling and normalisation, single thread, untimed), then
+    the timed region: one complete solve by the reference's serial solver algorithm on all host
+    threads, to 1e-10, iterations counted on the CPU.  The K steps are the solve's iterations in
+    K consecutive runs of equal length (the first also holds the factorisation), so
+    ms_per_step * steps is the solve's wall time.  Loads no GPU library."""
     if D_.rank != 0:
         return
-    from vshe import gpu
-    ctx = gpu.Context(D_.local)
-    P = build_problem(args, ctx, "fp64")
-    P.assemble(3)
-    rp, ci, v, b = P.export("reduced")   # input preparation (not timed)
-    P.free()
-    st = reference_iterations(ctx, rp, ci, v, b)
-    ctx.close()
-    # The reference's serial solver is single-threaded; with all the host's cores it serves as
-    # many solves at once, one per process, so the host's rate is the sum over the processes.
-    import multiprocessing as mp
-    workers = host_workers()
-    tmpd = tempfile.mkdtemp()
-    path = os.path.join(tmpd, "reduced.npz")
-    np.savez(path, rp=rp, ci=ci, v=v, b=b)
-    per_step = max(args.cpu_seconds / max(1, args.warmup + args.steps), 3.0)
-    vals, samples = [], []
-    try:
-        with mp.get_context("spawn").Pool(workers) as pool:
-            for k in range(args.warmup + args.steps):
-                res = pool.starmap(_cpu_worker, [(path, st["iterations"], per_step)] * workers)
-                if k >= args.warmup:
-                    vals.append(sum(r["value"] for r in res))
-                    samples.append(res[0]["sample"])
-    finally:
-        os.unlink(path)
-        os.rmdir(tmpd)
-    val = statistics.median(vals)
-    sample = ("%d concurrent host processes (one per core, as host memory allows), each: %s" % (workers, samples[-1]))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_api as O
+    from vshe import devices as D
+    if args.workload == "mosfet":
+        dev, cfg = D.config5(nx=240 // args.mos_shrink, ny=80 // args.mos_shrink)
+    else:
+        dev, cfg = D.config2(nx=args.nx, ny=args.ny, n_energies=args.ne, L=args.L)
+    t0 = time.perf_counter()
+    P = O.OracleProblem(dev, cfg, O.golden_coupling(cfg.max_expansion_order))
+    info = dict(n_even=P.n_even, n_odd=P.n_odd, nnz_full=P.nnz[0], nnz_reduced=P.nnz[3], n_energies=P.NH)
+    A = P.matrix(3)
+    del P
+    t_build = time.perf_counter() - t0
+    # warm-up: factorisation and `warmup` iterations (pages of the system and the factor touched)
+    O.serial_solve_mt(A, A.rhs, tol=0.0, maxit=max(1, args.warmup), threads=0)
+    st = cpu_solve(A.rp, A.ci, A.v, A.rhs)
+    total_s = st["wall_s"]
+    it_s = st["iter_s"]
+    k = max(1, args.steps)
+    bounds = [int(round(st["iters"] * j / k)) for j in range(k + 1)]
+    step_ms = [1000.0 * ((st["t_factor"] if j == 0 else 0.0) + it_s[bounds[j + 1]] - it_s[bounds[j]]) for j in range(k)]
+    res = float(np.linalg.norm(O.spmv(A, st["x"]) - A.rhs) / np.linalg.norm(A.rhs))
+    value = 1.0 / total_s
+    cb = cpu_baseline_line(st, A.n, A.nnz, "built by the oracle on the host")
     line = {
-        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / val,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / k,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args), "n_unknowns": int(len(b)), "nnz": int(len(v))},
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
-        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "reference_solve": {"iterations": st["iterations"], "rel_residual": st["rel_residual"]},
+        "config": config_dict(args, info),
+        "cpu_baseline": dict(cb, value=value),
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_solve": {"iterations": st["iters"], "rc": st["rc"], "recursive_rel_residual": st["relres"],
+                            "true_rel_residual": res, "threads": st["threads"], "wall_s": total_s,
+                            "step_ms": step_ms, "host_build_s": t_build,
+                            "timed_region": "one complete solve (factorisation + BiCGStab to 1e-10); steps = "
+                                            "consecutive runs of equal iteration count"},
     }
     print(json.dumps(line), flush=True)
 
@@ -474,9 +462,12 @@ def run_ours(args, D_):
     if dominant == "trsv":
         avg_ms = prof["trsv_ms"] / max(prof["trsv_launches"], 1)
         dbytes = trsv_bytes
-        kname = ("k_trsv_flow<float> (incomplete-LU apply, barrier-free forward then backward SELL-32 sweeps)"
-                 if st.get("sweep_mode") == 4 else
-                 "k_trsv_persistent<float> (incomplete-LU apply, forward then backward SELL-32 sweeps)")
+        kname = {4: "k_trsv_flow<float> (incomplete-LU apply, barrier-free forward then backward SELL-32 sweeps)",
+                 5: "k_trsv_task<float> (incomplete-LU apply, one CTA per energy slab, factor slices staged through "
+                    "shared memory by bulk copies, forward then backward SELL-32 sweeps)",
+                 3: "k_trsv_task<float> (incomplete-LU apply, one CTA per system, factor slices staged through shared "
+                    "memory by bulk copies)"}.get(
+            st.get("sweep_mode"), "k_trsv_persistent<float> (incomplete-LU apply, forward then backward SELL-32 sweeps)")
     else:
         avg_ms = prof["spmv_ms"] / max(prof["spmv_launches"], 1)
         dbytes = spmv_bytes
@@ -503,24 +494,21 @@ def run_ours(args, D_):
     except Exception:
         pass
     cpu = None
-    if D_.rank == 0 and not args.no_cpu:
-        st_ref = reference_iterations(ctx, rp, ci, v, b)
-        cpu = cpu_sample(rp, ci, v, b, st_ref["iterations"], args.cpu_seconds)
+    if D_.rank == 0 and D_.world == 1 and not args.no_cpu:
+        cst = cpu_solve(rp, ci, v, b)
+        cpu = cpu_baseline_line(cst, n, nnz, "exported from the device pass; bit-identical in pattern, 1e-12 in values to the oracle's")
     if D_.rank == 0:
         lat = np.asarray(ms, float)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D_.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * tmax / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 Krylov / f32-stored ILU factors", "data": "synthetic",
-            "config": {"workload": workload_name(args), "n_unknowns_reduced": n, "nnz_reduced": nnz, "nnz_factor": nnz_lu,
-                       "n_unknowns_full": int(info["n_even"] + info["n_odd"]), "nnz_full": int(info["nnz_full"]),
-                       "n_energies": int(info["n_energies"]),
-                       "preconditioner": ("block-ILU(%d) per energy slab, node %s colouring" % (args.fill_level, "distance-2" if args.fill_level else "4-colour")
-                                          if args.workload == "bar"
-                                          else "ILUT(%d, %g), natural order" % (args.ilut_entries, args.ilut_drop)
-                                          if args.mos_precond == "ilut" else "block-ILU(0) per energy slab, node 4-colour colouring"),
-                       "l2": "inputs larger than L2 (reduced system %.2f GB)" % (nnz * 12 / 1e9),
-                       "parallelism": "replicas" if D_.world > 1 else "single"},
+            "config": config_dict(args, info),
+            "preconditioner": ("block-ILU(%d) per energy slab, node %s colouring" % (args.fill_level, "distance-2" if args.fill_level else "4-colour")
+                               if args.workload == "bar"
+                               else "ILUT(%d, %g), natural order" % (args.ilut_entries, args.ilut_drop)
+                               if args.mos_precond == "ilut" else "block-ILU(0) per energy slab, node 4-colour colouring"),
+            "nnz_factor": nnz_lu,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "fp64_solves_per_s": fp64_value, "mixed_over_fp64": (value / max(D_.world, 1)) / fp64_value if fp64_value else None,
             "fp64": {"iterations": st64["iterations"], "rel_residual": st64["rel_residual"], "ms": [float(x) for x in ms64]},

@@ -16,6 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "_build", "libvshe_oracle.so")
+LIB_MT = os.path.join(HERE, "_build", "libvshe_oracle_mt.so")
 sys.path.insert(0, os.path.join(ROOT, "viennashe-dev_b200"))
 from vshe.abi import DeviceDesc, she_config_c, Coupling, ptr  # noqa: E402
 
@@ -24,6 +25,7 @@ i64p = C.POINTER(C.c_int64)
 f64p = C.POINTER(C.c_double)
 
 _lib = None
+_lib_mt = None
 
 
 def build():
@@ -274,6 +276,38 @@ def bench_serial(A: CSR, b, iters):
     done = lib().vsheo_bench_serial(A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double),
                                     ptr(b, C.c_double), iters, ptr(tf, C.c_double), ptr(ti, C.c_double), ptr(rr, C.c_double))
     return dict(iters=int(done), t_factor=float(tf[0]), t_per_iter=float(ti[0]), relres=float(rr[0]))
+
+
+def lib_mt():
+    global _lib_mt
+    if _lib_mt is None:
+        if not os.path.exists(LIB_MT):
+            build()
+        L = C.CDLL(LIB_MT)
+        L.vsheo_serial_solve_mt.argtypes = [C.c_int64, i64p, i32p, f64p, f64p, f64p, C.c_double, C.c_int32, C.c_int32, f64p, f64p]
+        L.vsheo_serial_solve_mt.restype = C.c_int
+        _lib_mt = L
+    return _lib_mt
+
+
+def serial_solve_mt(A: CSR, b, tol=1e-10, maxit=20000, threads=0, trace=False):
+    """The reference's serial solver (natural-order ILU(0) + BiCGStab with r^ = r_0) on `threads`
+    host threads (0: all), from x0 = 0 (serial_solver_mt.cpp).  Returns x and a dict with rc (0
+    converged, 1 iteration limit, -1 breakdown, -2 a row without diagonal), iterations, the
+    recursive relative residual, the factorisation and iteration seconds, the threads used and
+    (trace=True) the elapsed seconds after every iteration."""
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(A.n)
+    out = np.zeros(5)
+    it_s = np.zeros(maxit + 1) if trace else None
+    rc = lib_mt().vsheo_serial_solve_mt(A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double),
+                                        ptr(b, C.c_double), ptr(x, C.c_double), float(tol), int(maxit), int(threads),
+                                        ptr(out, C.c_double), None if it_s is None else ptr(it_s, C.c_double))
+    d = dict(rc=int(rc), iters=int(out[0]), relres=float(out[1]), t_factor=float(out[2]), t_iter=float(out[3]),
+             threads=int(out[4]))
+    if trace:
+        d["iter_s"] = it_s[:d["iters"] + 1]
+    return x, d
 
 
 def golden_coupling(L):
