@@ -130,7 +130,7 @@ int vshe_create(vshe_ctx **ctx, int device, size_t hbm_budget_bytes);
 int vshe_destroy(vshe_ctx *ctx);
 const char *vshe_errstr(int code);
 const char *vshe_last_error(vshe_ctx *ctx);
-/* Bytes of device memory currently held by the context's systems. */
+/* Bytes of device memory currently held by the context's systems and SHE problems. */
 size_t vshe_bytes_in_use(vshe_ctx *ctx);
 /* Per-kernel-class device timing (CUDA events around every launch of the next
  * solves; off by default).  vshe_get_profile returns, for the last solve, ms spent
@@ -158,10 +158,15 @@ int64_t vshe_kernel_launches(void);
  * FP64 values), rhs and x are host arrays of length n.  Checks, in the
  * reference's order (src/solvers/solve.hpp:54-66): empty rows -> VSHE_E_EMPTY_ROW,
  * non-finite rhs -> VSHE_E_NAN, ||rhs|| == 0 -> x = 0.  Host buffers are copied
- * in and out inside the call. */
+ * in and out inside the call.  The context keeps the system of the last call resident (its
+ * solver order, schedules and device buffers; counted in vshe_bytes_in_use): a following call
+ * with the same row offsets, columns and options (a Gummel loop's next step) uploads only the
+ * values and rhs.  Not kept for VSHE_PRECOND_ILUT, whose pattern depends on the values.
+ * vshe_solve_csr_release frees the kept system (vshe_destroy does too). */
 int vshe_solve_csr(vshe_ctx *ctx, int64_t n, int64_t nnz, const int64_t *row_ptr, const int32_t *col,
                    const double *val, const double *rhs, const vshe_solve_opts *opts, double *x,
                    vshe_solve_stats *stats);
+int vshe_solve_csr_release(vshe_ctx *ctx);
 
 /* ---- resident systems: upload once, refactor/solve many times ----
  * vshe_system_create copies the CSR (host) to the device and builds the
@@ -289,6 +294,10 @@ int vshe_she_results(vshe_ctx *ctx, int64_t handle, double *x_full, double *dens
 int vshe_she_export(vshe_ctx *ctx, int64_t handle, int32_t which, int64_t *row_ptr, int32_t *col, double *val, double *rhs);
 /* Unknown scaling s and column scale factors of the reduced system (length n_even). */
 int vshe_she_scaling(vshe_ctx *ctx, int64_t handle, double *scaling, double *scale_factors);
+/* Energy-slab row blocks of the reduced system (n_energies + 1 row offsets; slab H = rows
+ * [block_ptr[H], block_ptr[H+1]), empty for the end slabs): what fill_block_indices
+ * (viennashe/she/linear_solver.hpp:44-83) puts into linear_solver_config::block_preconditioner_boundaries(). */
+int vshe_she_blocks(vshe_ctx *ctx, int64_t handle, int64_t *block_ptr);
 int vshe_she_free(vshe_ctx *ctx, int64_t handle);
 
 /* ---- served stream: continuous batching of SHE solves ----

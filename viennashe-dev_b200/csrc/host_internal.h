@@ -196,6 +196,12 @@ struct Ctx {
   // with VSHE_E_TIMEOUT
   unsigned long long spin_limit = kDefaultSpinLimit;
   std::map<int64_t, std::unique_ptr<System>> systems;
+  // vshe_solve_csr's pattern cache: the system of its last call (0 = none) and the options it was
+  // created with (with copies of the option arrays)
+  int64_t csr_cache = 0;
+  vshe_solve_opts csr_cache_opts{};
+  std::vector<int64_t> csr_cache_blocks;
+  std::vector<int32_t> csr_cache_perm;
   std::map<std::vector<int64_t>, std::unique_ptr<Batch>> batches;
   // kernel-class timings of the last profiled solve (ms): spmv, trsv, vector, reliable, factor
   double prof[5] = {0, 0, 0, 0, 0};
@@ -211,6 +217,8 @@ struct Ctx {
 
 // releases the SHE problems of a context (she_pipeline.cpp)
 void she_release_all(Ctx *ctx);
+// device memory held by the context's SHE problems (she_pipeline.cpp)
+size_t she_bytes(Ctx *ctx);
 
 }  // namespace vshe
 

@@ -1564,7 +1564,7 @@ size_t vshe_bytes_in_use(vshe_ctx *ctx) {
   size_t t = 0;
   for (auto &kv : ctx->systems) t += kv.second->arena.total;
   for (auto &kv : ctx->batches) t += kv.second->arena.total + kv.second->tile_arena.total;
-  return t;
+  return t + vshe::she_bytes(ctx);
 }
 
 int vshe_set_spin_limit(vshe_ctx *ctx, uint64_t polls) {
@@ -1712,15 +1712,74 @@ int vshe_system_free(vshe_ctx *ctx, int64_t h) {
   return VSHE_OK;
 }
 
+// Pattern cache of vshe_solve_csr: the system of the last call stays resident with its solver
+// order, schedules and tuned launch shapes; a call whose pattern (row offsets and columns,
+// compared entry by entry) and options equal it uploads only values and rhs.  ILUT systems are
+// not kept (their factor pattern comes from the values at creation).
+static bool same_solve_opts(const vshe_solve_opts &a, const vshe_solve_opts &b) {
+  return a.precision == b.precision && a.precond == b.precond && a.ordering == b.ordering && a.tol == b.tol &&
+         a.max_iters == b.max_iters && a.n_blocks == b.n_blocks && a.trsv_mode == b.trsv_mode && a.check_every == b.check_every &&
+         a.shadow == b.shadow && a.fill_level == b.fill_level && a.ilut_entries == b.ilut_entries && a.ilut_drop == b.ilut_drop;
+}
+
 int vshe_solve_csr(vshe_ctx *ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *v,
                    const double *rhs, const vshe_solve_opts *opts, double *x, vshe_solve_stats *stats) {
-  if (!ctx || !x || !rhs) return VSHE_E_INVALID_ARGUMENT;
+  if (!ctx || !x || !rhs || !rp || !ci || !v || n <= 0 || nnz <= 0) return VSHE_E_INVALID_ARGUMENT;
+  vshe_solve_opts o;
+  if (opts) o = *opts; else vshe_default_opts(&o);
+  const bool keep = o.precond != VSHE_PRECOND_ILUT;
+  const bool has_blocks = o.n_blocks > 0 && o.block_ptr;
+  bool hit = false;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->systems.find(ctx->csr_cache);
+    if (keep && it != ctx->systems.end()) {
+      const System *S = it->second.get();
+      const bool blocks_same = has_blocks ? (ctx->csr_cache_blocks.size() == size_t(o.n_blocks) + 1 &&
+                                             std::equal(ctx->csr_cache_blocks.begin(), ctx->csr_cache_blocks.end(), o.block_ptr))
+                                          : ctx->csr_cache_blocks.empty();
+      const bool perm_same = o.perm ? (ctx->csr_cache_perm.size() == size_t(n) && std::equal(ctx->csr_cache_perm.begin(), ctx->csr_cache_perm.end(), o.perm))
+                                    : ctx->csr_cache_perm.empty();
+      hit = S->n == n && S->nnz == nnz && same_solve_opts(ctx->csr_cache_opts, o) && blocks_same && perm_same &&
+            std::memcmp(S->rp.data(), rp, sizeof(int64_t) * size_t(n + 1)) == 0 &&
+            std::memcmp(S->ci.data(), ci, sizeof(int32_t) * size_t(nnz)) == 0;
+    }
+  }
+  int rc;
+  if (hit) {
+    rc = vshe_system_set_values(ctx, ctx->csr_cache, v, rhs);
+    if (rc) return rc;
+    return vshe_system_solve(ctx, ctx->csr_cache, x, stats);
+  }
+  if (ctx->csr_cache) {
+    vshe_system_free(ctx, ctx->csr_cache);
+    ctx->csr_cache = 0;
+  }
   int64_t h = 0;
-  int rc = vshe_system_create(ctx, n, nnz, rp, ci, v, rhs, opts, &h);
+  rc = vshe_system_create(ctx, n, nnz, rp, ci, v, rhs, &o, &h);
   if (rc) return rc;
   rc = vshe_system_solve(ctx, h, x, stats);
-  vshe_system_free(ctx, h);
+  if (!keep) {
+    vshe_system_free(ctx, h);
+    return rc;
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->csr_cache = h;
+  ctx->csr_cache_opts = o;
+  ctx->csr_cache_opts.block_ptr = nullptr;
+  ctx->csr_cache_opts.perm = nullptr;
+  if (has_blocks) ctx->csr_cache_blocks.assign(o.block_ptr, o.block_ptr + o.n_blocks + 1);
+  else ctx->csr_cache_blocks.clear();
+  if (o.perm) ctx->csr_cache_perm.assign(o.perm, o.perm + n);
+  else ctx->csr_cache_perm.clear();
   return rc;
+}
+
+int vshe_solve_csr_release(vshe_ctx *ctx) {
+  if (!ctx) return VSHE_E_INVALID_ARGUMENT;
+  if (ctx->csr_cache) vshe_system_free(ctx, ctx->csr_cache);
+  ctx->csr_cache = 0;
+  return VSHE_OK;
 }
 
 int vshe_system_spmv(vshe_ctx *ctx, int64_t h, int32_t precision, const double *x, double *y) {

@@ -339,6 +339,22 @@ static std::map<vshe::Ctx *, std::map<int64_t, std::unique_ptr<SheProblem>>> g_s
 static std::map<vshe::Ctx *, std::map<std::vector<int64_t>, std::unique_ptr<Batch>>> g_she_batches;
 static std::mutex g_she_mu;
 
+static size_t problem_bytes(const SheProblem *S) {
+  size_t b = S->arena.total;
+  if (S->sys) b += S->sys->arena.total;
+  if (S->batch) b += S->batch->arena.total + S->batch->tile_arena.total;
+  return b;
+}
+
+size_t she_bytes(Ctx *ctx) {
+  std::lock_guard<std::mutex> lk(g_she_mu);
+  size_t t = 0;
+  auto it = g_she.find(ctx);
+  if (it != g_she.end())
+    for (auto &kv : it->second) t += problem_bytes(kv.second.get());
+  return t;
+}
+
 static SheProblem *find_she(vshe_ctx *ctx, int64_t h) {
   std::lock_guard<std::mutex> lk(g_she_mu);
   auto it = g_she.find(ctx);
@@ -522,6 +538,15 @@ int vshe_she_scaling(vshe_ctx *ctx, int64_t h, double *scaling, double *scale_fa
   return VSHE_OK;
 }
 
+int vshe_she_blocks(vshe_ctx *ctx, int64_t h, int64_t *block_ptr) {
+  if (!ctx || !block_ptr) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  SheProblem *S = find_she(ctx, h);
+  if (!S) return ctx->fail(VSHE_E_NOT_FOUND, "");
+  std::copy(S->slab_ptr.begin(), S->slab_ptr.end(), block_ptr);
+  return VSHE_OK;
+}
+
 int vshe_she_free(vshe_ctx *ctx, int64_t h) {
   if (!ctx) return VSHE_E_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(ctx->mu);
@@ -672,12 +697,6 @@ struct Server {
   void complete(ServeRequest *r, int status);
 };
 
-static size_t problem_bytes(const SheProblem *S) {
-  size_t b = S->arena.total;
-  if (S->sys) b += S->sys->arena.total;
-  if (S->batch) b += S->batch->arena.total + S->batch->tile_arena.total;
-  return b;
-}
 
 void Server::complete(ServeRequest *r, int status) {
   r->t_done = std::chrono::steady_clock::now();

@@ -64,6 +64,7 @@ def lib():
         L.vshe_system_time_spmv.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, f64p]
         L.vshe_set_profiling.argtypes = [vp, C.c_int32]
         L.vshe_set_spin_limit.argtypes = [vp, C.c_uint64]
+        L.vshe_solve_csr_release.argtypes = [vp]
         L.vshe_get_profile.argtypes = [vp, f64p, i64p]
         L.vshe_kernel_launches.restype = C.c_int64
         L.vshe_kernel_launches.argtypes = []
@@ -177,6 +178,10 @@ class Context:
 
     def set_profiling(self, on=True):
         self._check(lib().vshe_set_profiling(self.h, 1 if on else 0))
+
+    def release_csr_cache(self):
+        """Frees the system vshe_solve_csr keeps resident for its last pattern."""
+        self._check(lib().vshe_solve_csr_release(self.h))
 
     def set_spin_limit(self, polls=0):
         """Polls of every bounded device-side wait before VSHE_E_TIMEOUT (0: the default)."""
@@ -313,6 +318,7 @@ def _she_lib():
         L.vshe_she_results.argtypes = [vp, C.c_int64, f64p, f64p, f64p]
         L.vshe_she_export.argtypes = [vp, C.c_int64, C.c_int32, i64p, i32p, f64p, f64p]
         L.vshe_she_scaling.argtypes = [vp, C.c_int64, f64p, f64p]
+        L.vshe_she_blocks.argtypes = [vp, C.c_int64, i64p]
         L.vshe_she_free.argtypes = [vp, C.c_int64]
         L.vshe_she_bench.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, f64p, C.POINTER(SolveStatsC)]
         L.vshe_she_run_batch.argtypes = [vp, C.c_int32, i64p, C.POINTER(SolveStatsC), f64p, f64p]
@@ -410,6 +416,12 @@ class SheProblem:
         b = np.zeros(n)
         self.ctx._check(_she_lib().vshe_she_export(self.ctx.h, self.h, w, ptr(rp, C.c_int64), ptr(ci, C.c_int32), ptr(v, C.c_double), ptr(b, C.c_double)))
         return rp, ci, v, b
+
+    def blocks(self):
+        """Energy-slab row offsets of the reduced system (n_energies + 1)."""
+        b = np.zeros(self.info["n_energies"] + 1, np.int64)
+        self.ctx._check(_she_lib().vshe_she_blocks(self.ctx.h, self.h, ptr(b, C.c_int64)))
+        return b
 
     def scaling(self):
         n = self.info["n_even"]
