@@ -346,7 +346,7 @@ static size_t problem_bytes(const SheProblem *S) {
   return b;
 }
 
-size_t she_bytes(Ctx *ctx) {
+size_t vshe::she_bytes(Ctx *ctx) {
   std::lock_guard<std::mutex> lk(g_she_mu);
   size_t t = 0;
   auto it = g_she.find(ctx);
