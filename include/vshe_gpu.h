@@ -254,6 +254,8 @@ typedef struct vshe_she_info {
   int64_t bytes_device;
   int32_t levels_L, levels_U;
   int64_t nnz_factor;       /* strict lower + upper entries the ILU(0) preconditioner keeps */
+  int64_t bytes_estimate;   /* the upper bound of bytes_device computed from the host set-up alone, which
+                               vshe_she_create and the server compare with the HBM budget before allocating */
 } vshe_she_info;
 
 /* 6 * ((L+1)^2)^2 doubles, layout of vshe_coupling_tables.data; no GPU needed. */

@@ -51,6 +51,9 @@ struct SheProblem {
   int stage = 0;
 
   int create(Ctx &ctx, const vshe_device_desc &d, const vshe_she_config &c, const vshe_coupling_tables &ct, const vshe_solve_opts &o);
+  int setup_host(Ctx &ctx, const vshe_device_desc &d, const vshe_she_config &c, const vshe_coupling_tables &ct, const vshe_solve_opts &o);
+  size_t estimate_bytes() const;
+  int create_device(Ctx &ctx);
   int symbolic_full(Ctx &ctx);
   int fill_full(Ctx &ctx);
   int assemble(Ctx &ctx, int upto);
@@ -86,10 +89,48 @@ int SheProblem::check(Ctx &ctx, const char *what) {
 }
 
 int SheProblem::create(Ctx &ctx, const vshe_device_desc &d, const vshe_she_config &c, const vshe_coupling_tables &ct, const vshe_solve_opts &o) {
+  int rc = setup_host(ctx, d, c, ct, o);
+  if (rc) return rc;
+  return create_device(ctx);
+}
+
+// The host part of the set-up (energies, orders, mapping, boundary values): no device work.
+int SheProblem::setup_host(Ctx &ctx, const vshe_device_desc &d, const vshe_she_config &c, const vshe_coupling_tables &ct, const vshe_solve_opts &o) {
   std::string msg = H.build(d, c, ct);
   if (!msg.empty()) return ctx.fail(VSHE_E_INVALID_ARGUMENT, msg);
   opts = o;
   for (int i = 0; i < H.nc; ++i) ncontacts = std::max(ncontacts, H.contact[i] + 1);
+  return VSHE_OK;
+}
+
+// Upper bound of the device memory the problem will hold, from the host set-up alone, so that
+// admission against an HBM budget happens before any allocation.  Row lengths are bounded by the
+// mesh and the harmonics per node: a full-system even row holds its diagonal, two optical
+// in-scattering entries and at most o(L) odd couplings per facet of its cell (2 dim facets); an
+// odd row its diagonal and at most e(L) couplings to each of its two cells; a reduced row its
+// diagonal, the in-scattering pair and at most e(L) columns for its cell and each neighbour.  The
+// factor keeps at most (1 + k) times the reduced pattern for ILU(k), and 2 p + 1 entries per row
+// more for ILUT(p).  Per entry and per row, the bytes of every buffer the pipeline, the solver
+// (SELL copies of A, L and U, factorisation CSR and maps, Krylov vectors) and the batch hold.
+size_t SheProblem::estimate_bytes() const {
+  int64_t e = 0;
+  for (int l = 0; l <= H.L; l += 2) e += 2 * l + 1;
+  const int64_t o = int64_t(H.L + 1) * (H.L + 1) - e;
+  const int64_t ne = H.n_even, no = H.n_odd, nfull = ne + no;
+  const int64_t nnz_full = ne * (3 + 2 * H.dim * o) + no * (1 + 2 * e);
+  const int64_t nnz_red = ne * (3 + (1 + 2 * H.dim) * e);
+  const int64_t nnz_f = opts.precond == VSHE_PRECOND_ILUT
+                            ? nnz_red + ne * (2 * int64_t(opts.ilut_entries > 0 ? opts.ilut_entries : 60) + 1)
+                            : nnz_red * (1 + std::max(0, int(opts.fill_level)));
+  const int64_t tsz = opts.precision == VSHE_PRECISION_MIXED ? 4 : 8;
+  const int64_t tables = (int64_t(H.nc) + H.nf) * H.NH * 48 + int64_t(H.nc + H.nf) * 256 + (int64_t(1) << 20);
+  const int64_t pipeline = nnz_full * 12 + nfull * 40 + nnz_red * 20 + ne * 72;
+  const int64_t solver = nnz_red * 24 + nnz_f * (32 + 2 * (4 + tsz)) + ne * (11 * 8 + 48 + tsz);
+  const int64_t batch = (ne / 256 + 64) * 64 + (int64_t(1) << 20);
+  return size_t(tables + pipeline + (solver * 11) / 10 + batch);
+}
+
+int SheProblem::create_device(Ctx &ctx) {
   int rc = 0;
   cudaError_t e;
 #define UP(dst, vec) dst = upload(ctx, arena, vec, rc); if (rc) return rc;
@@ -387,7 +428,12 @@ int vshe_she_create(vshe_ctx *ctx, const vshe_device_desc *d, const vshe_she_con
   vshe_solve_opts o;
   if (opts) o = *opts; else vshe_default_opts(&o);
   std::unique_ptr<SheProblem> S(new SheProblem);
-  int rc = S->create(*ctx, *d, *c, *ct, o);
+  int rc = S->setup_host(*ctx, *d, *c, *ct, o);
+  if (rc) return rc;
+  // admission against the context's HBM budget before any allocation
+  const size_t est = S->estimate_bytes();
+  if (vshe_bytes_in_use(ctx) + est > ctx->budget) return ctx->fail(VSHE_E_BUDGET, std::to_string(est) + " bytes (upper bound) requested");
+  rc = S->create_device(*ctx);
   if (rc) return rc;
   int64_t h = ++ctx->next_handle;
   std::lock_guard<std::mutex> lk2(g_she_mu);
@@ -414,6 +460,7 @@ int vshe_she_info_get(vshe_ctx *ctx, int64_t h, vshe_she_info *info) {
   info->levels_L = S->sys ? S->sys->nlevL : 0;
   info->levels_U = S->sys ? S->sys->nlevU : 0;
   info->nnz_factor = S->sys ? S->sys->nnzL + S->sys->nnzU : 0;
+  info->bytes_estimate = int64_t(S->estimate_bytes());
   return VSHE_OK;
 }
 
@@ -721,11 +768,13 @@ int Server::admit(std::vector<ServeRequest *> &fresh) {
       if (pending.empty() || int(active.size() + fresh.size()) >= opts.max_active) break;
       r = pending.front();
     }
+    // the host set-up and the footprint bound first: nothing is allocated on the device for a
+    // request that has to wait or is refused
     std::unique_ptr<SheProblem> S(new SheProblem);
-    int rc = S->create(c, r->d, r->c, r->t, r->o);
-    const size_t need = rc ? 0 : problem_bytes(S.get());
+    int rc = S->setup_host(c, r->d, r->c, r->t, r->o);
+    const size_t need = rc ? 0 : S->estimate_bytes();
     if (!rc && held + need > opts.hbm_budget && !(active.empty() && fresh.empty())) {
-      break;  // wait for resident problems to finish (S is released here)
+      break;  // wait for resident problems to finish
     }
     {
       std::lock_guard<std::mutex> lk(mu);
@@ -733,6 +782,7 @@ int Server::admit(std::vector<ServeRequest *> &fresh) {
     }
     r->t_admit = std::chrono::steady_clock::now();
     if (!rc && held + need > opts.hbm_budget) rc = c.fail(VSHE_E_BUDGET, "request alone exceeds the server's HBM budget");
+    if (!rc) rc = S->create_device(c);
     if (!rc) rc = S->assemble(c, 3);
     if (!rc) {
       S->sys->prepare(c);

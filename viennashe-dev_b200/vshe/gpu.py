@@ -297,7 +297,7 @@ class SheInfoC(C.Structure):
         ("nnz_full", C.c_int64), ("nnz_reduced", C.c_int64),
         ("n_cells", C.c_int32), ("n_facets", C.c_int32), ("n_contacts", C.c_int32),
         ("hbar_omega", C.c_double), ("bytes_device", C.c_int64),
-        ("levels_L", C.c_int32), ("levels_U", C.c_int32), ("nnz_factor", C.c_int64),
+        ("levels_L", C.c_int32), ("levels_U", C.c_int32), ("nnz_factor", C.c_int64), ("bytes_estimate", C.c_int64),
     ]
 
 
