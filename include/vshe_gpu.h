@@ -318,6 +318,9 @@ typedef struct vshe_server_opts {
   size_t  hbm_budget;       /* bytes the resident problems may hold (0: the context's budget) */
   int32_t max_active;       /* resident problems at most (0: 256) */
   vshe_solve_opts solve;    /* default solver options of a request */
+  int32_t stagnation_iters; /* a request whose recursive residual has not halved within this many
+                               iterations ends early with VSHE_E_NOT_CONVERGED, freeing its slot
+                               (0: 400; negative: never, only max_iters ends it) */
 } vshe_server_opts;
 typedef struct vshe_server_result {
   int32_t status;           /* VSHE_OK or the error of this request */

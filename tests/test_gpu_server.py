@@ -57,3 +57,29 @@ def test_server_admits_as_slots_free(gpu_ctx):
     out = _serve(gpu_ctx, _mix(), max_active=2)
     assert all(r["status"] == 0 for r, _, _ in out)
     assert max(r["queue_ms"] for r, _, _ in out) > 0.0
+
+
+def test_stagnation_stop_frees_the_slot(gpu_ctx):
+    """A 2D bar at L = 5 with block-ILU(0) per slab, where BiCGStab stalls (the oracle: no
+    convergence on a 25 x 10 x 60 bar), ends early as not converged once its residual has not
+    halved in 100 iterations, far below its iteration cap; the request queued behind it is
+    served."""
+    dev5, cfg5 = cases.bar_small(L=5, nx=25, ny=10, n_energies=60)
+    dev1, cfg1 = cases.diode_small(L=1, boxes=40, bias=0.3)
+    srv = gpu.Server(gpu_ctx, max_active=1, stagnation_iters=100, precision="mixed", precond="ilu0", tol=1e-10,
+                     max_iters=3000, check_every=8)
+    try:
+        t5 = srv.submit(dev5, cfg5, coupling=O.golden_coupling(5), ordering="multicolor", precond="block_ilu0")
+        t1 = srv.submit(dev1, cfg1, coupling=O.golden_coupling(1), ordering="natural")
+        try:
+            res5, _, _ = srv.wait(t5)
+            code = res5["status"]
+        except gpu.VsheError as e:  # a diverging iterate ends as a breakdown, also early
+            code, res5 = e.code, None
+        assert code in (-6, -5)
+        if res5 is not None:
+            assert res5["iterations"] < 1500 and res5["rel_residual"] >= 1e-10
+        res1, _, _ = srv.wait(t1)
+        assert res1["status"] == 0 and res1["rel_residual"] < 1e-10
+    finally:
+        srv.close()

@@ -722,6 +722,10 @@ struct ServeRequest {
   bool collected = false;   // the caller has its result: the worker may free the record
   int replacements = 0;
   bool needs_start = true;
+  // stagnation watch: the best recursive residual so far and the iteration it was reached at
+  double best_res = 1e300;
+  int best_iter = 0;
+  bool stagnated = false;
 };
 
 struct Server {
@@ -850,9 +854,19 @@ int Server::step() {
   std::vector<int32_t> fin(active.size(), 0);
   bool any = false;
   for (size_t k = 0; k < active.size(); ++k) {
-    active[k]->state.assign(st.begin() + bsz * k, st.begin() + bsz * (k + 1));
-    const BiState *b = (const BiState *)active[k]->state.data();
-    if (b->done) { fin[k] = 1; any = true; }
+    ServeRequest *r = active[k];
+    r->state.assign(st.begin() + bsz * k, st.begin() + bsz * (k + 1));
+    const BiState *b = (const BiState *)r->state.data();
+    if (b->done) { fin[k] = 1; any = true; continue; }
+    // stagnation stop: no halving of the recursive residual within stagnation_iters iterations
+    if (b->res < 0.5 * r->best_res) {
+      r->best_res = b->res;
+      r->best_iter = b->iter;
+    } else if (opts.stagnation_iters > 0 && b->iter - r->best_iter >= opts.stagnation_iters) {
+      r->stagnated = true;
+      fin[k] = 1;
+      any = true;
+    }
   }
   if (!any) return VSHE_OK;
   // true FP64 residual of the members that stopped
@@ -866,7 +880,7 @@ int Server::step() {
     ServeRequest *r = active[k];
     if (!fin[k]) { keep.push_back(r); continue; }
     const BiState *b = (const BiState *)r->state.data();
-    if (b->status == 0 && rel[k] >= o.tol && b->iter < o.max_iters && r->replacements < 3) {
+    if (!r->stagnated && b->status == 0 && rel[k] >= o.tol && b->iter < o.max_iters && r->replacements < 3) {
       r->replacements++;
       resume[k] = 1;
       any_resume = true;
@@ -876,6 +890,7 @@ int Server::step() {
     SheProblem *S = r->prob.get();
     vk_permute(S->sys->n, S->sys->d_perm, (const double *)S->sys->kv[0], S->sys->d_x64, 0, c.stream);
     int status = b->status;
+    if (r->stagnated && status == 0) status = VSHE_E_NOT_CONVERGED;
     if (status == 0 && rel[k] >= o.tol) status = VSHE_E_NOT_CONVERGED;
     if (status != 0 && rel[k] < o.tol) status = 0;
     int frc = S->finish(c);
@@ -953,6 +968,7 @@ int vshe_server_create(vshe_ctx *ctx, const vshe_server_opts *opts, vshe_server 
   else { std::memset(&s->opts, 0, sizeof(s->opts)); vshe_default_opts(&s->opts.solve); }
   if (s->opts.hbm_budget == 0) s->opts.hbm_budget = ctx->budget;
   if (s->opts.max_active <= 0) s->opts.max_active = 256;
+  if (s->opts.stagnation_iters == 0) s->opts.stagnation_iters = 400;
   vshe_server *p = s.get();
   p->worker = std::thread([p] { p->run(); });
   *out = s.release();

@@ -446,7 +446,7 @@ def she_run_batch(ctx: Context, problems):
 
 # ---------------------------------------------------------------- served stream
 class ServerOptsC(C.Structure):
-    _fields_ = [("hbm_budget", C.c_size_t), ("max_active", C.c_int32), ("solve", SolveOptsC)]
+    _fields_ = [("hbm_budget", C.c_size_t), ("max_active", C.c_int32), ("solve", SolveOptsC), ("stagnation_iters", C.c_int32)]
 
 
 class ServerResultC(C.Structure):
@@ -458,7 +458,7 @@ class ServerResultC(C.Structure):
 class Server:
     """Continuous-batching request loop on one context (vshe_server_*)."""
 
-    def __init__(self, ctx: Context, hbm_budget=0, max_active=0, **solve):
+    def __init__(self, ctx: Context, hbm_budget=0, max_active=0, stagnation_iters=0, **solve):
         L = lib()
         L.vshe_server_create.argtypes = [C.c_void_p, C.POINTER(ServerOptsC), C.POINTER(C.c_void_p)]
         L.vshe_server_submit.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveOptsC), C.POINTER(C.c_int64)]
@@ -468,6 +468,7 @@ class Server:
         o = ServerOptsC()
         o.hbm_budget = int(hbm_budget)
         o.max_active = int(max_active)
+        o.stagnation_iters = int(stagnation_iters)
         so, self._keep = make_opts(**solve)
         o.solve = so
         h = C.c_void_p()
