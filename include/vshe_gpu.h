@@ -113,7 +113,8 @@ typedef struct vshe_solve_stats {
   int32_t levels_L;         /* level-schedule depth of the L and U solves */
   int32_t levels_U;
   int64_t bytes_device;     /* device memory held by the system */
-  int32_t sweep_ctas;       /* CTAs of the grid-wide triangular sweep (autotuned; 0 = none) */
+  int32_t sweep_ctas;       /* CTAs of the grid-wide triangular sweep (autotuned; 0 = none); for a
+                               member swept per task, the CTAs per task (1 = staged single CTA) */
   int32_t tile_rows;        /* rows per reduction tile of this system (autotuned) */
   int32_t sweep_mode;       /* grid-wide sweep used: VSHE_TRSV_PERSISTENT, _PER_LEVEL or _FLOW (0 = none) */
 } vshe_solve_stats;
@@ -142,6 +143,13 @@ int vshe_set_profiling(vshe_ctx *ctx, int32_t on);
  * VSHE_E_TIMEOUT and the context stays usable.  0 restores the default (20,000,000 polls, about
  * 1-2 s).  No reference counterpart: failure handling of the device-side waits. */
 int vshe_set_spin_limit(vshe_ctx *ctx, uint64_t polls);
+/* Sweep kernel of the members swept one task per CTA or cluster (VSHE_TRSV_PER_BLOCK,
+ * VSHE_TRSV_PER_SYSTEM and their AUTO cases): -1 (default) times the candidates on each batch's
+ * own factors before its first iteration and keeps the fastest; 0 one CTA per task with the
+ * factor slices staged through shared memory by bulk copies; 2, 4 or 8 one thread-block cluster
+ * of that many CTAs per task with a cluster barrier per level.  Every choice gives bitwise the same
+ * results.  No reference counterpart: scheduling control of the triangular sweeps. */
+int vshe_set_task_sweep(vshe_ctx *ctx, int32_t kernel);
 int vshe_get_profile(vshe_ctx *ctx, double *ms, int64_t *counts);
 /* Autotuner record: the rows per reduction tile chosen for systems of n's size class
  * (floor(log2 n)) on this context, and ms[0..3] = the timed FP64 SpMV for 512, 1024, 2048 and

@@ -280,9 +280,18 @@ def test_per_block_sweep_bitwise_equal():
                 out[(mode, precision)] = (x, st)
         assert out[("auto", "mixed")][1]["sweep_mode"] == 5 and out[("per_block", "fp64")][1]["sweep_mode"] == 5
         assert out[("persistent", "mixed")][1]["sweep_mode"] == 1 and out[("per_system", "mixed")][1]["sweep_mode"] == 3
+        # each task kernel forced: one staged CTA, clusters of 2, 4 and 8 CTAs
+        for kern in (0, 2, 4, 8):
+            ctx.set_task_sweep(kern)
+            for precision in ("mixed", "fp64"):
+                x, st = ctx.solve_csr(A.rp, A.ci, A.v, A.rhs, precision=precision, precond="block_ilu0", ordering="multicolor",
+                                      blocks=blocks, fill_level=1, trsv="per_block", tol=1e-10, max_iters=4000)
+                assert st["sweep_ctas"] == max(kern, 1)
+                out[("kernel%d" % kern, precision)] = (x, st)
+        ctx.set_task_sweep(-1)
         for precision in ("mixed", "fp64"):
             x0, st0 = out[("persistent", precision)]
-            for mode in ("per_block", "auto", "per_system"):
+            for mode in ("per_block", "auto", "per_system", "kernel0", "kernel2", "kernel4", "kernel8"):
                 x, st = out[(mode, precision)]
                 assert st["iterations"] == st0["iterations"], (mode, precision, st["iterations"], st0["iterations"])
                 assert np.array_equal(x, x0), (mode, precision, np.max(np.abs(x - x0)))

@@ -128,7 +128,13 @@ struct Batch {
   // schedule of the grid-wide sweep (grid_group)
   int ntasks = 0;
   std::vector<int32_t> task_kind;  // per member: 0 grid-wide sweep, 1 one task per system, 2 one task per block
-  void *d_tasks = nullptr, *d_chunks = nullptr;
+  void *d_tasks = nullptr, *d_chunks = nullptr, *d_ctasks = nullptr;
+  int64_t *d_clv = nullptr;
+  int task_kernel = 4;                 // 0 staged single CTA per task, K > 0 cluster of K CTAs per task
+  bool tasks_tuned = false;
+  std::vector<double> task_tune_ms;    // ms per apply: staged, clusters of 2, 4, 8
+  int launch_tasks(Ctx &ctx, int which);
+  int autotune_tasks(Ctx &ctx);
   bool grid_group = true;
   // the BiCGStab iteration chunk (check_every iterations) captured once as a CUDA graph and
   // replayed; graph_failed: capture was refused (then the chunk is launched directly)
@@ -195,6 +201,9 @@ struct Ctx {
   // polls of a device-side wait (grid barrier, flow poll, stage barrier) before it gives up
   // with VSHE_E_TIMEOUT
   unsigned long long spin_limit = kDefaultSpinLimit;
+  // task sweep of one-CTA/cluster-per-task members: -1 autotuned per batch, 0 one CTA with staged
+  // factor slices, K = 2, 4, 8 a cluster of K CTAs
+  int task_sweep = -1;
   std::map<int64_t, std::unique_ptr<System>> systems;
   // vshe_solve_csr's pattern cache: the system of its last call (0 = none) and the options it was
   // created with (with copies of the option arrays)

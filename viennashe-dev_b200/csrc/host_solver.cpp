@@ -824,6 +824,8 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   }
   std::vector<TaskDev> tasks;
   std::vector<ChunkDev> chunks;
+  std::vector<ClusterTask> ctasks;
+  std::vector<int64_t> clv;
   {
     const int64_t cap = mixed ? vk_task_stage_slots_f32() : vk_task_stage_slots_f64();
     // chunks of the slices [a, b) of one level: runs of whole slices that fit one stage; a wider
@@ -844,6 +846,7 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
       chunks.back().flags |= kChunkLevelEnd;
     };
     std::vector<std::pair<int64_t, TaskDev>> tw;  // (work in slots, task)
+    std::vector<std::vector<int64_t>> twl, twu;    // per task: level slice ranges (pairs) of L and U
     for (int k = 0; k < nsys; ++k) {
       if (!on_task[size_t(k)]) continue;
       const System *S = sys[size_t(k)];
@@ -861,7 +864,14 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
           work += S->uoff_h[size_t(r.second)] - S->uoff_h[size_t(r.first)] + 32 * (r.second - r.first);
         }
         t.cU1 = int32_t(chunks.size());
-        if (t.cL1 > t.cL0 || t.cU1 > t.cU0) tw.push_back({work, t});
+        if (t.cL1 > t.cL0 || t.cU1 > t.cU0) {
+          t.pad = int32_t(tw.size());  // index into twl / twu until the tasks are sorted
+          tw.push_back({work, t});
+          twl.emplace_back();
+          twu.emplace_back();
+          for (auto &r : lv_l) { twl.back().push_back(r.first); twl.back().push_back(r.second); }
+          for (auto &r : lv_u) { twu.back().push_back(r.first); twu.back().push_back(r.second); }
+        }
       };
       if (on_task[size_t(k)] == 1) {
         std::vector<std::pair<int64_t, int64_t>> l, u;
@@ -878,7 +888,16 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
       }
     }
     std::stable_sort(tw.begin(), tw.end(), [](const std::pair<int64_t, TaskDev> &a, const std::pair<int64_t, TaskDev> &b) { return a.first > b.first; });
-    for (auto &t : tw) tasks.push_back(t.second);
+    for (auto &t : tw) {
+      const std::vector<int64_t> &l = twl[size_t(t.second.pad)], &u = twu[size_t(t.second.pad)];
+      ClusterTask c{t.second.sys, int32_t(l.size() / 2), int32_t(u.size() / 2), 0, int64_t(clv.size()), 0};
+      clv.insert(clv.end(), l.begin(), l.end());
+      c.offU = int64_t(clv.size());
+      clv.insert(clv.end(), u.begin(), u.end());
+      ctasks.push_back(c);
+      t.second.pad = 0;
+      tasks.push_back(t.second);
+    }
     ntasks = int(tasks.size());
   }
   grid_group = false;
@@ -940,6 +959,9 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   if (!d_tasks) return ctx.cuda_fail(e, "cudaMalloc tasks");
   d_chunks = arena.alloc(sizeof(ChunkDev) * std::max<size_t>(chunks.size(), 1), e);
   if (!d_chunks) return ctx.cuda_fail(e, "cudaMalloc chunks");
+  d_ctasks = arena.alloc(sizeof(ClusterTask) * std::max<size_t>(ctasks.size(), 1), e);
+  if (!d_ctasks) return ctx.cuda_fail(e, "cudaMalloc cluster tasks");
+  ALLOC(d_clv, int64_t, std::max<size_t>(clv.size(), 1));
   d_sysdev = arena.alloc(vk_sysdev_size() * size_t(nsys), e);
   if (!d_sysdev) return ctx.cuda_fail(e, "cudaMalloc sysdev");
   d_state = arena.alloc(vk_bistate_size() * size_t(nsys), e);
@@ -991,6 +1013,8 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   H2D(d_factdev, fd.data(), fd.size());
   if (!tasks.empty()) { H2D(d_tasks, tasks.data(), sizeof(TaskDev) * tasks.size()); }
   if (!chunks.empty()) { H2D(d_chunks, chunks.data(), sizeof(ChunkDev) * chunks.size()); }
+  if (!ctasks.empty()) { H2D(d_ctasks, ctasks.data(), sizeof(ClusterTask) * ctasks.size()); }
+  if (!clv.empty()) { H2D(d_clv, clv.data(), sizeof(int64_t) * clv.size()); }
   if (has_pc) {
     H2D(d_cptrL, cptrL.data(), sizeof(int64_t) * cptrL.size());
     H2D(d_cptrU, cptrU.data(), sizeof(int64_t) * cptrU.size());
@@ -1164,6 +1188,54 @@ int Batch::factor(Ctx &ctx) {
 // batch on its own factors (one forward + backward apply, CUDA events), before the first
 // iteration; the choice does not change any result (each slice is computed the same way by
 // whichever warp, in either kind).
+// The task sweep launched: task_kernel 0 = one CTA per task with the factor slices staged
+// through shared memory (k_trsv_task), K > 0 = one thread-block cluster of K CTAs per task
+// (k_trsv_cluster).
+int Batch::launch_tasks(Ctx &ctx, int which) {
+  cudaStream_t s = ctx.stream;
+  if (task_kernel == 0)
+    return mixed ? vk_trsv_task_f32(ntasks, d_sysdev, d_state, d_active, d_tasks, d_chunks, which, d_bar, d_err, s)
+                 : vk_trsv_task_f64(ntasks, d_sysdev, d_state, d_active, d_tasks, d_chunks, which, d_bar, d_err, s);
+  return mixed ? vk_trsv_cluster_f32(ntasks, task_kernel, d_sysdev, d_state, d_active, d_ctasks, d_clv, which, s)
+               : vk_trsv_cluster_f64(ntasks, task_kernel, d_sysdev, d_state, d_active, d_ctasks, d_clv, which, s);
+}
+
+// Autotuner of the task sweep: one apply of each candidate (staged single CTA; clusters of 2, 4
+// and 8 CTAs) timed on the batch's own factors with CUDA events, once per batch before its first
+// iteration; the fastest is kept.  Every candidate computes every row the same way, so the
+// choice changes no result.
+int Batch::autotune_tasks(Ctx &ctx) {
+  if (ctx.task_sweep >= 0 && task_kernel != ctx.task_sweep) {
+    task_kernel = ctx.task_sweep;
+    if (chunk_exec) { cudaGraphExecDestroy(chunk_exec); chunk_exec = nullptr; }
+  }
+  if (ctx.task_sweep >= 0 || tasks_tuned || !has_pc || ntasks == 0) return VSHE_OK;
+  tasks_tuned = true;
+  cudaStream_t s = ctx.stream;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a); cudaEventCreate(&b);
+  double best = 1e30;
+  int best_k = task_kernel;
+  task_tune_ms.clear();
+  for (int k : {0, 2, 4, 8}) {
+    task_kernel = k;
+    int rc = launch_tasks(ctx, 0);  // warm-up
+    cudaEventRecord(a, s);
+    for (int r = 0; r < 3; ++r) rc |= launch_tasks(ctx, 0);
+    cudaEventRecord(b, s);
+    cudaError_t e = cudaEventSynchronize(b);
+    if (rc || e != cudaSuccess) { cudaEventDestroy(a); cudaEventDestroy(b); return ctx.cuda_fail(e != cudaSuccess ? e : cudaError_t(rc), "autotune task sweeps"); }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    task_tune_ms.push_back(ms / 3.0);
+    if (ms < best) { best = ms; best_k = k; }
+  }
+  cudaEventDestroy(a); cudaEventDestroy(b);
+  task_kernel = best_k;
+  if (chunk_exec) { cudaGraphExecDestroy(chunk_exec); chunk_exec = nullptr; }
+  return check_err(ctx, "autotune task sweeps");
+}
+
 int Batch::autotune_trsv(Ctx &ctx) {
   const int mode = sys[0]->opts.trsv_mode;
   if (mode == VSHE_TRSV_FLOW) trsv_kernel = 3;
@@ -1298,8 +1370,7 @@ int Batch::run_chunk(Ctx &ctx, int every) {
     if (!has_pc) { vk_precond_copy(ntiles, d_sysdev, d_state, &tiles, d_active, which, s); return 0; }
     int rc = 0;
     if (ntasks) {
-      rc = mixed ? vk_trsv_task_f32(ntasks, d_sysdev, d_state, d_active, d_tasks, d_chunks, which, d_bar, d_err, s)
-                 : vk_trsv_task_f64(ntasks, d_sysdev, d_state, d_active, d_tasks, d_chunks, which, d_bar, d_err, s);
+      rc = launch_tasks(ctx, which);
       if (rc) return rc;
     }
     if (!grid_group) return 0;
@@ -1440,6 +1511,7 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
   rc = factor(ctx);
   if (rc) return rc;
   if ((rc = autotune_trsv(ctx))) return rc;
+  if ((rc = autotune_tasks(ctx))) return rc;
   cudaEventRecord(e1, s);
   const vshe_solve_opts &o = sys[0]->opts;
   int it = 0;
@@ -1490,7 +1562,7 @@ int Batch::solve(Ctx &ctx, std::vector<vshe_solve_stats> &stats) {
     st.levels_U = S->nlevU;
     st.bytes_device = int64_t(S->arena.total);
     const int tk = task_kind.empty() ? 0 : task_kind[size_t(k)];
-    st.sweep_ctas = !has_pc ? 0 : tk ? 0 : trsv_grid;
+    st.sweep_ctas = !has_pc ? 0 : tk ? (task_kernel > 0 ? task_kernel : 1) : trsv_grid;
     st.sweep_mode = !has_pc ? 0
                     : tk == 1 ? VSHE_TRSV_PER_SYSTEM
                     : tk == 2 ? VSHE_TRSV_PER_BLOCK
@@ -1565,6 +1637,13 @@ size_t vshe_bytes_in_use(vshe_ctx *ctx) {
   for (auto &kv : ctx->systems) t += kv.second->arena.total;
   for (auto &kv : ctx->batches) t += kv.second->arena.total + kv.second->tile_arena.total;
   return t + vshe::she_bytes(ctx);
+}
+
+int vshe_set_task_sweep(vshe_ctx *ctx, int32_t kernel) {
+  if (!ctx || kernel < -1 || kernel > 8 || kernel == 1 || (kernel > 2 && kernel != 4 && kernel != 8)) return VSHE_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->task_sweep = kernel;
+  return VSHE_OK;
 }
 
 int vshe_set_spin_limit(vshe_ctx *ctx, uint64_t polls) {

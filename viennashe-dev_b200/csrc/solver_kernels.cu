@@ -25,6 +25,7 @@
 // that BiCGStab's short recurrences do not tolerate: on the 2D bar they cost 2-6x the
 // iterations or break down.
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <atomic>
 #include <cstdint>
@@ -852,6 +853,49 @@ __global__ void __launch_bounds__(kTaskThreads, 2) k_trsv_task(const SysDev<P> *
   }
 }
 
+// ------------------------------------------------- per-task sweeps on thread-block clusters
+// The incomplete-LU apply of one task (a preconditioner block, or a whole system) on one
+// thread-block cluster of K CTAs: the cluster's warps take the slices of a level in turn (one
+// slice per warp, one row per lane, the arithmetic of k_trsv_persistent, so both give bitwise
+// the same results) and a cluster barrier (barrier.cluster, release / acquire at cluster scope)
+// closes each level instead of a grid barrier.  Clusters are independent: tasks need no
+// co-residency, and tasks ordered by decreasing work put the smallest last.  A warp loads its
+// first slice of the next level (factor entries and the row's own operand, which do not depend
+// on the sweep) before the barrier that closes the current level; only the gathers of solved
+// values wait for it.  Solved values written by other CTAs of the cluster are read through L2.
+template <typename P>
+__global__ void __launch_bounds__(kThreads, 4) k_trsv_cluster(const SysDev<P> *sys, const BiState *st, const int32_t *active,
+                                                          const ClusterTask *tasks, const int64_t *lv, int which) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int nb = (int)cl.num_blocks();
+  const ClusterTask T = tasks[blockIdx.x / nb];
+  const int s = T.sys;
+  if (!active[s] || st[s].done || (which == 1 && st[s].s_conv)) return;  // uniform over the cluster
+  const SysDev<P> &S = sys[s];
+  const int w = (int)cl.block_rank() * kWarps + (threadIdx.x >> 5), nw = nb * kWarps;
+  for (int pass = 0; pass < 2; ++pass) {
+    const bool lower = pass == 0;
+    const int nlev = lower ? T.nlevL : T.nlevU;
+    const int64_t *lvp = lv + (lower ? T.offL : T.offU);
+    TrsvSlice<P, true> cur;
+    if (nlev > 0 && lvp[0] + w < lvp[1]) cur.load_slice(S, (int)(lvp[0] + w), lower, which);
+    for (int k = 0; k < nlev; ++k) {
+      const int64_t j0 = lvp[2 * k], j1 = lvp[2 * k + 1];
+      TrsvSlice<P, true> nxt;
+      if (k + 1 < nlev && lvp[2 * k + 2] + w < lvp[2 * k + 3]) nxt.load_slice(S, (int)(lvp[2 * k + 2] + w), lower, which);
+      cur.finish();
+      for (int64_t j = j0 + w + nw; j < j1; j += nw) {
+        TrsvSlice<P, true> extra;
+        extra.load_slice(S, (int)j, lower, which);
+        extra.finish();
+      }
+      cl.sync();
+      cur = nxt;
+    }
+  }
+}
+
 // ------------------------------------------------------ ILU(0) factorisation
 // Row-wise IKJ ILU(0) (Saad, Alg. 10.4) restricted to within-block entries,
 // one warp per row, rows of a level in parallel.  Values in FP64.
@@ -1171,6 +1215,22 @@ void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles 
     return (int)cudaGetLastError();                                                                                  \
   }                                                                                                                  \
   int vk_task_stage_slots_##SUF(void) { return stage_slots<P>(); }                                                  \
+  int vk_trsv_cluster_##SUF(int ntasks, int csize, const void *sys, const void *st, const int32_t *act, const void *tasks, \
+                            const int64_t *lv, int which, cudaStream_t s) {                                          \
+    cudaLaunchConfig_t cfg = {};                                                                                     \
+    cudaLaunchAttribute at[1];                                                                                       \
+    at[0].id = cudaLaunchAttributeClusterDimension;                                                                  \
+    at[0].val.clusterDim.x = (unsigned)csize; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;                \
+    cfg.gridDim = dim3((unsigned)(ntasks * csize));                                                                  \
+    cfg.blockDim = dim3(kThreads);                                                                                   \
+    cfg.dynamicSmemBytes = 0;                                                                                        \
+    cfg.stream = s;                                                                                                  \
+    cfg.attrs = at;                                                                                                  \
+    cfg.numAttrs = 1;                                                                                                \
+    g_launches += 1;                                                                                                 \
+    return (int)cudaLaunchKernelEx(&cfg, k_trsv_cluster<P>, (const SysDev<P> *)sys, (const BiState *)st, act,        \
+                                   (const ClusterTask *)tasks, lv, which);                                           \
+  }                                                                                                                  \
   int vk_trsv_##SUF(int mode, int grid, const void *sys, const void *st, const int32_t *act, const VkLevels *lL,     \
                     const VkLevels *lU, int which, unsigned *bar, int32_t *err, cudaStream_t s) {                    \
     return launch_trsv_t<P>(mode, grid, (const SysDev<P> *)sys, (const BiState *)st, act, *(const Levels *)lL,       \

@@ -113,6 +113,14 @@ struct ChunkDev {
   int32_t s0, s1, lvl_s0, flags;
 };
 
+// Cluster sweep tasks (k_trsv_cluster): the same units as TaskDev, walked by one thread-block
+// cluster each, level by level, with the slices of level k of the forward (backward) sweep in
+// [lv[offL + 2k], lv[offL + 2k + 1]) ([lv[offU + 2k], ...)).
+struct ClusterTask {
+  int32_t sys, nlevL, nlevU, pad;
+  int64_t offL, offU;
+};
+
 // FP64 residual view of one system (solver order): r = b - A x.
 struct RefDev {
   int64_t n;

@@ -64,6 +64,7 @@ def lib():
         L.vshe_system_time_spmv.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, f64p]
         L.vshe_set_profiling.argtypes = [vp, C.c_int32]
         L.vshe_set_spin_limit.argtypes = [vp, C.c_uint64]
+        L.vshe_set_task_sweep.argtypes = [vp, C.c_int32]
         L.vshe_solve_csr_release.argtypes = [vp]
         L.vshe_get_profile.argtypes = [vp, f64p, i64p]
         L.vshe_kernel_launches.restype = C.c_int64
@@ -182,6 +183,10 @@ class Context:
     def release_csr_cache(self):
         """Frees the system vshe_solve_csr keeps resident for its last pattern."""
         self._check(lib().vshe_solve_csr_release(self.h))
+
+    def set_task_sweep(self, kernel=-1):
+        """Task sweep kernel: -1 autotuned, 0 staged single CTA, 2 / 4 / 8 CTAs per cluster."""
+        self._check(lib().vshe_set_task_sweep(self.h, int(kernel)))
 
     def set_spin_limit(self, polls=0):
         """Polls of every bounded device-side wait before VSHE_E_TIMEOUT (0: the default)."""
