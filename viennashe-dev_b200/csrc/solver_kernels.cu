@@ -46,9 +46,10 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kSpmvU = 8;  // SELL entries per lane whose loads are issued together
 constexpr int kDotU = 6;   // the same inside the tile kernels, which also carry reduction state
 constexpr int kTrsvU = 8;  // entries of a factor row loaded at once (factor rows hold ~5 entries)
-// CTAs per SM the grid-wide sweeps are compiled for (40 registers, a few spilled): up to 6 CTAs
-// of slices in flight per SM.  The autotuner picks 1 .. 6; on the 2D bar 6 beat 4 by 3 %.
-constexpr int kTrsvCtasPerSm = 6;
+// CTAs per SM the grid-wide sweeps are compiled for (64 registers): up to 4 CTAs of slices in
+// flight per SM; the autotuner picks 1 .. 4.  The row sums walk the entries of a wide slice 8 at a
+// time, which needs the registers more than a 5th or 6th CTA per SM.
+constexpr int kTrsvCtasPerSm = 4;
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -153,8 +154,9 @@ __device__ __forceinline__ double sell_rowsum(int64_t off, int width, const int3
 
 // Continues a SELL-32 row sum from entry k0 (entries below k0 already summed into `sum`), kU
 // entries per round trip; CG: x is written by other CTAs of the same launch (L2 reads).  The
-// triangular sweeps use kU = 1: wider groups cost registers, and with them occupancy, which
-// measured slower on the 2D bar (0.47 vs 0.40 ms per apply).
+// triangular sweeps use kU = kTrsvU: the incomplete factors of the 2D bar have slices up to 37
+// entries wide (ILU(1) fill), and one entry per round trip left every level waiting on the
+// widest slice's chain of dependent loads.
 template <typename V, bool CG, int kU>
 __device__ __forceinline__ double sell_rowsum_from(int64_t off, int width, int k0, const int32_t *__restrict__ col, const V *__restrict__ val,
                                                 const double *x, double sum) {
@@ -576,7 +578,7 @@ struct TrsvSlice {
       }
       if (lane < nr) st_flow(dst + row, (base - sum) * dinv);
     } else {
-      if (width > kTrsvU) sum = sell_rowsum_from<P, CG, 1>(off, width, kTrsvU, col, val, src, sum);
+      if (width > kTrsvU) sum = sell_rowsum_from<P, CG, kTrsvU>(off, width, kTrsvU, col, val, src, sum);
       if (lane < nr) dst[row] = (base - sum) * dinv;
     }
   }
