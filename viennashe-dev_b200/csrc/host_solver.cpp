@@ -805,6 +805,12 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   constexpr int64_t kCtaMaxRows = int64_t(2) << 20;  // beyond, one SM's bandwidth bounds the sweep
   constexpr int64_t kTaskMaxRows = int64_t(1) << 18;
   std::vector<char> on_task((size_t)nsys, 0);  // 0 grid, 1 whole system, 2 per block
+  int64_t num_sms_hint = 148;
+  {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+      num_sms_hint = sms;
+  }
   ntasks = 0;
   if (has_pc) {
     for (int k = 0; k < nsys; ++k) {
@@ -879,12 +885,53 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
         for (int32_t v = 0; v < S->nlevU; ++v) u.push_back({S->lvsU[size_t(v)], S->lvsU[size_t(v) + 1]});
         make(l, u);
       } else {
+        // runs of consecutive blocks: a block of more than the target work is a task of its own,
+        // smaller neighbours share one (the level slices of consecutive blocks are contiguous,
+        // blocks being ordered inside every level), so that the tasks of the batch fit one wave
+        // of one CTA per SM
         int32_t nb = 0;
         for (int32_t b : S->blk) nb = std::max(nb, b + 1);
-        std::vector<std::vector<std::pair<int64_t, int64_t>>> l((size_t)nb), u((size_t)nb);
-        for (size_t g = 0; g + 1 < S->lgrp_s0.size(); ++g) l[size_t(S->lgrp_blk[g])].push_back({S->lgrp_s0[g], S->lgrp_s0[g + 1]});
-        for (size_t g = 0; g + 1 < S->ugrp_s0.size(); ++g) u[size_t(S->ugrp_blk[g])].push_back({S->ugrp_s0[g], S->ugrp_s0[g + 1]});
-        for (int32_t b = 0; b < nb; ++b) make(l[size_t(b)], u[size_t(b)]);
+        std::vector<int64_t> wb((size_t)nb, 0);
+        for (size_t g = 0; g + 1 < S->lgrp_s0.size(); ++g)
+          wb[size_t(S->lgrp_blk[g])] += S->loff_h[size_t(S->lgrp_s0[g + 1])] - S->loff_h[size_t(S->lgrp_s0[g])];
+        for (size_t g = 0; g + 1 < S->ugrp_s0.size(); ++g)
+          wb[size_t(S->ugrp_blk[g])] += S->uoff_h[size_t(S->ugrp_s0[g + 1])] - S->uoff_h[size_t(S->ugrp_s0[g])];
+        int64_t total = 0, wmax = 0;
+        for (int64_t w : wb) { total += w; wmax = std::max(wmax, w); }
+        const int64_t slots = std::max<int64_t>(1, num_sms_hint - int64_t(nsys) + 1);
+        std::vector<int32_t> gstart;  // first block of each task
+        for (int64_t target = std::max<int64_t>(wmax, (total + slots - 1) / slots);; target += std::max<int64_t>(1, target / 20)) {
+          gstart.clear();
+          int64_t acc = 0;
+          for (int32_t b = 0; b < nb; ++b) {
+            if (wb[size_t(b)] == 0) continue;
+            if (gstart.empty() || acc + wb[size_t(b)] > target) { gstart.push_back(b); acc = 0; }
+            acc += wb[size_t(b)];
+          }
+          if (int64_t(gstart.size()) <= slots) break;
+        }
+        std::vector<int32_t> task_of((size_t)nb, -1);
+        for (size_t t = 0; t < gstart.size(); ++t) {
+          const int32_t e = t + 1 < gstart.size() ? gstart[t + 1] : nb;
+          for (int32_t b = gstart[t]; b < e; ++b) task_of[size_t(b)] = int32_t(t);
+        }
+        // merged level ranges of each task: the task's groups of one level are adjacent slices
+        std::vector<std::vector<std::pair<int64_t, int64_t>>> l(gstart.size()), u(gstart.size());
+        auto add = [&](std::vector<std::pair<int64_t, int64_t>> &v, int32_t lev, std::vector<int32_t> &lastlev, size_t t, int64_t a, int64_t b) {
+          if (!v.empty() && lastlev[t] == lev && v.back().second == a) v.back().second = b;
+          else v.push_back({a, b});
+          lastlev[t] = lev;
+        };
+        std::vector<int32_t> lastL(gstart.size(), -1), lastU(gstart.size(), -1);
+        for (size_t g = 0; g + 1 < S->lgrp_s0.size(); ++g) {
+          const int32_t t = task_of[size_t(S->lgrp_blk[g])];
+          if (t >= 0) add(l[size_t(t)], S->lgrp_lev[g], lastL, size_t(t), S->lgrp_s0[g], S->lgrp_s0[g + 1]);
+        }
+        for (size_t g = 0; g + 1 < S->ugrp_s0.size(); ++g) {
+          const int32_t t = task_of[size_t(S->ugrp_blk[g])];
+          if (t >= 0) add(u[size_t(t)], S->ugrp_lev[g], lastU, size_t(t), S->ugrp_s0[g], S->ugrp_s0[g + 1]);
+        }
+        for (size_t t = 0; t < gstart.size(); ++t) make(l[t], u[t]);
       }
     }
     std::stable_sort(tw.begin(), tw.end(), [](const std::pair<int64_t, TaskDev> &a, const std::pair<int64_t, TaskDev> &b) { return a.first > b.first; });

@@ -46,10 +46,9 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kSpmvU = 8;  // SELL entries per lane whose loads are issued together
 constexpr int kDotU = 6;   // the same inside the tile kernels, which also carry reduction state
 constexpr int kTrsvU = 8;  // entries of a factor row loaded at once (factor rows hold ~5 entries)
-// CTAs per SM the grid-wide sweeps are compiled for (64 registers): up to 4 CTAs of slices in
-// flight per SM; the autotuner picks 1 .. 4.  The row sums walk the entries of a wide slice 8 at a
-// time, which needs the registers more than a 5th or 6th CTA per SM.
-constexpr int kTrsvCtasPerSm = 4;
+// CTAs per SM the grid-wide sweeps are compiled for (40 registers, some spilled): up to 6 CTAs
+// of slices in flight per SM.  The autotuner picks 1 .. 6; on the 2D bar 6 beat 4 by 3 %.
+constexpr int kTrsvCtasPerSm = 6;
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -154,9 +153,8 @@ __device__ __forceinline__ double sell_rowsum(int64_t off, int width, const int3
 
 // Continues a SELL-32 row sum from entry k0 (entries below k0 already summed into `sum`), kU
 // entries per round trip; CG: x is written by other CTAs of the same launch (L2 reads).  The
-// triangular sweeps use kU = kTrsvU: the incomplete factors of the 2D bar have slices up to 37
-// entries wide (ILU(1) fill), and one entry per round trip left every level waiting on the
-// widest slice's chain of dependent loads.
+// global-load sweeps use kU = 1: 8 per round trip cost registers and spills, and measured slower
+// on the 2D bar with ILU(1) (cluster sweep 1.00 vs 0.76 ms per apply).
 template <typename V, bool CG, int kU>
 __device__ __forceinline__ double sell_rowsum_from(int64_t off, int width, int k0, const int32_t *__restrict__ col, const V *__restrict__ val,
                                                 const double *x, double sum) {
@@ -578,7 +576,7 @@ struct TrsvSlice {
       }
       if (lane < nr) st_flow(dst + row, (base - sum) * dinv);
     } else {
-      if (width > kTrsvU) sum = sell_rowsum_from<P, CG, kTrsvU>(off, width, kTrsvU, col, val, src, sum);
+      if (width > kTrsvU) sum = sell_rowsum_from<P, CG, 1>(off, width, kTrsvU, col, val, src, sum);
       if (lane < nr) dst[row] = (base - sum) * dinv;
     }
   }
@@ -718,10 +716,11 @@ __device__ __noinline__ void trsv_slice_direct(const SysDev<P> &S, int j, bool l
   a.finish();
 }
 
-constexpr int kTaskConsumers = 16;                          // warps that sum rows
+constexpr int kTaskConsumers = 31;                          // warps that sum rows
 constexpr int kTaskThreads = 32 * (kTaskConsumers + 1);     // + one warp that issues the bulk copies
 constexpr int kStageBytes = 32768;                          // one chunk: its columns, then its values
-constexpr int kStages = 3;                                  // chunks in flight per CTA
+constexpr int kStages = 6;                                  // chunks in flight per CTA
+constexpr int kTaskG = 16;                                  // gathers of a row issued together
 constexpr int kTaskSmem = kStages * kStageBytes;
 template <typename P>
 __host__ __device__ constexpr int stage_slots() { return (kStageBytes / int(4 + sizeof(P))) & ~31; }
@@ -740,7 +739,7 @@ __host__ __device__ constexpr int stage_slots() { return (kStageBytes / int(4 + 
 // is bounded (bar[2..3] polls); after a failed wait a consumer stops reading the stages but keeps
 // arriving on the barriers, and the producer stops issuing and drains its copies in flight.
 template <typename P>
-__global__ void __launch_bounds__(kTaskThreads, 2) k_trsv_task(const SysDev<P> *sys, const BiState *st, const int32_t *active,
+__global__ void __launch_bounds__(kTaskThreads, 1) k_trsv_task(const SysDev<P> *sys, const BiState *st, const int32_t *active,
                                                                 const TaskDev *tasks, const ChunkDev *chunks, int which,
                                                                 const unsigned *bar, int32_t *err) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -831,20 +830,15 @@ __global__ void __launch_bounds__(kTaskThreads, 2) k_trsv_task(const SysDev<P> *
         const int32_t *cj = scol + (oj - o0) + lane;
         const P *vj = sval + (oj - o0) + lane;
         double sum = 0.0;
-        for (int k = 0; k < width; k += kTrsvU) {
-          int32_t cc[kTrsvU];
-          P aa[kTrsvU];
-          double xx[kTrsvU];
+        // kTaskG gathers in flight per lane; the values are read from shared memory as they are
+        // multiplied, in index order
+        for (int k = 0; k < width; k += kTaskG) {
+          double xx[kTaskG];
 #pragma unroll
-          for (int u = 0; u < kTrsvU; ++u) {
-            cc[u] = 0; aa[u] = P(0);
-            if (k + u < width) { cc[u] = cj[32 * (k + u)]; aa[u] = vj[32 * (k + u)]; }
-          }
+          for (int u = 0; u < kTaskG; ++u) xx[u] = k + u < width ? __ldcg(src + cj[32 * (k + u)]) : 0.0;
 #pragma unroll
-          for (int u = 0; u < kTrsvU; ++u) xx[u] = k + u < width ? __ldcg(src + cc[u]) : 0.0;
-#pragma unroll
-          for (int u = 0; u < kTrsvU; ++u)
-            if (k + u < width) sum = fma((double)aa[u], xx[u], sum);
+          for (int u = 0; u < kTaskG; ++u)
+            if (k + u < width) sum = fma((double)vj[32 * (k + u)], xx[u], sum);
         }
         if (lane < nr) dst[row] = (base - sum) * dinv;
       }
