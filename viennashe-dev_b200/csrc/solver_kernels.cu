@@ -720,7 +720,8 @@ constexpr int kTaskConsumers = 31;                          // warps that sum ro
 constexpr int kTaskThreads = 32 * (kTaskConsumers + 1);     // + one warp that issues the bulk copies
 constexpr int kStageBytes = 32768;                          // one chunk: its columns, then its values
 constexpr int kStages = 6;                                  // chunks in flight per CTA
-constexpr int kTaskG = 16;                                  // gathers of a row issued together
+constexpr int kTaskG = 8;                                   // gathers of a row issued together (16 measured
+                                                            // 3.9x slower in FP32 on the 2D bar: register-bound)
 constexpr int kTaskSmem = kStages * kStageBytes;
 template <typename P>
 __host__ __device__ constexpr int stage_slots() { return (kStageBytes / int(4 + sizeof(P))) & ~31; }
@@ -831,7 +832,7 @@ __global__ void __launch_bounds__(kTaskThreads, 1) k_trsv_task(const SysDev<P> *
         const P *vj = sval + (oj - o0) + lane;
         double sum = 0.0;
         // kTaskG gathers in flight per lane; the values are read from shared memory as they are
-        // multiplied, in index order
+        // multiplied, in index order (loading them into registers first measured 3.5x slower)
         for (int k = 0; k < width; k += kTaskG) {
           double xx[kTaskG];
 #pragma unroll
