@@ -211,8 +211,8 @@ int vshe_system_time_spmv(vshe_ctx *ctx, int64_t handle, int32_t precision, int3
  * queued on `stream` (a cudaStream_t; NULL = the default stream) and the call returns without
  * waiting.  Its scratch (one partial-sum pair per 2048 rows) is a fixed 512 KiB array in the
  * library's device image, so n is limited to 64 Mi rows (67,108,864): larger n returns
- * VSHE_E_CAPACITY.  The first call on each device looks up that array and clears it, so it
- * synchronises the device once and should come before any stream capture.  All calls share
+ * VSHE_E_CAPACITY.  The first call on each device looks up that array's address and clears its
+ * ticket counter, so it synchronises the device once and should come before any stream capture.  All calls share
  * the array: calls whose kernels overlap on the GPU (other streams or threads on the same
  * device) race on it.  Nothing is allocated or freed by this call. */
 int vshe_csr_residual_noalloc(int64_t n, int64_t nnz, const int64_t *d_row_ptr, const int32_t *d_col,

@@ -7,15 +7,17 @@ and writes the values as golden fixtures (tests/golden/coupling_L{L}.json),
 which the tests use to pin (a) the library's own quadrature of the coupling
 integrals and (b) assembly parity when the reference's own tables are fed in.
 
-Run from the repository root:  python tests/golden/make_coupling_golden.py
-(it needs the reference tree at /root/reference; the fixtures are committed).
+Run from the repository root:  python tests/golden/make_coupling_golden.py [viennashe-dev root]
+(the reference tree: the argument, else $VIENNASHE_REF_ROOT, else /root/reference; the fixtures
+are committed).
 """
 import json
 import os
 import re
 import sys
 
-REF = "/root/reference/viennashe/she/harmonics_coupling.hpp"
+REF_ROOT = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("VIENNASHE_REF_ROOT", "/root/reference")
+REF = os.path.join(REF_ROOT, "viennashe", "she", "harmonics_coupling.hpp")
 HERE = os.path.dirname(os.path.abspath(__file__))
 NAMES = ["a_x", "a_y", "a_z", "b_x", "b_y", "b_z"]
 
