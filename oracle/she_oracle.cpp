@@ -1469,6 +1469,38 @@ int vsheo_ilu0_apply(int64_t n, const int64_t *rp, const int32_t *ci, const doub
   return 0;
 }
 
+// The oracle's scalar physics at given arguments, numbered like oracle/ref_physics.cpp's probe
+// of the reference's own headers (tests/test_oracle_ref.py compares the two): 0 DOS(in[0]);
+// 1 velocity(in[0]); 2 optical phonon number(in[0], T = in[1]); 3 built-in potential(T, N_D, N_A);
+// 4 ohmic contact electron density(T, N_D, N_A); 5 acoustic rate(T = in[0], fit factor in[1]);
+// 6 optical processes(spacing in[0], T in[1], kinetic energy in[2], fit factor in[3]) -> the rates
+// of emission, emission into the state, absorption, absorption into the state, and the snapped
+// phonon energy; 7 band weight(T).
+int vsheo_physics_probe(int what, const double *in, double *out) {
+  Problem p;
+  switch (what) {
+    case 0: out[0] = dos(in[0]); return 0;
+    case 1: out[0] = velocity(in[0]); return 0;
+    case 2: out[0] = optical_phonon_number(in[0], in[1]); return 0;
+    case 3: out[0] = built_in_potential(in[0], in[1], in[2]); return 0;
+    case 4: out[0] = contact_carrier_ohm_n(in[0], in[1], in[2]); return 0;
+    case 5:
+      p.T = in[0]; p.cfg.acoustic_fit_factor = in[1];
+      out[0] = acoustic_rate(p);
+      return 0;
+    case 6: {
+      p.cfg.energy_spacing = in[0]; p.T = in[1]; p.cfg.optical_fit_factor = in[3];
+      snap_phonon_energy(p);
+      const double r = optical_rate(p), N = optical_phonon_number(p.hbar_omega, p.T);
+      out[0] = r * (N + 1.0); out[1] = r * (N + 1.0); out[2] = r * N; out[3] = r * N;
+      out[4] = p.hbar_omega;
+      return 0;
+    }
+    case 7: out[0] = band_weight(in[0]); return 0;
+  }
+  return -1;
+}
+
 // Spherical-harmonics index sequence of an iterator type (0 all, 1 even, 2 odd) up to order L.
 int vsheo_harmonics(int L, int type, int64_t *out, int cap) {
   int k = 0;

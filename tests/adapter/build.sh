@@ -14,7 +14,7 @@ fi
 mkdir -p "$HERE/_build"
 g++ -std=c++11 -O1 -fPIC -shared -Wall -Wno-unused-parameter -Wno-unused-variable -Wno-unused-but-set-variable \
     -Wno-deprecated-declarations \
-    -I"$ROOT/viennashe-dev_b200/adapter" -I"$ROOT/include" -I"$REF" -I"$HERE/stub" \
+    -I"$ROOT/viennashe-dev_b200/adapter" -I"$ROOT/include" -I"$REF" -I"$ROOT/oracle/ref_stub/grid" \
     -o "$HERE/_build/libadapter_check.so" "$HERE/adapter_check.cpp" \
     -L"$ROOT/viennashe-dev_b200/lib" -lvshe_b200 -Wl,-rpath,'$ORIGIN/../../../viennashe-dev_b200/lib'
 echo "built $HERE/_build/libadapter_check.so"
