@@ -496,16 +496,19 @@ class Server:
         self._meta[t.value] = (dev.n_cells, dev.n_contacts)
         return t.value
 
-    def wait(self, ticket, timeout_ms=-1.0):
-        """-> (result dict, densities, currents); raises on a failed request."""
+    def wait(self, ticket, timeout_ms=-1.0, raise_on_error=True):
+        """-> (result dict, densities, currents); raises on a failed request (other than not
+        converged) unless raise_on_error is False, in which case the result carries the status."""
         nc, ncont = self._meta.pop(ticket)
         r = ServerResultC()
         dens = np.zeros(nc)
         cur = np.zeros(max(ncont, 1))
         rc = lib().vshe_server_wait(self.h, ticket, float(timeout_ms), C.byref(r), ptr(dens, C.c_double), ptr(cur, C.c_double))
         res = {k: getattr(r, k) for k, _ in ServerResultC._fields_}
-        if rc and rc != -6:
+        if rc and rc != -6 and raise_on_error:
             raise VsheError(rc, "served request %d failed (%s)" % (ticket, ERRORS.get(rc, "?")))
+        if rc:
+            res["status"] = rc
         return res, dens, cur[:ncont]
 
     def close(self):
