@@ -230,6 +230,20 @@ std::string SheSetup::build(const vshe_device_desc &d, const vshe_she_config &c,
   }
   slab_ptr[NH] = idx;
   n_even = idx;
+  // the slab bounds as fill_block_indices (viennashe/she/linear_solver.hpp:44-83) writes them:
+  // block H starts at the first unknown of the most recent slab <= H that has unknowns, so the
+  // rows of a slab followed by an empty one carry the empty one's index (the row partition is
+  // the same)
+  {
+    int64_t last_found = 0;
+    std::vector<int64_t> first(size_t(NH) + 1, 0);
+    for (int H = 0; H < NH; ++H) {
+      if (slab_ptr[size_t(H) + 1] > slab_ptr[size_t(H)]) last_found = slab_ptr[size_t(H)];
+      first[size_t(H)] = last_found;
+    }
+    first[size_t(NH)] = n_even;
+    slab_ptr.swap(first);
+  }
   for (int H = 0; H < NH; ++H) {
     for (int f = 0; f < nf; ++f) {
       const size_t a = size_t(f) * NH + H;
