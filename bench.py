@@ -487,13 +487,15 @@ def run_ours(args, D_):
         dbytes = spmv_bytes
         kname = "k_spmv_dot (SELL-32 SpMV FP64 + fused dots)"
     achieved = dbytes / (avg_ms / 1000.0) / 1e9
-    # DRAM traffic per launch: ncu --set full captures of the same kernels on the 200 x 50 x 80
-    # bar (the sweeps as now compiled: 40 registers) measured dram__bytes_read.sum +
-    # dram__bytes_write.sum at 0.967 (SpMV + dots) and 0.980 (ILU(1) apply) of the algorithmic
-    # bytes; the traffic grows in proportion with the units processed, so a full launch's is
-    # that ratio times its algorithmic bytes.
-    traffic_ratio = {"spmv": 383372032 / 396606924, "trsv": (421555456 + 19777280) / 450235320}
-    traffic = dbytes * traffic_ratio[dominant] if args.workload == "bar" and (dominant == "spmv" or st.get("sweep_mode") == 1) else None
+    # DRAM traffic per launch: ncu captures of the same kernels on the 200 x 50 x 80 bar measured
+    # dram__bytes_read.sum + dram__bytes_write.sum at 0.967 of the algorithmic bytes for the SpMV
+    # + dots, 0.980 for the grid-barrier ILU(1) apply (40 registers) and 1.071 for the per-slab
+    # apply; the traffic grows in proportion with the units processed, so a full launch's is that
+    # ratio times its algorithmic bytes.
+    traffic_ratio = {"spmv": 383372032 / 396606924, 1: (421555456 + 19777280) / 450235320,
+                     5: (442529280 + 39483392) / 450235320}
+    key = dominant if dominant == "spmv" else st.get("sweep_mode")
+    traffic = dbytes * traffic_ratio[key] if args.workload == "bar" and key in traffic_ratio else None
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_source": peak_src,
                 "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                 "traffic_source": "ncu capture of the 200x50x80 bar scaled by algorithmic bytes" if traffic else None,
