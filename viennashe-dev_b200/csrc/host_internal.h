@@ -19,6 +19,9 @@ const char *errstr(int code);
 
 // polls of a device-side wait before it gives up with VSHE_E_TIMEOUT (about 1-2 s with backoff)
 constexpr unsigned long long kDefaultSpinLimit = 20000000ull;
+// Entries allocated past n in the Krylov vectors and in urow / udinv: the per-task sweep stages
+// row ranges rounded up to a multiple of 4 entries, which may reach up to 3 entries past n.
+constexpr int64_t kVecPad = 8;
 
 // Device allocations owned by one object, freed together.
 struct DevArena {
@@ -73,6 +76,7 @@ struct System {
   std::vector<int64_t> lgrp_s0, ugrp_s0;  // (level, block) slice groups (Layout)
   std::vector<int32_t> lgrp_lev, lgrp_blk, ugrp_lev, ugrp_blk;
   std::vector<int64_t> loff_h, uoff_h;    // SELL slot offsets of the L and U slices (host copies)
+  std::vector<int64_t> lrow0_h, uslot0_h; // first solver row / slot of every L / U slice (host copies)
   int32_t nlevL = 0, nlevU = 0;
   int64_t nslA = 0, nslL = 0, nslU = 0;     // SELL slices
   int64_t padA = 0, padL = 0, padU = 0;     // SELL slots (incl. padding)
@@ -97,7 +101,7 @@ struct System {
   int64_t *d_loff = nullptr, *d_uoff = nullptr, *d_lvsL = nullptr, *d_lvsU = nullptr;
   void *d_lval = nullptr, *d_uval = nullptr, *d_udinv = nullptr;
   double *d_ytmp = nullptr;
-  void *kv[9] = {nullptr};  // x r rh p v s t ph sh (FP64, solver order, n + 1 entries; entry n stays 0)
+  void *kv[9] = {nullptr};  // x r rh p v s t ph sh (FP64, solver order, n + kVecPad entries; entry n stays 0)
   int64_t tile_rows = 0;    // rows per reduction tile (0: not chosen yet; see Batch::autotune_tiles)
 
   int create(Ctx &ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *v,
@@ -128,7 +132,7 @@ struct Batch {
   // schedule of the grid-wide sweep (grid_group)
   int ntasks = 0;
   std::vector<int32_t> task_kind;  // per member: 0 grid-wide sweep, 1 one task per system, 2 one task per block
-  void *d_tasks = nullptr, *d_chunks = nullptr, *d_ctasks = nullptr;
+  void *d_tasks = nullptr, *d_chunks = nullptr, *d_ctasks = nullptr, *d_sdesc = nullptr;
   int64_t *d_clv = nullptr;
   int task_kernel = 4;                 // 0 staged single CTA per task, K > 0 cluster of K CTAs per task
   bool tasks_tuned = false;

@@ -662,6 +662,7 @@ int System::setup_pattern(Ctx &ctx, const double *host_val) {
   lgrp_s0 = Lt.lgrp_s0; lgrp_lev = Lt.lgrp_lev; lgrp_blk = Lt.lgrp_blk;
   ugrp_s0 = Lt.ugrp_s0; ugrp_lev = Lt.ugrp_lev; ugrp_blk = Lt.ugrp_blk;
   loff_h = Lt.loff; uoff_h = Lt.uoff;
+  lrow0_h.assign(Lt.lstart.begin(), Lt.lstart.end()); uslot0_h.assign(Lt.ustart.begin(), Lt.ustart.end());
   nlevL = Lt.nlevL; nlevU = Lt.nlevU; nslA = Lt.nslA; nslL = Lt.nslL; nslU = Lt.nslU;
   padA = Lt.padA; padL = Lt.padL; padU = Lt.padU; nnzL = Lt.nnzL; nnzU = Lt.nnzU; nnzF = Lt.nnzF;
   const auto &prp = Lt.prp; const auto &pci = Lt.pci; const auto &pdiag = Lt.pdiag; const auto &amap = Lt.amap;
@@ -678,7 +679,7 @@ int System::setup_pattern(Ctx &ctx, const double *host_val) {
   ptr = arena.alloc(tsz * size_t(count), e);                                 \
   if (!ptr) return ctx.cuda_fail(e, "cudaMalloc " #ptr);
   // Krylov vectors x r rh p v s t ph sh (FP64, solver order) with the zero entry n
-  for (int k = 0; k < 9; ++k) { ALLOC(kv[k], double, n + 1); }
+  for (int k = 0; k < 9; ++k) { ALLOC(kv[k], double, n + kVecPad); }
   ALLOC(d_x64, double, n);
   ALLOC(d_bp, double, n + 1);
   ALLOC(d_perm, int32_t, n);
@@ -700,14 +701,14 @@ int System::setup_pattern(Ctx &ctx, const double *host_val) {
     ALLOC(d_loff, int64_t, nslL + 1);
     ALLOC(d_uslot0, int32_t, nslU + 1);
     ALLOC(d_uoff, int64_t, nslU + 1);
-    ALLOC(d_urow, int32_t, n);
+    ALLOC(d_urow, int32_t, n + kVecPad);
     ALLOC(d_lvsL, int64_t, lvsL.size());
     ALLOC(d_lvsU, int64_t, lvsU.size());
     ALLOC(d_lcol, int32_t, std::max<int64_t>(padL, 1));
     ALLOC(d_ucol, int32_t, std::max<int64_t>(padU, 1));
     ALLOCT(d_lval, std::max<int64_t>(padL, 1));
     ALLOCT(d_uval, std::max<int64_t>(padU, 1));
-    ALLOCT(d_udinv, n);
+    ALLOCT(d_udinv, n + kVecPad);
     ALLOC(d_ytmp, double, n + 1);
   }
 #undef ALLOC
@@ -715,7 +716,7 @@ int System::setup_pattern(Ctx &ctx, const double *host_val) {
   cudaStream_t s = ctx.stream;
   // every vector starts at 0 (entry n is the SELL padding target and is never written)
   for (int k = 0; k < 9; ++k)
-    if ((e = cudaMemsetAsync(kv[k], 0, sizeof(double) * size_t(n + 1), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+    if ((e = cudaMemsetAsync(kv[k], 0, sizeof(double) * size_t(n + kVecPad), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   if ((e = cudaMemsetAsync(d_bp, 0, sizeof(double) * size_t(n + 1), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   if ((e = cudaMemsetAsync(d_x64, 0, sizeof(double) * size_t(n), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
 #define H2D(dst, vec)                                                                                        \
@@ -747,6 +748,8 @@ int System::setup_pattern(Ctx &ctx, const double *host_val) {
     if ((e = cudaMemsetAsync(d_lval, 0, tsz * size_t(std::max<int64_t>(padL, 1)), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
     if ((e = cudaMemsetAsync(d_uval, 0, tsz * size_t(std::max<int64_t>(padU, 1)), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
     if ((e = cudaMemsetAsync(d_ytmp, 0, sizeof(double) * size_t(n + 1), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+    if ((e = cudaMemsetAsync(d_urow + n, 0, sizeof(int32_t) * size_t(kVecPad), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
+    if ((e = cudaMemsetAsync((char *)d_udinv + tsz * size_t(n), 0, tsz * size_t(kVecPad), s)) != cudaSuccess) return ctx.cuda_fail(e, "memset");
   }
 #undef H2D
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return ctx.cuda_fail(e, "upload pattern");
@@ -795,15 +798,19 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   // Triangular sweeps.  A member sweeps either as tasks, one CTA each walking its levels with
   // a CTA barrier per level (k_trsv_task), or in the merged level schedule of the grid-wide sweep
   // (k_trsv_persistent).  Tasks are whole systems for members with many short levels (fewer than
-  // kCtaRowsPerLevel rows per forward level on average, more than kCtaMinLevels levels and at
-  // most kCtaMaxRows rows: 1D devices), and preconditioner blocks for block-ILU members with at
-  // least two blocks of at most kTaskMaxRows rows (energy slabs: the factor has no entry between
-  // blocks, so they sweep independently).  VSHE_TRSV_PER_SYSTEM / VSHE_TRSV_PER_BLOCK force the
-  // former / latter for every member; the grid-wide modes force the merged schedule.
+  // kCtaRowsPerLevel rows per forward level on average and more than kCtaMinLevels levels: 1D
+  // devices) whose apply one SM finishes sooner than the grid-wide sweep, and preconditioner
+  // blocks for block-ILU members with at least two blocks of at most kTaskMaxRows rows (energy
+  // slabs: the factor has no entry between blocks, so they sweep independently).
+  // VSHE_TRSV_PER_SYSTEM / VSHE_TRSV_PER_BLOCK force the former / latter for every member; the
+  // grid-wide modes force the merged schedule.  The time estimates use rates measured on the 2D
+  // bar: one CTA streams a task's factor and vectors at about kTaskBytesPerUs, and a level of the
+  // grid-wide sweep costs about kGridLevelUs (its grid barrier and the latency of the level's
+  // rows) on top of the apply's bytes at kGridBytesPerUs.
   constexpr int64_t kCtaRowsPerLevel = 4096;
   constexpr int32_t kCtaMinLevels = 32;
-  constexpr int64_t kCtaMaxRows = int64_t(2) << 20;  // beyond, one SM's bandwidth bounds the sweep
   constexpr int64_t kTaskMaxRows = int64_t(1) << 18;
+  constexpr double kTaskBytesPerUs = 3.0e4, kGridBytesPerUs = 3.0e6, kGridLevelUs = 4.0;
   std::vector<char> on_task((size_t)nsys, 0);  // 0 grid, 1 whole system, 2 per block
   int64_t num_sms_hint = 148;
   {
@@ -821,7 +828,9 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
       std::vector<int64_t> bsz((size_t)nb, 0);
       for (int32_t b : S->blk) bsz[size_t(b)]++;
       const int64_t bmax = nb ? *std::max_element(bsz.begin(), bsz.end()) : 0;
-      const bool per_sys = S->nlevL > kCtaMinLevels && S->n / std::max(S->nlevL, 1) < kCtaRowsPerLevel && S->n <= kCtaMaxRows;
+      const double apply_bytes = double(4 + (mixed ? 4 : 8)) * double(S->padL + S->padU) + 40.0 * double(S->n);
+      const bool one_sm_sooner = apply_bytes / kTaskBytesPerUs < kGridLevelUs * double(S->nlevL + S->nlevU) + apply_bytes / kGridBytesPerUs;
+      const bool per_sys = S->nlevL > kCtaMinLevels && S->n / std::max(S->nlevL, 1) < kCtaRowsPerLevel && one_sm_sooner;
       const bool per_blk = S->opts.precond == VSHE_PRECOND_BLOCK_ILU0 && nb >= 2 && bmax <= kTaskMaxRows;
       if (mode == VSHE_TRSV_PER_SYSTEM) on_task[size_t(k)] = 1;
       else if (mode == VSHE_TRSV_PER_BLOCK) on_task[size_t(k)] = 2;
@@ -830,23 +839,45 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   }
   std::vector<TaskDev> tasks;
   std::vector<ChunkDev> chunks;
+  std::vector<SliceDesc> sdesc;
   std::vector<ClusterTask> ctasks;
   std::vector<int64_t> clv;
   {
-    const int64_t cap = mixed ? vk_task_stage_slots_f32() : vk_task_stage_slots_f64();
-    // chunks of the slices [a, b) of one level: runs of whole slices that fit one stage; a wider
-    // slice is its own chunk, read from global memory
-    auto add_level = [&](const std::vector<int64_t> &off, int64_t a, int64_t b) {
+    const int vbytes = mixed ? int(sizeof(float)) : int(sizeof(double));
+    // chunks of the slices [a, b) of one level of one system's L (lower) or U sweep: runs of
+    // whole slices whose descriptors, factor slots and row operands fit one stage, with their
+    // slice descriptors; a slice too wide for a stage is its own chunk, read from global memory
+    auto add_level = [&](const System *S, bool lower, int64_t a, int64_t b) {
       if (a >= b) return;
+      const std::vector<int64_t> &off = lower ? S->loff_h : S->uoff_h;
+      const std::vector<int64_t> &rs = lower ? S->lrow0_h : S->uslot0_h;
+      auto bytes = [&](int64_t j0, int64_t e) {
+        return task_chunk_bytes(e - j0, off[size_t(e)] - off[size_t(j0)], rs[size_t(j0)] & ~int64_t(3),
+                                (rs[size_t(e)] + 3) & ~int64_t(3), lower, vbytes);
+      };
       for (int64_t j = a; j < b;) {
-        const int64_t sz = off[size_t(j) + 1] - off[size_t(j)];
-        if (sz > cap) { chunks.push_back({int32_t(j), int32_t(j + 1), int32_t(a), kChunkDirect}); ++j; continue; }
-        int64_t e = j, tot = 0;
-        while (e < b && off[size_t(e) + 1] - off[size_t(e)] <= cap && tot + (off[size_t(e) + 1] - off[size_t(e)]) <= cap) {
-          tot += off[size_t(e) + 1] - off[size_t(e)];
-          ++e;
+        ChunkDev c{};
+        c.s0 = int32_t(j);
+        c.o0 = off[size_t(j)];
+        c.d0 = int64_t(sdesc.size());
+        c.rot = int32_t((j - a) % kTaskConsumers);
+        if (bytes(j, j + 1) > kTaskStageBytes) {
+          c.s1 = int32_t(j + 1);
+          c.flags = kChunkDirect;
+          chunks.push_back(c);
+          ++j;
+          continue;
         }
-        chunks.push_back({int32_t(j), int32_t(e), int32_t(a), 0});
+        int64_t e = j + 1;
+        while (e < b && bytes(j, e + 1) <= kTaskStageBytes) ++e;
+        c.s1 = int32_t(e);
+        c.nslot = int32_t(off[size_t(e)] - off[size_t(j)]);
+        c.r0 = int32_t(rs[size_t(j)] & ~int64_t(3));
+        c.r1 = int32_t((rs[size_t(e)] + 3) & ~int64_t(3));
+        for (int64_t i = j; i < e; ++i)
+          sdesc.push_back({int32_t(off[size_t(i)] - off[size_t(j)]), int32_t((off[size_t(i) + 1] - off[size_t(i)]) >> 5),
+                           int32_t(rs[size_t(i)]), int32_t(rs[size_t(i) + 1] - rs[size_t(i)])});
+        chunks.push_back(c);
         j = e;
       }
       chunks.back().flags |= kChunkLevelEnd;
@@ -860,13 +891,13 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
         TaskDev t{k, int32_t(chunks.size()), 0, 0, 0, 0};
         int64_t work = 0;
         for (auto &r : lv_l) {
-          add_level(S->loff_h, r.first, r.second);
+          add_level(S, true, r.first, r.second);
           work += S->loff_h[size_t(r.second)] - S->loff_h[size_t(r.first)] + 32 * (r.second - r.first);
         }
         t.cL1 = int32_t(chunks.size());
         t.cU0 = int32_t(chunks.size());
         for (auto &r : lv_u) {
-          add_level(S->uoff_h, r.first, r.second);
+          add_level(S, false, r.first, r.second);
           work += S->uoff_h[size_t(r.second)] - S->uoff_h[size_t(r.first)] + 32 * (r.second - r.first);
         }
         t.cU1 = int32_t(chunks.size());
@@ -1006,6 +1037,8 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   if (!d_tasks) return ctx.cuda_fail(e, "cudaMalloc tasks");
   d_chunks = arena.alloc(sizeof(ChunkDev) * std::max<size_t>(chunks.size(), 1), e);
   if (!d_chunks) return ctx.cuda_fail(e, "cudaMalloc chunks");
+  d_sdesc = arena.alloc(sizeof(SliceDesc) * std::max<size_t>(sdesc.size(), 1), e);
+  if (!d_sdesc) return ctx.cuda_fail(e, "cudaMalloc slice descriptors");
   d_ctasks = arena.alloc(sizeof(ClusterTask) * std::max<size_t>(ctasks.size(), 1), e);
   if (!d_ctasks) return ctx.cuda_fail(e, "cudaMalloc cluster tasks");
   ALLOC(d_clv, int64_t, std::max<size_t>(clv.size(), 1));
@@ -1060,6 +1093,7 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
   H2D(d_factdev, fd.data(), fd.size());
   if (!tasks.empty()) { H2D(d_tasks, tasks.data(), sizeof(TaskDev) * tasks.size()); }
   if (!chunks.empty()) { H2D(d_chunks, chunks.data(), sizeof(ChunkDev) * chunks.size()); }
+  if (!sdesc.empty()) { H2D(d_sdesc, sdesc.data(), sizeof(SliceDesc) * sdesc.size()); }
   if (!ctasks.empty()) { H2D(d_ctasks, ctasks.data(), sizeof(ClusterTask) * ctasks.size()); }
   if (!clv.empty()) { H2D(d_clv, clv.data(), sizeof(int64_t) * clv.size()); }
   if (has_pc) {
@@ -1241,8 +1275,8 @@ int Batch::factor(Ctx &ctx) {
 int Batch::launch_tasks(Ctx &ctx, int which) {
   cudaStream_t s = ctx.stream;
   if (task_kernel == 0)
-    return mixed ? vk_trsv_task_f32(ntasks, d_sysdev, d_state, d_active, d_tasks, d_chunks, which, d_bar, d_err, s)
-                 : vk_trsv_task_f64(ntasks, d_sysdev, d_state, d_active, d_tasks, d_chunks, which, d_bar, d_err, s);
+    return mixed ? vk_trsv_task_f32(ntasks, d_sysdev, d_state, d_active, d_tasks, d_chunks, d_sdesc, which, d_bar, d_err, s)
+                 : vk_trsv_task_f64(ntasks, d_sysdev, d_state, d_active, d_tasks, d_chunks, d_sdesc, which, d_bar, d_err, s);
   return mixed ? vk_trsv_cluster_f32(ntasks, task_kernel, d_sysdev, d_state, d_active, d_ctasks, d_clv, which, s)
                : vk_trsv_cluster_f64(ntasks, task_kernel, d_sysdev, d_state, d_active, d_ctasks, d_clv, which, s);
 }

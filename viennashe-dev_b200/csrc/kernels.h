@@ -50,8 +50,8 @@ void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles 
                     const VkLevels *lL, const VkLevels *lU, int which, unsigned *bar, int32_t *err, cudaStream_t s);    \
   int vk_trsv_occupancy_##SUF(int *blocks_per_sm);                                                                     \
   int vk_trsv_task_##SUF(int ntasks, const void *sys, const void *st, const int32_t *act, const void *tasks,          \
-                         const void *chunks, int which, const unsigned *bar, int32_t *err, cudaStream_t s);      \
-  int vk_task_stage_slots_##SUF(void);                                                                               \
+                         const void *chunks, const void *sdesc, int which, const unsigned *bar, int32_t *err,      \
+                         cudaStream_t s);                                                                           \
   int vk_trsv_cluster_##SUF(int ntasks, int csize, const void *sys, const void *st, const int32_t *act, const void *tasks, \
                             const int64_t *lv, int which, cudaStream_t s);                                           \
   void vk_split_factor_##SUF(int64_t nnz, int64_t n, const double *lu, const int64_t *fmap, const int64_t *diag,       \

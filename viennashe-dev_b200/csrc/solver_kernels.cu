@@ -716,36 +716,59 @@ __device__ __noinline__ void trsv_slice_direct(const SysDev<P> &S, int j, bool l
   a.finish();
 }
 
-constexpr int kTaskConsumers = 31;                          // warps that sum rows
 constexpr int kTaskThreads = 32 * (kTaskConsumers + 1);     // + one warp that issues the bulk copies
-constexpr int kStageBytes = 32768;                          // one chunk: its columns, then its values
-constexpr int kStages = 6;                                  // chunks in flight per CTA
-constexpr int kTaskG = 8;                                   // gathers of a row issued together (16 measured
-                                                            // 3.9x slower in FP32 on the 2D bar: register-bound)
-constexpr int kTaskSmem = kStages * kStageBytes;
+constexpr int kStages = 6;                                  // chunks in flight per CTA (4 measured 3.5x slower)
+// gathers of a row issued together: 4 with FP32 factor values (5 or more spill at 64 registers, and
+// 8 measured 13 % slower on the 2D bar), 8 with FP64 ones (3 % faster than 4)
 template <typename P>
-__host__ __device__ constexpr int stage_slots() { return (kStageBytes / int(4 + sizeof(P))) & ~31; }
+__host__ __device__ constexpr int task_gathers() { return sizeof(P) == 4 ? 4 : 8; }
+constexpr int kTaskSmem = kStages * kTaskStageBytes;
+
+// Row sum of one slice row from a stage: sum_k val[32 k] * src[col[32 k]] in index order with
+// FP64 FMAs, task_gathers<P>() gathers in flight; the values are read from shared memory as they
+// are multiplied (loading them into registers first measured 3.5x slower).
+template <typename P>
+__device__ __forceinline__ double task_row_sum(const double *src, const int32_t *cj, const P *vj, int width) {
+  constexpr int G = task_gathers<P>();
+  double sum = 0.0;
+  for (int k = 0; k < width; k += G) {
+    double xx[G];
+#pragma unroll
+    for (int u = 0; u < G; ++u) xx[u] = k + u < width ? __ldcg(src + cj[32 * (k + u)]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < G; ++u)
+      if (k + u < width) sum = fma((double)vj[32 * (k + u)], xx[u], sum);
+  }
+  return sum;
+}
 
 // The incomplete-LU apply of one task (a preconditioner block, or a whole system) on one CTA:
 // out = U^{-1} L^{-1} in over the task's SELL-32 slices, level after level, a CTA barrier
-// between levels instead of a grid barrier.  The factor columns and values of a level do not
-// depend on the sweep, so one producer thread streams them chunk by chunk into a ring of
-// kStages shared-memory stages with bulk copies (chunks of later levels are in flight while
-// the consumer warps work on the current one), and the consumer warps read them from there.
-// Slice j of a level is summed by consumer warp (j - level's first slice) mod kTaskConsumers,
-// one row per lane, in index order with FP64 FMAs: the same arithmetic as k_trsv_persistent,
-// so both give bitwise the same results.  The gathers of solved values (written by other warps
-// of this CTA before the last CTA barrier) read through L2.  Grid = one CTA per task, tasks
-// ordered by decreasing work, so the CTAs that start late take the smallest tasks.  Every wait
-// is bounded (bar[2..3] polls); after a failed wait a consumer stops reading the stages but keeps
-// arriving on the barriers, and the producer stops issuing and drains its copies in flight.
+// between levels instead of a grid barrier.  Everything a slice needs except the solved values
+// it gathers -- its descriptor (slot offset, width, rows), the factor columns and values, and its
+// rows' operands (the input vector's entries in the forward sweep; urow and udinv in the
+// backward sweep) -- does not depend on the sweep, so one producer thread streams it chunk by
+// chunk (the layout of solver_kernels.cuh) into a ring of kStages shared-memory stages with bulk
+// copies, chunks of later levels in flight while the consumer warps work on the current one.
+// A consumer then reads global memory only for the gathers of solved values and, in the
+// backward sweep, its row's forward result.
+// Slice j of a chunk is summed by consumer warp (rot + j - s0) mod kTaskConsumers, one row per
+// lane, in index order with FP64 FMAs: the same arithmetic as k_trsv_persistent, so both give
+// bitwise the same results.  The gathers of solved values (written by other warps of this CTA
+// before the last CTA barrier) read through L2.  Grid = one CTA per task, tasks ordered by
+// decreasing work, so the CTAs that start late take the smallest tasks.  Every wait is bounded
+// (bar[2..3] polls); after a failed wait a consumer stops reading the stages but keeps arriving
+// on the barriers and taking the level barriers (their sequence comes from the chunk flags in
+// global memory, never from a stage), and the producer stops issuing and drains its copies in
+// flight.
 template <typename P>
 __global__ void __launch_bounds__(kTaskThreads, 1) k_trsv_task(const SysDev<P> *sys, const BiState *st, const int32_t *active,
-                                                                const TaskDev *tasks, const ChunkDev *chunks, int which,
-                                                                const unsigned *bar, int32_t *err) {
+                                                                const TaskDev *tasks, const ChunkDev *chunks,
+                                                                const SliceDesc *sdesc, int which, const unsigned *bar,
+                                                                int32_t *err) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
-  constexpr int CAP = stage_slots<P>();
+  __shared__ int4 smeta[kStages][2];  // per stage: (s0, s1, rot, r0), (values, rows, udinv byte offsets, flags)
   const TaskDev T = tasks[blockIdx.x];
   const int s = T.sys;
   if (!active[s] || st[s].done || (which == 1 && st[s].s_conv)) return;
@@ -758,6 +781,7 @@ __global__ void __launch_bounds__(kTaskThreads, 1) k_trsv_task(const SysDev<P> *
   __syncthreads();
   const int nL = T.cL1 - T.cL0, nch = nL + (T.cU1 - T.cU0);
   const unsigned long long spin_limit = spin_limit_of(bar);
+  const double *in = which == 0 ? S.p : S.s;
 
   if (warp == kTaskConsumers) {
     // producer: one thread issues the chunks in sweep order, each into the stage its
@@ -770,14 +794,24 @@ __global__ void __launch_bounds__(kTaskThreads, 1) k_trsv_task(const SysDev<P> *
       const int stg = g % kStages, round = g / kStages;
       if (round > 0 && !mbar_wait(&empty[stg], (round - 1) & 1, spin_limit, err)) break;
       if (*((volatile int32_t *)err) != 0) break;  // after a failed wait the stages may hold copies in flight
-      const int64_t *off = lower ? S.loff : S.uoff;
-      const int64_t o0 = off[c.s0];
-      const unsigned nslot = (unsigned)(off[c.s1] - o0);
-      if ((c.flags & kChunkDirect) || nslot == 0) { mbar_arrive(&full[stg]); issued = g + 1; continue; }
-      unsigned char *base = smem + stg * kStageBytes;
-      mbar_arrive_expect_tx(&full[stg], nslot * (4u + (unsigned)sizeof(P)));
-      bulk_g2s(base, (lower ? S.lcol : S.ucol) + o0, nslot * 4u, &full[stg]);
-      bulk_g2s(base + CAP * 4, (lower ? S.lval : S.uval) + o0, nslot * (unsigned)sizeof(P), &full[stg]);
+      const unsigned ns = (unsigned)(c.s1 - c.s0), nslot = (unsigned)c.nslot, nrow = (unsigned)(c.r1 - c.r0);
+      const unsigned offA = 16u * ns, offB = offA + 4u * nslot, offC = offB + (unsigned)sizeof(P) * nslot, offD = offC + 4u * nrow;
+      smeta[stg][0] = make_int4(c.s0, c.s1, c.rot, c.r0);
+      smeta[stg][1] = make_int4((int)offB, (int)offC, (int)offD, c.flags);
+      if (c.flags & kChunkDirect) { mbar_arrive(&full[stg]); issued = g + 1; continue; }
+      unsigned char *base = smem + stg * kTaskStageBytes;
+      mbar_arrive_expect_tx(&full[stg], offC + nrow * (lower ? 8u : 4u + (unsigned)sizeof(P)));
+      bulk_g2s(base, sdesc + c.d0, offA, &full[stg]);
+      if (nslot) {
+        bulk_g2s(base + offA, (lower ? S.lcol : S.ucol) + c.o0, 4u * nslot, &full[stg]);
+        bulk_g2s(base + offB, (lower ? S.lval : S.uval) + c.o0, (unsigned)sizeof(P) * nslot, &full[stg]);
+      }
+      if (lower) {
+        bulk_g2s(base + offC, in + c.r0, 8u * nrow, &full[stg]);
+      } else {
+        bulk_g2s(base + offC, S.urow + c.r0, 4u * nrow, &full[stg]);
+        bulk_g2s(base + offD, S.udinv + c.r0, (unsigned)sizeof(P) * nrow, &full[stg]);
+      }
       issued = g + 1;
     }
     // leave only once this thread's copies have landed: every chunk before the last kStages
@@ -788,65 +822,61 @@ __global__ void __launch_bounds__(kTaskThreads, 1) k_trsv_task(const SysDev<P> *
   }
 
   // consumers
-  const double *in = which == 0 ? S.p : S.s;
   double *out = which == 0 ? S.ph : S.sh;
   double *ytmp = S.ytmp;
   bool ok = true;
   for (int g = 0; g < nch; ++g) {
     const bool lower = g < nL;
-    const ChunkDev c = chunks[lower ? T.cL0 + g : T.cU0 + (g - nL)];
     const int stg = g % kStages;
     if (ok && !mbar_wait(&full[stg], (g / kStages) & 1, spin_limit, err)) ok = false;
+    // the chunk's flags: from its stage, or from global memory once a wait has failed (the stage
+    // may then be stale, and every consumer warp must take the same level barriers)
+    int32_t flags;
     if (ok) {
-      const int64_t *off = lower ? S.loff : S.uoff;
-      const int64_t o0 = off[c.s0];
-      const int32_t *scol = (const int32_t *)(smem + stg * kStageBytes);
-      const P *sval = (const P *)(smem + stg * kStageBytes + CAP * 4);
-      int j = c.s0 + ((warp - (c.s0 - c.lvl_s0) % kTaskConsumers) + kTaskConsumers) % kTaskConsumers;
-      for (; j < c.s1; j += kTaskConsumers) {
-        if (c.flags & kChunkDirect) { trsv_slice_direct<P>(S, j, lower, which); continue; }
-        const int64_t oj = off[j];
-        const int width = (int)((off[j + 1] - oj) >> 5);
-        const double *src;
-        double *dst;
-        int32_t row = 0;
-        int nr;
-        double base = 0.0, dinv = 1.0;
+      const int4 m0 = smeta[stg][0], m1 = smeta[stg][1];
+      flags = m1.w;
+      const int s0 = m0.x, s1 = m0.y;
+      int j = s0 + (warp - m0.z + kTaskConsumers) % kTaskConsumers;
+      if (flags & kChunkDirect) {
+        for (; j < s1; j += kTaskConsumers) trsv_slice_direct<P>(S, j, lower, which);
+      } else {
+        const unsigned char *stage = smem + stg * kTaskStageBytes;
+        const int4 *sd = (const int4 *)stage;
+        const int32_t *scol = (const int32_t *)(stage + 16 * (s1 - s0));
+        const P *sval = (const P *)(stage + m1.x);
         if (lower) {
-          const int32_t q0 = S.lrow0[j];
-          nr = S.lrow0[j + 1] - q0;
-          row = q0 + lane;
-          if (lane < nr) base = __ldcs(in + row);
-          src = ytmp; dst = ytmp;
-        } else {
-          const int32_t t0 = S.uslot0[j];
-          nr = S.uslot0[j + 1] - t0;
-          if (lane < nr) {
-            row = __ldcs(S.urow + t0 + lane);
-            dinv = (double)__ldcs(S.udinv + t0 + lane);
-            base = __ldcg(ytmp + row);
+          const double *sin = (const double *)(stage + m1.y);
+          for (; j < s1; j += kTaskConsumers) {
+            const int4 d = sd[j - s0];
+            const int row = d.z + lane;
+            const double base = lane < d.w ? sin[row - m0.w] : 0.0;
+            const double sum = task_row_sum<P>(ytmp, scol + d.x + lane, sval + d.x + lane, d.y);
+            if (lane < d.w) ytmp[row] = base - sum;
           }
-          src = out; dst = out;
+        } else {
+          const int32_t *surow = (const int32_t *)(stage + m1.y);
+          const P *sdinv = (const P *)(stage + m1.z);
+          for (; j < s1; j += kTaskConsumers) {
+            const int4 d = sd[j - s0];
+            int32_t row = 0;
+            double base = 0.0, dinv = 1.0;
+            if (lane < d.w) {
+              const int t = d.z + lane - m0.w;
+              row = surow[t];
+              dinv = (double)sdinv[t];
+              base = __ldcg(ytmp + row);
+            }
+            const double sum = task_row_sum<P>(out, scol + d.x + lane, sval + d.x + lane, d.y);
+            if (lane < d.w) out[row] = (base - sum) * dinv;
+          }
         }
-        const int32_t *cj = scol + (oj - o0) + lane;
-        const P *vj = sval + (oj - o0) + lane;
-        double sum = 0.0;
-        // kTaskG gathers in flight per lane; the values are read from shared memory as they are
-        // multiplied, in index order (loading them into registers first measured 3.5x slower)
-        for (int k = 0; k < width; k += kTaskG) {
-          double xx[kTaskG];
-#pragma unroll
-          for (int u = 0; u < kTaskG; ++u) xx[u] = k + u < width ? __ldcg(src + cj[32 * (k + u)]) : 0.0;
-#pragma unroll
-          for (int u = 0; u < kTaskG; ++u)
-            if (k + u < width) sum = fma((double)vj[32 * (k + u)], xx[u], sum);
-        }
-        if (lane < nr) dst[row] = (base - sum) * dinv;
       }
+    } else {
+      flags = chunks[lower ? T.cL0 + g : T.cU0 + (g - nL)].flags;
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[stg]);
-    if (c.flags & kChunkLevelEnd) consumers_sync(32 * kTaskConsumers);
+    if (flags & kChunkLevelEnd) consumers_sync(32 * kTaskConsumers);
   }
 }
 
@@ -1197,7 +1227,8 @@ void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles 
 
 #define VK_BODY_P(P, SUF)                                                                                             \
   int vk_trsv_task_##SUF(int ntasks, const void *sys, const void *st, const int32_t *act, const void *tasks,          \
-                         const void *chunks, int which, const unsigned *bar, int32_t *err, cudaStream_t s) {      \
+                         const void *chunks, const void *sdesc, int which, const unsigned *bar, int32_t *err,      \
+                         cudaStream_t s) {                                                                          \
     static bool attr = false;                                                                                        \
     if (!attr) {                                                                                                     \
       cudaError_t e = cudaFuncSetAttribute((const void *)k_trsv_task<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
@@ -1207,11 +1238,10 @@ void vk_precond_copy(int ntiles, const void *sys, const void *st, const VkTiles 
     }                                                                                                                \
     g_launches += 1;                                                                                                 \
     k_trsv_task<P><<<ntasks, kTaskThreads, kTaskSmem, s>>>((const SysDev<P> *)sys, (const BiState *)st, act,         \
-                                                           (const TaskDev *)tasks, (const ChunkDev *)chunks, which,   \
-                                                           bar, err);                                                 \
+                                                           (const TaskDev *)tasks, (const ChunkDev *)chunks,          \
+                                                           (const SliceDesc *)sdesc, which, bar, err);                \
     return (int)cudaGetLastError();                                                                                  \
   }                                                                                                                  \
-  int vk_task_stage_slots_##SUF(void) { return stage_slots<P>(); }                                                  \
   int vk_trsv_cluster_##SUF(int ntasks, int csize, const void *sys, const void *st, const int32_t *act, const void *tasks, \
                             const int64_t *lv, int which, cudaStream_t s) {                                          \
     cudaLaunchConfig_t cfg = {};                                                                                     \

@@ -99,19 +99,44 @@ struct FactDev {
 // Sweep tasks.  A task is one independent unit of the incomplete-LU apply that one CTA walks
 // alone: a preconditioner block of one system (an energy slab of block-ILU: its factor has no
 // entry outside the block, so blocks sweep independently), or a whole system.  Its forward
-// (L) and backward (U) sweeps are lists of chunks [cL0, cL1) and [cU0, cU1): a chunk is a run of
-// consecutive SELL slices [s0, s1) of one level (lvl_s0 = the level's first slice in the task)
-// whose factor slots fit one shared-memory stage and are staged there by bulk copies, or one
-// slice wider than a stage (kChunkDirect: read from global memory).  kChunkLevelEnd marks the
-// last chunk of a level: the CTA synchronises before the next level.
+// (L) and backward (U) sweeps are lists of chunks [cL0, cL1) and [cU0, cU1).
+//
+// A chunk is a run of consecutive SELL slices [s0, s1) of one level whose operands fit one
+// shared-memory stage of kTaskStageBytes, staged there by bulk copies in this layout (byte
+// offsets, each a multiple of 16):
+//   [0, 16 ns)                       ns = s1 - s0 slice descriptors (SliceDesc), from desc + d0
+//   [16 ns, +4 nslot)                factor columns of the chunk's slots [o0, o0 + nslot)
+//   [.., +sizeof(P) nslot)           factor values of the same slots
+//   [.., ..)                         forward sweep: the input vector's rows [r0, r1) (FP64);
+//                                    backward sweep: urow[r0, r1), then udinv[r0, r1)
+// r0 and r1 are the chunk's first row (L) or slot (U) rounded down, and its end rounded up, to
+// a multiple of 4, so that every copy starts and ends on a 16-byte boundary.  A slice too wide
+// for a stage is a chunk of its own (kChunkDirect) and is read from global memory.
+// kChunkLevelEnd marks the last chunk of a level: the CTA synchronises before the next level.
+// rot = (s0 - first slice of the level) mod the consumer warps: slice j of the chunk is summed by
+// consumer warp (rot + j - s0) mod the consumer warps, so the slices of a level go round the warps.
 constexpr int32_t kChunkLevelEnd = 1;
 constexpr int32_t kChunkDirect = 2;
+constexpr int32_t kTaskStageBytes = 32768;
+constexpr int32_t kTaskConsumers = 31;  // consumer warps of k_trsv_task (one more warp issues the copies)
 struct TaskDev {
   int32_t sys, cL0, cL1, cU0, cU1, pad;
 };
 struct ChunkDev {
-  int32_t s0, s1, lvl_s0, flags;
+  int32_t s0, s1, flags, nslot;
+  int64_t o0, d0;
+  int32_t r0, r1, rot, pad;
 };
+struct SliceDesc {
+  int32_t soff;   // first slot of the slice, relative to the chunk's o0
+  int32_t width;  // entries per row (slots / 32)
+  int32_t r0;     // first solver row (L) or slot (U) of the slice
+  int32_t nr;     // rows of the slice (at most 32)
+};
+// Bytes one chunk occupies in a stage (the layout above), for factor values of `vbytes` bytes.
+inline constexpr int64_t task_chunk_bytes(int64_t ns, int64_t nslot, int64_t r0, int64_t r1, bool lower, int vbytes) {
+  return 16 * ns + (4 + vbytes) * nslot + (r1 - r0) * (lower ? 8 : 4 + vbytes);
+}
 
 // Cluster sweep tasks (k_trsv_cluster): the same units as TaskDev, walked by one thread-block
 // cluster each, level by level, with the slices of level k of the forward (backward) sweep in
