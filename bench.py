@@ -324,14 +324,16 @@ def measure_batched_sweep(ctx, reps=3):
 
 def served_options(dev, cfg):
     """Solver options per request class (measured): 1D devices natural-order ILU(0) over the whole
-    system; 2D bars at L <= 3 node-coloured block-ILU(0) per energy slab; 2D bars at L = 5, where
-    ILU(0) stalls in every order, ILUT with the reference's defaults (60 entries, drop 1e-4:
-    viennashe/solvers/config.hpp:62-63), which the oracle converges on the smaller of the mix's two
-    L = 5 bars and not on the larger; the server's stagnation stop ends a request that stalls."""
+    system; 2D bars at L <= 3 node-coloured block-ILU(0) per energy slab; 2D bars at L = 5
+    node-coloured block-ILU(1) per energy slab, ended by the server's stagnation stop where it
+    stalls.  ILUT with the reference's defaults (60 entries, drop 1e-4:
+    viennashe/solvers/config.hpp:62-63) is not served here: on the smaller L = 5 bar of the mix
+    (1,064,868 unknowns) its pattern takes 50 s of serial host elimination and its natural-order
+    factor 20,462 forward levels, so one request would hold the server for minutes."""
     if dev.dim == 1:
         return dict(ordering="natural", precond="ilu0")
     if cfg.max_expansion_order >= 5:
-        return dict(ordering="natural", precond="ilut", ilut_entries=60, ilut_drop=1e-4)
+        return dict(ordering="multicolor", precond="block_ilu0", fill_level=1)
     return dict(ordering="multicolor", precond="block_ilu0")
 
 

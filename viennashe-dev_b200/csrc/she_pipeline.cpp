@@ -687,7 +687,8 @@ int vshe_she_run_batch(vshe_ctx *ctx, int32_t count, const int64_t *handles, vsh
 // A request is a device description + SHE configuration (+ solver options).  Its arrays are
 // copied at submission.  One worker thread per server admits queued requests in arrival
 // order while the HBM the resident problems hold stays within the budget (and at most
-// max_active are resident), sets each one up on the device (host set-up of the (x, H) space,
+// max_active are resident), a quarter second of set-up per scheduling step at most while
+// others are resident, sets each one up on the device (host set-up of the (x, H) space,
 // device assembly, odd elimination, normalisation, ILU(0) factorisation) and then iterates all
 // resident systems together, chunk by chunk, in one batch (shared launches of the SELL SpMV,
 // the sweeps and the vector kernels).  After every chunk a converged member leaves the batch:
@@ -760,12 +761,20 @@ void Server::complete(ServeRequest *r, int status) {
   cv.notify_all();
 }
 
-// Admits queued requests while memory and slots allow; returns the first error of a set-up.
+// Admits queued requests while memory and slots allow, for at most kAdmitSliceMs of set-up per
+// step once a request is resident or admitted in this step (then the residents iterate and the
+// rest of the queue is admitted in later steps, so that a long set-up at the back of the queue
+// does not hold up the requests in front of it); returns the first error of a set-up.
+constexpr double kAdmitSliceMs = 250.0;
 int Server::admit(std::vector<ServeRequest *> &fresh) {
   Ctx &c = *ctx;
   size_t held = 0;
   for (ServeRequest *r : active) held += problem_bytes(r->prob.get());
+  const auto t0 = std::chrono::steady_clock::now();
   while (true) {
+    if ((!active.empty() || !fresh.empty()) &&
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() > kAdmitSliceMs)
+      break;
     ServeRequest *r = nullptr;
     {
       std::lock_guard<std::mutex> lk(mu);

@@ -717,7 +717,7 @@ __device__ __noinline__ void trsv_slice_direct(const SysDev<P> &S, int j, bool l
 }
 
 constexpr int kTaskThreads = 32 * (kTaskConsumers + 1);     // + one warp that issues the bulk copies
-constexpr int kStages = 6;                                  // chunks in flight per CTA (4 measured 3.5x slower)
+constexpr int kStages = 3;                                  // chunks of 64 KB in flight per CTA (6 of 32 KB: 3.5 % slower)
 // gathers of a row issued together: 4 with FP32 factor values (5 or more spill at 64 registers, and
 // 8 measured 13 % slower on the 2D bar), 8 with FP64 ones (3 % faster than 4)
 template <typename P>

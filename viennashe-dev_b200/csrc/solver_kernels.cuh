@@ -117,7 +117,7 @@ struct FactDev {
 // consumer warp (rot + j - s0) mod the consumer warps, so the slices of a level go round the warps.
 constexpr int32_t kChunkLevelEnd = 1;
 constexpr int32_t kChunkDirect = 2;
-constexpr int32_t kTaskStageBytes = 32768;
+constexpr int32_t kTaskStageBytes = 65536;
 constexpr int32_t kTaskConsumers = 31;  // consumer warps of k_trsv_task (one more warp issues the copies)
 struct TaskDev {
   int32_t sys, cL0, cL1, cU0, cU1, pad;
