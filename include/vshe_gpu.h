@@ -314,7 +314,8 @@ int vshe_she_free(vshe_ctx *ctx, int64_t handle);
  * No reference counterpart: the reference solves one device at a time (simulator::run).  A
  * server owns a worker thread that admits submitted requests in arrival order while the device
  * memory of its resident problems stays within hbm_budget and at most max_active are resident
- * (with problems resident, a quarter second of set-up per scheduling step at most, so that the
+ * (with problems resident, a quarter second of set-up per scheduling step at most, and the host
+ * layout of a request of 262,144 or more reduced unknowns on a thread of its own, so that the
  * residents keep iterating while a long queue is set up), iterates all resident problems together (one batch, chunks of check_every iterations), and
  * retires each one as soon as it converges, its place taken by the next request.  A served
  * result equals the result of the same request solved alone (per-system reductions in a fixed

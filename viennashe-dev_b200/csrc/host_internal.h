@@ -112,6 +112,11 @@ struct System {
                       int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o, const double *host_val = nullptr);
   int set_values(Ctx &ctx, const double *v, const double *rhs);
   int setup_pattern(Ctx &ctx, const double *host_val);  // ordering, schedules, device buffers
+  // the two halves of create_borrowed: the host copies of the pattern and the device pointers,
+  // and (after Layout::build on those copies, which needs no device) the device buffers
+  int init_borrowed(Ctx &ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, int64_t *d_rp_,
+                    int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o);
+  int setup_from_layout(Ctx &ctx, const Layout &Lt);
   // gathers the caller-order values and rhs into the solver-order SELL A, the factorisation
   // CSR and b_p (on the context's stream)
   void prepare(Ctx &ctx);

@@ -132,6 +132,13 @@ int System::create(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_, const
 
 int System::create_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_, const int32_t *ci_, int64_t *d_rp_,
                             int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o, const double *host_val) {
+  int rc = init_borrowed(ctx, n_, nnz_, rp_, ci_, d_rp_, d_ci_, d_val, d_rhs, o);
+  if (rc) return rc;
+  return setup_pattern(ctx, host_val);
+}
+
+int System::init_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_, const int32_t *ci_, int64_t *d_rp_,
+                          int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o) {
   n = n_; nnz = nnz_; opts = o; borrowed = true;
   if (n <= 0 || nnz <= 0) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "empty system");
   if (n >= (int64_t(1) << 31) - 64) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "more than 2^31 - 64 rows");
@@ -141,7 +148,7 @@ int System::create_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *r
     if (rp[i + 1] == rp[i]) return ctx.fail(VSHE_E_EMPTY_ROW, "row " + std::to_string(i));
   d_rp = d_rp_; d_ci = d_ci_; d_av64 = d_val; d_b64 = d_rhs;
   bnorm_host = 1.0;  // the trivial-rhs test uses the device-side norm
-  return setup_pattern(ctx, host_val);
+  return VSHE_OK;
 }
 
 int System::set_values(Ctx &ctx, const double *v, const double *rhs) {
@@ -651,13 +658,17 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
 }
 
 int System::setup_pattern(Ctx &ctx, const double *host_val) {
-  has_pc = opts.precond != VSHE_PRECOND_NONE;
-  mixed = opts.precision == VSHE_PRECISION_MIXED;
-  cudaError_t e;
   Layout Lt;
   std::string err;
   int rc = Lt.build(n, nnz, rp, ci, opts, host_val, err);
   if (rc) return ctx.fail(rc, err);
+  return setup_from_layout(ctx, Lt);
+}
+
+int System::setup_from_layout(Ctx &ctx, const Layout &Lt) {
+  has_pc = opts.precond != VSHE_PRECOND_NONE;
+  mixed = opts.precision == VSHE_PRECISION_MIXED;
+  cudaError_t e;
   perm = Lt.perm; blk = Lt.blk; lvr = Lt.lvr; lvsL = Lt.lvsL; lvsU = Lt.lvsU;
   lgrp_s0 = Lt.lgrp_s0; lgrp_lev = Lt.lgrp_lev; lgrp_blk = Lt.lgrp_blk;
   ugrp_s0 = Lt.ugrp_s0; ugrp_lev = Lt.ugrp_lev; ugrp_blk = Lt.ugrp_blk;

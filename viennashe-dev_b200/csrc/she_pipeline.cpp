@@ -47,13 +47,24 @@ struct SheProblem {
   std::vector<int64_t> slab_ptr;
   std::unique_ptr<System> sys;
   std::unique_ptr<Batch> batch;
+  // between create_device_pattern and create_device_finish: the solver options with the node
+  // colouring and slab bounds they point at, the values ILUT's pattern needs, the layout
+  vshe_solve_opts so_{};
+  std::vector<int32_t> node_perm_;
+  std::vector<double> hval_;
+  std::unique_ptr<Layout> layout_;
+  int layout_rc_ = 0;
+  std::string layout_err_;
   double full_residual = -1.0;
   int stage = 0;
 
   int create(Ctx &ctx, const vshe_device_desc &d, const vshe_she_config &c, const vshe_coupling_tables &ct, const vshe_solve_opts &o);
   int setup_host(Ctx &ctx, const vshe_device_desc &d, const vshe_she_config &c, const vshe_coupling_tables &ct, const vshe_solve_opts &o);
   size_t estimate_bytes() const;
-  int create_device(Ctx &ctx);
+  int create_device(Ctx &ctx);  // = create_device_pattern, build_layout, create_device_finish
+  int create_device_pattern(Ctx &ctx);
+  void build_layout();
+  int create_device_finish(Ctx &ctx);
   int symbolic_full(Ctx &ctx);
   int fill_full(Ctx &ctx);
   int assemble(Ctx &ctx, int upto);
@@ -131,6 +142,14 @@ size_t SheProblem::estimate_bytes() const {
 }
 
 int SheProblem::create_device(Ctx &ctx) {
+  int rc = create_device_pattern(ctx);
+  if (rc) return rc;
+  build_layout();
+  return create_device_finish(ctx);
+}
+
+// Device set-up up to the reduced system's pattern on the host (the system's host copies).
+int SheProblem::create_device_pattern(Ctx &ctx) {
   int rc = 0;
   cudaError_t e;
 #define UP(dst, vec) dst = upload(ctx, arena, vec, rc); if (rc) return rc;
@@ -241,8 +260,9 @@ int SheProblem::create_device(Ctx &ctx) {
   if ((e = cudaMemcpyAsync(hrp.data(), d_rrp, sizeof(int64_t) * hrp.size(), cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "pattern");
   if ((e = cudaMemcpyAsync(hci.data(), d_rci, sizeof(int32_t) * hci.size(), cudaMemcpyDeviceToHost, ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "pattern");
   if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "pattern");
-  vshe_solve_opts so = opts;
-  std::vector<int32_t> node_perm;
+  vshe_solve_opts &so = so_;
+  so = opts;
+  std::vector<int32_t> &node_perm = node_perm_;
   if (so.ordering == VSHE_ORDER_MULTICOLOR && !so.perm && so.precond != VSHE_PRECOND_NONE) {
     // Colour the (cell, H) nodes so that no two coupled nodes share a colour: cells by a
     // greedy colouring of the mesh graph, energies by the parity of H / n_op (in-scattering
@@ -289,7 +309,7 @@ int SheProblem::create_device(Ctx &ctx) {
     so.n_blocks = int64_t(slab_ptr.size()) - 1;
     so.block_ptr = slab_ptr.data();
   }
-  std::vector<double> hval;
+  std::vector<double> &hval = hval_;
   if (so.precond == VSHE_PRECOND_ILUT) {
     // the ILUT pattern is found from the values of this first assembly
     hval.resize((size_t)nnz_red);
@@ -297,10 +317,27 @@ int SheProblem::create_device(Ctx &ctx) {
     if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess) return ctx.cuda_fail(e, "values");
   }
   sys.reset(new System);
-  rc = sys->create_borrowed(ctx, n_red, nnz_red, hrp.data(), hci.data(), d_rrp, d_rci, d_rval, d_rrhs, so, hval.empty() ? nullptr : hval.data());
+  return sys->init_borrowed(ctx, n_red, nnz_red, hrp.data(), hci.data(), d_rrp, d_rci, d_rval, d_rrhs, so);
+}
+
+// The solver layout of the reduced system (ordering, ILU(k) or ILUT pattern, level schedules,
+// SELL tables) from its host pattern: host work only, no device or context call, so it may run
+// on another thread while the context serves other work.
+void SheProblem::build_layout() {
+  layout_.reset(new Layout);
+  layout_rc_ = layout_->build(sys->n, sys->nnz, sys->rp, sys->ci, sys->opts, hval_.empty() ? nullptr : hval_.data(), layout_err_);
+}
+
+// Device buffers of the reduced system from the layout, and the problem's own batch.
+int SheProblem::create_device_finish(Ctx &ctx) {
+  if (!layout_) return ctx.fail(VSHE_E_INVALID_ARGUMENT, "layout not built");
+  int rc = layout_rc_ ? ctx.fail(layout_rc_, layout_err_) : sys->setup_from_layout(ctx, *layout_);
+  layout_.reset();
+  std::vector<double>().swap(hval_);
   if (rc) return rc;
   sys->opts.block_ptr = nullptr;  // the pointers above are only read during creation
   sys->opts.perm = nullptr;
+  std::vector<int32_t>().swap(node_perm_);
   batch.reset(new Batch);
   std::vector<System *> mem{sys.get()};
   return batch->build(ctx, mem);
@@ -688,7 +725,8 @@ int vshe_she_run_batch(vshe_ctx *ctx, int32_t count, const int64_t *handles, vsh
 // copied at submission.  One worker thread per server admits queued requests in arrival
 // order while the HBM the resident problems hold stays within the budget (and at most
 // max_active are resident), a quarter second of set-up per scheduling step at most while
-// others are resident, sets each one up on the device (host set-up of the (x, H) space,
+// others are resident (the host layout of a large request on a thread of its own), sets each
+// one up on the device (host set-up of the (x, H) space,
 // device assembly, odd elimination, normalisation, ILU(0) factorisation) and then iterates all
 // resident systems together, chunk by chunk, in one batch (shared launches of the SELL SpMV,
 // the sweeps and the vector kernels).  After every chunk a converged member leaves the batch:
@@ -698,6 +736,7 @@ int vshe_she_run_batch(vshe_ctx *ctx, int32_t count, const int64_t *handles, vsh
 // not depend on the batch (per-system reductions in a fixed order, per-system tiles), so a
 // result in the mix equals the same request served alone.
 // =======================================================================
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -723,6 +762,9 @@ struct ServeRequest {
   bool collected = false;   // the caller has its result: the worker may free the record
   int replacements = 0;
   bool needs_start = true;
+  size_t need = 0;                       // the footprint bound it was admitted with
+  std::thread layout_thread;             // host layout of a large request, off the worker thread
+  std::atomic<bool> layout_done{false};
   // stagnation watch: the best recursive residual so far and the iteration it was reached at
   double best_res = 1e300;
   int best_iter = 0;
@@ -738,6 +780,7 @@ struct Server {
   std::deque<ServeRequest *> pending;
   std::map<int64_t, std::unique_ptr<ServeRequest>> all;
   std::vector<ServeRequest *> active;
+  std::vector<ServeRequest *> setting_up;  // admitted, host layout running on its own thread
   std::unique_ptr<Batch> batch;
   int64_t next_ticket = 0;
   std::thread worker;
@@ -745,6 +788,8 @@ struct Server {
 
   void run();
   int admit(std::vector<ServeRequest *> &fresh);
+  int finish_setup(ServeRequest *r);
+  void end_setting_up(int status);
   int step();
   void complete(ServeRequest *r, int status);
 };
@@ -762,23 +807,67 @@ void Server::complete(ServeRequest *r, int status) {
 }
 
 // Admits queued requests while memory and slots allow, for at most kAdmitSliceMs of set-up per
-// step once a request is resident or admitted in this step (then the residents iterate and the
-// rest of the queue is admitted in later steps, so that a long set-up at the back of the queue
-// does not hold up the requests in front of it); returns the first error of a set-up.
+// step once a request is resident, admitted in this step or being set up (then the residents
+// iterate and the rest of the queue is admitted in later steps, so that a long set-up at the
+// back of the queue does not hold up the requests in front of it); returns the first error of
+// a set-up.  The host layout of a request with at least kAsyncLayoutRows reduced unknowns (its
+// ordering, ILU(k) or ILUT pattern and level schedules: seconds of host work for millions of
+// rows) runs on a thread of its own; the request joins the batch in the first step after it.
 constexpr double kAdmitSliceMs = 250.0;
+constexpr int64_t kAsyncLayoutRows = int64_t(1) << 18;
+
+// Device set-up after the layout: device buffers, assembly, factorisation.
+int Server::finish_setup(ServeRequest *r) {
+  Ctx &c = *ctx;
+  SheProblem *S = r->prob.get();
+  int rc = S->create_device_finish(c);
+  if (!rc) rc = S->assemble(c, 3);
+  if (!rc) {
+    S->sys->prepare(c);
+    rc = S->batch->autotune_tiles(c);
+  }
+  if (!rc) rc = S->batch->factor(c);
+  if (rc) { r->res.status = rc; return rc; }
+  r->res.n_unknowns = S->n_red;
+  r->phase = 1;
+  r->needs_start = true;
+  return VSHE_OK;
+}
+
+// Waits for every running layout thread and ends its request with `status`.
+void Server::end_setting_up(int status) {
+  for (ServeRequest *r : setting_up) {
+    if (r->layout_thread.joinable()) r->layout_thread.join();
+    r->res.status = status;
+    complete(r, status);
+  }
+  setting_up.clear();
+}
+
 int Server::admit(std::vector<ServeRequest *> &fresh) {
   Ctx &c = *ctx;
   size_t held = 0;
   for (ServeRequest *r : active) held += problem_bytes(r->prob.get());
+  for (ServeRequest *r : setting_up) held += r->need;
+  // requests whose layout has finished
+  for (auto it = setting_up.begin(); it != setting_up.end();) {
+    ServeRequest *r = *it;
+    if (!r->layout_done.load()) { ++it; continue; }
+    r->layout_thread.join();
+    it = setting_up.erase(it);
+    const int rc = finish_setup(r);
+    if (rc) { held -= r->need; complete(r, rc); continue; }
+    fresh.push_back(r);
+  }
   const auto t0 = std::chrono::steady_clock::now();
   while (true) {
-    if ((!active.empty() || !fresh.empty()) &&
+    if ((!active.empty() || !fresh.empty() || !setting_up.empty()) &&
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() > kAdmitSliceMs)
       break;
     ServeRequest *r = nullptr;
     {
       std::lock_guard<std::mutex> lk(mu);
-      if (pending.empty() || int(active.size() + fresh.size()) >= opts.max_active) break;
+      if (pending.empty() || int(active.size() + fresh.size() + setting_up.size()) >= opts.max_active) break;
       r = pending.front();
     }
     // the host set-up and the footprint bound first: nothing is allocated on the device for a
@@ -786,7 +875,7 @@ int Server::admit(std::vector<ServeRequest *> &fresh) {
     std::unique_ptr<SheProblem> S(new SheProblem);
     int rc = S->setup_host(c, r->d, r->c, r->t, r->o);
     const size_t need = rc ? 0 : S->estimate_bytes();
-    if (!rc && held + need > opts.hbm_budget && !(active.empty() && fresh.empty())) {
+    if (!rc && held + need > opts.hbm_budget && !(active.empty() && fresh.empty() && setting_up.empty())) {
       break;  // wait for resident problems to finish
     }
     {
@@ -795,19 +884,25 @@ int Server::admit(std::vector<ServeRequest *> &fresh) {
     }
     r->t_admit = std::chrono::steady_clock::now();
     if (!rc && held + need > opts.hbm_budget) rc = c.fail(VSHE_E_BUDGET, "request alone exceeds the server's HBM budget");
-    if (!rc) rc = S->create_device(c);
-    if (!rc) rc = S->assemble(c, 3);
-    if (!rc) {
-      S->sys->prepare(c);
-      rc = S->batch->autotune_tiles(c);
-    }
-    if (!rc) rc = S->batch->factor(c);
+    if (!rc) rc = S->create_device_pattern(c);
     if (rc) { r->res.status = rc; complete(r, rc); continue; }
-    r->res.n_unknowns = S->n_red;
     r->prob = std::move(S);
-    r->phase = 1;
-    r->needs_start = true;
+    r->need = need;
     held += need;
+    if (r->prob->n_red >= kAsyncLayoutRows) {
+      r->layout_done.store(false);
+      r->layout_thread = std::thread([this, r] {
+        r->prob->build_layout();
+        r->layout_done.store(true);
+        std::lock_guard<std::mutex> lk(mu);
+        cv.notify_all();
+      });
+      setting_up.push_back(r);
+      continue;
+    }
+    r->prob->build_layout();
+    rc = finish_setup(r);
+    if (rc) { held -= need; complete(r, rc); continue; }
     fresh.push_back(r);
   }
   return VSHE_OK;
@@ -939,9 +1034,17 @@ void Server::run() {
   while (true) {
     {
       std::unique_lock<std::mutex> lk(mu);
-      cv.wait(lk, [&] { return stop || !pending.empty() || !active.empty(); });
-      if (stop && active.empty() && pending.empty()) return;
-      if (stop && active.empty()) {
+      if (active.empty() && !setting_up.empty()) {
+        // nothing to iterate: wait for a layout (polled, its thread notifies too)
+        cv.wait_for(lk, std::chrono::milliseconds(2), [&] {
+          for (ServeRequest *r : setting_up)
+            if (r->layout_done.load()) return true;
+          return false;
+        });
+      } else {
+        cv.wait(lk, [&] { return stop || !pending.empty() || !active.empty(); });
+      }
+      if (stop && active.empty() && setting_up.empty()) {
         // drop what is still queued
         for (ServeRequest *r : pending) { r->res.status = VSHE_E_NOT_FOUND; r->phase = 2; }
         pending.clear();
@@ -951,12 +1054,13 @@ void Server::run() {
     }
     int rc = step();
     if (rc) {
-      // a device error ends every resident request with that error
+      // a device error ends every resident request, and every one being set up, with that error
       std::vector<ServeRequest *> act = active;
       active.clear();
       batch.reset();
       for (ServeRequest *r : act)
         if (r->phase != 2) complete(r, rc);
+      end_setting_up(rc);
       std::lock_guard<std::mutex> lk(mu);
       error = ctx->last_error;
     }
