@@ -44,6 +44,7 @@ namespace vshe {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSpmvU = 8;  // SELL entries per lane whose loads are issued together
+constexpr int kVecU = 4;   // rows per thread whose loads the vector updates issue together
 constexpr int kDotU = 6;   // the same inside the tile kernels, which also carry reduction state
 constexpr int kTrsvU = 8;  // entries of a factor row loaded at once (factor rows hold ~5 entries)
 // CTAs per SM the grid-wide sweeps are compiled for (40 registers, some spilled): up to 6 CTAs
@@ -250,8 +251,22 @@ __device__ __forceinline__ void k_update_p_tile(const SysK *sys, BiState *st, co
     for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) S.p[i] = S.r[i];
   } else {
     const double beta = (b.rho / b.rho_old) * (b.alpha / b.omega);
-    for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads)
-      S.p[i] = S.r[i] + beta * (S.p[i] - b.omega * S.v[i]);
+    const double *__restrict__ r = S.r;
+    const double *__restrict__ v = S.v;
+    double *__restrict__ p = S.p;
+    const int64_t i1 = tl.tile_row1[tile];
+    // kVecU rows per thread in flight: all loads of a group, then the updates
+    for (int64_t i0 = tl.tile_row0[tile] + threadIdx.x; i0 < i1; i0 += kVecU * kThreads) {
+      double rr[kVecU], pp[kVecU], vv[kVecU];
+#pragma unroll
+      for (int u = 0; u < kVecU; ++u) {
+        const int64_t i = i0 + u * kThreads;
+        rr[u] = i < i1 ? r[i] : 0.0; pp[u] = i < i1 ? p[i] : 0.0; vv[u] = i < i1 ? v[i] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kVecU; ++u)
+        if (i0 + u * kThreads < i1) p[i0 + u * kThreads] = rr[u] + beta * (pp[u] - b.omega * vv[u]);
+    }
   }
 }
 __global__ void __launch_bounds__(kThreads) k_update_p(const SysK *sys, BiState *st, Tiles tl, const int32_t *active) {
@@ -307,10 +322,26 @@ __device__ __forceinline__ void k_update_s_tile(const SysK *sys, BiState *st, co
   const SysK S = sys[s];
   const double alpha = st[s].alpha;
   double acc[1] = {0.0};
-  for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) {
-    const double v = S.r[i] - alpha * S.v[i];
-    S.s[i] = v;
-    acc[0] += v * v;
+  const double *__restrict__ r = S.r;
+  const double *__restrict__ vp = S.v;
+  double *__restrict__ sp = S.s;
+  const int64_t i1 = tl.tile_row1[tile];
+  for (int64_t i0 = tl.tile_row0[tile] + threadIdx.x; i0 < i1; i0 += kVecU * kThreads) {
+    double rr[kVecU], vv[kVecU];
+#pragma unroll
+    for (int u = 0; u < kVecU; ++u) {
+      const int64_t i = i0 + u * kThreads;
+      rr[u] = i < i1 ? r[i] : 0.0; vv[u] = i < i1 ? vp[i] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kVecU; ++u) {
+      const int64_t i = i0 + u * kThreads;
+      if (i < i1) {
+        const double v = rr[u] - alpha * vv[u];
+        sp[i] = v;
+        acc[0] += v * v;
+      }
+    }
   }
   double tot[1];
   if (tile_finish<1>(acc, tile, s, tl, partials, counters, tot)) {
@@ -340,12 +371,34 @@ __device__ __forceinline__ void k_update_xr_tile(const SysK *sys, BiState *st, c
       acc[1] += S.rh[i] * r;
     }
   } else {
-    for (int64_t i = tl.tile_row0[tile] + threadIdx.x; i < tl.tile_row1[tile]; i += kThreads) {
-      S.x[i] += b0.alpha * S.ph[i] + b0.omega * S.sh[i];
-      const double r = S.s[i] - b0.omega * S.t[i];
-      S.r[i] = r;
-      acc[0] += r * r;
-      acc[1] += S.rh[i] * r;
+    double *__restrict__ x = S.x;
+    double *__restrict__ rp = S.r;
+    const double *__restrict__ ph = S.ph;
+    const double *__restrict__ sh = S.sh;
+    const double *__restrict__ sv = S.s;
+    const double *__restrict__ tv = S.t;
+    const double *__restrict__ rh = S.rh;
+    const int64_t i1 = tl.tile_row1[tile];
+    for (int64_t i0 = tl.tile_row0[tile] + threadIdx.x; i0 < i1; i0 += kVecU * kThreads) {
+      double xx[kVecU], pp[kVecU], ss[kVecU], sv_[kVecU], tt[kVecU], hh[kVecU];
+#pragma unroll
+      for (int u = 0; u < kVecU; ++u) {
+        const int64_t i = i0 + u * kThreads;
+        const bool in = i < i1;
+        xx[u] = in ? x[i] : 0.0; pp[u] = in ? ph[i] : 0.0; ss[u] = in ? sh[i] : 0.0;
+        sv_[u] = in ? sv[i] : 0.0; tt[u] = in ? tv[i] : 0.0; hh[u] = in ? rh[i] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kVecU; ++u) {
+        const int64_t i = i0 + u * kThreads;
+        if (i < i1) {
+          x[i] = xx[u] + (b0.alpha * pp[u] + b0.omega * ss[u]);
+          const double r = sv_[u] - b0.omega * tt[u];
+          rp[i] = r;
+          acc[0] += r * r;
+          acc[1] += hh[u] * r;
+        }
+      }
     }
   }
   double tot[2];
