@@ -501,12 +501,23 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     }
   }
   // solver order: by level, then block (each block's rows of a level are one run, which the
-  // per-block sweeps walk), then longest rows first (less SELL padding), then base position
+  // per-block sweeps walk), then longest rows first (less SELL padding), then by the base
+  // position of the row's first neighbour (the lanes of a slice then gather nearby entries:
+  // 4 % faster sweeps on the 2D bar than base position), then base position
   perm = base;
+  std::vector<int32_t> nbk((size_t)n, 0);
+  for (int64_t o = 0; o < n; ++o) {
+    int32_t m = INT32_MAX;
+    for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k)
+      if (fci[size_t(k)] != o) m = std::min(m, binv[size_t(fci[size_t(k)])]);
+    nbk[size_t(o)] = m;
+  }
   std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) {
     if (lev[size_t(a)] != lev[size_t(b)]) return lev[size_t(a)] < lev[size_t(b)];
     if (blk0[size_t(a)] != blk0[size_t(b)]) return blk0[size_t(a)] < blk0[size_t(b)];
-    return rp[size_t(a) + 1] - rp[size_t(a)] > rp[size_t(b) + 1] - rp[size_t(b)];
+    const int64_t la = rp[size_t(a) + 1] - rp[size_t(a)], lb = rp[size_t(b) + 1] - rp[size_t(b)];
+    if (la != lb) return la > lb;
+    return nbk[size_t(a)] < nbk[size_t(b)];
   });
   std::vector<int32_t> inv((size_t)(n));
   for (int64_t i = 0; i < n; ++i) inv[size_t(perm[size_t(i)])] = int32_t(i);
