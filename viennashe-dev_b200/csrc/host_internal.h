@@ -141,6 +141,7 @@ struct Batch {
   int64_t *d_clv = nullptr;
   int task_kernel = 4;                 // 0 staged single CTA per task, K > 0 cluster of K CTAs per task
   bool tasks_tuned = false;
+  int64_t tune_key_tasks = -1, tune_key_grid = -1;  // shape classes of the task and grid-wide sweeps
   std::vector<double> task_tune_ms;    // ms per apply: staged, clusters of 2, 4, 8
   int launch_tasks(Ctx &ctx, int which);
   int autotune_tasks(Ctx &ctx);
@@ -229,6 +230,11 @@ struct Ctx {
   // iterates) does not depend on the batch it is solved in
   std::map<int, int64_t> tile_choice;
   std::map<int, std::vector<double>> tile_timings;  // ms per SpMV for 512, 1024, 2048, 4096 rows
+  // autotuned sweep choices per batch shape class (Batch::tune_key_*): a later batch of the same
+  // class (a served batch rebuilt on an admission, say) reuses the choice instead of timing again;
+  // every choice gives bitwise the same results
+  std::map<int64_t, int> task_choice;
+  std::map<int64_t, std::pair<int, int>> trsv_choice;  // (grid, kernel)
   int fail(int code, const std::string &msg);
   int cuda_fail(cudaError_t e, const char *what);
 };

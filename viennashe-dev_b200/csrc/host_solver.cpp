@@ -999,9 +999,20 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
       tasks.push_back(t.second);
     }
     ntasks = int(tasks.size());
+    // shape class of the task sweep: precision, the largest task's work and the task count (the
+    // apply's time is the largest task's walk, in waves of one CTA per SM)
+    auto log2c = [](int64_t v) { int c = 0; while (v > 1) { v >>= 1; ++c; } return c; };
+    if (!tw.empty()) tune_key_tasks = (int64_t(mixed ? 1 : 0) << 40) | (int64_t(log2c(tw.front().first)) << 20) | int64_t(log2c(ntasks));
   }
   grid_group = false;
-  for (int k = 0; k < nsys; ++k) if (!on_task[size_t(k)]) grid_group = true;
+  {
+    int64_t grid_rows = 0;
+    for (int k = 0; k < nsys; ++k)
+      if (!on_task[size_t(k)]) { grid_group = true; grid_rows += sys[size_t(k)]->n; }
+    int c = 0;
+    for (int64_t v = grid_rows; v > 1; v >>= 1) ++c;
+    tune_key_grid = (int64_t(mixed ? 1 : 0) << 40) | (int64_t(sys[0]->opts.trsv_mode) << 32) | int64_t(c);
+  }
   task_kind.assign(on_task.begin(), on_task.end());
   std::vector<int64_t> cptrL, cptrU, fptr;
   std::vector<int32_t> csL, cqL, csU, cqU, fsys, frow;
@@ -1314,6 +1325,16 @@ int Batch::autotune_tasks(Ctx &ctx) {
   }
   if (ctx.task_sweep >= 0 || tasks_tuned || !has_pc || ntasks == 0) return VSHE_OK;
   tasks_tuned = true;
+  {
+    auto it = ctx.task_choice.find(tune_key_tasks);
+    if (it != ctx.task_choice.end()) {
+      if (task_kernel != it->second) {
+        task_kernel = it->second;
+        if (chunk_exec) { cudaGraphExecDestroy(chunk_exec); chunk_exec = nullptr; }
+      }
+      return VSHE_OK;
+    }
+  }
   cudaStream_t s = ctx.stream;
   cudaEvent_t a, b;
   cudaEventCreate(&a); cudaEventCreate(&b);
@@ -1335,6 +1356,7 @@ int Batch::autotune_tasks(Ctx &ctx) {
   }
   cudaEventDestroy(a); cudaEventDestroy(b);
   task_kernel = best_k;
+  ctx.task_choice[tune_key_tasks] = best_k;
   if (chunk_exec) { cudaGraphExecDestroy(chunk_exec); chunk_exec = nullptr; }
   return check_err(ctx, "autotune task sweeps");
 }
@@ -1344,6 +1366,17 @@ int Batch::autotune_trsv(Ctx &ctx) {
   if (mode == VSHE_TRSV_FLOW) trsv_kernel = 3;
   if (trsv_tuned || !has_pc || !grid_group || mode == VSHE_TRSV_PER_LEVEL) return VSHE_OK;
   trsv_tuned = true;
+  {
+    auto it = ctx.trsv_choice.find(tune_key_grid);
+    if (it != ctx.trsv_choice.end()) {
+      if (trsv_grid != it->second.first || trsv_kernel != it->second.second) {
+        trsv_grid = it->second.first;
+        trsv_kernel = it->second.second;
+        if (chunk_exec) { cudaGraphExecDestroy(chunk_exec); chunk_exec = nullptr; }
+      }
+      return VSHE_OK;
+    }
+  }
   cudaStream_t s = ctx.stream;
   cudaEvent_t a, b;
   cudaEventCreate(&a); cudaEventCreate(&b);
@@ -1373,6 +1406,7 @@ int Batch::autotune_trsv(Ctx &ctx) {
   cudaEventDestroy(a); cudaEventDestroy(b);
   trsv_grid = best_grid;
   trsv_kernel = best_kernel;
+  ctx.trsv_choice[tune_key_grid] = {best_grid, best_kernel};
   if (chunk_exec) { cudaGraphExecDestroy(chunk_exec); chunk_exec = nullptr; }  // the graph holds the old grid
   return check_err(ctx, "autotune sweeps");
 }
