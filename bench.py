@@ -417,11 +417,27 @@ def run_ours(args, D_):
 
     # plain FP64 solver on the same problem
     fp64_value, ms64, st64 = None, [], {"iterations": None, "rel_residual": None}
+    currents = None
     if args.fp64_steps > 0:
         P64 = build_problem(args, ctx, "fp64")
         ms64, st64 = P64.bench(1, args.fp64_steps)
         fp64_value = args.fp64_steps / (float(np.sum(ms64)) / 1000.0)
         P64.free()
+        # terminal currents of the timed mixed pass against a plain FP64 solve of the same
+        # problem to 1e-13 (untimed)
+        if args.workload == "bar":
+            _, _, cur = P.results()
+            from vshe import devices as D
+            dev, cfg = D.config2(nx=args.nx, ny=args.ny, n_energies=args.ne, L=args.L)
+            P13 = gpu.SheProblem(ctx, dev, cfg, precision="fp64", tol=1e-13, max_iters=20000, check_every=16,
+                                 **solver_options(args))
+            st13, _ = P13.run()
+            _, _, cur13 = P13.results()
+            P13.free()
+            scale = float(np.max(np.abs(cur13)))
+            currents = {"mixed_1e-10": [float(c) for c in cur], "fp64_tight": [float(c) for c in cur13],
+                        "tight_rel_residual": st13["rel_residual"], "tight_iterations": st13["iterations"],
+                        "max_rel_diff": float(np.max(np.abs(np.asarray(cur) - np.asarray(cur13)))) / scale if scale > 0 else None}
 
     # drop-in path: the reduced system as host CSR through the C ABI with host buffers, with the
     # options the drop-in adapter (viennashe-dev_b200/adapter/vshe_gpu_solver.hpp) derives from the
@@ -530,6 +546,7 @@ def run_ours(args, D_):
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "fp64_solves_per_s": fp64_value, "mixed_over_fp64": (value / max(D_.world, 1)) / fp64_value if fp64_value else None,
             "fp64": {"iterations": st64["iterations"], "rel_residual": st64["rel_residual"], "ms": [float(x) for x in ms64]},
+            "terminal_currents": currents,
             "solve": solve, "kernels_ms": kern,
             "spmv_gbs": ({"fp64": plain_bytes / (spmv_ms / 1000) / 1e9, "frac": plain_bytes / (spmv_ms / 1000) / 1e9 / hbm, "ms": spmv_ms,
                           "kernel": "k_spmv_plain (SELL-32 FP64 y = A x)", "algorithmic_bytes": plain_bytes}
