@@ -356,6 +356,40 @@ int vshe_server_wait(vshe_server *server, int64_t ticket, double timeout_ms, vsh
 /* Finishes the resident requests, drops the queued ones and joins the worker. */
 int vshe_server_destroy(vshe_server *server);
 
+/* ---- outer loop: Gummel update of the electrostatic potential ----
+ * One spatial step of the reference's Gummel iteration (viennashe/simulator.hpp:1029-1052) on
+ * the device: the linearised Poisson system of viennashe/assemble.hpp:165-345 (finite volumes
+ * on the cell mesh, harmonic-mean permittivity across facets, homogeneous Neumann at the domain
+ * boundary, Dirichlet at contact cells with the description's potential there, the Gummel term
+ * q (n + p) / V_T on the diagonal of semiconductor cells, the charge q (n - N_D - p + N_A) in the
+ * rhs; no fixed or trapped charge), solved for the update in FP64, then the damped update of
+ * simulator.hpp:606-647: psi <- (1 - alpha) psi + alpha (psi + dpsi) (contact cells keep their
+ * value).  The unknowns are the non-contact cells, in cell order.  Every cell that is not a
+ * contact needs a non-metal material.  facet_centroid (n_facets * dim) gives the facet centres
+ * the permittivity mean weights by (viennagrid::centroid of the facet in the reference). */
+typedef struct vshe_poisson_stats {
+  int32_t status;            /* of the linear solve */
+  int32_t iterations;
+  double  rel_residual;      /* of the linear solve */
+  double  rhs_norm;          /* ||b||_2: the reference's current_residual_norm term */
+  double  update_norm;       /* ||dpsi||_2: the reference's potential_norm_increment */
+  int64_t n_unknowns;
+} vshe_poisson_stats;
+/* opts: FP64 solver options (NULL: ILU(0) in natural order, tol 1e-12, 10000 iterations;
+ * the precision is always FP64). */
+int vshe_poisson_create(vshe_ctx *ctx, const vshe_device_desc *dev, const double *facet_centroid,
+                        const vshe_solve_opts *opts, int64_t *handle);
+/* potential (n_cells, host) is the current iterate; n and p (n_cells, host, m^-3) the carrier
+ * densities; the damped new potential goes to potential_out (n_cells, host; may alias
+ * potential).  damping in (0, 1]. */
+int vshe_poisson_update(vshe_ctx *ctx, int64_t handle, const double *potential, const double *n, const double *p,
+                        double damping, double *potential_out, vshe_poisson_stats *stats);
+/* The last assembled system: row offsets (n_unknowns + 1), columns and values (nnz), rhs
+ * (n_unknowns); NULL pointers are skipped; *nnz receives the entry count. */
+int vshe_poisson_export(vshe_ctx *ctx, int64_t handle, int64_t *row_ptr, int32_t *col, double *val, double *rhs,
+                        int64_t *nnz);
+int vshe_poisson_free(vshe_ctx *ctx, int64_t handle);
+
 #ifdef __cplusplus
 }
 #endif

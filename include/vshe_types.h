@@ -16,7 +16,11 @@ extern "C" {
 #endif
 
 /* Material ids, same numbering as viennashe/materials/all.hpp (si::id = 0, metal::id = 100). */
-#define VSHE_MATERIAL_SI     0
+#define VSHE_MATERIAL_SI     0    /* materials/all.hpp: si, the semiconductor */
+#define VSHE_MATERIAL_SIO2   1    /* insulators (Poisson only): sio2, hfo2, sion, gas */
+#define VSHE_MATERIAL_HFO2   2
+#define VSHE_MATERIAL_SION   3
+#define VSHE_MATERIAL_GAS    4
 #define VSHE_MATERIAL_METAL  100
 
 /* SHE boundary condition types (viennashe/forwards.h boundary_type_id subset used by SHE). */

@@ -159,6 +159,55 @@ class OracleProblem:
         return xf, dens, cur, float(res[0])
 
 
+def poisson_assemble(dev, facet_centroid, psi, n, p) -> CSR:
+    """The Gummel-linearised Poisson system of the reference (poisson_oracle.cpp:
+    viennashe/assemble.hpp:165-345) for the potential psi and densities n, p; rows are the
+    non-contact cells in cell order."""
+    L = lib()
+    if not getattr(L, "_poisson_ready", False):
+        L.vsheo_poisson_assemble.restype = C.c_int64
+        L.vsheo_poisson_assemble.argtypes = [C.c_void_p, f64p, f64p, f64p, f64p, C.c_int64, i64p, i32p, f64p, f64p, i64p]
+        L._poisson_ready = True
+    desc = DeviceDesc(dev)
+    fc = np.ascontiguousarray(facet_centroid, np.float64)
+    psi = np.ascontiguousarray(psi, np.float64)
+    n = np.ascontiguousarray(n, np.float64)
+    p = np.ascontiguousarray(p, np.float64)
+    nc = dev.n_cells
+    cap = nc * (2 * dev.dim + 2) + 16
+    rp = np.zeros(nc + 1, np.int64)
+    ci = np.zeros(cap, np.int32)
+    v = np.zeros(cap)
+    b = np.zeros(nc)
+    nnz = np.zeros(1, np.int64)
+    nu = L.vsheo_poisson_assemble(C.byref(desc.c), ptr(fc, C.c_double), ptr(psi, C.c_double), ptr(n, C.c_double),
+                                  ptr(p, C.c_double), cap, ptr(rp, C.c_int64), ptr(ci, C.c_int32), ptr(v, C.c_double),
+                                  ptr(b, C.c_double), ptr(nnz, C.c_int64))
+    if nu < 0:
+        raise ValueError("poisson_assemble: capacity or material error")
+    k = int(nnz[0])
+    return CSR(rp[:nu + 1], ci[:k], v[:k], b[:nu])
+
+
+def poisson_update(dev, facet_centroid, psi, n, p, damping=1.0, tol=1e-13):
+    """One Gummel step of the potential (viennashe/simulator.hpp:1029-1052, 606-647): assemble,
+    solve A dpsi = b (the oracle's ILU(0) + BiCGStab), psi_new = psi + dpsi on unknown cells and
+    the description's potential on contact cells, then (1 - damping) psi + damping psi_new.
+    -> (psi_out, dpsi, A)."""
+    A = poisson_assemble(dev, facet_centroid, psi, n, p)
+    if np.any(A.rhs != 0.0):
+        dpsi, st = csr_solve(A, A.rhs, precond=1, tol=tol, maxit=20000)
+        if st["rc"] != 0:
+            raise RuntimeError("oracle Poisson solve: %s" % st)
+    else:
+        dpsi = np.zeros(A.n)
+    psi = np.asarray(psi, np.float64)
+    unk = dev.contact_id < 0
+    new = np.array(dev.potential, np.float64)
+    new[unk] = psi[unk] + dpsi
+    return psi * (1.0 - damping) + new * damping, dpsi, A
+
+
 def csr_solve(A: CSR, b, precond=1, tol=1e-10, maxit=5000, ilut_p=20, ilut_tau=1e-3, blocks=None):
     b = np.ascontiguousarray(b, np.float64)
     x = np.zeros(A.n)

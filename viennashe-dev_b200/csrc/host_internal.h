@@ -243,6 +243,8 @@ struct Ctx {
 void she_release_all(Ctx *ctx);
 // device memory held by the context's SHE problems (she_pipeline.cpp)
 size_t she_bytes(Ctx *ctx);
+void poisson_release_all(Ctx *ctx);
+size_t poisson_bytes(Ctx *ctx);
 
 }  // namespace vshe
 

@@ -1759,6 +1759,7 @@ int vshe_destroy(vshe_ctx *ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   vshe::she_release_all(ctx);
+  vshe::poisson_release_all(ctx);
   ctx->batches.clear();
   ctx->systems.clear();
   cudaStreamDestroy(ctx->stream);
@@ -1773,7 +1774,7 @@ size_t vshe_bytes_in_use(vshe_ctx *ctx) {
   size_t t = 0;
   for (auto &kv : ctx->systems) t += kv.second->arena.total;
   for (auto &kv : ctx->batches) t += kv.second->arena.total + kv.second->tile_arena.total;
-  return t + vshe::she_bytes(ctx);
+  return t + vshe::she_bytes(ctx) + vshe::poisson_bytes(ctx);
 }
 
 int vshe_set_task_sweep(vshe_ctx *ctx, int32_t kernel) {

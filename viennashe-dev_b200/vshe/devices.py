@@ -98,6 +98,17 @@ class Device:
         return int(self.contact_id.max()) + 1 if (self.contact_id >= 0).any() else 0
 
 
+def facet_centres(dev: Device) -> np.ndarray:
+    """Facet centres (n_facets, dim) for the outer loop's Poisson system: the midpoint of the two
+    cell centroids of an interior facet (exact on the uniform tensor meshes built here), the
+    cell centroid on a boundary facet (which the Poisson system does not use)."""
+    fc = dev.facet_cells
+    cen = dev.cell_centroid.reshape(dev.n_cells, dev.dim)
+    c1 = cen[fc[:, 0]]
+    c2 = np.where((fc[:, 1] >= 0)[:, None], cen[np.maximum(fc[:, 1], 0)], c1)
+    return np.ascontiguousarray(0.5 * (c1 + c2))
+
+
 @dataclasses.dataclass
 class SheConfig:
     """Mirror of vshe_she_config; defaults follow viennashe/config.hpp:131-159."""

@@ -342,6 +342,65 @@ def coupling_tables(L):
     return Coupling(L, out)
 
 
+class PoissonStatsC(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("rel_residual", C.c_double),
+                ("rhs_norm", C.c_double), ("update_norm", C.c_double), ("n_unknowns", C.c_int64)]
+
+
+class PoissonProblem:
+    """The outer loop's Gummel update of the potential on the device (vshe_poisson_*)."""
+
+    def __init__(self, ctx: Context, dev, facet_centroid=None, **opts):
+        from .abi import DeviceDesc
+        from .devices import facet_centres
+        L = lib()
+        i64p, i32p, f64p = C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_double)
+        L.vshe_poisson_create.argtypes = [C.c_void_p, C.c_void_p, f64p, C.c_void_p, i64p]
+        L.vshe_poisson_update.argtypes = [C.c_void_p, C.c_int64, f64p, f64p, f64p, C.c_double, f64p, C.c_void_p]
+        L.vshe_poisson_export.argtypes = [C.c_void_p, C.c_int64, i64p, i32p, f64p, f64p, i64p]
+        L.vshe_poisson_free.argtypes = [C.c_void_p, C.c_int64]
+        self.ctx, self.dev = ctx, dev
+        self._desc = DeviceDesc(dev)
+        self._fc = np.ascontiguousarray(facet_centres(dev) if facet_centroid is None else facet_centroid, np.float64)
+        o, self._keep = make_opts(precision="fp64", **opts) if opts else (None, None)
+        h = C.c_int64()
+        ctx._check(L.vshe_poisson_create(ctx.h, C.byref(self._desc.c), ptr(self._fc, C.c_double),
+                                         C.byref(o) if o is not None else None, C.byref(h)))
+        self.h = h.value
+
+    def update(self, potential, n, p, damping=1.0):
+        """-> (new potential, stats dict); raises on a failed solve."""
+        nc = self.dev.n_cells
+        psi = np.ascontiguousarray(potential, np.float64)
+        nn = np.ascontiguousarray(n, np.float64)
+        pp = np.ascontiguousarray(p, np.float64)
+        out = np.zeros(nc)
+        st = PoissonStatsC()
+        rc = lib().vshe_poisson_update(self.ctx.h, self.h, ptr(psi, C.c_double), ptr(nn, C.c_double), ptr(pp, C.c_double),
+                                       float(damping), ptr(out, C.c_double), C.byref(st))
+        self.ctx._check(rc)
+        return out, {k: getattr(st, k) for k, _ in PoissonStatsC._fields_}
+
+    def export(self):
+        """-> (row_ptr, col, val, rhs) of the last assembled system."""
+        nnz = C.c_int64()
+        L = lib()
+        self.ctx._check(L.vshe_poisson_export(self.ctx.h, self.h, None, None, None, None, C.byref(nnz)))
+        nu = int(np.sum(self.dev.contact_id < 0))
+        rp = np.zeros(nu + 1, np.int64)
+        ci = np.zeros(nnz.value, np.int32)
+        v = np.zeros(nnz.value)
+        b = np.zeros(nu)
+        self.ctx._check(L.vshe_poisson_export(self.ctx.h, self.h, ptr(rp, C.c_int64), ptr(ci, C.c_int32), ptr(v, C.c_double),
+                                              ptr(b, C.c_double), C.byref(nnz)))
+        return rp, ci, v, b
+
+    def free(self):
+        if self.h:
+            lib().vshe_poisson_free(self.ctx.h, self.h)
+            self.h = 0
+
+
 class SheProblem:
     """A SHE problem assembled, eliminated, normalised and solved on the device (vshe_she_*)."""
 
