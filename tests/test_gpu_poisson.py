@@ -55,10 +55,12 @@ def test_assembly_and_update_match_oracle(gpu_ctx, name):
     assert np.max(np.abs(b - M.rhs)) <= 1e-12 * np.max(np.abs(M.rhs))
     assert st["status"] == 0 and st["rel_residual"] < 1e-13
     assert abs(st["rhs_norm"] - np.linalg.norm(M.rhs)) <= 1e-12 * np.linalg.norm(M.rhs)
-    assert abs(st["update_norm"] - np.linalg.norm(dpsi)) <= 1e-9 * np.linalg.norm(dpsi)
+    # two solves of one system to a 1e-13 residual differ by up to its condition number times
+    # that (about 1e6 on the MOSFET, whose gate and body differ by 1 V over 1e23 m^-3 doping)
+    assert abs(st["update_norm"] - np.linalg.norm(dpsi)) <= 1e-6 * np.linalg.norm(dpsi)
     contact = dev.contact_id >= 0
     assert np.array_equal(out[contact], psi[contact] * 0.4 + dev.potential[contact] * 0.6)
-    assert np.max(np.abs(out - ref_out)) <= 1e-9 * np.max(np.abs(dpsi))
+    assert np.max(np.abs(out - ref_out)) <= 1e-6 * np.max(np.abs(dpsi))
 
 
 def test_errors(gpu_ctx):
@@ -105,7 +107,7 @@ def test_gummel_loop_on_device_follows_oracle_steps(gpu_ctx):
             p = NI * NI / np.maximum(n, 1.0)
             new, pst = G.update(psi, n, p, damping=0.5)
             ref, dpsi, _ = O.poisson_update(dev0, fc, psi, n, p, damping=0.5, tol=1e-13)
-            assert np.max(np.abs(new - ref)) <= 1e-9 * max(np.max(np.abs(dpsi)), 1e-12)
+            assert np.max(np.abs(new - ref)) <= 1e-6 * max(np.max(np.abs(dpsi)), 1e-12)
             assert np.all(np.isfinite(new))
             norms.append(pst["rhs_norm"])
             psi = new
