@@ -390,6 +390,39 @@ int vshe_poisson_export(vshe_ctx *ctx, int64_t handle, int64_t *row_ptr, int32_t
                         int64_t *nnz);
 int vshe_poisson_free(vshe_ctx *ctx, int64_t handle);
 
+/* The self-consistent electron SHE + Poisson Gummel loop of simulator::run
+ * (viennashe/simulator.hpp:895-1130, electrons only, the SHE equation for electrons): each
+ * iteration takes the Gummel update of the potential for the current electron and hole
+ * densities (vshe_poisson_update), then solves the SHE for the new potential on the device
+ * (vshe_she_create / _run / _results) and updates the electron density with logarithmic damping,
+ * n <- n^(1 - alpha) n_SHE^alpha with n_SHE >= 1e-10 n (simulator.hpp:560-577).  The holes stay
+ * at their initial density (hole equation off).  The loop ends, as the reference's does, after
+ * one more undamped update once the Poisson rhs norm has fallen below 1e-10 of its first value
+ * or the potential increment below tol, or at max_iters (the last iteration undamped).  The SHE
+ * rhs is not part of the residual norm here (the reference adds ||b_SHE||).  Each iteration
+ * builds the SHE problem for its potential on the host (energies, orders, mapping). */
+typedef struct vshe_gummel_opts {
+  int32_t max_iters;   /* the reference's default 100 (solvers/config.hpp:256-257) */
+  double  tol;         /* on ||dpsi||_2, default 1e-8 */
+  double  damping;     /* default 0.3 */
+} vshe_gummel_opts;
+typedef struct vshe_gummel_stats {
+  int32_t status;
+  int32_t iterations;          /* Gummel iterations done */
+  double  potential_increment; /* ||dpsi||_2 of the last iteration */
+  double  rhs_norm;            /* ||b_Poisson||_2 of the last iteration */
+  double  initial_rhs_norm;    /* ... of the first */
+  int64_t she_iterations;      /* BiCGStab iterations over all SHE solves */
+} vshe_gummel_stats;
+/* density0 / p0: initial electron and hole densities (n_cells, m^-3).  The potential starts at
+ * the description's.  Outputs (n_cells / one per contact, host, may be NULL): the final
+ * potential, electron density and terminal currents of the last SHE solve.  history, if not NULL,
+ * receives per iteration (||b_Poisson||, ||dpsi||, SHE iterations), 3 * max_iters doubles. */
+int vshe_gummel_solve(vshe_ctx *ctx, const vshe_device_desc *dev, const double *facet_centroid, const vshe_she_config *cfg,
+                      const vshe_coupling_tables *coupling, const vshe_solve_opts *she_opts, const vshe_gummel_opts *gopts,
+                      const double *density0, const double *p0, double *potential_out, double *density_out,
+                      double *currents_out, double *history, vshe_gummel_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

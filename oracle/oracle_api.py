@@ -208,6 +208,49 @@ def poisson_update(dev, facet_centroid, psi, n, p, damping=1.0, tol=1e-13):
     return psi * (1.0 - damping) + new * damping, dpsi, A
 
 
+def gummel_solve(dev, cfg, cpl, n0, p0, max_iters=100, tol=1e-8, damping=0.3, she_tol=1e-12):
+    """The electron SHE + Poisson Gummel loop of viennashe/simulator.hpp:895-1130 on the oracle:
+    the Poisson step (poisson_update), the oracle SHE for the new potential, the logarithmic
+    density damping of simulator.hpp:560-577 and the reference's stopping rules.
+    -> (potential, density, currents, history (||b||, ||dpsi||, SHE iterations) per iteration)."""
+    import dataclasses
+    from vshe import devices as D
+    fc = D.facet_centres(dev)
+    psi = np.array(dev.potential, np.float64)
+    n = np.array(n0, np.float64)
+    p = np.array(p0, np.float64)
+    semi = (dev.contact_id < 0) & (dev.cell_material == D.SI)
+    no_damping = break_after = False
+    initial = 0.0
+    hist, cur = [], None
+    for it in range(1, max_iters + 1):
+        if it == max_iters:
+            no_damping = True
+        alpha = 1.0 if no_damping else damping
+        A = poisson_assemble(dev, fc, psi, n, p)
+        res, psi, dpsi = float(np.linalg.norm(A.rhs)), *poisson_update(dev, fc, psi, n, p, damping=alpha)[:2]
+        P = OracleProblem(dataclasses.replace(dev, potential=psi.copy()), cfg, cpl)
+        M = P.matrix(3)
+        x, st = csr_solve(M, M.rhs, precond=1, tol=she_tol, maxit=20000)
+        if st["rc"] != 0:
+            raise RuntimeError("oracle SHE solve: %s" % st)
+        _, dens, cur, _ = P.finish(x)
+        if no_damping:
+            n[semi] = dens[semi]
+        else:
+            nv = np.maximum(dens[semi], n[semi] * 1e-10)
+            n[semi] = np.power(n[semi], 1.0 - alpha) * np.power(nv, alpha)
+        inc = float(np.linalg.norm(dpsi))
+        hist.append((res, inc, st["iters"]))
+        if break_after or res == 0.0:
+            break
+        if it == 1:
+            initial = res
+        elif res / initial < 1e-10 or inc < tol:
+            no_damping = break_after = True
+    return psi, n, cur, np.array(hist)
+
+
 def csr_solve(A: CSR, b, precond=1, tol=1e-10, maxit=5000, ilut_p=20, ilut_tau=1e-3, blocks=None):
     b = np.ascontiguousarray(b, np.float64)
     x = np.zeros(A.n)

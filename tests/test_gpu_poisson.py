@@ -114,3 +114,28 @@ def test_gummel_loop_on_device_follows_oracle_steps(gpu_ctx):
     finally:
         G.free()
     assert len(norms) == 3 and all(np.isfinite(norms))
+
+
+def test_gummel_solve_matches_oracle_loop(gpu_ctx):
+    """vshe_gummel_solve (device SHE + device Poisson, the reference's damping and stopping rules)
+    against the oracle's restatement of the same loop: the same iteration at which the potential
+    increment falls below tol, the same norms per iteration, the same final potential and
+    density.  (Past about 1e-6 V the increments of this loop stop falling on both sides: the
+    energy grid is rebuilt for every potential.)"""
+    dev = D.nin_diode_1d(boxes=60, bias=0.3)
+    cfg = D.SheConfig(max_expansion_order=1, energy_spacing=D.HBAR_OMEGA_OP / 4.0, min_kinetic_energy_range=1.0 * D.Q)
+    n0 = dev.doping_n.copy()
+    p0 = NI * NI / n0
+    cpl = O.golden_coupling(1)
+    psi, dens, cur, hist, st = gpu.gummel_solve(gpu_ctx, dev, cfg, n0, p0, coupling=cpl, tol=3e-2, damping=0.3,
+                                                max_iters=100, precision="fp64", precond="ilu0", ordering="natural")
+    r_psi, r_n, r_cur, r_hist = O.gummel_solve(dev, cfg, cpl, n0, p0, max_iters=100, tol=3e-2, damping=0.3)
+    assert st["rc"] == 0 and st["status"] == 0, st
+    assert st["iterations"] == len(r_hist) < 100
+    assert np.allclose(hist[:, 0], r_hist[:, 0], rtol=1e-6, atol=0)
+    assert np.allclose(hist[:, 1], r_hist[:, 1], rtol=1e-6, atol=0)
+    assert hist[-2, 1] < 3e-2  # stopped one undamped update after the increment fell below tol
+    assert np.max(np.abs(psi - r_psi)) <= 1e-7 * np.max(np.abs(r_psi))
+    semi = dev.contact_id < 0
+    assert np.max(np.abs(dens[semi] - r_n[semi]) / r_n[semi]) <= 1e-6
+    assert np.max(np.abs(cur - r_cur)) <= 1e-5 * np.max(np.abs(r_cur))

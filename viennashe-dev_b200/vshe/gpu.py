@@ -401,6 +401,48 @@ class PoissonProblem:
             self.h = 0
 
 
+class GummelOptsC(C.Structure):
+    _fields_ = [("max_iters", C.c_int32), ("tol", C.c_double), ("damping", C.c_double)]
+
+
+class GummelStatsC(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("potential_increment", C.c_double),
+                ("rhs_norm", C.c_double), ("initial_rhs_norm", C.c_double), ("she_iterations", C.c_int64)]
+
+
+def gummel_solve(ctx: Context, dev, cfg, density0, p0, coupling=None, facet_centroid=None, max_iters=100, tol=1e-8,
+                 damping=0.3, she_tol=1e-12, she_max_iters=20000, **she_opts):
+    """Self-consistent electron SHE + Poisson (vshe_gummel_solve) -> (potential, density, currents,
+    history (iterations x 3: ||b_Poisson||, ||dpsi||, SHE iterations), stats dict)."""
+    from .abi import DeviceDesc, she_config_c
+    from .devices import facet_centres
+    L = _she_lib()
+    f64p = C.POINTER(C.c_double)
+    L.vshe_gummel_solve.argtypes = [C.c_void_p, C.c_void_p, f64p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    f64p, f64p, f64p, f64p, f64p, f64p, C.c_void_p]
+    desc = DeviceDesc(dev)
+    cfgc = she_config_c(cfg)
+    cpl = coupling if coupling is not None else coupling_tables(cfg.max_expansion_order)
+    fc = np.ascontiguousarray(facet_centres(dev) if facet_centroid is None else facet_centroid, np.float64)
+    o, keep = make_opts(tol=she_tol, max_iters=she_max_iters, **she_opts)
+    g = GummelOptsC(int(max_iters), float(tol), float(damping))
+    n0 = np.ascontiguousarray(density0, np.float64)
+    pp = np.ascontiguousarray(p0, np.float64)
+    psi = np.zeros(dev.n_cells)
+    dens = np.zeros(dev.n_cells)
+    cur = np.zeros(max(dev.n_contacts, 1))
+    hist = np.zeros(3 * int(max_iters))
+    st = GummelStatsC()
+    rc = L.vshe_gummel_solve(ctx.h, C.byref(desc.c), ptr(fc, C.c_double), C.byref(cfgc), C.byref(cpl.c), C.byref(o), C.byref(g),
+                             ptr(n0, C.c_double), ptr(pp, C.c_double), ptr(psi, C.c_double), ptr(dens, C.c_double),
+                             ptr(cur, C.c_double), ptr(hist, C.c_double), C.byref(st))
+    stats = {k: getattr(st, k) for k, _ in GummelStatsC._fields_}
+    if rc and rc != -6:
+        ctx._check(rc)
+    stats["rc"] = rc
+    return psi, dens, cur[:dev.n_contacts], hist.reshape(-1, 3)[:stats["iterations"]], stats
+
+
 class SheProblem:
     """A SHE problem assembled, eliminated, normalised and solved on the device (vshe_she_*)."""
 
