@@ -1057,6 +1057,51 @@ __device__ void keep_largest(double *lu, int64_t lo, int64_t hi, int pkeep) {
   __syncwarp();
 }
 
+// One row of the IKJ elimination (ILU(0) / ILU(k), no dropping) on a group of kRowLanes lanes,
+// with the row's columns and values held in the group's shared-memory row cache: the same
+// operations in the same order as the general path below, with the searches and updates of row
+// i in shared memory instead of global memory.  Rows of earlier levels (the pivots and the U
+// parts) are read from global memory, where they are final.  A warp works on 32 / kRowLanes rows
+// at once (the U part of a pivot row is rarely wider than 8 entries).
+constexpr int kRowCache = 64;
+constexpr int kRowLanes = 8;
+constexpr int kRowGroups = kWarps * (32 / kRowLanes);
+__device__ __forceinline__ void ilu_row_cached(const FactDev &F, int64_t a, int64_t b, int64_t d, int32_t bi, int32_t *scol,
+                                               double *sval, unsigned mask, int32_t *err) {
+  const int g = threadIdx.x & (kRowLanes - 1);
+  const int w = (int)(b - a);
+  for (int k = g; k < w; k += kRowLanes) { scol[k] = F.ci[a + k]; sval[k] = __ldcg(&F.lu[a + k]); }
+  __syncwarp(mask);
+  for (int64_t kp = a; kp < d; ++kp) {
+    const int q = (int)(kp - a);
+    const int32_t c = scol[q];
+    if (F.blk[c] != bi) continue;
+    const double piv = __ldcg(&F.lu[F.diag[c]]);
+    if (piv == 0.0) {
+      if (g == 0) atomicExch(err, VSHE_E_ZERO_PIVOT_DEV);
+      break;
+    }
+    const double l = sval[q] / piv;
+    __syncwarp(mask);
+    if (g == 0) sval[q] = l;
+    for (int64_t kk = F.diag[c] + 1 + g; kk < F.rp[c + 1]; kk += kRowLanes) {
+      const int32_t j = F.ci[kk];
+      if (F.blk[j] != bi) continue;
+      int lo = q + 1, hi = w - 1, pos = -1;
+      while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int32_t cm = scol[mid];
+        if (cm == j) { pos = mid; break; }
+        if (cm < j) lo = mid + 1; else hi = mid - 1;
+      }
+      if (pos >= 0) sval[pos] = sval[pos] - l * __ldcg(&F.lu[kk]);
+    }
+    __syncwarp(mask);
+  }
+  for (int k = g; k < w; k += kRowLanes) F.lu[a + k] = sval[k];
+  __syncwarp(mask);
+}
+
 // level entries are solver rows ent_row[e] of system ent_sys[e] (row e of system 0 when NULL).
 // ILU(0) / ILU(k) / ILU on a pattern: Saad's IKJ elimination inside the row's pattern.  With
 // F.ilut the two ILUT dropping rules (Saad Alg. 10.6) are applied on the way: multipliers below
@@ -1064,16 +1109,34 @@ __device__ void keep_largest(double *lu, int64_t lo, int64_t hi, int pkeep) {
 // tau ||a_i|| are dropped and only the pkeep largest of L and of U stay; a zero pivot is replaced
 // by tau ||a_i|| (or 1), as ILUT does.
 __device__ void ilu0_level_rows(const FactDev *fs, Levels lv, int k, int32_t *err) {
+  __shared__ int32_t s_col[kRowGroups][kRowCache];
+  __shared__ double s_val[kRowGroups][kRowCache];
   const int lane = threadIdx.x & 31;
   const int64_t gid = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
   const int64_t e0 = lv.lvl_ptr[k], e1 = lv.lvl_ptr[k + 1];
+  // pass 1: rows without dropping that fit the row cache, one lane group each
+  {
+    const int grp = threadIdx.x / kRowLanes;
+    const unsigned mask = ((1u << kRowLanes) - 1u) << (lane & ~(kRowLanes - 1));
+    const int64_t gg = (int64_t)blockIdx.x * kRowGroups + grp, ng = (int64_t)gridDim.x * kRowGroups;
+    for (int64_t e = e0 + gg; e < e1; e += ng) {
+      const FactDev &F = fs[lv.ent_sys ? lv.ent_sys[e] : 0];
+      const int64_t i = lv.ent_row ? lv.ent_row[e] : e;
+      const int64_t a = F.rp[i], b = F.rp[i + 1];
+      if (F.ilut || b - a > kRowCache) continue;
+      ilu_row_cached(F, a, b, F.diag[i], F.blk[i], s_col[grp], s_val[grp], mask, err);
+    }
+  }
+  __syncwarp();
+  // pass 2: the other rows (ILUT, or longer than the cache), one warp each
   for (int64_t e = e0 + gid; e < e1; e += nw) {
     const int s = lv.ent_sys ? lv.ent_sys[e] : 0;
     const FactDev F = fs[s];
     const int64_t i = lv.ent_row ? lv.ent_row[e] : e;
     const int64_t a = F.rp[i], b = F.rp[i + 1], d = F.diag[i];
     const int32_t bi = F.blk[i];
+    if (!F.ilut && b - a <= kRowCache) continue;  // done in pass 1
     double ti = 0.0;
     if (F.ilut) {
       double ss = 0.0;
