@@ -17,12 +17,14 @@
 //     (src/solvers/viennacl/parallel_linear_solver.hpp:82-93).
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <thread>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -151,11 +153,45 @@ int System::init_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_
   return VSHE_OK;
 }
 
+// Runs fn(begin, end) over [0, n) in contiguous chunks of at least `grain` on up to 16 host
+// threads (the host-side checks of the drop-in call on arrays of hundreds of MB).
+static void host_parallel(int64_t n, int64_t grain, const std::function<void(int64_t, int64_t)> &fn) {
+  const int64_t hw = std::max<int64_t>(1, int64_t(std::thread::hardware_concurrency()));
+  const int64_t T = std::min<int64_t>(std::min<int64_t>(hw, 16), std::max<int64_t>(1, n / std::max<int64_t>(grain, 1)));
+  if (T <= 1) { fn(0, n); return; }
+  std::vector<std::thread> th;
+  for (int64_t t = 0; t < T; ++t) th.emplace_back(fn, n * t / T, n * (t + 1) / T);
+  for (auto &x : th) x.join();
+}
+
+// First index in [0, n) whose value is not finite, or n.
+static int64_t first_nonfinite(const double *v, int64_t n) {
+  std::atomic<int64_t> first{n};
+  host_parallel(n, int64_t(1) << 20, [&](int64_t a, int64_t b) {
+    for (int64_t k = a; k < b && k < first.load(std::memory_order_relaxed); ++k)
+      if (!std::isfinite(v[k])) {
+        int64_t cur = first.load();
+        while (k < cur && !first.compare_exchange_weak(cur, k)) {}
+        return;
+      }
+  });
+  return first.load();
+}
+
+// memcmp(a, b, bytes) == 0, on several host threads for large arrays.
+static bool host_equal(const void *a, const void *b, size_t bytes) {
+  std::atomic<bool> eq{true};
+  host_parallel(int64_t(bytes), int64_t(1) << 24, [&](int64_t x, int64_t y) {
+    if (eq.load(std::memory_order_relaxed) && std::memcmp((const char *)a + x, (const char *)b + x, size_t(y - x)) != 0) eq = false;
+  });
+  return eq.load();
+}
+
 int System::set_values(Ctx &ctx, const double *v, const double *rhs) {
   cudaStream_t s = ctx.stream;
   cudaError_t e;
-  for (int64_t k = 0; k < nnz; ++k)
-    if (!std::isfinite(v[k])) return ctx.fail(VSHE_E_NAN, "matrix entry " + std::to_string(k));
+  const int64_t bad = first_nonfinite(v, nnz);
+  if (bad < nnz) return ctx.fail(VSHE_E_NAN, "matrix entry " + std::to_string(bad));
   bnorm_host = 0.0;
   for (int64_t i = 0; i < n; ++i) {
     if (!std::isfinite(rhs[i])) return ctx.fail(VSHE_E_NAN, "rhs entry " + std::to_string(i));
@@ -1958,8 +1994,8 @@ int vshe_solve_csr(vshe_ctx *ctx, int64_t n, int64_t nnz, const int64_t *rp, con
       const bool perm_same = o.perm ? (ctx->csr_cache_perm.size() == size_t(n) && std::equal(ctx->csr_cache_perm.begin(), ctx->csr_cache_perm.end(), o.perm))
                                     : ctx->csr_cache_perm.empty();
       hit = S->n == n && S->nnz == nnz && same_solve_opts(ctx->csr_cache_opts, o) && blocks_same && perm_same &&
-            std::memcmp(S->rp.data(), rp, sizeof(int64_t) * size_t(n + 1)) == 0 &&
-            std::memcmp(S->ci.data(), ci, sizeof(int32_t) * size_t(nnz)) == 0;
+            host_equal(S->rp.data(), rp, sizeof(int64_t) * size_t(n + 1)) &&
+            host_equal(S->ci.data(), ci, sizeof(int32_t) * size_t(nnz));
     }
   }
   int rc;

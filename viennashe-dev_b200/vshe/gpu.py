@@ -209,14 +209,16 @@ class Context:
         self._check(L.vshe_autotune_info(self.h, int(n), C.byref(rows), ptr(ms, C.c_double)))
         return int(rows.value), ms
 
-    def solve_csr(self, rp, ci, v, b, **kw):
-        """The drop-in call: host CSR + rhs in, host x out (copies inside)."""
+    def solve_csr(self, rp, ci, v, b, out=None, **kw):
+        """The drop-in call: host CSR + rhs in, host x out (copies inside); `out` (n float64,
+        contiguous) receives x when given."""
         rp = np.ascontiguousarray(rp, np.int64)
         ci = np.ascontiguousarray(ci, np.int32)
         v = np.ascontiguousarray(v, np.float64)
         b = np.ascontiguousarray(b, np.float64)
         n = len(rp) - 1
-        x = np.zeros(n)
+        x = np.zeros(n) if out is None else out
+        assert x.dtype == np.float64 and x.flags["C_CONTIGUOUS"] and x.shape == (n,)
         o, keep = make_opts(**kw)
         st = SolveStatsC()
         rc = lib().vshe_solve_csr(self.h, n, int(rp[-1]), ptr(rp, C.c_int64), ptr(ci, C.c_int32), ptr(v, C.c_double),
