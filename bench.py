@@ -521,11 +521,11 @@ def run_ours(args, D_):
     achieved = dbytes / (avg_ms / 1000.0) / 1e9
     # DRAM traffic per launch: ncu captures of the same kernels on the 200 x 50 x 80 bar measured
     # dram__bytes_read.sum + dram__bytes_write.sum at 0.967 of the algorithmic bytes for the SpMV
-    # + dots, 0.980 for the grid-barrier ILU(1) apply (40 registers) and 1.073 for the per-slab
+    # + dots, 0.980 for the grid-barrier ILU(1) apply (40 registers) and 1.046 for the per-slab
     # apply; the traffic grows in proportion with the units processed, so a full launch's is that
     # ratio times its algorithmic bytes.
     traffic_ratio = {"spmv": 383372032 / 396606924, 1: (421555456 + 19777280) / 450235320,
-                     5: (443091968 + 40048384) / 450235320}
+                     5: (429628416 + 41189376) / 450235320}
     key = dominant if dominant == "spmv" else st.get("sweep_mode")
     traffic = dbytes * traffic_ratio[key] if args.workload == "bar" and key in traffic_ratio else None
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "peak_source": peak_src,
