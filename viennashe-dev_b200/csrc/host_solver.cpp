@@ -210,8 +210,20 @@ void System::prepare(Ctx &ctx) {
   vk_permute(n, d_perm, d_b64, d_bp, 1, s);
 }
 
+
+// Contiguous runs of equal block id: run r = rows [runs[r], runs[r + 1]).
+static std::vector<int64_t> block_runs(const std::vector<int32_t> &blk) {
+  std::vector<int64_t> runs(1, 0);
+  for (size_t i = 1; i < blk.size(); ++i)
+    if (blk[i] != blk[i - 1]) runs.push_back(int64_t(i));
+  runs.push_back(int64_t(blk.size()));
+  return runs;
+}
+
 // Greedy colouring of the symmetrised pattern within blocks: distance 1 (coupled rows differ)
-// or distance 2 (rows with a common neighbour differ as well).
+// or distance 2 (rows with a common neighbour differ as well).  Rows are coloured in index
+// order; a row's colour depends only on rows of its own block, so runs of rows of one block are
+// coloured on several host threads with the same result.
 static void greedy_colours(int64_t n, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci, const std::vector<int32_t> &blk,
                            std::vector<int32_t> &col, int distance) {
   std::vector<int64_t> tcnt((size_t)(n) + 1, 0);
@@ -223,26 +235,30 @@ static void greedy_colours(int64_t n, const std::vector<int64_t> &rp, const std:
   for (int64_t i = 0; i < n; ++i)
     for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tci[size_t(pos[size_t(ci[k])]++)] = int32_t(i);
   col.assign(size_t(n), -1);
-  std::vector<int64_t> mark(64, -1);
   auto neighbours = [&](int64_t i, auto &&fn) {
     for (int64_t k = rp[i]; k < rp[i + 1]; ++k) fn(ci[k]);
     for (int64_t k = tcnt[size_t(i)]; k < tcnt[size_t(i) + 1]; ++k) fn(tci[size_t(k)]);
   };
-  for (int64_t i = 0; i < n; ++i) {
-    auto visit = [&](int32_t j) {
-      if (j == i || col[size_t(j)] < 0 || blk[size_t(j)] != blk[size_t(i)]) return;
-      int32_t c = col[size_t(j)];
-      if (c >= int32_t(mark.size())) mark.resize(size_t(c) + 1, -1);
-      mark[size_t(c)] = i;
-    };
-    neighbours(i, [&](int32_t j) {
-      visit(j);
-      if (distance > 1 && blk[size_t(j)] == blk[size_t(i)]) neighbours(j, visit);
-    });
-    int32_t c = 0;
-    while (c < int32_t(mark.size()) && mark[size_t(c)] == i) ++c;
-    col[size_t(i)] = c;
-  }
+  const std::vector<int64_t> runs = block_runs(blk);
+  const int64_t nruns = int64_t(runs.size()) - 1;
+  host_parallel(nruns, 1, [&](int64_t r0, int64_t r1) {
+    std::vector<int64_t> mark(64, -1);
+    for (int64_t i = runs[size_t(r0)]; i < runs[size_t(r1)]; ++i) {
+      auto visit = [&](int32_t j) {
+        if (j == i || blk[size_t(j)] != blk[size_t(i)] || col[size_t(j)] < 0) return;
+        int32_t c = col[size_t(j)];
+        if (c >= int32_t(mark.size())) mark.resize(size_t(c) + 1, -1);
+        mark[size_t(c)] = i;
+      };
+      neighbours(i, [&](int32_t j) {
+        visit(j);
+        if (distance > 1 && blk[size_t(j)] == blk[size_t(i)]) neighbours(j, visit);
+      });
+      int32_t c = 0;
+      while (c < int32_t(mark.size()) && mark[size_t(c)] == i) ++c;
+      col[size_t(i)] = c;
+    }
+  });
 }
 
 // SELL-32 layout of a row sequence rows[t] (t = 0..m-1) made of groups: group g is the run
@@ -341,14 +357,16 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   } else {
     // base-order rows of A: (base column, entry)
     std::vector<int64_t> brp((size_t)n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) brp[size_t(i) + 1] = brp[size_t(i)] + (rp[size_t(base[size_t(i)]) + 1] - rp[size_t(base[size_t(i)])]);
     std::vector<std::pair<int32_t, int64_t>> bent((size_t)nnz);
-    for (int64_t i = 0; i < n; ++i) {
-      const int32_t o = base[size_t(i)];
-      int64_t p = brp[size_t(i)];
-      for (int64_t k = rp[size_t(o)]; k < rp[size_t(o) + 1]; ++k) bent[size_t(p++)] = {binv[size_t(ci[size_t(k)])], k};
-      std::sort(bent.begin() + brp[size_t(i)], bent.begin() + p);
-      brp[size_t(i) + 1] = p;
-    }
+    host_parallel(n, int64_t(1) << 16, [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; ++i) {
+        const int32_t o = base[size_t(i)];
+        int64_t p = brp[size_t(i)];
+        for (int64_t k = rp[size_t(o)]; k < rp[size_t(o) + 1]; ++k) bent[size_t(p++)] = {binv[size_t(ci[size_t(k)])], k};
+        std::sort(bent.begin() + brp[size_t(i)], bent.begin() + p);
+      }
+    });
     std::vector<std::vector<std::pair<int32_t, int64_t>>> rows((size_t)n);  // base order: (base column, entry or -1)
     if (ilut) {
       // ILUT(p, tau), Saad Alg. 10.6, in base order: the row is eliminated with the kept rows
@@ -438,52 +456,74 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
         for (int32_t j : cols) { nz[size_t(j)] = 0; w[size_t(j)] = 0.0; }
       }
     } else {
-      // symbolic ILU(k): the final rows' upper parts (column, level) feed later rows
-      std::vector<int64_t> urp((size_t)n + 1, 0);
-      std::vector<int32_t> ucolv, ulevv;
-      std::vector<int32_t> lvl((size_t)n, -1);
-      std::vector<int64_t> src((size_t)n, -1);
-      std::vector<int32_t> cols, heap;
-      for (int64_t i = 0; i < n; ++i) {
-        const int32_t bi = blk0[size_t(base[size_t(i)])];
-        cols.clear(); heap.clear();
-        for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) {
-          const int32_t j = bent[size_t(k)].first;
-          lvl[size_t(j)] = 0; src[size_t(j)] = bent[size_t(k)].second; cols.push_back(j);
-          if (j < i) heap.push_back(j);
+      // symbolic ILU(k): the final rows' upper parts (column, level) feed later rows.  A row
+      // reads only earlier rows of its own block, so when every block is one run of base
+      // positions the runs are processed on several host threads (each with its own scratch
+      // and its own store of upper parts), with the same result.
+      std::vector<int32_t> bblk((size_t)n);
+      for (int64_t i = 0; i < n; ++i) bblk[size_t(i)] = blk0[size_t(base[size_t(i)])];
+      const std::vector<int64_t> runs = block_runs(bblk);
+      const int64_t nruns = int64_t(runs.size()) - 1;
+      bool contiguous = true;
+      {
+        std::vector<char> seen;
+        for (int64_t r = 0; r < nruns && contiguous; ++r) {
+          const int32_t b = bblk[size_t(runs[size_t(r)])];
+          if (b >= int32_t(seen.size())) seen.resize(size_t(b) + 1, 0);
+          if (seen[size_t(b)]) contiguous = false;
+          seen[size_t(b)] = 1;
         }
-        std::make_heap(heap.begin(), heap.end(), std::greater<int32_t>());
-        int32_t last = -1;
-        while (!heap.empty()) {
-          std::pop_heap(heap.begin(), heap.end(), std::greater<int32_t>());
-          const int32_t k = heap.back(); heap.pop_back();
-          if (k == last) continue;
-          last = k;
-          if (blk0[size_t(base[size_t(k)])] != bi) continue;
-          const int32_t lik = lvl[size_t(k)];
-          for (int64_t kk = urp[size_t(k)]; kk < urp[size_t(k) + 1]; ++kk) {
-            const int32_t j = ucolv[size_t(kk)];
-            if (blk0[size_t(base[size_t(j)])] != bi) continue;
-            const int32_t l = lik + ulevv[size_t(kk)] + 1;
-            if (l > kfill) continue;
-            if (lvl[size_t(j)] < 0) {
-              lvl[size_t(j)] = l; src[size_t(j)] = -1; cols.push_back(j);
-              if (j < i) { heap.push_back(j); std::push_heap(heap.begin(), heap.end(), std::greater<int32_t>()); }
-            } else if (l < lvl[size_t(j)]) {
-              lvl[size_t(j)] = l;
+      }
+      std::vector<int64_t> ub((size_t)n, 0), ue((size_t)n, 0);  // upper part of row k: [ub[k], ue[k]) in its thread's store
+      auto symbolic = [&](int64_t r0, int64_t r1) {
+        std::vector<int32_t> ucolv, ulevv;
+        std::vector<int32_t> lvl((size_t)n, -1);
+        std::vector<int64_t> src((size_t)n, -1);
+        std::vector<int32_t> cols, heap;
+        for (int64_t i = runs[size_t(r0)]; i < runs[size_t(r1)]; ++i) {
+          const int32_t bi = bblk[size_t(i)];
+          cols.clear(); heap.clear();
+          for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) {
+            const int32_t j = bent[size_t(k)].first;
+            lvl[size_t(j)] = 0; src[size_t(j)] = bent[size_t(k)].second; cols.push_back(j);
+            if (j < i) heap.push_back(j);
+          }
+          std::make_heap(heap.begin(), heap.end(), std::greater<int32_t>());
+          int32_t last = -1;
+          while (!heap.empty()) {
+            std::pop_heap(heap.begin(), heap.end(), std::greater<int32_t>());
+            const int32_t k = heap.back(); heap.pop_back();
+            if (k == last) continue;
+            last = k;
+            if (bblk[size_t(k)] != bi) continue;
+            const int32_t lik = lvl[size_t(k)];
+            for (int64_t kk = ub[size_t(k)]; kk < ue[size_t(k)]; ++kk) {
+              const int32_t j = ucolv[size_t(kk)];
+              if (bblk[size_t(j)] != bi) continue;
+              const int32_t l = lik + ulevv[size_t(kk)] + 1;
+              if (l > kfill) continue;
+              if (lvl[size_t(j)] < 0) {
+                lvl[size_t(j)] = l; src[size_t(j)] = -1; cols.push_back(j);
+                if (j < i) { heap.push_back(j); std::push_heap(heap.begin(), heap.end(), std::greater<int32_t>()); }
+              } else if (l < lvl[size_t(j)]) {
+                lvl[size_t(j)] = l;
+              }
             }
           }
+          std::sort(cols.begin(), cols.end());
+          auto &row = rows[size_t(i)];
+          row.reserve(cols.size());
+          ub[size_t(i)] = int64_t(ucolv.size());
+          for (int32_t j : cols) {
+            row.push_back({j, src[size_t(j)]});
+            if (j > i) { ucolv.push_back(j); ulevv.push_back(lvl[size_t(j)]); }
+            lvl[size_t(j)] = -1; src[size_t(j)] = -1;
+          }
+          ue[size_t(i)] = int64_t(ucolv.size());
         }
-        std::sort(cols.begin(), cols.end());
-        auto &row = rows[size_t(i)];
-        row.reserve(cols.size());
-        for (int32_t j : cols) {
-          row.push_back({j, src[size_t(j)]});
-          if (j > i) { ucolv.push_back(j); ulevv.push_back(lvl[size_t(j)]); }
-          lvl[size_t(j)] = -1; src[size_t(j)] = -1;
-        }
-        urp[size_t(i) + 1] = int64_t(ucolv.size());
-      }
+      };
+      if (contiguous) host_parallel(nruns, 1, symbolic);
+      else symbolic(0, nruns);
     }
     // back to the caller's numbering, columns ascending
     frp.assign((size_t)n + 1, 0);
@@ -491,16 +531,18 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     for (int64_t i = 0; i < n; ++i) frp[size_t(i) + 1] += frp[size_t(i)];
     fci.resize(size_t(frp[size_t(n)]));
     fsrc.resize(size_t(frp[size_t(n)]));
-    std::vector<std::pair<int32_t, int64_t>> tmp;
-    for (int64_t i = 0; i < n; ++i) {
-      const int32_t o = base[size_t(i)];
-      tmp.clear();
-      for (auto &e : rows[size_t(i)]) tmp.push_back({base[size_t(e.first)], e.second});
-      std::sort(tmp.begin(), tmp.end());
-      int64_t p = frp[size_t(o)];
-      for (auto &e : tmp) { fci[size_t(p)] = e.first; fsrc[size_t(p)] = e.second; ++p; }
-      std::vector<std::pair<int32_t, int64_t>>().swap(rows[size_t(i)]);
-    }
+    host_parallel(n, int64_t(1) << 16, [&](int64_t i0, int64_t i1) {
+      std::vector<std::pair<int32_t, int64_t>> tmp;
+      for (int64_t i = i0; i < i1; ++i) {
+        const int32_t o = base[size_t(i)];
+        tmp.clear();
+        for (auto &e : rows[size_t(i)]) tmp.push_back({base[size_t(e.first)], e.second});
+        std::sort(tmp.begin(), tmp.end());
+        int64_t p = frp[size_t(o)];
+        for (auto &e : tmp) { fci[size_t(p)] = e.first; fsrc[size_t(p)] = e.second; ++p; }
+        std::vector<std::pair<int32_t, int64_t>>().swap(rows[size_t(i)]);
+      }
+    });
   }
   const int64_t fnnz = frp[size_t(n)];
   nnzF = fnnz;
@@ -567,22 +609,26 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   prp.assign((size_t)n + 1, 0); pdiag.assign((size_t)n, -1); amap.assign((size_t)fnnz, 0);
   pci.assign((size_t)fnnz, 0);
   {
-    std::vector<std::pair<int32_t, int64_t>> row;
-    for (int64_t i = 0; i < n; ++i) {
-      const int64_t o = perm[size_t(i)];
-      row.clear();
-      for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k) row.push_back({inv[size_t(fci[size_t(k)])], fsrc[size_t(k)]});
-      std::sort(row.begin(), row.end());
-      int64_t p = prp[size_t(i)];
-      for (auto &x : row) {
-        if (x.first == i) pdiag[size_t(i)] = p;
-        pci[size_t(p)] = x.first;
-        amap[size_t(p)] = x.second;
-        ++p;
+    for (int64_t i = 0; i < n; ++i) prp[size_t(i) + 1] = prp[size_t(i)] + (frp[size_t(perm[size_t(i)]) + 1] - frp[size_t(perm[size_t(i)])]);
+    host_parallel(n, int64_t(1) << 16, [&](int64_t i0, int64_t i1) {
+      std::vector<std::pair<int32_t, int64_t>> row;
+      for (int64_t i = i0; i < i1; ++i) {
+        const int64_t o = perm[size_t(i)];
+        row.clear();
+        for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k) row.push_back({inv[size_t(fci[size_t(k)])], fsrc[size_t(k)]});
+        std::sort(row.begin(), row.end());
+        int64_t p = prp[size_t(i)];
+        for (auto &x : row) {
+          if (x.first == i) pdiag[size_t(i)] = p;
+          pci[size_t(p)] = x.first;
+          amap[size_t(p)] = x.second;
+          ++p;
+        }
       }
-      prp[size_t(i) + 1] = p;
-      if (has_pc && pdiag[size_t(i)] < 0) { err = "no diagonal entry in row " + std::to_string(o); return VSHE_E_ZERO_PIVOT; }
-    }
+    });
+    if (has_pc)
+      for (int64_t i = 0; i < n; ++i)
+        if (pdiag[size_t(i)] < 0) { err = "no diagonal entry in row " + std::to_string(perm[size_t(i)]); return VSHE_E_ZERO_PIVOT; }
   }
   const int32_t PAD = int32_t(n);  // padding column: entry n of every vector stays 0
 
