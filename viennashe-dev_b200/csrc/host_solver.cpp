@@ -563,20 +563,44 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       for (int64_t i = 0; i < n; ++i)
         for (int64_t k = frp[size_t(i)]; k < frp[size_t(i) + 1]; ++k) tr[size_t(pos[size_t(fci[size_t(k)])]++)] = int32_t(i);
     }
-    for (int64_t i = 0; i < n; ++i) {
-      const int32_t o = base[size_t(i)];
-      int32_t m = -1;
-      for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k) {
-        const int32_t j = fci[size_t(k)];
-        if (binv[size_t(j)] < i && blk0[size_t(j)] == blk0[size_t(o)]) m = std::max(m, lev[size_t(j)]);
+    // a row reads only earlier rows of its own block: runs of one block in base order are
+    // levelled on several host threads when every block is one run
+    std::vector<int32_t> bblk((size_t)n);
+    for (int64_t i = 0; i < n; ++i) bblk[size_t(i)] = blk0[size_t(base[size_t(i)])];
+    const std::vector<int64_t> runs = block_runs(bblk);
+    const int64_t nruns = int64_t(runs.size()) - 1;
+    bool contiguous = true;
+    {
+      std::vector<char> seen;
+      for (int64_t r = 0; r < nruns && contiguous; ++r) {
+        const int32_t b = bblk[size_t(runs[size_t(r)])];
+        if (b >= int32_t(seen.size())) seen.resize(size_t(b) + 1, 0);
+        if (seen[size_t(b)]) contiguous = false;
+        seen[size_t(b)] = 1;
       }
-      for (int64_t k = tp[size_t(o)]; k < tp[size_t(o) + 1]; ++k) {
-        const int32_t j = tr[size_t(k)];
-        if (binv[size_t(j)] < i && blk0[size_t(j)] == blk0[size_t(o)]) m = std::max(m, lev[size_t(j)]);
-      }
-      lev[size_t(o)] = m + 1;
-      nlevL = std::max(nlevL, m + 2);
     }
+    std::mutex mu;
+    auto level = [&](int64_t r0, int64_t r1) {
+      int32_t nl = 1;
+      for (int64_t i = runs[size_t(r0)]; i < runs[size_t(r1)]; ++i) {
+        const int32_t o = base[size_t(i)];
+        int32_t m = -1;
+        for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k) {
+          const int32_t j = fci[size_t(k)];
+          if (binv[size_t(j)] < i && blk0[size_t(j)] == blk0[size_t(o)]) m = std::max(m, lev[size_t(j)]);
+        }
+        for (int64_t k = tp[size_t(o)]; k < tp[size_t(o) + 1]; ++k) {
+          const int32_t j = tr[size_t(k)];
+          if (binv[size_t(j)] < i && blk0[size_t(j)] == blk0[size_t(o)]) m = std::max(m, lev[size_t(j)]);
+        }
+        lev[size_t(o)] = m + 1;
+        nl = std::max(nl, m + 2);
+      }
+      std::lock_guard<std::mutex> lk(mu);
+      nlevL = std::max(nlevL, nl);
+    };
+    if (contiguous) host_parallel(nruns, 1, level);
+    else level(0, nruns);
   }
   // solver order: by level, then block (each block's rows of a level are one run, which the
   // per-block sweeps walk), then longest rows first (less SELL padding), then by the base
