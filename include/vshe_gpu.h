@@ -143,6 +143,11 @@ int vshe_set_profiling(vshe_ctx *ctx, int32_t on);
  * VSHE_E_TIMEOUT and the context stays usable.  0 restores the default (20,000,000 polls, about
  * 1-2 s).  No reference counterpart: failure handling of the device-side waits. */
 int vshe_set_spin_limit(vshe_ctx *ctx, uint64_t polls);
+/* Host threads the library uses for its host work (the layout of a pattern: colouring, symbolic
+ * ILU(k) per block, levels, pattern conversions; the drop-in call's value checks and pattern
+ * comparison), for every context of the process: 0 (default) up to 16, limited by the cores.
+ * Every choice gives the same layout and results.  No reference counterpart. */
+int vshe_set_host_threads(int32_t threads);
 /* Sweep kernel of the members swept one task per CTA or cluster (VSHE_TRSV_PER_BLOCK,
  * VSHE_TRSV_PER_SYSTEM and their AUTO cases): -1 (default) times the candidates on each batch's
  * own factors before its first iteration and keeps the fastest; 0 one CTA per task with the

@@ -153,11 +153,16 @@ int System::init_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_
   return VSHE_OK;
 }
 
+// Host threads of the library's host work (vshe_set_host_threads; 0: up to 16).
+static std::atomic<int> g_host_threads{0};
+
 // Runs fn(begin, end) over [0, n) in contiguous chunks of at least `grain` on up to 16 host
-// threads (the host-side checks of the drop-in call on arrays of hundreds of MB).
+// threads (the host-side checks of the drop-in call on arrays of hundreds of MB, the layout).
 static void host_parallel(int64_t n, int64_t grain, const std::function<void(int64_t, int64_t)> &fn) {
   const int64_t hw = std::max<int64_t>(1, int64_t(std::thread::hardware_concurrency()));
-  const int64_t T = std::min<int64_t>(std::min<int64_t>(hw, 16), std::max<int64_t>(1, n / std::max<int64_t>(grain, 1)));
+  const int cap = g_host_threads.load();
+  const int64_t tmax = cap > 0 ? int64_t(cap) : std::min<int64_t>(hw, 16);
+  const int64_t T = std::min<int64_t>(tmax, std::max<int64_t>(1, n / std::max<int64_t>(grain, 1)));
   if (T <= 1) { fn(0, n); return; }
   std::vector<std::thread> th;
   for (int64_t t = 0; t < T; ++t) th.emplace_back(fn, n * t / T, n * (t + 1) / T);
@@ -1887,6 +1892,12 @@ int vshe_set_task_sweep(vshe_ctx *ctx, int32_t kernel) {
   if (!ctx || kernel < -1 || kernel > 8 || kernel == 1 || (kernel > 2 && kernel != 4 && kernel != 8)) return VSHE_E_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->task_sweep = kernel;
+  return VSHE_OK;
+}
+
+int vshe_set_host_threads(int32_t threads) {
+  if (threads < 0) return VSHE_E_INVALID_ARGUMENT;
+  g_host_threads.store(threads);
   return VSHE_OK;
 }
 

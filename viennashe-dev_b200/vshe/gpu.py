@@ -114,6 +114,15 @@ def kernel_launches():
     return int(lib().vshe_kernel_launches())
 
 
+def set_host_threads(threads=0):
+    """vshe_set_host_threads: host threads of the library's host work (0: up to 16)."""
+    L = lib()
+    L.vshe_set_host_threads.argtypes = [C.c_int32]
+    rc = L.vshe_set_host_threads(int(threads))
+    if rc:
+        raise VsheError(rc, "vshe_set_host_threads")
+
+
 def make_opts(precision="mixed", precond="ilu0", tol=1e-10, max_iters=1000, inner_tol=1e-5,
               max_refinements=10, blocks=None, trsv="auto", check_every=8, ordering="natural", perm=None,
               shadow="dense", fill_level=0, ilut_entries=20, ilut_drop=1e-3):
