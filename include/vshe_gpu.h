@@ -273,6 +273,12 @@ typedef struct vshe_she_info {
 
 /* 6 * ((L+1)^2)^2 doubles, layout of vshe_coupling_tables.data; no GPU needed. */
 int vshe_coupling_tables_compute(int32_t L, double *out);
+/* The host set-up of a SHE problem alone, no GPU needed (capacity planning before a request is
+ * submitted): fills n_energies, n_even, n_odd, n_cells, n_facets, n_contacts, hbar_omega and
+ * bytes_estimate (the footprint bound vshe_she_create and the server admit by) of *info, the
+ * other fields 0.  opts may be NULL (the defaults). */
+int vshe_she_plan(const vshe_device_desc *dev, const vshe_she_config *cfg, const vshe_coupling_tables *coupling,
+                  const vshe_solve_opts *opts, vshe_she_info *info);
 int vshe_she_create(vshe_ctx *ctx, const vshe_device_desc *dev, const vshe_she_config *cfg,
                     const vshe_coupling_tables *coupling, const vshe_solve_opts *opts, int64_t *handle);
 int vshe_she_info_get(vshe_ctx *ctx, int64_t handle, vshe_she_info *info);

@@ -54,3 +54,13 @@ def test_vtk_point_cloud_reads_back(tmp_path):
     assert np.array_equal(pts[:, 0], dev.cell_centroid.reshape(-1)) and np.all(pts[:, 1:] == 0)
     assert np.array_equal(fields["potential"], dev.potential)
     assert np.array_equal(fields["electron_density"], dev.doping_n)
+
+
+def test_she_plan_sizes_match_oracle():
+    """vshe_she_plan (the host set-up alone, no GPU): the sizes the oracle's set-up gives."""
+    from vshe import gpu
+    for dev, cfg in (D.config1(), D.config2(nx=20, ny=5, n_energies=30, L=3)):
+        info = gpu.she_plan(dev, cfg, coupling=O.golden_coupling(cfg.max_expansion_order))
+        P = O.OracleProblem(dev, cfg, O.golden_coupling(cfg.max_expansion_order))
+        assert info["n_even"] == P.n_even and info["n_odd"] == P.n_odd and info["n_energies"] == P.NH
+        assert info["bytes_estimate"] > 0

@@ -479,6 +479,26 @@ int vshe_she_create(vshe_ctx *ctx, const vshe_device_desc *d, const vshe_she_con
   return VSHE_OK;
 }
 
+int vshe_she_plan(const vshe_device_desc *d, const vshe_she_config *c, const vshe_coupling_tables *ct,
+                  const vshe_solve_opts *opts, vshe_she_info *info) {
+  if (!d || !c || !ct || !info) return VSHE_E_INVALID_ARGUMENT;
+  SheProblem S;
+  if (opts) S.opts = *opts; else vshe_default_opts(&S.opts);
+  if (!S.H.build(*d, *c, *ct).empty()) return VSHE_E_INVALID_ARGUMENT;
+  std::memset(info, 0, sizeof(*info));
+  int ncont = 0;
+  for (int i = 0; i < S.H.nc; ++i) ncont = std::max(ncont, S.H.contact[i] + 1);
+  info->n_energies = S.H.NH;
+  info->n_even = S.H.n_even;
+  info->n_odd = S.H.n_odd;
+  info->n_cells = S.H.nc;
+  info->n_facets = S.H.nf;
+  info->n_contacts = ncont;
+  info->hbar_omega = S.H.hbar_omega;
+  info->bytes_estimate = int64_t(S.estimate_bytes());
+  return VSHE_OK;
+}
+
 int vshe_she_info_get(vshe_ctx *ctx, int64_t h, vshe_she_info *info) {
   if (!ctx || !info) return VSHE_E_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(ctx->mu);

@@ -353,6 +353,24 @@ def coupling_tables(L):
     return Coupling(L, out)
 
 
+def she_plan(dev, cfg, coupling=None, **opts):
+    """vshe_she_plan: the host set-up of a SHE problem alone (no GPU) -> dict of the sizes and the
+    footprint bound the library admits the problem by."""
+    from .abi import DeviceDesc, she_config_c
+    L = _she_lib()
+    L.vshe_she_plan.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SheInfoC)]
+    desc = DeviceDesc(dev)
+    cfgc = she_config_c(cfg)
+    cpl = coupling if coupling is not None else coupling_tables(cfg.max_expansion_order)
+    o, keep = make_opts(**opts) if opts else (None, None)
+    inf = SheInfoC()
+    rc = L.vshe_she_plan(C.byref(desc.c), C.byref(cfgc), C.byref(cpl.c), C.byref(o) if o is not None else None, C.byref(inf))
+    if rc:
+        raise VsheError(rc, "vshe_she_plan")
+    keys = ("n_energies", "n_even", "n_odd", "n_cells", "n_facets", "n_contacts", "hbar_omega", "bytes_estimate")
+    return {k: getattr(inf, k) for k in keys}
+
+
 class PoissonStatsC(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("rel_residual", C.c_double),
                 ("rhs_norm", C.c_double), ("update_norm", C.c_double), ("n_unknowns", C.c_int64)]
