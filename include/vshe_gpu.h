@@ -279,6 +279,18 @@ int vshe_coupling_tables_compute(int32_t L, double *out);
  * other fields 0.  opts may be NULL (the defaults). */
 int vshe_she_plan(const vshe_device_desc *dev, const vshe_she_config *cfg, const vshe_coupling_tables *coupling,
                   const vshe_solve_opts *opts, vshe_she_info *info);
+/* The (x, H) space of the same set-up, no GPU needed, so that a caller can read the unknowns of
+ * x_full (vshe_she_results) per cell and energy -- the quantity the reference's distribution
+ * function wrappers look up (viennashe/she/df_wrappers.hpp:45-90, 230-260): the N_H total
+ * energies (J); per cell and energy, at [cell * N_H + H], the index in x_full of the node's first
+ * even unknown (-1: no unknown there; the node's harmonics follow in the order of
+ * spherical_harmonics.hpp:213-252), its expansion order, the kinetic energy H - E_c(cell) (J) and
+ * the density of states there (Modena dispersion, viennashe/physics/dispersion.hpp:207-286); per
+ * facet and energy, at [facet * N_H + H], the first odd unknown's index and the order.  Sizes are
+ * vshe_she_plan's n_energies, n_cells and n_facets.  Any output pointer may be NULL. */
+int vshe_she_space(const vshe_device_desc *dev, const vshe_she_config *cfg, const vshe_coupling_tables *coupling,
+                   double *energies, int64_t *even_index, int32_t *even_order, double *kinetic_energy,
+                   double *density_of_states, int64_t *odd_index, int32_t *odd_order);
 int vshe_she_create(vshe_ctx *ctx, const vshe_device_desc *dev, const vshe_she_config *cfg,
                     const vshe_coupling_tables *coupling, const vshe_solve_opts *opts, int64_t *handle);
 int vshe_she_info_get(vshe_ctx *ctx, int64_t handle, vshe_she_info *info);

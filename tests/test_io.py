@@ -64,3 +64,91 @@ def test_she_plan_sizes_match_oracle():
         P = O.OracleProblem(dev, cfg, O.golden_coupling(cfg.max_expansion_order))
         assert info["n_even"] == P.n_even and info["n_odd"] == P.n_odd and info["n_energies"] == P.NH
         assert info["bytes_estimate"] > 0
+
+
+def _space_case():
+    return D.config2(nx=12, ny=4, n_energies=20, L=3)
+
+
+def test_she_space_matches_oracle_mapping():
+    """vshe_she_space (host set-up, no GPU): the oracle's energies and (x, H) mapping, entry for
+    entry, and the density of states of the oracle's restatement of the Modena dispersion."""
+    import ctypes as C
+    from vshe import gpu
+    for dev, cfg in (D.config1(), _space_case()):
+        cpl = O.golden_coupling(cfg.max_expansion_order)
+        sp = gpu.she_space(dev, cfg, coupling=cpl)
+        P = O.OracleProblem(dev, cfg, cpl)
+        H, sc, sf, _ = P.energies()
+        ic, jf, oc, of, _ = P.mapping()
+        nc, nf, nh = dev.n_cells, dev.n_facets, P.NH
+        assert np.array_equal(sp["energies"], H)
+        assert np.array_equal(sp["even_index"], ic.reshape(nc, nh))
+        assert np.array_equal(sp["odd_index"], jf.reshape(nf, nh))
+        assert np.array_equal(sp["even_order"], oc.reshape(nc, nh))
+        assert np.array_equal(sp["odd_order"], of.reshape(nf, nh))
+        assert np.array_equal(sp["kinetic_energy"], H[None, :] - sc[:, None])
+        probe = O.lib().vsheo_physics_probe
+        probe.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        eps = sp["kinetic_energy"].reshape(-1)
+        ref = np.zeros_like(eps)
+        out = np.zeros(8)
+        for k in range(0, eps.size, max(1, eps.size // 200)):
+            a = np.array([eps[k]])
+            probe(0, a.ctypes.data_as(C.POINTER(C.c_double)), out.ctypes.data_as(C.POINTER(C.c_double)))
+            ref[k] = out[0]
+            assert sp["density_of_states"].reshape(-1)[k] == ref[k]
+        # every even unknown belongs to exactly one node
+        used = sp["even_index"][sp["even_index"] >= 0]
+        assert np.unique(used).size == used.size and used.max() < P.n_even
+
+
+def test_gnuplot_edf_layouts(tmp_path):
+    """The two layouts of the reference's EDF writer (gnuplot_writer_edf.hpp:54-110, 117-175) from
+    a full solution of the oracle (the tiny bar's reduced system solved on the CPU)."""
+    from vshe import gpu
+    dev, cfg = _space_case()
+    cpl = O.golden_coupling(cfg.max_expansion_order)
+    sp = gpu.she_space(dev, cfg, coupling=cpl)
+    P = O.OracleProblem(dev, cfg, cpl)
+    A = P.matrix(3)
+    x_red, st = O.csr_solve(A, A.rhs, tol=1e-12)
+    assert st["rc"] == 0 and st["relres"] <= 1e-12
+    xf = P.finish(x_red)[0]
+    y00 = 1.0 / np.sqrt(4.0 * np.pi)
+    edf = vio.edf_values(sp, xf)
+    m = sp["even_index"] >= 0
+    assert np.allclose(edf[m], xf[sp["even_index"][m]] * y00, rtol=1e-15, atol=0)
+    cen = dev.cell_centroid.reshape(dev.n_cells, 2)
+    # filtered writer: the cells of the bottom row
+    cells = [c for c in range(dev.n_cells) if cen[c, 1] == cen[0, 1]]
+    path = tmp_path / "edf.dat"
+    vio.write_gnuplot_edf(path, dev, sp, xf, cells=lambda c: cen[c, 1] == cen[0, 1])
+    want = []
+    for c in cells:
+        for h in range(1, P.NH - 1):
+            if sp["even_index"][c, h] > -1 and sp["kinetic_energy"][c, h] > 0:
+                want.append("%g %g %g %g %g" % (cen[c, 0], cen[c, 1], sp["kinetic_energy"][c, h] / 1.602176565e-19,
+                                                edf[c, h], sp["density_of_states"][c, h]))
+        want += ["", ""]
+    got = open(path).read().split("\n")
+    k = 0
+    for w in want:
+        if w:
+            assert got[k] == w, (k, got[k], w)
+        else:
+            assert got[k] == ""
+        k += 1
+    # line writer at the first column's x: sorted by (y, kinetic energy), a blank line per y
+    path2 = tmp_path / "edf_line.dat"
+    x0 = cen[int(np.argmax((sp["even_index"] >= 0).sum(axis=1))), 0]
+    vio.write_gnuplot_edf_line(path2, dev, sp, xf, x0)
+    lines = open(path2).read().split("\n")[:-1]
+    col = [c for c in range(dev.n_cells) if cen[c, 0] == x0]
+    expect = []
+    for c in sorted(col, key=lambda c: cen[c, 1]):
+        rows = sorted((sp["kinetic_energy"][c, h], edf[c, h]) for h in range(1, P.NH - 1) if sp["even_index"][c, h] > -1)
+        expect += [""] * bool(rows) + ["%g %g %g" % (cen[c, 1], e, v) for e, v in rows]
+    assert len(expect) > 4 * len(col) and lines == expect
+    # the EDF is positive where the carrier population lives (well above the band edge)
+    assert np.all(edf[m & (sp["kinetic_energy"] > 0)] > 0)

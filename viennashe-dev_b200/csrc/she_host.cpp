@@ -67,6 +67,8 @@ double contact_carrier_ohm_n(double T, double nd, double na) {
 }
 }  // namespace
 
+double density_of_states(double eps) { return dos(eps); }
+
 // ------------------------------------------------------------------ build
 std::string SheSetup::build(const vshe_device_desc &d, const vshe_she_config &c, const vshe_coupling_tables &ct) {
   if (d.dim < 1 || d.dim > 2) return "dim must be 1 or 2";

@@ -63,6 +63,10 @@ struct SheSetup {
   double ekin_f(int f, int H) const { return Hval[H] - shift_f[f]; }
 };
 
+// Density of states of the Modena dispersion for silicon electrons at kinetic energy eps (J),
+// per unit volume and energy (viennashe/physics/dispersion.hpp:207-286); 0 for eps <= 0.
+double density_of_states(double eps);
+
 // Spherical-harmonics coupling tables a_{x,y,z}, b_{x,y,z} of order L computed by
 // quadrature of the integrals that define them (viennashe/she/harmonics_coupling.hpp:39-200,
 // 216-278): out has 6 * D * D entries, values below 1e-8 in magnitude set to 0.

@@ -499,6 +499,27 @@ int vshe_she_plan(const vshe_device_desc *d, const vshe_she_config *c, const vsh
   return VSHE_OK;
 }
 
+int vshe_she_space(const vshe_device_desc *d, const vshe_she_config *c, const vshe_coupling_tables *ct, double *energies,
+                   int64_t *even_index, int32_t *even_order, double *kinetic_energy, double *density_of_states,
+                   int64_t *odd_index, int32_t *odd_order) {
+  if (!d || !c || !ct) return VSHE_E_INVALID_ARGUMENT;
+  SheSetup H;
+  if (!H.build(*d, *c, *ct).empty()) return VSHE_E_INVALID_ARGUMENT;
+  const size_t nh = size_t(H.NH), cells = size_t(H.nc) * nh, facets = size_t(H.nf) * nh;
+  if (energies) std::copy(H.Hval.begin(), H.Hval.end(), energies);
+  if (even_index) std::copy(H.idx_c.begin(), H.idx_c.begin() + cells, even_index);
+  if (even_order) std::copy(H.ord_c.begin(), H.ord_c.begin() + cells, even_order);
+  if (odd_index) std::copy(H.idx_f.begin(), H.idx_f.begin() + facets, odd_index);
+  if (odd_order) std::copy(H.ord_f.begin(), H.ord_f.begin() + facets, odd_order);
+  for (int i = 0; i < H.nc; ++i)
+    for (int h = 0; h < H.NH; ++h) {
+      const double eps = H.ekin_c(i, h);
+      if (kinetic_energy) kinetic_energy[size_t(i) * nh + size_t(h)] = eps;
+      if (density_of_states) density_of_states[size_t(i) * nh + size_t(h)] = vshe::density_of_states(eps);
+    }
+  return VSHE_OK;
+}
+
 int vshe_she_info_get(vshe_ctx *ctx, int64_t h, vshe_she_info *info) {
   if (!ctx || !info) return VSHE_E_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(ctx->mu);

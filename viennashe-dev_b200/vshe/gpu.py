@@ -371,6 +371,29 @@ def she_plan(dev, cfg, coupling=None, **opts):
     return {k: getattr(inf, k) for k in keys}
 
 
+def she_space(dev, cfg, coupling=None):
+    """vshe_she_space: the (x, H) space of the host set-up (no GPU) -> dict of "energies" (N_H),
+    per cell and energy (shape (n_cells, N_H)) "even_index" (first even unknown in x_full, -1:
+    none), "even_order", "kinetic_energy" and "density_of_states", per facet and energy
+    "odd_index" and "odd_order"."""
+    from .abi import DeviceDesc, she_config_c
+    info = she_plan(dev, cfg, coupling)
+    L = _she_lib()
+    L.vshe_she_space.argtypes = [C.c_void_p] * 10
+    desc = DeviceDesc(dev)
+    cfgc = she_config_c(cfg)
+    cpl = coupling if coupling is not None else coupling_tables(cfg.max_expansion_order)
+    nh, nc, nf = info["n_energies"], info["n_cells"], info["n_facets"]
+    out = {"energies": np.zeros(nh), "even_index": np.zeros((nc, nh), np.int64), "even_order": np.zeros((nc, nh), np.int32),
+           "kinetic_energy": np.zeros((nc, nh)), "density_of_states": np.zeros((nc, nh)),
+           "odd_index": np.zeros((nf, nh), np.int64), "odd_order": np.zeros((nf, nh), np.int32)}
+    order = ("energies", "even_index", "even_order", "kinetic_energy", "density_of_states", "odd_index", "odd_order")
+    rc = L.vshe_she_space(C.byref(desc.c), C.byref(cfgc), C.byref(cpl.c), *[out[k].ctypes.data for k in order])
+    if rc:
+        raise VsheError(rc, "vshe_she_space")
+    return out
+
+
 class PoissonStatsC(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("rel_residual", C.c_double),
                 ("rhs_norm", C.c_double), ("update_norm", C.c_double), ("n_unknowns", C.c_int64)]

@@ -8,6 +8,10 @@
   (viennashe/io/gnuplot_writer.hpp:47-118): a ``## ViennaSHE - gnuplot output`` line, then one
   line per cell with the centroid coordinates and the value, each followed by a space, numbers
   as C++ streams print doubles by default (``%g``).
+* ``write_gnuplot_edf`` / ``write_gnuplot_edf_line``: the energy distribution function of a
+  solved problem, in the layouts of the reference's EDF writer
+  (viennashe/io/gnuplot_writer_edf.hpp:54-110 and :117-175), from ``x_full`` and the (x, H)
+  space of ``vshe.gpu.she_space``.
 * ``write_vtk``: per-cell quantities as a legacy-format VTK point cloud at the cell centroids.
   The reference's VTK writers (viennashe/io/she_vtk_writer.hpp) write the mesh cells; a
   ``vshe_device_desc`` carries no vertices, so the cells are written as points.
@@ -15,6 +19,7 @@
 from __future__ import annotations
 
 import dataclasses
+import math
 
 import numpy as np
 
@@ -65,6 +70,79 @@ def write_gnuplot(path, dev: Device, values, cells=None):
             v = vals[c]
             line += "".join("%g " % x for x in np.atleast_1d(v))
             f.write(line + "\n")
+
+
+_Q = 1.602176565e-19   # viennashe/physics/constants.hpp
+# Y_0^0 as the reference evaluates it (viennashe/math/spherical_harmonics.hpp:100-115): the
+# normalisation sqrt((2l+1) (l-m)! / (2 pi (l+m)!)) times P_0^0 = 1, over sqrt(2) for m = 0
+_Y00 = math.sqrt((2.0 * 0 + 1.0) * 1.0 / (2.0 * math.pi * 1.0)) * 1.0 / math.sqrt(2.0)
+
+
+def edf_values(space, x_full):
+    """The energy distribution function f_00 Y_00 per cell and energy (shape (n_cells, N_H)) from a
+    full solution, as the reference's edf_wrapper returns it at a node's own kinetic energy
+    (viennashe/she/df_wrappers.hpp:517-562, even-odd DF discretisation): the node's first even
+    unknown times Y_0^0; 0 where the node has no unknown."""
+    idx = space["even_index"]
+    x = np.asarray(x_full, np.float64)
+    out = np.zeros(idx.shape)
+    m = idx >= 0
+    out[m] = x[idx[m]] * _Y00
+    return out
+
+
+def _cell_list(dev, cells):
+    if cells is None:
+        return range(dev.n_cells)
+    if callable(cells):
+        return [c for c in range(dev.n_cells) if cells(c)]
+    return cells
+
+
+def write_gnuplot_edf(path, dev: Device, space, x_full, cells=None):
+    """The reference's EDF writer with a cell filter (gnuplot_writer_edf.hpp:117-175): for every
+    cell that passes (cells: None = all, a callable on the cell index, or a list of cells), one
+    line per interior energy with an unknown and a positive kinetic energy -- the centroid
+    coordinates, the kinetic energy in eV, the EDF and the density of states -- then two empty
+    lines (a gnuplot block).  Numbers as C++ streams print doubles by default (%g)."""
+    cen = np.asarray(dev.cell_centroid, np.float64).reshape(dev.n_cells, dev.dim)
+    idx, eps, dos = space["even_index"], space["kinetic_energy"], space["density_of_states"]
+    f_edf = edf_values(space, x_full)
+    nh = idx.shape[1]
+    with open(path, "w") as f:
+        for c in _cell_list(dev, cells):
+            pre = "".join("%g " % v for v in cen[c])
+            for h in range(1, nh - 1):
+                if idx[c, h] > -1 and eps[c, h] > 0:
+                    f.write(pre + "%g %g %g\n" % (eps[c, h] / _Q, f_edf[c, h], dos[c, h]))
+            f.write("\n\n")
+
+
+def write_gnuplot_edf_line(path, dev: Device, space, x_full, coordinate_x):
+    """The reference's EDF writer along a vertical line of a 2D device (gnuplot_writer_edf.hpp:
+    54-110): the cells whose centroid has x == coordinate_x, every interior energy with an unknown,
+    as lines "y kinetic_energy(J) EDF" sorted by (y, kinetic energy), with an empty line before
+    each new y (and before the first, as the reference starts from y = -1)."""
+    if dev.dim < 2:
+        raise ValueError("write_gnuplot_edf_line needs a 2D device (it sorts by the centroid's y)")
+    cen = np.asarray(dev.cell_centroid, np.float64).reshape(dev.n_cells, dev.dim)
+    idx, eps = space["even_index"], space["kinetic_energy"]
+    f_edf = edf_values(space, x_full)
+    nh = idx.shape[1]
+    values = {}
+    for c in range(dev.n_cells):
+        if cen[c, 0] != coordinate_x:
+            continue
+        for h in range(1, nh - 1):
+            if idx[c, h] > -1:
+                values[(float(cen[c, 1]), float(eps[c, h]))] = f_edf[c, h]
+    last_y = -1.0
+    with open(path, "w") as f:
+        for (y, e) in sorted(values):
+            if y != last_y:
+                f.write("\n")
+                last_y = y
+            f.write("%g %g %g\n" % (y, e, values[(y, e)]))
 
 
 def write_vtk(path, dev: Device, fields: dict, title="ViennaSHE B200 results"):
