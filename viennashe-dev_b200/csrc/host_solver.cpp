@@ -156,17 +156,79 @@ int System::init_borrowed(Ctx &ctx, int64_t n_, int64_t nnz_, const int64_t *rp_
 // Host threads of the library's host work (vshe_set_host_threads; 0: up to 16).
 static std::atomic<int> g_host_threads{0};
 
-// Runs fn(begin, end) over [0, n) in contiguous chunks of at least `grain` on up to 16 host
-// threads (the host-side checks of the drop-in call on arrays of hundreds of MB, the layout).
-static void host_parallel(int64_t n, int64_t grain, const std::function<void(int64_t, int64_t)> &fn) {
+// Host threads for n items in chunks of at least `grain`: up to 16 (or the vshe_set_host_threads cap).
+static int64_t host_threads(int64_t n, int64_t grain) {
   const int64_t hw = std::max<int64_t>(1, int64_t(std::thread::hardware_concurrency()));
   const int cap = g_host_threads.load();
   const int64_t tmax = cap > 0 ? int64_t(cap) : std::min<int64_t>(hw, 16);
-  const int64_t T = std::min<int64_t>(tmax, std::max<int64_t>(1, n / std::max<int64_t>(grain, 1)));
+  return std::min<int64_t>(tmax, std::max<int64_t>(1, n / std::max<int64_t>(grain, 1)));
+}
+
+// Runs fn(begin, end) over [0, n) in contiguous chunks of at least `grain` on up to 16 host
+// threads (the host-side checks of the drop-in call on arrays of hundreds of MB, the layout).
+static void host_parallel(int64_t n, int64_t grain, const std::function<void(int64_t, int64_t)> &fn) {
+  const int64_t T = host_threads(n, grain);
   if (T <= 1) { fn(0, n); return; }
   std::vector<std::thread> th;
   for (int64_t t = 0; t < T; ++t) th.emplace_back(fn, n * t / T, n * (t + 1) / T);
   for (auto &x : th) x.join();
+}
+
+// Runs fn(r0, r1) over the runs of a row partition (run r = rows [runs[r], runs[r + 1])) on the
+// host threads, in contiguous chunks of whole runs that hold about the same number of rows.
+static void host_parallel_runs(const std::vector<int64_t> &runs, const std::function<void(int64_t, int64_t)> &fn) {
+  const int64_t nruns = int64_t(runs.size()) - 1;
+  if (nruns <= 0) return;
+  const int64_t T = host_threads(nruns, 1);
+  if (T <= 1) { fn(0, nruns); return; }
+  const int64_t first = runs.front(), rows = runs.back() - runs.front();
+  std::vector<int64_t> cut(1, 0);
+  for (int64_t t = 1; t < T; ++t) {
+    const int64_t r = int64_t(std::lower_bound(runs.begin(), runs.end() - 1, first + rows * t / T) - runs.begin());
+    if (r > cut.back() && r < nruns) cut.push_back(r);
+  }
+  cut.push_back(nruns);
+  std::vector<std::thread> th;
+  for (size_t c = 0; c + 1 < cut.size(); ++c) th.emplace_back(fn, cut[c], cut[c + 1]);
+  for (auto &x : th) x.join();
+}
+
+// Transpose of the pattern (rp, ci) of n rows over n columns: tp (n + 1 offsets) and tr, the rows
+// holding each column, ascending (the order a serial pass over the rows writes them in).
+static void transpose_pattern(int64_t n, const int64_t *rp, const int32_t *ci, std::vector<int64_t> &tp, std::vector<int32_t> &tr) {
+  std::unique_ptr<std::atomic<int64_t>[]> cur(new std::atomic<int64_t>[size_t(n)]);
+  host_parallel(n, int64_t(1) << 16, [&](int64_t a, int64_t b) {
+    for (int64_t i = a; i < b; ++i) cur[size_t(i)].store(0, std::memory_order_relaxed);
+  });
+  host_parallel(n, int64_t(1) << 16, [&](int64_t a, int64_t b) {
+    for (int64_t i = a; i < b; ++i)
+      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) cur[size_t(ci[k])].fetch_add(1, std::memory_order_relaxed);
+  });
+  tp.assign(size_t(n) + 1, 0);
+  for (int64_t i = 0; i < n; ++i) {
+    tp[size_t(i) + 1] = tp[size_t(i)] + cur[size_t(i)].load(std::memory_order_relaxed);
+    cur[size_t(i)].store(tp[size_t(i)], std::memory_order_relaxed);
+  }
+  tr.resize(size_t(tp[size_t(n)]));
+  host_parallel(n, int64_t(1) << 16, [&](int64_t a, int64_t b) {
+    for (int64_t i = a; i < b; ++i)
+      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tr[size_t(cur[size_t(ci[k])].fetch_add(1, std::memory_order_relaxed))] = int32_t(i);
+  });
+  host_parallel(n, int64_t(1) << 16, [&](int64_t a, int64_t b) {
+    for (int64_t j = a; j < b; ++j) std::sort(tr.begin() + tp[size_t(j)], tr.begin() + tp[size_t(j) + 1]);
+  });
+}
+
+// Stable counting sort of seq by key(x) in [0, range): equal keys keep their order.
+template <class Key>
+static void counting_sort_by(std::vector<int32_t> &seq, int64_t range, Key key) {
+  if (range <= 1) return;
+  std::vector<int64_t> pos(size_t(range) + 1, 0);
+  for (int32_t x : seq) pos[size_t(key(x)) + 1]++;
+  for (int64_t k = 0; k < range; ++k) pos[size_t(k) + 1] += pos[size_t(k)];
+  std::vector<int32_t> out(seq.size());
+  for (int32_t x : seq) out[size_t(pos[size_t(key(x))]++)] = x;
+  seq.swap(out);
 }
 
 // First index in [0, n) whose value is not finite, or n.
@@ -231,22 +293,39 @@ static std::vector<int64_t> block_runs(const std::vector<int32_t> &blk) {
 // coloured on several host threads with the same result.
 static void greedy_colours(int64_t n, const std::vector<int64_t> &rp, const std::vector<int32_t> &ci, const std::vector<int32_t> &blk,
                            std::vector<int32_t> &col, int distance) {
-  std::vector<int64_t> tcnt((size_t)(n) + 1, 0);
-  for (int64_t i = 0; i < n; ++i)
-    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tcnt[size_t(ci[k]) + 1]++;
-  for (int64_t i = 0; i < n; ++i) tcnt[size_t(i) + 1] += tcnt[size_t(i)];
-  std::vector<int32_t> tci(size_t(tcnt[size_t(n)]));
-  std::vector<int64_t> pos(tcnt.begin(), tcnt.end() - 1);
-  for (int64_t i = 0; i < n; ++i)
-    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tci[size_t(pos[size_t(ci[k])]++)] = int32_t(i);
+  // neighbours of every row in the symmetrised pattern, each once and without the row itself (a
+  // row's colour depends only on the set of colours around it): the union of its row and its
+  // column, on the host threads
+  std::vector<int64_t> sp(size_t(n) + 1, 0);
+  std::vector<int32_t> sj;
+  {
+    std::vector<int64_t> tcnt;
+    std::vector<int32_t> tci;
+    transpose_pattern(n, rp.data(), ci.data(), tcnt, tci);
+    auto gather = [&](int64_t i, std::vector<int32_t> &v) {
+      v.clear();
+      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) if (ci[k] != i) v.push_back(ci[k]);
+      for (int64_t k = tcnt[size_t(i)]; k < tcnt[size_t(i) + 1]; ++k) if (tci[size_t(k)] != i) v.push_back(tci[size_t(k)]);
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+    };
+    host_parallel(n, int64_t(1) << 16, [&](int64_t a, int64_t b) {
+      std::vector<int32_t> v;
+      for (int64_t i = a; i < b; ++i) { gather(i, v); sp[size_t(i) + 1] = int64_t(v.size()); }
+    });
+    for (int64_t i = 0; i < n; ++i) sp[size_t(i) + 1] += sp[size_t(i)];
+    sj.resize(size_t(sp[size_t(n)]));
+    host_parallel(n, int64_t(1) << 16, [&](int64_t a, int64_t b) {
+      std::vector<int32_t> v;
+      for (int64_t i = a; i < b; ++i) { gather(i, v); std::copy(v.begin(), v.end(), sj.begin() + sp[size_t(i)]); }
+    });
+  }
   col.assign(size_t(n), -1);
   auto neighbours = [&](int64_t i, auto &&fn) {
-    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) fn(ci[k]);
-    for (int64_t k = tcnt[size_t(i)]; k < tcnt[size_t(i) + 1]; ++k) fn(tci[size_t(k)]);
+    for (int64_t k = sp[size_t(i)]; k < sp[size_t(i) + 1]; ++k) fn(sj[size_t(k)]);
   };
   const std::vector<int64_t> runs = block_runs(blk);
-  const int64_t nruns = int64_t(runs.size()) - 1;
-  host_parallel(nruns, 1, [&](int64_t r0, int64_t r1) {
+  host_parallel_runs(runs, [&](int64_t r0, int64_t r1) {
     std::vector<int64_t> mark(64, -1);
     for (int64_t i = runs[size_t(r0)]; i < runs[size_t(r1)]; ++i) {
       auto visit = [&](int32_t j) {
@@ -322,6 +401,7 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       for (int64_t i = bp[b]; i < bp[b + 1]; ++i) blk0[size_t(i)] = int32_t(b);
     }
   }
+  const int64_t nblk = int64_t(*std::max_element(blk0.begin(), blk0.end())) + 1;
   // base ordering of the preconditioner: base[i] = caller row at base position i
   std::vector<int32_t> base((size_t)n);
   if (opts.perm) {
@@ -337,11 +417,10 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     // ILU(k > 0): rows two steps apart get different colours too, so that the fill (which
     // couples such rows) does not chain rows of one colour into extra levels
     greedy_colours(n, rp, ci, blk0, col, opts.fill_level > 0 ? 2 : 1);
+    // by block, then colour, then row (two stable counting passes)
     std::iota(base.begin(), base.end(), 0);
-    std::stable_sort(base.begin(), base.end(), [&](int32_t a, int32_t b) {
-      if (blk0[size_t(a)] != blk0[size_t(b)]) return blk0[size_t(a)] < blk0[size_t(b)];
-      return col[size_t(a)] < col[size_t(b)];
-    });
+    counting_sort_by(base, int64_t(*std::max_element(col.begin(), col.end())) + 1, [&](int32_t a) { return col[size_t(a)]; });
+    counting_sort_by(base, nblk, [&](int32_t a) { return blk0[size_t(a)]; });
   } else {
     std::iota(base.begin(), base.end(), 0);
   }
@@ -372,7 +451,18 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
         std::sort(bent.begin() + brp[size_t(i)], bent.begin() + p);
       }
     });
-    std::vector<std::vector<std::pair<int32_t, int64_t>>> rows((size_t)n);  // base order: (base column, entry or -1)
+    // rows of F in base order, (base column, entry or -1), in one flat store per host thread:
+    // row i is (*rstore[rsid[i]])[roff[i] .. roff[i] + rcnt[i])
+    typedef std::vector<std::pair<int32_t, int64_t>> RowStore;
+    std::vector<std::unique_ptr<RowStore>> rstore;
+    std::mutex rmu;
+    std::vector<int32_t> rsid((size_t)n, 0);
+    std::vector<int64_t> roff((size_t)n, 0), rcnt((size_t)n, 0);
+    auto new_store = [&]() {
+      std::lock_guard<std::mutex> lk(rmu);
+      rstore.emplace_back(new RowStore);
+      return int32_t(rstore.size() - 1);
+    };
     if (ilut) {
       // ILUT(p, tau), Saad Alg. 10.6, in base order: the row is eliminated with the kept rows
       // above it in increasing column order; a multiplier or entry below tau * ||a_i|| is
@@ -389,6 +479,8 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       std::vector<char> nz((size_t)n, 0);
       std::vector<int32_t> cols, heap;
       std::vector<std::pair<double, int32_t>> lo, up;
+      const int32_t sid = new_store();
+      RowStore &st = *rstore[size_t(sid)];
       for (int64_t i = 0; i < n; ++i) {
         cols.clear(); heap.clear();
         double rn = 0.0;
@@ -450,14 +542,15 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
         for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) pat.push_back(bent[size_t(k)].first);
         std::sort(pat.begin(), pat.end());
         pat.erase(std::unique(pat.begin(), pat.end()), pat.end());
-        auto &row = rows[size_t(i)];
-        row.reserve(pat.size());
+        rsid[size_t(i)] = sid;
+        roff[size_t(i)] = int64_t(st.size());
         int64_t ka = brp[size_t(i)];
         for (int32_t j : pat) {
           while (ka < brp[size_t(i) + 1] && bent[size_t(ka)].first < j) ++ka;
           const bool in_a = ka < brp[size_t(i) + 1] && bent[size_t(ka)].first == j;
-          row.push_back({j, in_a ? bent[size_t(ka)].second : int64_t(-1)});
+          st.push_back({j, in_a ? bent[size_t(ka)].second : int64_t(-1)});
         }
+        rcnt[size_t(i)] = int64_t(st.size()) - roff[size_t(i)];
         for (int32_t j : cols) { nz[size_t(j)] = 0; w[size_t(j)] = 0.0; }
       }
     } else {
@@ -482,15 +575,22 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       std::vector<int64_t> ub((size_t)n, 0), ue((size_t)n, 0);  // upper part of row k: [ub[k], ue[k]) in its thread's store
       auto symbolic = [&](int64_t r0, int64_t r1) {
         std::vector<int32_t> ucolv, ulevv;
-        std::vector<int32_t> lvl((size_t)n, -1);
-        std::vector<int64_t> src((size_t)n, -1);
+        // scratch over all columns: lvl1[j] = level of fill of column j + 1 (0: not in the row),
+        // src[j] its entry of A; calloc'd and left uninitialised, so that a thread touches only the
+        // pages of the columns its rows reach
+        std::unique_ptr<int32_t, void (*)(void *)> lvl1((int32_t *)std::calloc(size_t(n), sizeof(int32_t)), std::free);
+        std::unique_ptr<int64_t[]> src(new int64_t[size_t(n)]);
+        if (!lvl1) throw std::bad_alloc();
+        int32_t *lvl = lvl1.get();
+        const int32_t sid = new_store();
+        RowStore &st = *rstore[size_t(sid)];
         std::vector<int32_t> cols, heap;
         for (int64_t i = runs[size_t(r0)]; i < runs[size_t(r1)]; ++i) {
           const int32_t bi = bblk[size_t(i)];
           cols.clear(); heap.clear();
           for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) {
             const int32_t j = bent[size_t(k)].first;
-            lvl[size_t(j)] = 0; src[size_t(j)] = bent[size_t(k)].second; cols.push_back(j);
+            lvl[size_t(j)] = 1; src[size_t(j)] = bent[size_t(k)].second; cols.push_back(j);
             if (j < i) heap.push_back(j);
           }
           std::make_heap(heap.begin(), heap.end(), std::greater<int32_t>());
@@ -501,38 +601,39 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
             if (k == last) continue;
             last = k;
             if (bblk[size_t(k)] != bi) continue;
-            const int32_t lik = lvl[size_t(k)];
+            const int32_t lik = lvl[size_t(k)] - 1;
             for (int64_t kk = ub[size_t(k)]; kk < ue[size_t(k)]; ++kk) {
               const int32_t j = ucolv[size_t(kk)];
               if (bblk[size_t(j)] != bi) continue;
               const int32_t l = lik + ulevv[size_t(kk)] + 1;
               if (l > kfill) continue;
-              if (lvl[size_t(j)] < 0) {
-                lvl[size_t(j)] = l; src[size_t(j)] = -1; cols.push_back(j);
+              if (lvl[size_t(j)] == 0) {
+                lvl[size_t(j)] = l + 1; src[size_t(j)] = -1; cols.push_back(j);
                 if (j < i) { heap.push_back(j); std::push_heap(heap.begin(), heap.end(), std::greater<int32_t>()); }
-              } else if (l < lvl[size_t(j)]) {
-                lvl[size_t(j)] = l;
+              } else if (l < lvl[size_t(j)] - 1) {
+                lvl[size_t(j)] = l + 1;
               }
             }
           }
           std::sort(cols.begin(), cols.end());
-          auto &row = rows[size_t(i)];
-          row.reserve(cols.size());
+          rsid[size_t(i)] = sid;
+          roff[size_t(i)] = int64_t(st.size());
           ub[size_t(i)] = int64_t(ucolv.size());
           for (int32_t j : cols) {
-            row.push_back({j, src[size_t(j)]});
-            if (j > i) { ucolv.push_back(j); ulevv.push_back(lvl[size_t(j)]); }
-            lvl[size_t(j)] = -1; src[size_t(j)] = -1;
+            st.push_back({j, src[size_t(j)]});
+            if (j > i) { ucolv.push_back(j); ulevv.push_back(lvl[size_t(j)] - 1); }
+            lvl[size_t(j)] = 0;
           }
+          rcnt[size_t(i)] = int64_t(st.size()) - roff[size_t(i)];
           ue[size_t(i)] = int64_t(ucolv.size());
         }
       };
-      if (contiguous) host_parallel(nruns, 1, symbolic);
+      if (contiguous) host_parallel_runs(runs, symbolic);
       else symbolic(0, nruns);
     }
     // back to the caller's numbering, columns ascending
     frp.assign((size_t)n + 1, 0);
-    for (int64_t i = 0; i < n; ++i) frp[size_t(base[size_t(i)]) + 1] = int64_t(rows[size_t(i)].size());
+    for (int64_t i = 0; i < n; ++i) frp[size_t(base[size_t(i)]) + 1] = rcnt[size_t(i)];
     for (int64_t i = 0; i < n; ++i) frp[size_t(i) + 1] += frp[size_t(i)];
     fci.resize(size_t(frp[size_t(n)]));
     fsrc.resize(size_t(frp[size_t(n)]));
@@ -541,11 +642,11 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       for (int64_t i = i0; i < i1; ++i) {
         const int32_t o = base[size_t(i)];
         tmp.clear();
-        for (auto &e : rows[size_t(i)]) tmp.push_back({base[size_t(e.first)], e.second});
+        const RowStore &st = *rstore[size_t(rsid[size_t(i)])];
+        for (int64_t q = roff[size_t(i)]; q < roff[size_t(i)] + rcnt[size_t(i)]; ++q) tmp.push_back({base[size_t(st[size_t(q)].first)], st[size_t(q)].second});
         std::sort(tmp.begin(), tmp.end());
         int64_t p = frp[size_t(o)];
         for (auto &e : tmp) { fci[size_t(p)] = e.first; fsrc[size_t(p)] = e.second; ++p; }
-        std::vector<std::pair<int32_t, int64_t>>().swap(rows[size_t(i)]);
       }
     });
   }
@@ -559,15 +660,9 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   std::vector<int32_t> lev((size_t)n, 0);
   nlevL = 1;
   if (has_pc) {
-    std::vector<int64_t> tp((size_t)n + 1, 0);
-    for (int64_t k = 0; k < fnnz; ++k) tp[size_t(fci[size_t(k)]) + 1]++;
-    for (int64_t i = 0; i < n; ++i) tp[size_t(i) + 1] += tp[size_t(i)];
-    std::vector<int32_t> tr((size_t)fnnz);
-    {
-      std::vector<int64_t> pos(tp.begin(), tp.end() - 1);
-      for (int64_t i = 0; i < n; ++i)
-        for (int64_t k = frp[size_t(i)]; k < frp[size_t(i) + 1]; ++k) tr[size_t(pos[size_t(fci[size_t(k)])]++)] = int32_t(i);
-    }
+    std::vector<int64_t> tp;
+    std::vector<int32_t> tr;
+    transpose_pattern(n, frp.data(), fci.data(), tp, tr);
     // a row reads only earlier rows of its own block: runs of one block in base order are
     // levelled on several host threads when every block is one run
     std::vector<int32_t> bblk((size_t)n);
@@ -604,28 +699,43 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       std::lock_guard<std::mutex> lk(mu);
       nlevL = std::max(nlevL, nl);
     };
-    if (contiguous) host_parallel(nruns, 1, level);
+    if (contiguous) host_parallel_runs(runs, level);
     else level(0, nruns);
   }
   // solver order: by level, then block (each block's rows of a level are one run, which the
   // per-block sweeps walk), then longest rows first (less SELL padding), then by the base
   // position of the row's first neighbour (the lanes of a slice then gather nearby entries:
   // 4 % faster sweeps on the 2D bar than base position), then base position
+  // (two stable counting passes give (level, block) groups in base order; each group is then
+  // sorted by the last three keys on the host threads)
   perm = base;
   std::vector<int32_t> nbk((size_t)n, 0);
-  for (int64_t o = 0; o < n; ++o) {
-    int32_t m = INT32_MAX;
-    for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k)
-      if (fci[size_t(k)] != o) m = std::min(m, binv[size_t(fci[size_t(k)])]);
-    nbk[size_t(o)] = m;
-  }
-  std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) {
-    if (lev[size_t(a)] != lev[size_t(b)]) return lev[size_t(a)] < lev[size_t(b)];
-    if (blk0[size_t(a)] != blk0[size_t(b)]) return blk0[size_t(a)] < blk0[size_t(b)];
-    const int64_t la = rp[size_t(a) + 1] - rp[size_t(a)], lb = rp[size_t(b) + 1] - rp[size_t(b)];
-    if (la != lb) return la > lb;
-    return nbk[size_t(a)] < nbk[size_t(b)];
+  host_parallel(n, int64_t(1) << 16, [&](int64_t o0, int64_t o1) {
+    for (int64_t o = o0; o < o1; ++o) {
+      int32_t m = INT32_MAX;
+      for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k)
+        if (fci[size_t(k)] != o) m = std::min(m, binv[size_t(fci[size_t(k)])]);
+      nbk[size_t(o)] = m;
+    }
   });
+  counting_sort_by(perm, nblk, [&](int32_t a) { return blk0[size_t(a)]; });
+  counting_sort_by(perm, int64_t(nlevL), [&](int32_t a) { return lev[size_t(a)]; });
+  {
+    std::vector<int64_t> grp(1, 0);
+    for (int64_t i = 1; i < n; ++i)
+      if (lev[size_t(perm[size_t(i)])] != lev[size_t(perm[size_t(i) - 1])] || blk0[size_t(perm[size_t(i)])] != blk0[size_t(perm[size_t(i) - 1])])
+        grp.push_back(i);
+    grp.push_back(n);
+    host_parallel_runs(grp, [&](int64_t g0, int64_t g1) {
+      for (int64_t g = g0; g < g1; ++g)
+        std::sort(perm.begin() + grp[size_t(g)], perm.begin() + grp[size_t(g) + 1], [&](int32_t a, int32_t b) {
+          const int64_t la = rp[size_t(a) + 1] - rp[size_t(a)], lb = rp[size_t(b) + 1] - rp[size_t(b)];
+          if (la != lb) return la > lb;
+          if (nbk[size_t(a)] != nbk[size_t(b)]) return nbk[size_t(a)] < nbk[size_t(b)];
+          return binv[size_t(a)] < binv[size_t(b)];
+        });
+    });
+  }
   std::vector<int32_t> inv((size_t)(n));
   for (int64_t i = 0; i < n; ++i) inv[size_t(perm[size_t(i)])] = int32_t(i);
   blk.resize(size_t(n));
@@ -666,8 +776,10 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   std::vector<int64_t> alvs;
   {
     std::vector<int64_t> len((size_t)n, 0);
-    for (int64_t i = 0; i < n; ++i)
-      for (int64_t p = prp[size_t(i)]; p < prp[size_t(i) + 1]; ++p) len[size_t(i)] += amap[size_t(p)] >= 0 ? 1 : 0;
+    host_parallel(n, int64_t(1) << 16, [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; ++i)
+        for (int64_t p = prp[size_t(i)]; p < prp[size_t(i) + 1]; ++p) len[size_t(i)] += amap[size_t(p)] >= 0 ? 1 : 0;
+    });
     std::vector<int64_t> one{0, n}, agrp;
     sell_layout(len, one, std::vector<int32_t>{0}, 1, aoff, astart, alvs, agrp);
   }
@@ -675,32 +787,36 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   padA = aoff.back();
   amapS.assign((size_t)padA, -1);
   acol.assign((size_t)padA, PAD);
-  for (int64_t j = 0; j < nslA; ++j) {
-    for (int64_t i = astart[size_t(j)]; i < astart[size_t(j) + 1]; ++i) {
-      const int lane = int(i - astart[size_t(j)]);
-      int64_t kk = 0;
-      for (int64_t p = prp[size_t(i)]; p < prp[size_t(i) + 1]; ++p) {
-        if (amap[size_t(p)] < 0) continue;
-        const int64_t slot = aoff[size_t(j)] + 32 * kk + lane;
-        acol[size_t(slot)] = pci[size_t(p)];
-        amapS[size_t(slot)] = amap[size_t(p)];
-        ++kk;
+  host_parallel(nslA, int64_t(1) << 12, [&](int64_t j0, int64_t j1) {
+    for (int64_t j = j0; j < j1; ++j) {
+      for (int64_t i = astart[size_t(j)]; i < astart[size_t(j) + 1]; ++i) {
+        const int lane = int(i - astart[size_t(j)]);
+        int64_t kk = 0;
+        for (int64_t p = prp[size_t(i)]; p < prp[size_t(i) + 1]; ++p) {
+          if (amap[size_t(p)] < 0) continue;
+          const int64_t slot = aoff[size_t(j)] + 32 * kk + lane;
+          acol[size_t(slot)] = pci[size_t(p)];
+          amapS[size_t(slot)] = amap[size_t(p)];
+          ++kk;
+        }
       }
     }
-  }
+  });
 
   // factor layouts
   if (has_pc) {
     // forward sweep: rows of a level are contiguous; L entries = in-block columns left of the diagonal
     std::vector<int64_t> llen((size_t)n), ulen((size_t)n);
-    for (int64_t i = 0; i < n; ++i) {
-      int64_t cl = 0, cu = 0;
-      for (int64_t k = prp[size_t(i)]; k < prp[size_t(i) + 1]; ++k) {
-        if (blk[size_t(pci[size_t(k)])] != blk[size_t(i)]) continue;
-        if (k < pdiag[size_t(i)]) ++cl; else if (k > pdiag[size_t(i)]) ++cu;
+    host_parallel(n, int64_t(1) << 16, [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; ++i) {
+        int64_t cl = 0, cu = 0;
+        for (int64_t k = prp[size_t(i)]; k < prp[size_t(i) + 1]; ++k) {
+          if (blk[size_t(pci[size_t(k)])] != blk[size_t(i)]) continue;
+          if (k < pdiag[size_t(i)]) ++cl; else if (k > pdiag[size_t(i)]) ++cu;
+        }
+        llen[size_t(i)] = cl; ulen[size_t(i)] = cu;
       }
-      llen[size_t(i)] = cl; ulen[size_t(i)] = cu;
-    }
+    });
     {
       std::vector<int64_t> gs;
       std::vector<int32_t> qlev((size_t)n);
@@ -711,25 +827,42 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     }
     nslL = int64_t(lstart.size()) - 1;
     padL = loff.back();
-    // backward levels in solver order (real U dependencies, block-restricted)
+    // backward levels in solver order (real U dependencies, block-restricted): a row reads only
+    // later rows of its own block, so the blocks are levelled on the host threads, each from its
+    // last solver row backwards
     std::vector<int32_t> levU((size_t)n, 0);
     nlevU = 1;
-    for (int64_t i = n - 1; i >= 0; --i) {
-      int32_t m = -1;
-      for (int64_t k = pdiag[size_t(i)] + 1; k < prp[size_t(i) + 1]; ++k) {
-        const int32_t j = pci[size_t(k)];
-        if (blk[size_t(j)] == blk[size_t(i)]) m = std::max(m, levU[size_t(j)]);
-      }
-      levU[size_t(i)] = m + 1;
-      nlevU = std::max(nlevU, m + 2);
+    {
+      std::vector<int32_t> byblk((size_t)n);
+      std::iota(byblk.begin(), byblk.end(), 0);
+      counting_sort_by(byblk, nblk, [&](int32_t a) { return blk[size_t(a)]; });
+      std::vector<int64_t> bruns(1, 0);
+      for (int64_t t = 1; t < n; ++t)
+        if (blk[size_t(byblk[size_t(t)])] != blk[size_t(byblk[size_t(t) - 1])]) bruns.push_back(t);
+      bruns.push_back(n);
+      std::mutex mu;
+      host_parallel_runs(bruns, [&](int64_t r0, int64_t r1) {
+        int32_t nl = 1;
+        for (int64_t r = r0; r < r1; ++r)
+          for (int64_t t = bruns[size_t(r) + 1] - 1; t >= bruns[size_t(r)]; --t) {
+            const int32_t i = byblk[size_t(t)];
+            int32_t m = -1;
+            for (int64_t k = pdiag[size_t(i)] + 1; k < prp[size_t(i) + 1]; ++k) {
+              const int32_t j = pci[size_t(k)];
+              if (blk[size_t(j)] == blk[size_t(i)]) m = std::max(m, levU[size_t(j)]);
+            }
+            levU[size_t(i)] = m + 1;
+            nl = std::max(nl, m + 2);
+          }
+        std::lock_guard<std::mutex> lk(mu);
+        nlevU = std::max(nlevU, nl);
+      });
     }
-    // backward-sweep slots: by backward level, then block, then solver row
+    // backward-sweep slots: by backward level, then block, then solver row (two stable counting passes)
     urow.resize((size_t)n);
     std::iota(urow.begin(), urow.end(), 0);
-    std::stable_sort(urow.begin(), urow.end(), [&](int32_t a, int32_t b) {
-      if (levU[size_t(a)] != levU[size_t(b)]) return levU[size_t(a)] < levU[size_t(b)];
-      return blk[size_t(a)] < blk[size_t(b)];
-    });
+    counting_sort_by(urow, nblk, [&](int32_t a) { return blk[size_t(a)]; });
+    counting_sort_by(urow, int64_t(nlevU), [&](int32_t a) { return levU[size_t(a)]; });
     std::vector<int64_t> ulen_t((size_t)n);
     dpos.resize((size_t)n);
     for (int64_t t = 0; t < n; ++t) { ulen_t[size_t(t)] = ulen[size_t(urow[size_t(t)])]; dpos[size_t(urow[size_t(t)])] = t; }
@@ -744,34 +877,38 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     fmap.assign((size_t)fnnz, -1);
     lcol.assign((size_t)padL, PAD);
     ucol.assign((size_t)padU, PAD);
-    nnzL = nnzU = 0;
-    for (int64_t j = 0; j < nslL; ++j) {
-      for (int64_t i = lstart[size_t(j)]; i < lstart[size_t(j) + 1]; ++i) {
-        const int lane = int(i - lstart[size_t(j)]);
-        int64_t kk = 0;
-        for (int64_t k = prp[size_t(i)]; k < pdiag[size_t(i)]; ++k) {
-          if (blk[size_t(pci[size_t(k)])] != blk[size_t(i)]) continue;
-          const int64_t slot = loff[size_t(j)] + 32 * kk + lane;
-          lcol[size_t(slot)] = pci[size_t(k)];
-          fmap[size_t(k)] = slot;
-          ++kk; ++nnzL;
+    nnzL = std::accumulate(llen.begin(), llen.end(), int64_t(0));
+    nnzU = std::accumulate(ulen.begin(), ulen.end(), int64_t(0));
+    // every slice writes its own slots, and every row's entries of fmap belong to one slice
+    host_parallel(nslL, int64_t(1) << 12, [&](int64_t j0, int64_t j1) {
+      for (int64_t j = j0; j < j1; ++j)
+        for (int64_t i = lstart[size_t(j)]; i < lstart[size_t(j) + 1]; ++i) {
+          const int lane = int(i - lstart[size_t(j)]);
+          int64_t kk = 0;
+          for (int64_t k = prp[size_t(i)]; k < pdiag[size_t(i)]; ++k) {
+            if (blk[size_t(pci[size_t(k)])] != blk[size_t(i)]) continue;
+            const int64_t slot = loff[size_t(j)] + 32 * kk + lane;
+            lcol[size_t(slot)] = pci[size_t(k)];
+            fmap[size_t(k)] = slot;
+            ++kk;
+          }
         }
-      }
-    }
-    for (int64_t j = 0; j < nslU; ++j) {
-      for (int64_t t = ustart[size_t(j)]; t < ustart[size_t(j) + 1]; ++t) {
-        const int lane = int(t - ustart[size_t(j)]);
-        const int32_t i = urow[size_t(t)];
-        int64_t kk = 0;
-        for (int64_t k = pdiag[size_t(i)] + 1; k < prp[size_t(i) + 1]; ++k) {
-          if (blk[size_t(pci[size_t(k)])] != blk[size_t(i)]) continue;
-          const int64_t slot = uoff[size_t(j)] + 32 * kk + lane;
-          ucol[size_t(slot)] = pci[size_t(k)];
-          fmap[size_t(k)] = -(slot + 2);
-          ++kk; ++nnzU;
+    });
+    host_parallel(nslU, int64_t(1) << 12, [&](int64_t j0, int64_t j1) {
+      for (int64_t j = j0; j < j1; ++j)
+        for (int64_t t = ustart[size_t(j)]; t < ustart[size_t(j) + 1]; ++t) {
+          const int lane = int(t - ustart[size_t(j)]);
+          const int32_t i = urow[size_t(t)];
+          int64_t kk = 0;
+          for (int64_t k = pdiag[size_t(i)] + 1; k < prp[size_t(i) + 1]; ++k) {
+            if (blk[size_t(pci[size_t(k)])] != blk[size_t(i)]) continue;
+            const int64_t slot = uoff[size_t(j)] + 32 * kk + lane;
+            ucol[size_t(slot)] = pci[size_t(k)];
+            fmap[size_t(k)] = -(slot + 2);
+            ++kk;
+          }
         }
-      }
-    }
+    });
   } else {
     nlevU = 1;
   }
