@@ -458,10 +458,12 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     std::mutex rmu;
     std::vector<int32_t> rsid((size_t)n, 0);
     std::vector<int64_t> roff((size_t)n, 0), rcnt((size_t)n, 0);
-    auto new_store = [&]() {
+    // a new store and its id (taken under the lock: another thread may grow rstore meanwhile)
+    auto new_store = [&](int32_t &sid) {
       std::lock_guard<std::mutex> lk(rmu);
       rstore.emplace_back(new RowStore);
-      return int32_t(rstore.size() - 1);
+      sid = int32_t(rstore.size() - 1);
+      return rstore.back().get();
     };
     if (ilut) {
       // ILUT(p, tau), Saad Alg. 10.6, in base order: the row is eliminated with the kept rows
@@ -479,8 +481,8 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       std::vector<char> nz((size_t)n, 0);
       std::vector<int32_t> cols, heap;
       std::vector<std::pair<double, int32_t>> lo, up;
-      const int32_t sid = new_store();
-      RowStore &st = *rstore[size_t(sid)];
+      int32_t sid = 0;
+      RowStore &st = *new_store(sid);
       for (int64_t i = 0; i < n; ++i) {
         cols.clear(); heap.clear();
         double rn = 0.0;
@@ -582,8 +584,8 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
         std::unique_ptr<int64_t[]> src(new int64_t[size_t(n)]);
         if (!lvl1) throw std::bad_alloc();
         int32_t *lvl = lvl1.get();
-        const int32_t sid = new_store();
-        RowStore &st = *rstore[size_t(sid)];
+        int32_t sid = 0;
+        RowStore &st = *new_store(sid);
         std::vector<int32_t> cols, heap;
         for (int64_t i = runs[size_t(r0)]; i < runs[size_t(r1)]; ++i) {
           const int32_t bi = bblk[size_t(i)];
