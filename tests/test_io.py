@@ -75,7 +75,9 @@ def test_she_space_matches_oracle_mapping():
     entry, and the density of states of the oracle's restatement of the Modena dispersion."""
     import ctypes as C
     from vshe import gpu
-    for dev, cfg in (D.config1(), _space_case()):
+    oxide = D.config1()
+    oxide[0].cell_material[oxide[0].n_cells // 2:] = 1  # SiO2 from the middle on: nodes without unknowns
+    for dev, cfg in (D.config1(), _space_case(), D.config5(nx=16, ny=8, n_energies=40, L=5), oxide):
         cpl = O.golden_coupling(cfg.max_expansion_order)
         sp = gpu.she_space(dev, cfg, coupling=cpl)
         P = O.OracleProblem(dev, cfg, cpl)
