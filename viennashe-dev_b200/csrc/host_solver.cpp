@@ -427,18 +427,33 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   std::vector<int32_t> binv((size_t)n);
   for (int64_t i = 0; i < n; ++i) binv[size_t(base[size_t(i)])] = int32_t(i);
 
-  // Pattern of the incomplete factor F, in the caller's numbering: A's entries (fsrc = entry
-  // of A) and, for ILU(k) with k = fill_level > 0, the fill of levels <= k (fsrc = -1) from the
-  // symbolic phase of Saad's Alg. 10.5 run in base order, fill kept inside the row's block.
+  // Blocks in base order, as runs of base positions; when every block is one run, the phases in
+  // which a row reads only earlier rows of its own block run on several host threads.
+  std::vector<int32_t> bblk((size_t)n);
+  for (int64_t i = 0; i < n; ++i) bblk[size_t(i)] = blk0[size_t(base[size_t(i)])];
+  const std::vector<int64_t> runs = block_runs(bblk);
+  const int64_t nruns = int64_t(runs.size()) - 1;
+  bool contiguous = true;
+  {
+    std::vector<char> seen;
+    for (int64_t r = 0; r < nruns && contiguous; ++r) {
+      const int32_t b = bblk[size_t(runs[size_t(r)])];
+      if (b >= int32_t(seen.size())) seen.resize(size_t(b) + 1, 0);
+      if (seen[size_t(b)]) contiguous = false;
+      seen[size_t(b)] = 1;
+    }
+  }
+
+  // Pattern of the incomplete factor F in base order (row i is caller row base[i]; columns are
+  // base positions, ascending; fsrc = entry of A, -1 for fill): A's entries and, for ILU(k) with
+  // k = fill_level > 0, the fill of levels <= k from the symbolic phase of Saad's Alg. 10.5 run
+  // in base order, fill kept inside the row's block; for ILUT, the positions that pass its drop
+  // test (below).
   std::vector<int64_t> frp;
   std::vector<int32_t> fci;
   std::vector<int64_t> fsrc;
   const int kfill = has_pc && !ilut ? std::max(0, int(opts.fill_level)) : 0;
-  if (kfill == 0 && !ilut) {
-    frp = rp; fci = ci;
-    fsrc.resize((size_t)nnz);
-    std::iota(fsrc.begin(), fsrc.end(), int64_t(0));
-  } else {
+  {
     // base-order rows of A: (base column, entry)
     std::vector<int64_t> brp((size_t)n + 1, 0);
     for (int64_t i = 0; i < n; ++i) brp[size_t(i) + 1] = brp[size_t(i)] + (rp[size_t(base[size_t(i)]) + 1] - rp[size_t(base[size_t(i)])]);
@@ -451,6 +466,14 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
         std::sort(bent.begin() + brp[size_t(i)], bent.begin() + p);
       }
     });
+    if (kfill == 0 && !ilut) {
+      frp.swap(brp);
+      fci.resize((size_t)nnz);
+      fsrc.resize((size_t)nnz);
+      host_parallel(nnz, int64_t(1) << 20, [&](int64_t k0, int64_t k1) {
+        for (int64_t k = k0; k < k1; ++k) { fci[size_t(k)] = bent[size_t(k)].first; fsrc[size_t(k)] = bent[size_t(k)].second; }
+      });
+    } else {
     // rows of F in base order, (base column, entry or -1), in one flat store per host thread:
     // row i is (*rstore[rsid[i]])[roff[i] .. roff[i] + rcnt[i])
     typedef std::vector<std::pair<int32_t, int64_t>> RowStore;
@@ -560,20 +583,6 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       // reads only earlier rows of its own block, so when every block is one run of base
       // positions the runs are processed on several host threads (each with its own scratch
       // and its own store of upper parts), with the same result.
-      std::vector<int32_t> bblk((size_t)n);
-      for (int64_t i = 0; i < n; ++i) bblk[size_t(i)] = blk0[size_t(base[size_t(i)])];
-      const std::vector<int64_t> runs = block_runs(bblk);
-      const int64_t nruns = int64_t(runs.size()) - 1;
-      bool contiguous = true;
-      {
-        std::vector<char> seen;
-        for (int64_t r = 0; r < nruns && contiguous; ++r) {
-          const int32_t b = bblk[size_t(runs[size_t(r)])];
-          if (b >= int32_t(seen.size())) seen.resize(size_t(b) + 1, 0);
-          if (seen[size_t(b)]) contiguous = false;
-          seen[size_t(b)] = 1;
-        }
-      }
       std::vector<int64_t> ub((size_t)n, 0), ue((size_t)n, 0);  // upper part of row k: [ub[k], ue[k]) in its thread's store
       auto symbolic = [&](int64_t r0, int64_t r1) {
         std::vector<int32_t> ucolv, ulevv;
@@ -633,24 +642,22 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       if (contiguous) host_parallel_runs(runs, symbolic);
       else symbolic(0, nruns);
     }
-    // back to the caller's numbering, columns ascending
+    // one CSR in base order (each stored row is already in ascending base column)
     frp.assign((size_t)n + 1, 0);
-    for (int64_t i = 0; i < n; ++i) frp[size_t(base[size_t(i)]) + 1] = rcnt[size_t(i)];
-    for (int64_t i = 0; i < n; ++i) frp[size_t(i) + 1] += frp[size_t(i)];
+    for (int64_t i = 0; i < n; ++i) frp[size_t(i) + 1] = frp[size_t(i)] + rcnt[size_t(i)];
     fci.resize(size_t(frp[size_t(n)]));
     fsrc.resize(size_t(frp[size_t(n)]));
     host_parallel(n, int64_t(1) << 16, [&](int64_t i0, int64_t i1) {
-      std::vector<std::pair<int32_t, int64_t>> tmp;
       for (int64_t i = i0; i < i1; ++i) {
-        const int32_t o = base[size_t(i)];
-        tmp.clear();
         const RowStore &st = *rstore[size_t(rsid[size_t(i)])];
-        for (int64_t q = roff[size_t(i)]; q < roff[size_t(i)] + rcnt[size_t(i)]; ++q) tmp.push_back({base[size_t(st[size_t(q)].first)], st[size_t(q)].second});
-        std::sort(tmp.begin(), tmp.end());
-        int64_t p = frp[size_t(o)];
-        for (auto &e : tmp) { fci[size_t(p)] = e.first; fsrc[size_t(p)] = e.second; ++p; }
+        int64_t p = frp[size_t(i)];
+        for (int64_t q = roff[size_t(i)]; q < roff[size_t(i)] + rcnt[size_t(i)]; ++q, ++p) {
+          fci[size_t(p)] = st[size_t(q)].first;
+          fsrc[size_t(p)] = st[size_t(q)].second;
+        }
       }
     });
+    }
   }
   const int64_t fnnz = frp[size_t(n)];
   nnzF = fnnz;
@@ -659,43 +666,27 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   // level is one more than the highest level of any coupled (F_ij or F_ji != 0) earlier row of
   // its block.  Sorting by these levels keeps the relative order of every coupled pair, so the
   // incomplete factorisation in the sorted order is the one in the base order, relabelled.
-  std::vector<int32_t> lev((size_t)n, 0);
+  std::vector<int32_t> lev((size_t)n, 0);   // by caller row
   nlevL = 1;
   if (has_pc) {
     std::vector<int64_t> tp;
     std::vector<int32_t> tr;
     transpose_pattern(n, frp.data(), fci.data(), tp, tr);
-    // a row reads only earlier rows of its own block: runs of one block in base order are
-    // levelled on several host threads when every block is one run
-    std::vector<int32_t> bblk((size_t)n);
-    for (int64_t i = 0; i < n; ++i) bblk[size_t(i)] = blk0[size_t(base[size_t(i)])];
-    const std::vector<int64_t> runs = block_runs(bblk);
-    const int64_t nruns = int64_t(runs.size()) - 1;
-    bool contiguous = true;
-    {
-      std::vector<char> seen;
-      for (int64_t r = 0; r < nruns && contiguous; ++r) {
-        const int32_t b = bblk[size_t(runs[size_t(r)])];
-        if (b >= int32_t(seen.size())) seen.resize(size_t(b) + 1, 0);
-        if (seen[size_t(b)]) contiguous = false;
-        seen[size_t(b)] = 1;
-      }
-    }
+    std::vector<int32_t> levb((size_t)n, 0);  // by base position
     std::mutex mu;
     auto level = [&](int64_t r0, int64_t r1) {
       int32_t nl = 1;
       for (int64_t i = runs[size_t(r0)]; i < runs[size_t(r1)]; ++i) {
-        const int32_t o = base[size_t(i)];
         int32_t m = -1;
-        for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k) {
+        for (int64_t k = frp[size_t(i)]; k < frp[size_t(i) + 1]; ++k) {
           const int32_t j = fci[size_t(k)];
-          if (binv[size_t(j)] < i && blk0[size_t(j)] == blk0[size_t(o)]) m = std::max(m, lev[size_t(j)]);
+          if (j < i && bblk[size_t(j)] == bblk[size_t(i)]) m = std::max(m, levb[size_t(j)]);
         }
-        for (int64_t k = tp[size_t(o)]; k < tp[size_t(o) + 1]; ++k) {
+        for (int64_t k = tp[size_t(i)]; k < tp[size_t(i) + 1]; ++k) {
           const int32_t j = tr[size_t(k)];
-          if (binv[size_t(j)] < i && blk0[size_t(j)] == blk0[size_t(o)]) m = std::max(m, lev[size_t(j)]);
+          if (j < i && bblk[size_t(j)] == bblk[size_t(i)]) m = std::max(m, levb[size_t(j)]);
         }
-        lev[size_t(o)] = m + 1;
+        levb[size_t(i)] = m + 1;
         nl = std::max(nl, m + 2);
       }
       std::lock_guard<std::mutex> lk(mu);
@@ -703,6 +694,7 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
     };
     if (contiguous) host_parallel_runs(runs, level);
     else level(0, nruns);
+    for (int64_t i = 0; i < n; ++i) lev[size_t(base[size_t(i)])] = levb[size_t(i)];
   }
   // solver order: by level, then block (each block's rows of a level are one run, which the
   // per-block sweeps walk), then longest rows first (less SELL padding), then by the base
@@ -712,12 +704,12 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   // sorted by the last three keys on the host threads)
   perm = base;
   std::vector<int32_t> nbk((size_t)n, 0);
-  host_parallel(n, int64_t(1) << 16, [&](int64_t o0, int64_t o1) {
-    for (int64_t o = o0; o < o1; ++o) {
+  host_parallel(n, int64_t(1) << 16, [&](int64_t i0, int64_t i1) {
+    for (int64_t i = i0; i < i1; ++i) {
       int32_t m = INT32_MAX;
-      for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k)
-        if (fci[size_t(k)] != o) m = std::min(m, binv[size_t(fci[size_t(k)])]);
-      nbk[size_t(o)] = m;
+      for (int64_t k = frp[size_t(i)]; k < frp[size_t(i) + 1]; ++k)
+        if (fci[size_t(k)] != i) m = std::min(m, fci[size_t(k)]);
+      nbk[size_t(base[size_t(i)])] = m;
     }
   });
   counting_sort_by(perm, nblk, [&](int32_t a) { return blk0[size_t(a)]; });
@@ -750,13 +742,19 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   prp.assign((size_t)n + 1, 0); pdiag.assign((size_t)n, -1); amap.assign((size_t)fnnz, 0);
   pci.assign((size_t)fnnz, 0);
   {
-    for (int64_t i = 0; i < n; ++i) prp[size_t(i) + 1] = prp[size_t(i)] + (frp[size_t(perm[size_t(i)]) + 1] - frp[size_t(perm[size_t(i)])]);
+    // solver position of every base position
+    std::vector<int32_t> sinv((size_t)n);
+    for (int64_t i = 0; i < n; ++i) sinv[size_t(i)] = inv[size_t(base[size_t(i)])];
+    for (int64_t i = 0; i < n; ++i) {
+      const int32_t b = binv[size_t(perm[size_t(i)])];
+      prp[size_t(i) + 1] = prp[size_t(i)] + (frp[size_t(b) + 1] - frp[size_t(b)]);
+    }
     host_parallel(n, int64_t(1) << 16, [&](int64_t i0, int64_t i1) {
       std::vector<std::pair<int32_t, int64_t>> row;
       for (int64_t i = i0; i < i1; ++i) {
-        const int64_t o = perm[size_t(i)];
+        const int32_t b = binv[size_t(perm[size_t(i)])];
         row.clear();
-        for (int64_t k = frp[size_t(o)]; k < frp[size_t(o) + 1]; ++k) row.push_back({inv[size_t(fci[size_t(k)])], fsrc[size_t(k)]});
+        for (int64_t k = frp[size_t(b)]; k < frp[size_t(b) + 1]; ++k) row.push_back({sinv[size_t(fci[size_t(k)])], fsrc[size_t(k)]});
         std::sort(row.begin(), row.end());
         int64_t p = prp[size_t(i)];
         for (auto &x : row) {
