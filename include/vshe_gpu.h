@@ -291,6 +291,15 @@ int vshe_she_plan(const vshe_device_desc *dev, const vshe_she_config *cfg, const
 int vshe_she_space(const vshe_device_desc *dev, const vshe_she_config *cfg, const vshe_coupling_tables *coupling,
                    double *energies, int64_t *even_index, int32_t *even_order, double *kinetic_energy,
                    double *density_of_states, int64_t *odd_index, int32_t *odd_order);
+/* The multicolour order of the reduced rows that vshe_she_create uses when opts->ordering is
+ * VSHE_ORDER_MULTICOLOR and opts->perm is NULL, no GPU needed: every (cell, H) node takes a colour,
+ * and all harmonics of a node share it.  The cell part is a greedy colouring of the mesh graph (at
+ * distance 2 for fill_level > 0).  The energy part is H / n_op in 2 classes (3 for fill_level >
+ * 0), since in-scattering couples H with H +- n_op.  perm[t] is the reduced row at position t, by
+ * colour and then by row; colour[row] is each row's colour.  Both hold n_even entries
+ * (vshe_she_plan); either may be NULL. */
+int vshe_she_node_order(const vshe_device_desc *dev, const vshe_she_config *cfg, const vshe_coupling_tables *coupling,
+                        int32_t fill_level, int32_t *perm, int32_t *colour);
 int vshe_she_create(vshe_ctx *ctx, const vshe_device_desc *dev, const vshe_she_config *cfg,
                     const vshe_coupling_tables *coupling, const vshe_solve_opts *opts, int64_t *handle);
 int vshe_she_info_get(vshe_ctx *ctx, int64_t handle, vshe_she_info *info);

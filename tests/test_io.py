@@ -154,3 +154,37 @@ def test_gnuplot_edf_layouts(tmp_path):
     assert len(expect) > 4 * len(col) and lines == expect
     # the EDF is positive where the carrier population lives (well above the band edge)
     assert np.all(edf[m & (sp["kinetic_energy"] > 0)] > 0)
+
+
+def _node_of_rows(sp, n_even):
+    """Node id (cell * N_H + H) of every reduced row, from the (x, H) space."""
+    idx, order = sp["even_index"].reshape(-1), sp["even_order"].reshape(-1)
+    node = np.full(n_even, -1, np.int64)
+    for a in np.nonzero(idx >= 0)[0]:
+        ne = sum(2 * l + 1 for l in range(0, int(order[a]) + 1, 2))
+        node[idx[a]:idx[a] + ne] = a
+    assert np.all(node >= 0)
+    return node
+
+
+def test_she_node_order_colours_against_the_oracle_pattern():
+    """vshe_she_node_order (host only): the SHE pipeline's multicolour order is a stable sort of
+    the rows by colour, and rows of different (cell, H) nodes that the oracle's reduced system
+    couples have different colours -- directly for ILU(0), at distance two (the pattern of A^2)
+    for ILU(k > 0)."""
+    import scipy.sparse as sps
+    from vshe import gpu
+    for dev, cfg in (D.config2(nx=16, ny=5, n_energies=40, L=3), D.config1()):
+        cpl = O.golden_coupling(cfg.max_expansion_order)
+        P = O.OracleProblem(dev, cfg, cpl)
+        A = P.matrix(3)
+        node = _node_of_rows(gpu.she_space(dev, cfg, coupling=cpl), P.n_even)
+        M = sps.csr_matrix((np.ones(A.nnz), A.ci, A.rp), shape=(A.n, A.n))
+        for fill, pat in ((0, M), (1, M @ M)):
+            perm, colour = gpu.she_node_order(dev, cfg, coupling=cpl, fill_level=fill)
+            assert np.array_equal(np.sort(perm), np.arange(P.n_even))
+            assert np.array_equal(perm, np.argsort(colour, kind="stable"))
+            coo = pat.tocoo()
+            other = node[coo.row] != node[coo.col]
+            assert np.all(colour[coo.row[other]] != colour[coo.col[other]]), (dev.name, fill)
+            assert colour.max() + 1 <= (64 * (3 if fill else 2))

@@ -344,6 +344,53 @@ std::string SheSetup::build(const vshe_device_desc &d, const vshe_she_config &c,
   return "";
 }
 
+// ------------------------------------------------------------ multicolour order of the reduced rows
+void node_colour_order(const SheSetup &H, int fill_level, std::vector<int32_t> &perm, std::vector<int32_t> *colour) {
+  // Colour the (cell, H) nodes so that no two coupled nodes share a colour: cells by a
+  // greedy colouring of the mesh graph, energies by the parity of H / n_op (in-scattering
+  // couples H and H +- n_op).  All harmonics of a node share its colour; rows are ordered
+  // by colour, then by their original position.
+  // ILU(k > 0) colours at distance 2 (cells with a common neighbour differ, and energies in
+  // three classes of H / n_op), so that the fill does not chain nodes of one colour.
+  const bool d2 = fill_level > 0;
+  std::vector<int32_t> ccol((size_t)H.nc, -1);
+  for (int c = 0; c < H.nc; ++c) {
+    uint64_t used = 0;
+    for (int k = H.cf_ptr[c]; k < H.cf_ptr[c + 1]; ++k) {
+      const int o = H.other_cell(H.cf_idx[k], c);
+      if (o < 0) continue;
+      if (ccol[(size_t)o] >= 0 && ccol[(size_t)o] < 64) used |= (uint64_t(1) << ccol[(size_t)o]);
+      if (!d2) continue;
+      for (int k2 = H.cf_ptr[o]; k2 < H.cf_ptr[o + 1]; ++k2) {
+        const int o2 = H.other_cell(H.cf_idx[k2], o);
+        if (o2 >= 0 && o2 != c && ccol[(size_t)o2] >= 0 && ccol[(size_t)o2] < 64) used |= (uint64_t(1) << ccol[(size_t)o2]);
+      }
+    }
+    int col = 0;
+    while (col < 63 && (used >> col) & 1) ++col;
+    ccol[(size_t)c] = col;
+  }
+  const int nop = std::max(1, int(std::lround(H.hbar_omega / H.cfg.energy_spacing)));
+  const int nh_classes = d2 ? 3 : 2;
+  std::vector<int32_t> rowcol((size_t)H.n_even);
+  for (size_t k = 0; k + 1 < H.even_nodes.size(); k += 2) {
+    const int c = H.even_nodes[k], h = H.even_nodes[k + 1];
+    const int64_t base = H.idx_c[(size_t)c * H.NH + h];
+    int ne = 0;
+    for (int l = 0; l <= H.ord_c[(size_t)c * H.NH + h]; l += 2) ne += 2 * l + 1;
+    const int32_t col = ccol[(size_t)c] * nh_classes + ((h / nop) % nh_classes);
+    for (int q = 0; q < ne; ++q) rowcol[(size_t)(base + q)] = col;
+  }
+  // rows by colour, then position: a stable counting sort over the few colours
+  const int32_t ncol = rowcol.empty() ? 1 : *std::max_element(rowcol.begin(), rowcol.end()) + 1;
+  std::vector<int64_t> cpos((size_t)ncol + 1, 0);
+  for (int32_t c : rowcol) cpos[(size_t)c + 1]++;
+  for (int32_t c = 0; c < ncol; ++c) cpos[(size_t)c + 1] += cpos[(size_t)c];
+  perm.resize((size_t)H.n_even);
+  for (int64_t i = 0; i < H.n_even; ++i) perm[(size_t)cpos[(size_t)rowcol[(size_t)i]]++] = int32_t(i);
+  if (colour) colour->swap(rowcol);
+}
+
 // ---------------------------------------------------------------- quadrature
 namespace {
 // associated Legendre P_n^m(x), m >= 0, with the (-1)^n factor on P_n^n

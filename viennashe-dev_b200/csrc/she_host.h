@@ -63,6 +63,11 @@ struct SheSetup {
   double ekin_f(int f, int H) const { return Hval[H] - shift_f[f]; }
 };
 
+// The multicolour order of the reduced rows (SHE problems with ordering = multicolor and no
+// caller permutation): perm[t] = reduced row at position t; colour (optional) receives every
+// row's colour.
+void node_colour_order(const SheSetup &H, int fill_level, std::vector<int32_t> &perm, std::vector<int32_t> *colour);
+
 // Density of states of the Modena dispersion for silicon electrons at kinetic energy eps (J),
 // per unit volume and energy (viennashe/physics/dispersion.hpp:207-286); 0 for eps <= 0.
 double density_of_states(double eps);

@@ -264,44 +264,7 @@ int SheProblem::create_device_pattern(Ctx &ctx) {
   so = opts;
   std::vector<int32_t> &node_perm = node_perm_;
   if (so.ordering == VSHE_ORDER_MULTICOLOR && !so.perm && so.precond != VSHE_PRECOND_NONE) {
-    // Colour the (cell, H) nodes so that no two coupled nodes share a colour: cells by a
-    // greedy colouring of the mesh graph, energies by the parity of H / n_op (in-scattering
-    // couples H and H +- n_op).  All harmonics of a node share its colour; rows are ordered
-    // by colour, then by their original position.
-    // ILU(k > 0) colours at distance 2 (cells with a common neighbour differ, and energies in
-    // three classes of H / n_op), so that the fill does not chain nodes of one colour.
-    const bool d2 = so.fill_level > 0;
-    std::vector<int32_t> ccol((size_t)H.nc, -1);
-    for (int c = 0; c < H.nc; ++c) {
-      uint64_t used = 0;
-      for (int k = H.cf_ptr[c]; k < H.cf_ptr[c + 1]; ++k) {
-        const int o = H.other_cell(H.cf_idx[k], c);
-        if (o < 0) continue;
-        if (ccol[(size_t)o] >= 0 && ccol[(size_t)o] < 64) used |= (uint64_t(1) << ccol[(size_t)o]);
-        if (!d2) continue;
-        for (int k2 = H.cf_ptr[o]; k2 < H.cf_ptr[o + 1]; ++k2) {
-          const int o2 = H.other_cell(H.cf_idx[k2], o);
-          if (o2 >= 0 && o2 != c && ccol[(size_t)o2] >= 0 && ccol[(size_t)o2] < 64) used |= (uint64_t(1) << ccol[(size_t)o2]);
-        }
-      }
-      int col = 0;
-      while (col < 63 && (used >> col) & 1) ++col;
-      ccol[(size_t)c] = col;
-    }
-    const int nop = std::max(1, int(std::lround(H.hbar_omega / H.cfg.energy_spacing)));
-    const int nh_classes = d2 ? 3 : 2;
-    std::vector<int32_t> rowcol((size_t)n_red);
-    for (size_t k = 0; k + 1 < H.even_nodes.size(); k += 2) {
-      const int c = H.even_nodes[k], h = H.even_nodes[k + 1];
-      const int64_t base = H.idx_c[(size_t)c * H.NH + h];
-      int ne = 0;
-      for (int l = 0; l <= H.ord_c[(size_t)c * H.NH + h]; l += 2) ne += 2 * l + 1;
-      const int32_t col = ccol[(size_t)c] * nh_classes + ((h / nop) % nh_classes);
-      for (int q = 0; q < ne; ++q) rowcol[(size_t)(base + q)] = col;
-    }
-    node_perm.resize((size_t)n_red);
-    for (int64_t i = 0; i < n_red; ++i) node_perm[(size_t)i] = int32_t(i);
-    std::stable_sort(node_perm.begin(), node_perm.end(), [&](int32_t a, int32_t b) { return rowcol[(size_t)a] < rowcol[(size_t)b]; });
+    node_colour_order(H, so.fill_level, node_perm, nullptr);
     so.perm = node_perm.data();
   }
   if (so.precond == VSHE_PRECOND_BLOCK_ILU0 && (so.n_blocks <= 0 || !so.block_ptr)) {
@@ -517,6 +480,18 @@ int vshe_she_space(const vshe_device_desc *d, const vshe_she_config *c, const vs
       if (kinetic_energy) kinetic_energy[size_t(i) * nh + size_t(h)] = eps;
       if (density_of_states) density_of_states[size_t(i) * nh + size_t(h)] = vshe::density_of_states(eps);
     }
+  return VSHE_OK;
+}
+
+int vshe_she_node_order(const vshe_device_desc *d, const vshe_she_config *c, const vshe_coupling_tables *ct, int32_t fill_level,
+                        int32_t *perm, int32_t *colour) {
+  if (!d || !c || !ct || fill_level < 0) return VSHE_E_INVALID_ARGUMENT;
+  SheSetup H;
+  if (!H.build(*d, *c, *ct).empty()) return VSHE_E_INVALID_ARGUMENT;
+  std::vector<int32_t> p, col;
+  node_colour_order(H, fill_level, p, &col);
+  if (perm) std::copy(p.begin(), p.end(), perm);
+  if (colour) std::copy(col.begin(), col.end(), colour);
   return VSHE_OK;
 }
 

@@ -394,6 +394,24 @@ def she_space(dev, cfg, coupling=None):
     return out
 
 
+def she_node_order(dev, cfg, coupling=None, fill_level=0):
+    """vshe_she_node_order: the multicolour order of the reduced rows the SHE pipeline uses (host
+    only) -> (perm, colour), n_even entries each."""
+    from .abi import DeviceDesc, she_config_c
+    info = she_plan(dev, cfg, coupling)
+    L = _she_lib()
+    L.vshe_she_node_order.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+    desc = DeviceDesc(dev)
+    cfgc = she_config_c(cfg)
+    cpl = coupling if coupling is not None else coupling_tables(cfg.max_expansion_order)
+    perm = np.zeros(info["n_even"], np.int32)
+    colour = np.zeros(info["n_even"], np.int32)
+    rc = L.vshe_she_node_order(C.byref(desc.c), C.byref(cfgc), C.byref(cpl.c), int(fill_level), perm.ctypes.data, colour.ctypes.data)
+    if rc:
+        raise VsheError(rc, "vshe_she_node_order")
+    return perm, colour
+
+
 class PoissonStatsC(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("rel_residual", C.c_double),
                 ("rhs_norm", C.c_double), ("update_norm", C.c_double), ("n_unknowns", C.c_int64)]
