@@ -246,6 +246,20 @@ int vshe_layout_export(int64_t n, int64_t nnz, const int64_t *row_ptr, const int
                        int32_t *perm, int64_t *lvr, int64_t *aoff, int32_t *acol, int64_t *amap_a,
                        int32_t *lrow0, int64_t *loff, int32_t *lcol, int64_t *lmap,
                        int32_t *uslot0, int64_t *uoff, int32_t *ucol, int64_t *umap, int32_t *urow);
+/* The sweep plan of that system alone, as a batch of one on a device of num_sms SMs (0: 148):
+ * - counts[0..3]: tasks, chunks, slice descriptors, and the system's sweep (0 grid-wide, 1 one
+ *   task for the system, 2 tasks of preconditioner blocks).
+ * - tasks[6 t ..]: system, first and end chunk of the forward sweep, first and end chunk of the
+ *   backward sweep, 0.
+ * - chunks[10 c ..]: first and end slice, flags (1: last chunk of its level, 2: read from global
+ *   memory), factor slots, first slot, first slice descriptor, first and end row operand, the
+ *   consumer rotation, and the bytes the chunk occupies in a 64 KiB shared-memory stage.
+ * - sdesc[4 d ..]: slot offset in the chunk, width, first row (L) or slot (U), and rows.
+ * Call once with NULL arrays for the counts, then with arrays of those sizes.  Host only; this
+ * is the plan the task sweeps (k_trsv_task) stage from, so tests check the stage bounds on it. */
+int vshe_layout_sweep_plan(int64_t n, int64_t nnz, const int64_t *row_ptr, const int32_t *col, const double *val,
+                           const vshe_solve_opts *opts, int32_t num_sms, int64_t *counts, int32_t *tasks,
+                           int64_t *chunks, int32_t *sdesc);
 
 /* ---- SHE path on the device: she::assemble + she::solve (secondary boundary) ----
  * vshe_she_create runs the host setup of the (x, H) space (energies, expansion

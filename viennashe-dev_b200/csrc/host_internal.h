@@ -117,6 +117,7 @@ struct System {
   int init_borrowed(Ctx &ctx, int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, int64_t *d_rp_,
                     int32_t *d_ci_, double *d_val, double *d_rhs, const vshe_solve_opts &o);
   int setup_from_layout(Ctx &ctx, const Layout &Lt);
+  void adopt_layout(const Layout &Lt);  // the host fields of setup_from_layout, no device work
   // gathers the caller-order values and rhs into the solver-order SELL A, the factorisation
   // CSR and b_p (on the context's stream)
   void prepare(Ctx &ctx);
@@ -124,6 +125,21 @@ struct System {
 };
 
 // Several systems solved together.
+// Sweep plan of a batch: per member 0 (grid-wide sweep), 1 (one task for the system) or 2 (tasks of
+// preconditioner blocks); the tasks, the chunks of their levels, the chunks' slice descriptors,
+// and the level slice ranges of the cluster sweeps.
+struct SweepPlan {
+  std::vector<char> on_task;
+  std::vector<TaskDev> tasks;
+  std::vector<ChunkDev> chunks;
+  std::vector<SliceDesc> sdesc;
+  std::vector<ClusterTask> ctasks;
+  std::vector<int64_t> clv;
+  int64_t tune_key_tasks = 0;
+  bool has_tune_key = false;
+};
+void plan_sweep_tasks(const std::vector<System *> &sys, bool mixed, bool has_pc, int64_t num_sms, SweepPlan &plan);
+
 struct Batch {
   std::vector<System *> sys;
   int nsys = 0;

@@ -924,10 +924,10 @@ int System::setup_pattern(Ctx &ctx, const double *host_val) {
   return setup_from_layout(ctx, Lt);
 }
 
-int System::setup_from_layout(Ctx &ctx, const Layout &Lt) {
+// The host copies of a layout's schedules and sizes (no device work).
+void System::adopt_layout(const Layout &Lt) {
   has_pc = opts.precond != VSHE_PRECOND_NONE;
   mixed = opts.precision == VSHE_PRECISION_MIXED;
-  cudaError_t e;
   perm = Lt.perm; blk = Lt.blk; lvr = Lt.lvr; lvsL = Lt.lvsL; lvsU = Lt.lvsU;
   lgrp_s0 = Lt.lgrp_s0; lgrp_lev = Lt.lgrp_lev; lgrp_blk = Lt.lgrp_blk;
   ugrp_s0 = Lt.ugrp_s0; ugrp_lev = Lt.ugrp_lev; ugrp_blk = Lt.ugrp_blk;
@@ -935,6 +935,11 @@ int System::setup_from_layout(Ctx &ctx, const Layout &Lt) {
   lrow0_h.assign(Lt.lstart.begin(), Lt.lstart.end()); uslot0_h.assign(Lt.ustart.begin(), Lt.ustart.end());
   nlevL = Lt.nlevL; nlevU = Lt.nlevU; nslA = Lt.nslA; nslL = Lt.nslL; nslU = Lt.nslU;
   padA = Lt.padA; padL = Lt.padL; padU = Lt.padU; nnzL = Lt.nnzL; nnzU = Lt.nnzU; nnzF = Lt.nnzF;
+}
+
+int System::setup_from_layout(Ctx &ctx, const Layout &Lt) {
+  adopt_layout(Lt);
+  cudaError_t e;
   const auto &prp = Lt.prp; const auto &pci = Lt.pci; const auto &pdiag = Lt.pdiag; const auto &amap = Lt.amap;
   const auto &aoff = Lt.aoff; const auto &amapS = Lt.amapS; const auto &acol = Lt.acol;
   const auto &fmap = Lt.fmap; const auto &dpos = Lt.dpos; const auto &loff = Lt.loff; const auto &uoff = Lt.uoff;
@@ -1056,39 +1061,30 @@ int Batch::sync_spin_limit(Ctx &ctx) {
   return VSHE_OK;
 }
 
-int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
-  int rc0 = 0;
-  sys = members;
-  nsys = int(sys.size());
-  mixed = sys[0]->mixed;
-  has_pc = sys[0]->has_pc;
-  for (System *S : sys)
-    if (S->mixed != mixed || S->has_pc != has_pc)
-      return ctx.fail(VSHE_E_INVALID_ARGUMENT, "systems in one batch need the same precision and preconditioner kind");
-  // Triangular sweeps.  A member sweeps either as tasks, one CTA each walking its levels with
-  // a CTA barrier per level (k_trsv_task), or in the merged level schedule of the grid-wide sweep
-  // (k_trsv_persistent).  Tasks are whole systems for members with many short levels (fewer than
-  // kCtaRowsPerLevel rows per forward level on average and more than kCtaMinLevels levels: 1D
-  // devices) whose apply one SM finishes sooner than the grid-wide sweep, and preconditioner
-  // blocks for block-ILU members with at least two blocks of at most kTaskMaxRows rows (energy
-  // slabs: the factor has no entry between blocks, so they sweep independently).
-  // VSHE_TRSV_PER_SYSTEM / VSHE_TRSV_PER_BLOCK force the former / latter for every member; the
-  // grid-wide modes force the merged schedule.  The time estimates use rates measured on the 2D
-  // bar: one CTA streams a task's factor and vectors at about kTaskBytesPerUs, and a level of the
-  // grid-wide sweep costs about kGridLevelUs (its grid barrier and the latency of the level's
-  // rows) on top of the apply's bytes at kGridBytesPerUs.
+// Sweep plan of a batch (host only): which members sweep as tasks (k_trsv_task, k_trsv_cluster)
+// and which in the grid-wide schedule, the tasks, the chunks of their levels with the chunks'
+// slice descriptors, and the level slice ranges of the cluster sweeps.
+//
+// Triangular sweeps.  A member sweeps either as tasks, one CTA each walking its levels with
+// a CTA barrier per level (k_trsv_task), or in the merged level schedule of the grid-wide sweep
+// (k_trsv_persistent).  Tasks are whole systems for members with many short levels (fewer than
+// kCtaRowsPerLevel rows per forward level on average and more than kCtaMinLevels levels: 1D
+// devices) whose apply one SM finishes sooner than the grid-wide sweep, and preconditioner
+// blocks for block-ILU members with at least two blocks of at most kTaskMaxRows rows (energy
+// slabs: the factor has no entry between blocks, so they sweep independently).
+// VSHE_TRSV_PER_SYSTEM / VSHE_TRSV_PER_BLOCK force the former / latter for every member; the
+// grid-wide modes force the merged schedule.  The time estimates use rates measured on the 2D
+// bar: one CTA streams a task's factor and vectors at about kTaskBytesPerUs, and a level of the
+// grid-wide sweep costs about kGridLevelUs (its grid barrier and the latency of the level's
+// rows) on top of the apply's bytes at kGridBytesPerUs.
+void plan_sweep_tasks(const std::vector<System *> &sys, bool mixed, bool has_pc, int64_t num_sms_hint, SweepPlan &P) {
   constexpr int64_t kCtaRowsPerLevel = 4096;
   constexpr int32_t kCtaMinLevels = 32;
   constexpr int64_t kTaskMaxRows = int64_t(1) << 18;
   constexpr double kTaskBytesPerUs = 3.0e4, kGridBytesPerUs = 3.0e6, kGridLevelUs = 4.0;
-  std::vector<char> on_task((size_t)nsys, 0);  // 0 grid, 1 whole system, 2 per block
-  int64_t num_sms_hint = 148;
-  {
-    int dev = 0, sms = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
-      num_sms_hint = sms;
-  }
-  ntasks = 0;
+  const int nsys = int(sys.size());
+  std::vector<char> &on_task = P.on_task;  // 0 grid, 1 whole system, 2 per block
+  on_task.assign((size_t)nsys, 0);
   if (has_pc) {
     for (int k = 0; k < nsys; ++k) {
       const System *S = sys[size_t(k)];
@@ -1107,11 +1103,11 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
       else if (mode == VSHE_TRSV_AUTO) on_task[size_t(k)] = per_blk ? 2 : per_sys ? 1 : 0;
     }
   }
-  std::vector<TaskDev> tasks;
-  std::vector<ChunkDev> chunks;
-  std::vector<SliceDesc> sdesc;
-  std::vector<ClusterTask> ctasks;
-  std::vector<int64_t> clv;
+  std::vector<TaskDev> &tasks = P.tasks;
+  std::vector<ChunkDev> &chunks = P.chunks;
+  std::vector<SliceDesc> &sdesc = P.sdesc;
+  std::vector<ClusterTask> &ctasks = P.ctasks;
+  std::vector<int64_t> &clv = P.clv;
   {
     const int vbytes = mixed ? int(sizeof(float)) : int(sizeof(double));
     // chunks of the slices [a, b) of one level of one system's L (lower) or U sweep: runs of
@@ -1246,12 +1242,43 @@ int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
       t.second.pad = 0;
       tasks.push_back(t.second);
     }
-    ntasks = int(tasks.size());
+    const int ntasks = int(tasks.size());
     // shape class of the task sweep: precision, the largest task's work and the task count (the
     // apply's time is the largest task's walk, in waves of one CTA per SM)
     auto log2c = [](int64_t v) { int c = 0; while (v > 1) { v >>= 1; ++c; } return c; };
-    if (!tw.empty()) tune_key_tasks = (int64_t(mixed ? 1 : 0) << 40) | (int64_t(log2c(tw.front().first)) << 20) | int64_t(log2c(ntasks));
+    if (!tw.empty()) {
+      P.tune_key_tasks = (int64_t(mixed ? 1 : 0) << 40) | (int64_t(log2c(tw.front().first)) << 20) | int64_t(log2c(ntasks));
+      P.has_tune_key = true;
+    }
   }
+}
+
+int Batch::build(Ctx &ctx, const std::vector<System *> &members) {
+  int rc0 = 0;
+  sys = members;
+  nsys = int(sys.size());
+  mixed = sys[0]->mixed;
+  has_pc = sys[0]->has_pc;
+  for (System *S : sys)
+    if (S->mixed != mixed || S->has_pc != has_pc)
+      return ctx.fail(VSHE_E_INVALID_ARGUMENT, "systems in one batch need the same precision and preconditioner kind");
+  // triangular sweeps: tasks or the grid-wide schedule per member (plan_sweep_tasks)
+  SweepPlan plan;
+  {
+    int64_t num_sms = 148;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+      num_sms = sms;
+    plan_sweep_tasks(sys, mixed, has_pc, num_sms, plan);
+  }
+  const std::vector<char> &on_task = plan.on_task;
+  const std::vector<TaskDev> &tasks = plan.tasks;
+  const std::vector<ChunkDev> &chunks = plan.chunks;
+  const std::vector<SliceDesc> &sdesc = plan.sdesc;
+  const std::vector<ClusterTask> &ctasks = plan.ctasks;
+  const std::vector<int64_t> &clv = plan.clv;
+  ntasks = int(tasks.size());
+  if (plan.has_tune_key) tune_key_tasks = plan.tune_key_tasks;
   grid_group = false;
   {
     int64_t grid_rows = 0;
@@ -2359,6 +2386,49 @@ static int layout_for(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *
   if (opts) o = *opts; else vshe_default_opts(&o);
   std::string err;
   return L.build(n, nnz, vrp, vci, o, val, err);
+}
+
+int vshe_layout_sweep_plan(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *val, const vshe_solve_opts *opts,
+                           int32_t num_sms, int64_t *counts, int32_t *tasks, int64_t *chunks, int32_t *sdesc) {
+  if (!counts) return VSHE_E_INVALID_ARGUMENT;
+  Layout L;
+  int rc = layout_for(n, nnz, rp, ci, val, opts, L);
+  if (rc) return rc;
+  System S;
+  S.n = n;
+  S.nnz = nnz;
+  if (opts) S.opts = *opts; else vshe_default_opts(&S.opts);
+  S.adopt_layout(L);
+  SweepPlan P;
+  plan_sweep_tasks(std::vector<System *>{&S}, S.mixed, S.has_pc, num_sms > 0 ? num_sms : 148, P);
+  counts[0] = int64_t(P.tasks.size());
+  counts[1] = int64_t(P.chunks.size());
+  counts[2] = int64_t(P.sdesc.size());
+  counts[3] = P.on_task.empty() ? 0 : int64_t(P.on_task[0]);
+  if (tasks)
+    for (size_t t = 0; t < P.tasks.size(); ++t) {
+      const TaskDev &d = P.tasks[t];
+      const int32_t v[6] = {d.sys, d.cL0, d.cL1, d.cU0, d.cU1, d.pad};
+      std::copy(v, v + 6, tasks + 6 * t);
+    }
+  if (chunks) {
+    const int vbytes = S.mixed ? int(sizeof(float)) : int(sizeof(double));
+    for (const TaskDev &d : P.tasks)
+      for (int32_t c = d.cL0; c < d.cU1; ++c) {
+        const ChunkDev &h = P.chunks[size_t(c)];
+        const bool lower = c < d.cL1;
+        const int64_t v[10] = {h.s0, h.s1, h.flags, h.nslot, h.o0, h.d0, h.r0, h.r1, h.rot,
+                               task_chunk_bytes(h.s1 - h.s0, h.nslot, h.r0, h.r1, lower, vbytes)};
+        std::copy(v, v + 10, chunks + 10 * size_t(c));
+      }
+  }
+  if (sdesc)
+    for (size_t k = 0; k < P.sdesc.size(); ++k) {
+      const SliceDesc &d = P.sdesc[k];
+      const int32_t v[4] = {d.soff, d.width, d.r0, d.nr};
+      std::copy(v, v + 4, sdesc + 4 * k);
+    }
+  return VSHE_OK;
 }
 
 int vshe_layout_sizes(int64_t n, int64_t nnz, const int64_t *rp, const int32_t *ci, const double *val, const vshe_solve_opts *opts,

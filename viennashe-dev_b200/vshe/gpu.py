@@ -109,6 +109,32 @@ def layout(rp, ci, values=None, **kw):
     return out
 
 
+def sweep_plan(rp, ci, values=None, num_sms=148, **kw):
+    """vshe_layout_sweep_plan: the task sweep plan of one system (host only) -> dict with "kind"
+    (0 grid-wide, 1 one task, 2 block tasks), "tasks" (t, 6), "chunks" (c, 10), "sdesc" (d, 4)."""
+    L = lib()
+    rp = np.ascontiguousarray(rp, np.int64)
+    ci = np.ascontiguousarray(ci, np.int32)
+    n = len(rp) - 1
+    o, keep = make_opts(**kw)
+    vals = None if values is None else np.ascontiguousarray(values, np.float64)
+    L.vshe_layout_sweep_plan.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveOptsC),
+                                         C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    cnt = np.zeros(4, np.int64)
+    vp = None if vals is None else vals.ctypes.data
+    args = (n, int(rp[-1]), rp.ctypes.data, ci.ctypes.data, vp, C.byref(o), int(num_sms))
+    rc = L.vshe_layout_sweep_plan(*args, cnt.ctypes.data, None, None, None)
+    if rc:
+        raise VsheError(rc, "vshe_layout_sweep_plan")
+    tasks = np.zeros((int(cnt[0]), 6), np.int32)
+    chunks = np.zeros((int(cnt[1]), 10), np.int64)
+    sdesc = np.zeros((int(cnt[2]), 4), np.int32)
+    rc = L.vshe_layout_sweep_plan(*args, cnt.ctypes.data, tasks.ctypes.data, chunks.ctypes.data, sdesc.ctypes.data)
+    if rc:
+        raise VsheError(rc, "vshe_layout_sweep_plan")
+    return {"kind": int(cnt[3]), "tasks": tasks, "chunks": chunks, "sdesc": sdesc}
+
+
 def kernel_launches():
     """This library's own kernel launches in the process so far."""
     return int(lib().vshe_kernel_launches())
