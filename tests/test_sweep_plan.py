@@ -8,7 +8,8 @@ so they are checked here on the CPU for the sweeps the bench and the tests run:
 * a chunk that does not fit is one slice, read from global memory;
 * the chunks of every task cover its slices in order, one level at a time, the last chunk of
   each level flagged; over all tasks every slice of the factor is swept exactly once;
-* the slice descriptors of a chunk are its slices' offsets, widths and rows."""
+* the slice descriptors of a chunk are its slices' offsets, widths and rows;
+* every solved value a chunk's rows read comes from the same task, before the level barrier."""
 import numpy as np
 import pytest
 
@@ -112,3 +113,48 @@ def test_sweep_plan_fits_the_stages(name):
     assert np.all(seen[True] == 1) and np.all(seen[False] == 1), "every slice swept exactly once"
     if name.startswith("band"):
         assert n_direct > 0
+
+
+@pytest.mark.parametrize("name", ["bar_block_ilu1_mixed", "diode_ilu0_mixed", "band_per_system_fp64"])
+def test_sweep_plan_honours_every_dependency(name):
+    """Every factor entry a chunk's row reads (a solved value of the same sweep) belongs to a row
+    of the same task swept in an earlier level of that task: tasks never wait on each other, and
+    a level's rows only read rows before the level barrier."""
+    make, kw, blocks, precision, kind = CASES[name]
+    rp, ci, bl = make()
+    kw = dict(kw, precision=precision)
+    if blocks:
+        kw["blocks"] = bl
+    n = len(rp) - 1
+    lay = gpu.layout(rp, ci, None, **kw)
+    plan = gpu.sweep_plan(rp, ci, None, **kw)
+    # backward slot of every solver row
+    slot_of_row = np.empty(n, np.int64)
+    slot_of_row[lay["urow"]] = np.arange(n)
+    for lower in (True, False):
+        off = lay["loff"] if lower else lay["uoff"]
+        rs = lay["lrow0"] if lower else lay["uslot0"]
+        col = lay["lcol"] if lower else lay["ucol"]
+        nsl = len(off) - 1
+        task_of = np.full(nsl, -1)
+        step_of = np.full(nsl, -1)
+        for ti, t in enumerate(plan["tasks"]):
+            c0, c1 = (t[1], t[2]) if lower else (t[3], t[4])
+            step = 0
+            for c in range(c0, c1):
+                s0, s1, flags = [int(v) for v in plan["chunks"][c][:3]]
+                task_of[s0:s1] = ti
+                step_of[s0:s1] = step
+                step += 1 if flags & LEVEL_END else 0
+        assert np.all(task_of >= 0)
+        # the slice holding every solver row (forward) or every backward slot
+        pos = np.arange(n) if lower else slot_of_row
+        slice_of_pos = np.searchsorted(rs, np.arange(n), side="right") - 1
+        for j in range(nsl):
+            cols = col[off[j]:off[j + 1]]
+            cols = cols[cols < n]
+            if cols.size == 0:
+                continue
+            dep = slice_of_pos[pos[cols]]
+            assert np.all(task_of[dep] == task_of[j]), ("cross-task read", lower, j)
+            assert np.all(step_of[dep] < step_of[j]), ("read inside its own level", lower, j)
