@@ -194,28 +194,25 @@ static void host_parallel_runs(const std::vector<int64_t> &runs, const std::func
 }
 
 // Transpose of the pattern (rp, ci) of n rows over n columns: tp (n + 1 offsets) and tr, the rows
-// holding each column, ascending (the order a serial pass over the rows writes them in).
+// holding each column, ascending.  Each host thread owns a range of columns and scans all rows
+// for them: no atomics, and every column's rows come out in row order.
 static void transpose_pattern(int64_t n, const int64_t *rp, const int32_t *ci, std::vector<int64_t> &tp, std::vector<int32_t> &tr) {
-  std::unique_ptr<std::atomic<int64_t>[]> cur(new std::atomic<int64_t>[size_t(n)]);
-  host_parallel(n, int64_t(1) << 16, [&](int64_t a, int64_t b) {
-    for (int64_t i = a; i < b; ++i) cur[size_t(i)].store(0, std::memory_order_relaxed);
-  });
-  host_parallel(n, int64_t(1) << 16, [&](int64_t a, int64_t b) {
-    for (int64_t i = a; i < b; ++i)
-      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) cur[size_t(ci[k])].fetch_add(1, std::memory_order_relaxed);
-  });
+  const int64_t T = host_threads(n, int64_t(1) << 16);
   tp.assign(size_t(n) + 1, 0);
-  for (int64_t i = 0; i < n; ++i) {
-    tp[size_t(i) + 1] = tp[size_t(i)] + cur[size_t(i)].load(std::memory_order_relaxed);
-    cur[size_t(i)].store(tp[size_t(i)], std::memory_order_relaxed);
-  }
-  tr.resize(size_t(tp[size_t(n)]));
-  host_parallel(n, int64_t(1) << 16, [&](int64_t a, int64_t b) {
-    for (int64_t i = a; i < b; ++i)
-      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tr[size_t(cur[size_t(ci[k])].fetch_add(1, std::memory_order_relaxed))] = int32_t(i);
+  auto own = [&](int64_t t, auto &&fn) {
+    const uint32_t c0 = uint32_t(n * t / T), w = uint32_t(n * (t + 1) / T) - c0;
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t k = rp[i]; k < rp[i + 1]; ++k)
+        if (uint32_t(ci[k]) - c0 < w) fn(i, ci[k]);
+  };
+  host_parallel(T, 1, [&](int64_t t0, int64_t t1) {
+    for (int64_t t = t0; t < t1; ++t) own(t, [&](int64_t, int32_t c) { tp[size_t(c) + 1]++; });
   });
-  host_parallel(n, int64_t(1) << 16, [&](int64_t a, int64_t b) {
-    for (int64_t j = a; j < b; ++j) std::sort(tr.begin() + tp[size_t(j)], tr.begin() + tp[size_t(j) + 1]);
+  for (int64_t i = 0; i < n; ++i) tp[size_t(i) + 1] += tp[size_t(i)];
+  tr.resize(size_t(tp[size_t(n)]));
+  std::vector<int64_t> cur(tp.begin(), tp.end() - 1);
+  host_parallel(T, 1, [&](int64_t t0, int64_t t1) {
+    for (int64_t t = t0; t < t1; ++t) own(t, [&](int64_t i, int32_t c) { tr[size_t(cur[size_t(c)]++)] = int32_t(i); });
   });
 }
 
