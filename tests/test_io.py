@@ -3,6 +3,7 @@ bit for bit (and the oracle builds the same system from it), the gnuplot file ha
 reference writer's layout (viennashe/io/gnuplot_writer.hpp:71-86), the VTK point cloud reads
 back."""
 import numpy as np
+import pytest
 
 from vshe import devices as D
 from vshe import io as vio
@@ -188,3 +189,28 @@ def test_she_node_order_colours_against_the_oracle_pattern():
             other = node[coo.row] != node[coo.col]
             assert np.all(colour[coo.row[other]] != colour[coo.col[other]]), (dev.name, fill)
             assert colour.max() + 1 <= (64 * (3 if fill else 2))
+
+
+def test_system_file_round_trip(tmp_path):
+    """A drop-in request (CSR system, slab bounds, options) survives the file bit for bit, and the
+    oracle solves the loaded system to the same x."""
+    from vshe import gpu
+    dev, cfg = D.config2(nx=12, ny=4, n_energies=24, L=3)
+    P = O.OracleProblem(dev, cfg, O.golden_coupling(3))
+    A = P.matrix(3)
+    path = tmp_path / "sys.npz"
+    vio.save_system(path, A.rp, A.ci, A.v, A.rhs, blocks=P.blocks(), precond="block_ilu0", fill_level=1,
+                    precision="mixed", tol=1e-10)
+    r = vio.load_system(path)
+    for a, b in ((r["rp"], A.rp), (r["ci"], A.ci), (r["values"], A.v), (r["rhs"], A.rhs), (r["blocks"], P.blocks())):
+        assert a.dtype == np.asarray(b).dtype or a.dtype.kind == np.asarray(b).dtype.kind
+        assert np.array_equal(a, b)
+    assert r["opts"] == dict(precond="block_ilu0", fill_level=1, precision="mixed", tol=1e-10)
+    o, _ = gpu.make_opts(blocks=r["blocks"], **r["opts"])  # the stored keywords are make_opts keywords
+    assert o.fill_level == 1 and o.precond == gpu.PRECOND["block_ilu0"] and o.n_blocks == len(P.blocks()) - 1
+    x1, s1 = O.csr_solve(A, A.rhs, tol=1e-12)
+    B = O.CSR(r["rp"], r["ci"], r["values"], r["rhs"])
+    x2, s2 = O.csr_solve(B, r["rhs"], tol=1e-12)
+    assert s1["iters"] == s2["iters"] and np.array_equal(x1, x2)
+    with pytest.raises(ValueError):
+        vio.save_system(tmp_path / "bad.npz", A.rp, A.ci, A.v, A.rhs[:-1])

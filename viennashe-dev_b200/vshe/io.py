@@ -4,6 +4,10 @@
   ``vshe_device_desc`` and the SHE configuration of ``vshe_she_config``) as one ``.npz`` file:
   flat arrays under the C field names, so a request can be replayed or exchanged without the
   generator that made it.
+* ``save_system`` / ``load_system``: a drop-in request -- the linear system the reference hands
+  to its solver slot (CSR row offsets, columns, values, rhs), the energy-slab bounds that
+  ``she::solve`` puts into the solver configuration, and the solver options as keyword
+  arguments of ``vshe.gpu.make_opts`` -- as one ``.npz`` file.
 * ``write_gnuplot``: a per-cell quantity in the layout of the reference's gnuplot writer
   (viennashe/io/gnuplot_writer.hpp:47-118): a ``## ViennaSHE - gnuplot output`` line, then one
   line per cell with the centroid coordinates and the value, each followed by a space, numbers
@@ -55,6 +59,41 @@ def load_request(path):
             v = z[key]
             ck[f.name] = v.item() if v.ndim == 0 else v
     return dev, SheConfig(**ck)
+
+
+_OPT_KEYS = ("precision", "precond", "ordering", "tol", "max_iters", "trsv", "check_every", "shadow",
+             "fill_level", "ilut_entries", "ilut_drop")
+
+
+def save_system(path, rp, ci, values, rhs, blocks=None, **opts):
+    """A CSR system with its slab bounds and solver options (make_opts keywords)."""
+    unknown = set(opts) - set(_OPT_KEYS)
+    if unknown:
+        raise ValueError("options not stored in a system file: %s" % sorted(unknown))
+    arrays = {"system.row_ptr": np.ascontiguousarray(rp, np.int64), "system.col": np.ascontiguousarray(ci, np.int32),
+              "system.val": np.ascontiguousarray(values, np.float64), "system.rhs": np.ascontiguousarray(rhs, np.float64)}
+    n = len(arrays["system.row_ptr"]) - 1
+    if arrays["system.row_ptr"][-1] != len(arrays["system.col"]) or len(arrays["system.col"]) != len(arrays["system.val"]):
+        raise ValueError("row_ptr, col and val do not describe one CSR matrix")
+    if len(arrays["system.rhs"]) != n:
+        raise ValueError("rhs has %d entries for %d rows" % (len(arrays["system.rhs"]), n))
+    if blocks is not None:
+        arrays["system.blocks"] = np.ascontiguousarray(blocks, np.int64)
+    for k, v in opts.items():
+        arrays["opts." + k] = np.asarray(v)
+    np.savez(path, **arrays)
+
+
+def load_system(path):
+    """-> dict(rp, ci, values, rhs, blocks (or None), opts: the make_opts keywords stored)."""
+    z = np.load(path, allow_pickle=False)
+    opts = {}
+    for k in _OPT_KEYS:
+        if "opts." + k in z:
+            v = z["opts." + k]
+            opts[k] = v.item() if v.ndim == 0 else v
+    return {"rp": z["system.row_ptr"], "ci": z["system.col"], "values": z["system.val"], "rhs": z["system.rhs"],
+            "blocks": z["system.blocks"] if "system.blocks" in z else None, "opts": opts}
 
 
 def write_gnuplot(path, dev: Device, values, cells=None):
