@@ -471,18 +471,22 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
         for (int64_t k = k0; k < k1; ++k) { fci[size_t(k)] = bent[size_t(k)].first; fsrc[size_t(k)] = bent[size_t(k)].second; }
       });
     } else {
-    // rows of F in base order, (base column, entry or -1), in one flat store per host thread:
-    // row i is (*rstore[rsid[i]])[roff[i] .. roff[i] + rcnt[i])
-    typedef std::vector<std::pair<int32_t, int64_t>> RowStore;
+    // rows of F in base order, (base column, entry or -1), in one store per host thread: a store
+    // holds the consecutive rows from row0 on, one after the other; rcnt[i] = entries of row i
+    struct RowStore {
+      int64_t row0 = 0;
+      std::vector<int32_t> col;
+      std::vector<int64_t> src;
+    };
     std::vector<std::unique_ptr<RowStore>> rstore;
     std::mutex rmu;
-    std::vector<int32_t> rsid((size_t)n, 0);
-    std::vector<int64_t> roff((size_t)n, 0), rcnt((size_t)n, 0);
-    // a new store and its id (taken under the lock: another thread may grow rstore meanwhile)
-    auto new_store = [&](int32_t &sid) {
+    std::vector<int64_t> rcnt((size_t)n, 0);
+    // a new store for the rows from row0 on (taken under the lock: another thread may grow
+    // rstore meanwhile)
+    auto new_store = [&](int64_t row0) {
       std::lock_guard<std::mutex> lk(rmu);
       rstore.emplace_back(new RowStore);
-      sid = int32_t(rstore.size() - 1);
+      rstore.back()->row0 = row0;
       return rstore.back().get();
     };
     if (ilut) {
@@ -501,8 +505,7 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       std::vector<char> nz((size_t)n, 0);
       std::vector<int32_t> cols, heap;
       std::vector<std::pair<double, int32_t>> lo, up;
-      int32_t sid = 0;
-      RowStore &st = *new_store(sid);
+      RowStore &st = *new_store(0);
       for (int64_t i = 0; i < n; ++i) {
         cols.clear(); heap.clear();
         double rn = 0.0;
@@ -564,15 +567,15 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
         for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) pat.push_back(bent[size_t(k)].first);
         std::sort(pat.begin(), pat.end());
         pat.erase(std::unique(pat.begin(), pat.end()), pat.end());
-        rsid[size_t(i)] = sid;
-        roff[size_t(i)] = int64_t(st.size());
+        const size_t before = st.col.size();
         int64_t ka = brp[size_t(i)];
         for (int32_t j : pat) {
           while (ka < brp[size_t(i) + 1] && bent[size_t(ka)].first < j) ++ka;
           const bool in_a = ka < brp[size_t(i) + 1] && bent[size_t(ka)].first == j;
-          st.push_back({j, in_a ? bent[size_t(ka)].second : int64_t(-1)});
+          st.col.push_back(j);
+          st.src.push_back(in_a ? bent[size_t(ka)].second : int64_t(-1));
         }
-        rcnt[size_t(i)] = int64_t(st.size()) - roff[size_t(i)];
+        rcnt[size_t(i)] = int64_t(st.col.size() - before);
         for (int32_t j : cols) { nz[size_t(j)] = 0; w[size_t(j)] = 0.0; }
       }
     } else {
@@ -590,8 +593,7 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
         std::unique_ptr<int64_t[]> src(new int64_t[size_t(n)]);
         if (!lvl1) throw std::bad_alloc();
         int32_t *lvl = lvl1.get();
-        int32_t sid = 0;
-        RowStore &st = *new_store(sid);
+        RowStore &st = *new_store(runs[size_t(r0)]);
         std::vector<int32_t> cols, heap;
         for (int64_t i = runs[size_t(r0)]; i < runs[size_t(r1)]; ++i) {
           const int32_t bi = bblk[size_t(i)];
@@ -624,34 +626,36 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
             }
           }
           std::sort(cols.begin(), cols.end());
-          rsid[size_t(i)] = sid;
-          roff[size_t(i)] = int64_t(st.size());
           ub[size_t(i)] = int64_t(ucolv.size());
           for (int32_t j : cols) {
-            st.push_back({j, src[size_t(j)]});
+            st.col.push_back(j);
+            st.src.push_back(src[size_t(j)]);
             if (j > i) { ucolv.push_back(j); ulevv.push_back(lvl[size_t(j)] - 1); }
             lvl[size_t(j)] = 0;
           }
-          rcnt[size_t(i)] = int64_t(st.size()) - roff[size_t(i)];
+          rcnt[size_t(i)] = int64_t(cols.size());
           ue[size_t(i)] = int64_t(ucolv.size());
         }
       };
       if (contiguous) host_parallel_runs(runs, symbolic);
       else symbolic(0, nruns);
     }
-    // one CSR in base order (each stored row is already in ascending base column)
+    // one CSR in base order: the stores' rows are consecutive and in ascending base column, so
+    // each store is one contiguous piece of it
     frp.assign((size_t)n + 1, 0);
     for (int64_t i = 0; i < n; ++i) frp[size_t(i) + 1] = frp[size_t(i)] + rcnt[size_t(i)];
+    {
+      size_t stored = 0;
+      for (const auto &st : rstore) stored += st->col.size();
+      if (stored != size_t(frp[size_t(n)])) { err = "factor pattern stores do not tile the rows"; return VSHE_E_INVALID_ARGUMENT; }
+    }
     fci.resize(size_t(frp[size_t(n)]));
     fsrc.resize(size_t(frp[size_t(n)]));
-    host_parallel(n, int64_t(1) << 16, [&](int64_t i0, int64_t i1) {
-      for (int64_t i = i0; i < i1; ++i) {
-        const RowStore &st = *rstore[size_t(rsid[size_t(i)])];
-        int64_t p = frp[size_t(i)];
-        for (int64_t q = roff[size_t(i)]; q < roff[size_t(i)] + rcnt[size_t(i)]; ++q, ++p) {
-          fci[size_t(p)] = st[size_t(q)].first;
-          fsrc[size_t(p)] = st[size_t(q)].second;
-        }
+    host_parallel(int64_t(rstore.size()), 1, [&](int64_t s0, int64_t s1) {
+      for (int64_t q = s0; q < s1; ++q) {
+        const RowStore &st = *rstore[size_t(q)];
+        std::copy(st.col.begin(), st.col.end(), fci.begin() + frp[size_t(st.row0)]);
+        std::copy(st.src.begin(), st.src.end(), fsrc.begin() + frp[size_t(st.row0)]);
       }
     });
     }
@@ -747,17 +751,20 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       prp[size_t(i) + 1] = prp[size_t(i)] + (frp[size_t(b) + 1] - frp[size_t(b)]);
     }
     host_parallel(n, int64_t(1) << 16, [&](int64_t i0, int64_t i1) {
-      std::vector<std::pair<int32_t, int64_t>> row;
+      // a row's columns are distinct: sort (solver column, position in the row) keys
+      std::vector<uint64_t> key;
       for (int64_t i = i0; i < i1; ++i) {
         const int32_t b = binv[size_t(perm[size_t(i)])];
-        row.clear();
-        for (int64_t k = frp[size_t(b)]; k < frp[size_t(b) + 1]; ++k) row.push_back({sinv[size_t(fci[size_t(k)])], fsrc[size_t(k)]});
-        std::sort(row.begin(), row.end());
+        const int64_t k0 = frp[size_t(b)];
+        key.clear();
+        for (int64_t k = k0; k < frp[size_t(b) + 1]; ++k) key.push_back((uint64_t(uint32_t(sinv[size_t(fci[size_t(k)])])) << 32) | uint64_t(k - k0));
+        std::sort(key.begin(), key.end());
         int64_t p = prp[size_t(i)];
-        for (auto &x : row) {
-          if (x.first == i) pdiag[size_t(i)] = p;
-          pci[size_t(p)] = x.first;
-          amap[size_t(p)] = x.second;
+        for (uint64_t x : key) {
+          const int32_t c = int32_t(x >> 32);
+          if (c == i) pdiag[size_t(i)] = p;
+          pci[size_t(p)] = c;
+          amap[size_t(p)] = fsrc[size_t(k0 + int64_t(x & 0xffffffffu))];
           ++p;
         }
       }
