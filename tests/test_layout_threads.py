@@ -17,6 +17,8 @@ CASES = {
     "bar_multicolour_ilu1": (lambda: D.config2(nx=24, ny=6, n_energies=24, L=3),
                              dict(precond="ilu0", ordering="multicolor", fill_level=1), False),
     "diode_natural": (lambda: D.config1(), dict(precond="ilu0", ordering="natural"), False),
+    "bar_ilut": (lambda: D.config2(nx=24, ny=6, n_energies=24, L=3),
+                 dict(precond="ilut", ordering="natural", ilut_entries=20, ilut_drop=1e-3), False),
 }
 
 
@@ -29,10 +31,11 @@ def test_layout_does_not_depend_on_host_threads(name):
     if blocks:
         kw = dict(kw, blocks=P.blocks())
     try:
+        vals = A.v if kw["precond"] == "ilut" else None  # the ILUT pattern comes from the values
         gpu.set_host_threads(1)
-        one = gpu.layout(A.rp, A.ci, None, **kw)
+        one = gpu.layout(A.rp, A.ci, vals, **kw)
         gpu.set_host_threads(8)
-        many = gpu.layout(A.rp, A.ci, None, **kw)
+        many = gpu.layout(A.rp, A.ci, vals, **kw)
     finally:
         gpu.set_host_threads(0)
     assert one.keys() == many.keys()
