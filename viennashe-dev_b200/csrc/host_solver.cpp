@@ -498,86 +498,111 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       // pattern (k_ilut), which reproduces ILUT for the values seen here.
       const int pkeep = opts.ilut_entries > 0 ? opts.ilut_entries : 60;
       const double tau = opts.ilut_drop > 0 ? opts.ilut_drop : 1e-4;
-      std::vector<int64_t> urp((size_t)n + 1, 0);
-      std::vector<int32_t> ucol;
-      std::vector<double> uval, udiag((size_t)n, 0.0);
-      std::vector<double> w((size_t)n, 0.0);
-      std::vector<char> nz((size_t)n, 0);
-      std::vector<int32_t> cols, heap;
-      std::vector<std::pair<double, int32_t>> lo, up;
-      RowStore &st = *new_store(0);
-      for (int64_t i = 0; i < n; ++i) {
-        cols.clear(); heap.clear();
-        double rn = 0.0;
-        for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) {
-          const int32_t j = bent[size_t(k)].first;
-          const double a = values[bent[size_t(k)].second];
-          w[size_t(j)] = a; nz[size_t(j)] = 1; cols.push_back(j);
-          rn += a * a;
-          if (j < i) heap.push_back(j);
-        }
-        const double ti = tau * std::sqrt(rn);
-        if (!nz[size_t(i)]) { nz[size_t(i)] = 1; w[size_t(i)] = 0.0; cols.push_back(int32_t(i)); }
-        std::make_heap(heap.begin(), heap.end(), std::greater<int32_t>());
-        int32_t last = -1;
-        while (!heap.empty()) {
-          std::pop_heap(heap.begin(), heap.end(), std::greater<int32_t>());
-          const int32_t k = heap.back(); heap.pop_back();
-          if (k == last) continue;
-          last = k;
-          if (udiag[size_t(k)] == 0.0) { w[size_t(k)] = 0.0; continue; }
-          const double wk = w[size_t(k)] / udiag[size_t(k)];
-          if (std::fabs(wk) < ti) { w[size_t(k)] = 0.0; continue; }
-          w[size_t(k)] = wk;
-          for (int64_t kk = urp[size_t(k)]; kk < urp[size_t(k) + 1]; ++kk) {
-            const int32_t j = ucol[size_t(kk)];
-            if (!nz[size_t(j)]) {
-              nz[size_t(j)] = 1; w[size_t(j)] = 0.0; cols.push_back(j);
-              if (j < i) { heap.push_back(j); std::push_heap(heap.begin(), heap.end(), std::greater<int32_t>()); }
+      //
+      // Rows are eliminated on the host threads in claims of consecutive rows, in increasing order.
+      // A row reads only rows above it: before it reads row k's pivot and kept upper part it waits
+      // until row k is final (done[k], set with release after they are written).  The row holding
+      // the first unfinished position never waits, so the elimination always progresses, and every
+      // row computes exactly what the serial elimination computes.
+      std::vector<std::vector<int32_t>> ucol((size_t)n);   // kept upper part of each row
+      std::vector<std::vector<double>> uval((size_t)n);
+      std::vector<double> udiag((size_t)n, 0.0);
+      std::unique_ptr<std::atomic<uint8_t>[]> done(new std::atomic<uint8_t>[size_t(n)]);
+      for (int64_t i = 0; i < n; ++i) done[size_t(i)].store(0, std::memory_order_relaxed);
+      std::atomic<int64_t> next_claim{0};
+      constexpr int64_t kClaimRows = 64;
+      auto eliminate = [&](int64_t, int64_t) {
+        // dense scratch over all columns, calloc'd: a thread touches only the pages its rows reach
+        std::unique_ptr<double, void (*)(void *)> wbuf((double *)std::calloc(size_t(n), sizeof(double)), std::free);
+        std::unique_ptr<char, void (*)(void *)> nzbuf((char *)std::calloc(size_t(n), 1), std::free);
+        if (!wbuf || !nzbuf) throw std::bad_alloc();
+        double *w = wbuf.get();
+        char *nz = nzbuf.get();
+        std::vector<int32_t> cols, heap;
+        std::vector<std::pair<double, int32_t>> lo, up;
+        for (;;) {
+          const int64_t c0 = next_claim.fetch_add(kClaimRows);
+          if (c0 >= n) break;
+          const int64_t c1 = std::min<int64_t>(n, c0 + kClaimRows);
+          RowStore &st = *new_store(c0);
+          for (int64_t i = c0; i < c1; ++i) {
+            cols.clear(); heap.clear();
+            double rn = 0.0;
+            for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) {
+              const int32_t j = bent[size_t(k)].first;
+              const double a = values[bent[size_t(k)].second];
+              w[size_t(j)] = a; nz[size_t(j)] = 1; cols.push_back(j);
+              rn += a * a;
+              if (j < i) heap.push_back(j);
             }
-            w[size_t(j)] -= wk * uval[size_t(kk)];
+            const double ti = tau * std::sqrt(rn);
+            if (!nz[size_t(i)]) { nz[size_t(i)] = 1; w[size_t(i)] = 0.0; cols.push_back(int32_t(i)); }
+            std::make_heap(heap.begin(), heap.end(), std::greater<int32_t>());
+            int32_t last = -1;
+            while (!heap.empty()) {
+              std::pop_heap(heap.begin(), heap.end(), std::greater<int32_t>());
+              const int32_t k = heap.back(); heap.pop_back();
+              if (k == last) continue;
+              last = k;
+              while (!done[size_t(k)].load(std::memory_order_acquire)) std::this_thread::yield();
+              if (udiag[size_t(k)] == 0.0) { w[size_t(k)] = 0.0; continue; }
+              const double wk = w[size_t(k)] / udiag[size_t(k)];
+              if (std::fabs(wk) < ti) { w[size_t(k)] = 0.0; continue; }
+              w[size_t(k)] = wk;
+              const std::vector<int32_t> &uck = ucol[size_t(k)];
+              const std::vector<double> &uvk = uval[size_t(k)];
+              for (size_t kk = 0; kk < uck.size(); ++kk) {
+                const int32_t j = uck[kk];
+                if (!nz[size_t(j)]) {
+                  nz[size_t(j)] = 1; w[size_t(j)] = 0.0; cols.push_back(j);
+                  if (j < i) { heap.push_back(j); std::push_heap(heap.begin(), heap.end(), std::greater<int32_t>()); }
+                }
+                w[size_t(j)] -= wk * uvk[kk];
+              }
+            }
+            lo.clear(); up.clear();
+            for (int32_t j : cols) {
+              if (j == i || w[size_t(j)] == 0.0 || std::fabs(w[size_t(j)]) < ti) continue;
+              (j < i ? lo : up).push_back({std::fabs(w[size_t(j)]), j});
+            }
+            auto keep = [&](std::vector<std::pair<double, int32_t>> &v) {
+              if (int(v.size()) > pkeep) {
+                std::nth_element(v.begin(), v.begin() + pkeep, v.end(),
+                [](const std::pair<double, int32_t> &a, const std::pair<double, int32_t> &b) { return a.first > b.first; });
+                v.resize(size_t(pkeep));
+              }
+            };
+            // the factor pattern of row i: every entry that survived the tau test (the device applies
+            // the p-largest rule itself, and multipliers beyond the p largest still take part in the
+            // elimination), the diagonal and A's own entries
+            std::vector<int32_t> pat;
+            for (auto &e : lo) pat.push_back(e.second);
+            pat.push_back(int32_t(i));
+            for (auto &e : up) pat.push_back(e.second);
+            keep(lo); keep(up);
+            double d = w[size_t(i)];
+            if (d == 0.0) d = ti > 0.0 ? ti : 1.0;
+            udiag[size_t(i)] = d;
+            std::sort(up.begin(), up.end(), [](const std::pair<double, int32_t> &a, const std::pair<double, int32_t> &b) { return a.second < b.second; });
+            for (auto &e : up) { ucol[size_t(i)].push_back(e.second); uval[size_t(i)].push_back(w[size_t(e.second)]); }
+            done[size_t(i)].store(1, std::memory_order_release);
+            for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) pat.push_back(bent[size_t(k)].first);
+            std::sort(pat.begin(), pat.end());
+            pat.erase(std::unique(pat.begin(), pat.end()), pat.end());
+            const size_t before = st.col.size();
+            int64_t ka = brp[size_t(i)];
+            for (int32_t j : pat) {
+              while (ka < brp[size_t(i) + 1] && bent[size_t(ka)].first < j) ++ka;
+              const bool in_a = ka < brp[size_t(i) + 1] && bent[size_t(ka)].first == j;
+              st.col.push_back(j);
+              st.src.push_back(in_a ? bent[size_t(ka)].second : int64_t(-1));
+            }
+            rcnt[size_t(i)] = int64_t(st.col.size() - before);
+            for (int32_t j : cols) { nz[size_t(j)] = 0; w[size_t(j)] = 0.0; }
           }
         }
-        lo.clear(); up.clear();
-        for (int32_t j : cols) {
-          if (j == i || w[size_t(j)] == 0.0 || std::fabs(w[size_t(j)]) < ti) continue;
-          (j < i ? lo : up).push_back({std::fabs(w[size_t(j)]), j});
-        }
-        auto keep = [&](std::vector<std::pair<double, int32_t>> &v) {
-          if (int(v.size()) > pkeep) {
-            std::nth_element(v.begin(), v.begin() + pkeep, v.end(),
-                             [](const std::pair<double, int32_t> &a, const std::pair<double, int32_t> &b) { return a.first > b.first; });
-            v.resize(size_t(pkeep));
-          }
-        };
-        // the factor pattern of row i: every entry that survived the tau test (the device applies
-        // the p-largest rule itself, and multipliers beyond the p largest still take part in the
-        // elimination), the diagonal and A's own entries
-        std::vector<int32_t> pat;
-        for (auto &e : lo) pat.push_back(e.second);
-        pat.push_back(int32_t(i));
-        for (auto &e : up) pat.push_back(e.second);
-        keep(lo); keep(up);
-        double d = w[size_t(i)];
-        if (d == 0.0) d = ti > 0.0 ? ti : 1.0;
-        udiag[size_t(i)] = d;
-        std::sort(up.begin(), up.end(), [](const std::pair<double, int32_t> &a, const std::pair<double, int32_t> &b) { return a.second < b.second; });
-        for (auto &e : up) { ucol.push_back(e.second); uval.push_back(w[size_t(e.second)]); }
-        urp[size_t(i) + 1] = int64_t(ucol.size());
-        for (int64_t k = brp[size_t(i)]; k < brp[size_t(i) + 1]; ++k) pat.push_back(bent[size_t(k)].first);
-        std::sort(pat.begin(), pat.end());
-        pat.erase(std::unique(pat.begin(), pat.end()), pat.end());
-        const size_t before = st.col.size();
-        int64_t ka = brp[size_t(i)];
-        for (int32_t j : pat) {
-          while (ka < brp[size_t(i) + 1] && bent[size_t(ka)].first < j) ++ka;
-          const bool in_a = ka < brp[size_t(i) + 1] && bent[size_t(ka)].first == j;
-          st.col.push_back(j);
-          st.src.push_back(in_a ? bent[size_t(ka)].second : int64_t(-1));
-        }
-        rcnt[size_t(i)] = int64_t(st.col.size() - before);
-        for (int32_t j : cols) { nz[size_t(j)] = 0; w[size_t(j)] = 0.0; }
-      }
+      };
+      host_parallel(host_threads(n, kClaimRows * 16), 1, eliminate);
     } else {
       // symbolic ILU(k): the final rows' upper parts (column, level) feed later rows.  A row
       // reads only earlier rows of its own block, so when every block is one run of base
