@@ -117,9 +117,10 @@ int SheProblem::setup_host(Ctx &ctx, const vshe_device_desc &d, const vshe_she_c
 // Upper bound of the device memory the problem will hold, from the host set-up alone, so that
 // admission against an HBM budget happens before any allocation.  Row lengths are bounded by the
 // mesh and the harmonics per node: a full-system even row holds its diagonal, two optical
-// in-scattering entries and at most o(L) odd couplings per facet of its cell (2 dim facets); an
-// odd row its diagonal and at most e(L) couplings to each of its two cells; a reduced row its
-// diagonal, the in-scattering pair and at most e(L) columns for its cell and each neighbour.  The
+// in-scattering entries and at most o(L) odd couplings per facet of its cell (at most f facets,
+// the mesh's largest cell; 2 dim on the structured meshes); an odd row its diagonal and at most
+// e(L) couplings to each of its two cells; a reduced row its diagonal, the in-scattering pair and
+// at most e(L) columns for its cell and each neighbour.  The
 // factor keeps at most (1 + k) times the reduced pattern for ILU(k), and 2 p + 1 entries per row
 // more for ILUT(p).  Per entry and per row, the bytes of every buffer the pipeline, the solver
 // (SELL copies of A, L and U, factorisation CSR and maps, Krylov vectors) and the batch hold.
@@ -128,8 +129,10 @@ size_t SheProblem::estimate_bytes() const {
   for (int l = 0; l <= H.L; l += 2) e += 2 * l + 1;
   const int64_t o = int64_t(H.L + 1) * (H.L + 1) - e;
   const int64_t ne = H.n_even, no = H.n_odd, nfull = ne + no;
-  const int64_t nnz_full = ne * (3 + 2 * H.dim * o) + no * (1 + 2 * e);
-  const int64_t nnz_red = ne * (3 + (1 + 2 * H.dim) * e);
+  int64_t f = 2 * H.dim;
+  for (int c = 0; c < H.nc; ++c) f = std::max<int64_t>(f, H.cf_ptr[size_t(c) + 1] - H.cf_ptr[size_t(c)]);
+  const int64_t nnz_full = ne * (3 + f * o) + no * (1 + 2 * e);
+  const int64_t nnz_red = ne * (3 + (1 + f) * e);
   const int64_t nnz_f = opts.precond == VSHE_PRECOND_ILUT
                             ? nnz_red + ne * (2 * int64_t(opts.ilut_entries > 0 ? opts.ilut_entries : 60) + 1)
                             : nnz_red * (1 + std::max(0, int(opts.fill_level)));
