@@ -57,7 +57,10 @@ extern "C" {
                                         values at system creation, every position whose entry passes the drop
                                         tolerance; the factorisation of every solve runs on the device inside
                                         that pattern with ILUT's two dropping rules (multipliers and entries
-                                        below tol * ||a_i||, then the ilut_entries largest of L and of U) */
+                                        below tol * ||a_i||, then the ilut_entries largest of L and of U).
+                                        With n_blocks / block_ptr the factorisation stays inside the blocks
+                                        (energy slabs): no elimination with, and no fill from, rows of other
+                                        blocks; tol * ||a_i|| uses the whole row */
 
 #define VSHE_ORDER_NATURAL     0   /* the caller's row order (the reference's) */
 #define VSHE_ORDER_MULTICOLOR  1   /* greedy colouring of the matrix graph, rows grouped by colour */

@@ -288,13 +288,22 @@ def iluk_csr(A: CSR, fill_level, blocks=None):
     return rp, ci, lu
 
 
-def ilut_csr(A: CSR, p, tau):
-    """ILUT(p, tau) factor (Saad Alg. 10.6) as one CSR (rp, ci, values), columns ascending."""
+def _blocks_arg(blocks):
+    bp = None if blocks is None else np.ascontiguousarray(blocks, np.int64)
+    return bp, (0 if bp is None else len(bp) - 1), (None if bp is None else ptr(bp, C.c_int64))
+
+
+def ilut_csr(A: CSR, p, tau, blocks=None):
+    """ILUT(p, tau) factor (Saad Alg. 10.6) as one CSR (rp, ci, values), columns ascending;
+    restricted to the blocks when they are given."""
     L = lib()
     L.vsheo_ilut_csr.argtypes = [C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int32,
-                                 C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+                                 C.c_double, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     nnz = np.zeros(1, np.int64)
-    args = (A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double), int(p), float(tau), ptr(nnz, C.c_int64))
+    bp, nb, bptr = _blocks_arg(blocks)
+    args = (A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double), int(p), float(tau), nb, bptr,
+            ptr(nnz, C.c_int64))
     if L.vsheo_ilut_csr(*args, None, None, None):
         raise RuntimeError("oracle ilut failed")
     rp = np.zeros(A.n + 1, np.int64)
@@ -305,14 +314,17 @@ def ilut_csr(A: CSR, p, tau):
     return rp, ci, lu
 
 
-def ilut_passed(A: CSR, p, tau):
+def ilut_passed(A: CSR, p, tau, blocks=None):
     """Per row, the columns whose entries passed ILUT(p, tau)'s tau test before the p-largest
-    rule (CSR pattern rp, ci)."""
+    rule (CSR pattern rp, ci); restricted to the blocks when they are given."""
     L = lib()
     L.vsheo_ilut_passed.argtypes = [C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int32,
-                                    C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+                                    C.c_double, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int32)]
     nnz = np.zeros(1, np.int64)
-    args = (A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double), int(p), float(tau), ptr(nnz, C.c_int64))
+    bp, nb, bptr = _blocks_arg(blocks)
+    args = (A.n, ptr(A.rp, C.c_int64), ptr(A.ci, C.c_int32), ptr(A.v, C.c_double), int(p), float(tau), nb, bptr,
+            ptr(nnz, C.c_int64))
     if L.vsheo_ilut_passed(*args, None, None):
         raise RuntimeError("oracle ilut failed")
     rp = np.zeros(A.n + 1, np.int64)

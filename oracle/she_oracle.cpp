@@ -968,8 +968,12 @@ static ILU iluk(int64_t n, const int64_t *rp, const int32_t *ci, const double *v
 }
 
 // ILUT(p, tau), Saad Alg. 10.6 (row-wise, dual dropping).
+// With blk (a block id per row), the factorisation is restricted to the blocks, as the library's
+// slab-restricted ILUT: a row is not eliminated with rows of other blocks and takes no fill from
+// them; tau * ||a_i|| uses the whole row, and the entries of other blocks take part in the
+// p-largest rule of L and of U, but are not part of the factor.
 static ILU ilut(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int p, double tau,
-                std::vector<std::vector<int32_t>> *passed = nullptr) {
+                std::vector<std::vector<int32_t>> *passed = nullptr, const std::vector<int32_t> *blk = nullptr) {
   ILU f; f.n = n; f.lrp.assign(1, 0); f.urp.assign(1, 0);
   std::vector<double> w(size_t(n), 0.0);
   std::vector<char> nz(size_t(n), 0);
@@ -990,11 +994,13 @@ static ILU ilut(int64_t n, const int64_t *rp, const int32_t *ci, const double *v
     while (!heap.empty()) {
       std::pop_heap(heap.begin(), heap.end(), std::greater<int32_t>());
       int32_t k = heap.back(); heap.pop_back();
+      if (blk && (*blk)[size_t(k)] != (*blk)[size_t(i)]) continue;  // another block: no elimination
       double wk = w[k] / f.uv[size_t(f.urp[k])];
       if (std::fabs(wk) < ti) { w[k] = 0.0; continue; }
       w[k] = wk;
       for (int64_t kk = f.urp[k] + 1; kk < f.urp[k + 1]; ++kk) {
         int32_t j = f.uci[size_t(kk)];
+        if (blk && (*blk)[size_t(j)] != (*blk)[size_t(i)]) continue;
         if (!nz[j]) { nz[j] = 1; w[j] = 0.0; cols.push_back(j); if (j < i) { heap.push_back(j); std::push_heap(heap.begin(), heap.end(), std::greater<int32_t>()); } }
         w[j] -= wk * f.uv[size_t(kk)];
       }
@@ -1020,6 +1026,11 @@ static ILU ilut(int64_t n, const int64_t *rp, const int32_t *ci, const double *v
       std::sort(ps.begin(), ps.end());
     }
     keep(lo); keep(up);
+    if (blk) {  // entries of other blocks are ranked above but are not part of the factor
+      auto other = [&](const std::pair<double, int32_t> &e) { return (*blk)[size_t(e.second)] != (*blk)[size_t(i)]; };
+      lo.erase(std::remove_if(lo.begin(), lo.end(), other), lo.end());
+      up.erase(std::remove_if(up.begin(), up.end(), other), up.end());
+    }
     for (auto &e : lo) { f.lci.push_back(e.second); f.lv.push_back(w[e.second]); }
     if (d == 0.0) d = (ti > 0 ? ti : 1.0);  // guard a zero pivot
     f.uci.push_back(int32_t(i)); f.uv.push_back(d);
@@ -1350,7 +1361,11 @@ int vsheo_csr_solve(int64_t n, const int64_t *rp, const int32_t *ci, const doubl
     auto t0 = std::chrono::steady_clock::now();
     ILU M; const ILU *pm = nullptr;
     if (precond == 1) { M = ilu0(n, rp, ci, v, 0, nullptr); pm = &M; }
-    else if (precond == 2) { M = ilut(n, rp, ci, v, ilut_p, ilut_tau); pm = &M; }
+    else if (precond == 2) {
+      const std::vector<int32_t> blk = row_blocks(n, nb, bptr);
+      M = ilut(n, rp, ci, v, ilut_p, ilut_tau, nullptr, nb > 0 ? &blk : nullptr);
+      pm = &M;
+    }
     else if (precond == 3) { M = ilu0(n, rp, ci, v, nb, bptr); pm = &M; }
     else if (precond == 4) { M = iluk(n, rp, ci, v, ilut_p, nb, bptr); pm = &M; }
     auto t1 = std::chrono::steady_clock::now();
@@ -1390,9 +1405,10 @@ int vsheo_iluk_csr(int64_t n, const int64_t *rp, const int32_t *ci, const double
 // ILUT(p, tau) factor as one CSR (L strictly lower, then U with its diagonal, columns ascending):
 // call with rp_out == NULL for the entry count, then with arrays of that size.
 int vsheo_ilut_csr(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int32_t p, double tau,
-                   int64_t *nnz_out, int64_t *rp_out, int32_t *ci_out, double *lu_out) {
+                   int64_t nb, const int64_t *bptr, int64_t *nnz_out, int64_t *rp_out, int32_t *ci_out, double *lu_out) {
   try {
-    ILU f = ilut(n, rp, ci, v, p, tau);
+    const std::vector<int32_t> blk = row_blocks(n, nb, bptr);
+    ILU f = ilut(n, rp, ci, v, p, tau, nullptr, nb > 0 ? &blk : nullptr);
     *nnz_out = int64_t(f.lci.size() + f.uci.size());
     if (!rp_out) return 0;
     int64_t q = 0;
@@ -1409,10 +1425,11 @@ int vsheo_ilut_csr(int64_t n, const int64_t *rp, const int32_t *ci, const double
 // Per row, the columns whose entries passed ILUT's tau test (before its p-largest rule), as a
 // CSR pattern: call with rp_out == NULL for the count.
 int vsheo_ilut_passed(int64_t n, const int64_t *rp, const int32_t *ci, const double *v, int32_t p, double tau,
-                      int64_t *nnz_out, int64_t *rp_out, int32_t *ci_out) {
+                      int64_t nb, const int64_t *bptr, int64_t *nnz_out, int64_t *rp_out, int32_t *ci_out) {
   try {
     std::vector<std::vector<int32_t>> passed((size_t)n);
-    ilut(n, rp, ci, v, p, tau, &passed);
+    const std::vector<int32_t> blk = row_blocks(n, nb, bptr);
+    ilut(n, rp, ci, v, p, tau, &passed, nb > 0 ? &blk : nullptr);
     int64_t q = 0;
     for (auto &r : passed) q += int64_t(r.size());
     *nnz_out = q;

@@ -9,6 +9,7 @@ oracle's CSR SpMV and ILU(0) apply (1e-13 relative, summation order differs).
 import numpy as np
 import pytest
 
+from vshe import devices as D
 from vshe import gpu
 import oracle_api as O
 import cases
@@ -292,3 +293,34 @@ def test_ilut_pattern_long_rows():
         want.update((i, int(j)) for j in A.ci[A.rp[i]:A.rp[i + 1]])
         want.add((i, i))
     assert got == want
+
+
+@pytest.mark.parametrize("p,tau", [(20, 1e-3), (60, 1e-4)])
+def test_slab_ilut_pattern_matches_oracle(p, tau):
+    """VSHE_PRECOND_ILUT with energy-slab blocks: the elimination stays inside each slab (no
+    elimination with, and no fill from, rows of other slabs; tau ||a_i|| over the whole row).  The
+    host analysis keeps, inside the slabs, exactly the positions that pass the oracle's
+    slab-restricted ILUT tau test, the diagonal and A's entries; the oracle's final factor lies
+    inside them; and the sweeps run one task per slab group."""
+    dev, cfg = D.config2(nx=16, ny=5, n_energies=40, L=5)
+    P = O.OracleProblem(dev, cfg, O.golden_coupling(5))
+    A = P.matrix(3)
+    bl = P.blocks()
+    blk = np.searchsorted(bl, np.arange(A.n), side="right") - 1
+    Lt = gpu.layout(A.rp, A.ci, values=A.v, precond="ilut", ilut_entries=p, ilut_drop=tau, blocks=bl)
+    perm = Lt["perm"]
+    got = set((int(perm[i]), int(perm[j])) for i, j in _slot_pattern(Lt))
+    rp, ci = O.ilut_passed(A, p, tau, blocks=bl)
+    want = set()
+    for i in range(A.n):
+        want.update((i, int(j)) for j in ci[rp[i]:rp[i + 1]] if blk[j] == blk[i])
+        want.update((i, int(j)) for j in A.ci[A.rp[i]:A.rp[i + 1]] if blk[j] == blk[i])
+        want.add((i, i))
+    assert got == want
+    frp, fci, _ = O.ilut_csr(A, p, tau, blocks=bl)
+    final = set((i, int(j)) for i in range(A.n) for j in fci[frp[i]:frp[i + 1]])
+    assert all(blk[j] == blk[i] for i, j in final) and final <= got
+    # without blocks the same options give the whole-matrix ILUT, which reaches across slabs
+    whole = O.ilut_passed(A, p, tau)
+    assert any(blk[int(j)] != blk[i] for i in range(A.n) for j in whole[1][whole[0][i]:whole[0][i + 1]] if j > i)
+    assert gpu.sweep_plan(A.rp, A.ci, A.v, precond="ilut", ilut_entries=p, ilut_drop=tau, blocks=bl)["kind"] == 2

@@ -19,6 +19,8 @@ CASES = {
     "diode_natural": (lambda: D.config1(), dict(precond="ilu0", ordering="natural"), False),
     "bar_ilut": (lambda: D.config2(nx=24, ny=6, n_energies=24, L=3),
                  dict(precond="ilut", ordering="natural", ilut_entries=20, ilut_drop=1e-3), False),
+    "bar_slab_ilut": (lambda: D.config2(nx=24, ny=6, n_energies=24, L=3),
+                      dict(precond="ilut", ordering="natural", ilut_entries=20, ilut_drop=1e-3), True),
 }
 
 

@@ -390,7 +390,8 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
   if (ilut && !values) { err = "the ILUT pattern needs the matrix values at creation"; return VSHE_E_INVALID_ARGUMENT; }
   // block ids in the caller's order
   std::vector<int32_t> blk0((size_t)(n), 0);
-  if (opts.precond == VSHE_PRECOND_BLOCK_ILU0 && opts.n_blocks > 0 && opts.block_ptr) {
+  // (block-ILU, and ILUT restricted to the blocks when the caller gives them)
+  if ((opts.precond == VSHE_PRECOND_BLOCK_ILU0 || opts.precond == VSHE_PRECOND_ILUT) && opts.n_blocks > 0 && opts.block_ptr) {
     const int64_t *bp = opts.block_ptr;
     if (bp[0] != 0 || bp[opts.n_blocks] != n) { err = "block_ptr must span [0, n]"; return VSHE_E_INVALID_ARGUMENT; }
     for (int64_t b = 0; b < opts.n_blocks; ++b) {
@@ -495,7 +496,9 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       // dropped, then the p largest of L and of U are kept (the diagonal always).  Only the
       // pattern is kept here: every position that survives the tau test, joined with A's.  The
       // device repeats the same elimination with the same two dropping rules inside that
-      // pattern (k_ilut), which reproduces ILUT for the values seen here.
+      // pattern (k_ilut), which reproduces ILUT for the values seen here.  With blocks the
+      // elimination stays inside the row's block (no elimination with, and no fill from, rows of
+      // other blocks), as the device's does; tau * ||a_i|| uses the whole row.
       const int pkeep = opts.ilut_entries > 0 ? opts.ilut_entries : 60;
       const double tau = opts.ilut_drop > 0 ? opts.ilut_drop : 1e-4;
       //
@@ -544,6 +547,7 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
               const int32_t k = heap.back(); heap.pop_back();
               if (k == last) continue;
               last = k;
+              if (bblk[size_t(k)] != bblk[size_t(i)]) continue;  // another block: no elimination
               while (!done[size_t(k)].load(std::memory_order_acquire)) std::this_thread::yield();
               if (udiag[size_t(k)] == 0.0) { w[size_t(k)] = 0.0; continue; }
               const double wk = w[size_t(k)] / udiag[size_t(k)];
@@ -553,6 +557,7 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
               const std::vector<double> &uvk = uval[size_t(k)];
               for (size_t kk = 0; kk < uck.size(); ++kk) {
                 const int32_t j = uck[kk];
+                if (bblk[size_t(j)] != bblk[size_t(i)]) continue;
                 if (!nz[size_t(j)]) {
                   nz[size_t(j)] = 1; w[size_t(j)] = 0.0; cols.push_back(j);
                   if (j < i) { heap.push_back(j); std::push_heap(heap.begin(), heap.end(), std::greater<int32_t>()); }
@@ -1126,7 +1131,8 @@ void plan_sweep_tasks(const std::vector<System *> &sys, bool mixed, bool has_pc,
       const double apply_bytes = double(4 + (mixed ? 4 : 8)) * double(S->padL + S->padU) + 40.0 * double(S->n);
       const bool one_sm_sooner = apply_bytes / kTaskBytesPerUs < kGridLevelUs * double(S->nlevL + S->nlevU) + apply_bytes / kGridBytesPerUs;
       const bool per_sys = S->nlevL > kCtaMinLevels && S->n / std::max(S->nlevL, 1) < kCtaRowsPerLevel && one_sm_sooner;
-      const bool per_blk = S->opts.precond == VSHE_PRECOND_BLOCK_ILU0 && nb >= 2 && bmax <= kTaskMaxRows;
+      const bool per_blk = (S->opts.precond == VSHE_PRECOND_BLOCK_ILU0 || S->opts.precond == VSHE_PRECOND_ILUT) && nb >= 2 &&
+                           bmax <= kTaskMaxRows;
       if (mode == VSHE_TRSV_PER_SYSTEM) on_task[size_t(k)] = 1;
       else if (mode == VSHE_TRSV_PER_BLOCK) on_task[size_t(k)] = 2;
       else if (mode == VSHE_TRSV_AUTO) on_task[size_t(k)] = per_blk ? 2 : per_sys ? 1 : 0;
