@@ -502,7 +502,9 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       const int pkeep = opts.ilut_entries > 0 ? opts.ilut_entries : 60;
       const double tau = opts.ilut_drop > 0 ? opts.ilut_drop : 1e-4;
       //
-      // Rows are eliminated on the host threads in claims of consecutive rows, in increasing order.
+      // With blocks that are runs of base positions, each host thread eliminates whole blocks.
+      // Otherwise rows are eliminated on the host threads in claims of consecutive rows, in
+      // increasing order.
       // A row reads only rows above it: before it reads row k's pivot and kept upper part it waits
       // until row k is final (done[k], set with release after they are written).  The row holding
       // the first unfinished position never waits, so the elimination always progresses, and every
@@ -514,7 +516,8 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
       for (int64_t i = 0; i < n; ++i) done[size_t(i)].store(0, std::memory_order_relaxed);
       std::atomic<int64_t> next_claim{0};
       constexpr int64_t kClaimRows = 64;
-      auto eliminate = [&](int64_t, int64_t) {
+      // eliminates the row ranges that next() hands out, one after the other
+      auto eliminate = [&](const std::function<bool(int64_t &, int64_t &)> &next) {
         // dense scratch over all columns, calloc'd: a thread touches only the pages its rows reach
         std::unique_ptr<double, void (*)(void *)> wbuf((double *)std::calloc(size_t(n), sizeof(double)), std::free);
         std::unique_ptr<char, void (*)(void *)> nzbuf((char *)std::calloc(size_t(n), 1), std::free);
@@ -523,10 +526,8 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
         char *nz = nzbuf.get();
         std::vector<int32_t> cols, heap;
         std::vector<std::pair<double, int32_t>> lo, up;
-        for (;;) {
-          const int64_t c0 = next_claim.fetch_add(kClaimRows);
-          if (c0 >= n) break;
-          const int64_t c1 = std::min<int64_t>(n, c0 + kClaimRows);
+        int64_t c0 = 0, c1 = 0;
+        while (next(c0, c1)) {
           RowStore &st = *new_store(c0);
           for (int64_t i = c0; i < c1; ++i) {
             cols.clear(); heap.clear();
@@ -607,7 +608,29 @@ int Layout::build(int64_t n, int64_t nnz, const std::vector<int64_t> &rp, const 
           }
         }
       };
-      host_parallel(host_threads(n, kClaimRows * 16), 1, eliminate);
+      if (contiguous && nruns > 1) {
+        // every block is one run of base positions and a row reads only rows of its block: whole
+        // blocks per thread, so no row waits
+        host_parallel_runs(runs, [&](int64_t r0, int64_t r1) {
+          bool given = false;
+          eliminate([&](int64_t &a, int64_t &b) {
+            if (given) return false;
+            given = true;
+            a = runs[size_t(r0)];
+            b = runs[size_t(r1)];
+            return true;
+          });
+        });
+      } else {
+        host_parallel(host_threads(n, kClaimRows * 16), 1, [&](int64_t, int64_t) {
+          eliminate([&](int64_t &a, int64_t &b) {
+            a = next_claim.fetch_add(kClaimRows);
+            if (a >= n) return false;
+            b = std::min<int64_t>(n, a + kClaimRows);
+            return true;
+          });
+        });
+      }
     } else {
       // symbolic ILU(k): the final rows' upper parts (column, level) feed later rows.  A row
       // reads only earlier rows of its own block, so when every block is one run of base
