@@ -26,14 +26,14 @@ def _bar():
     dev, cfg = D.config2(nx=40, ny=10, n_energies=48, L=3)
     P = O.OracleProblem(dev, cfg, O.golden_coupling(3))
     A = P.matrix(3)
-    return A.rp, A.ci, P.blocks()
+    return A.rp, A.ci, P.blocks(), A.v
 
 
 def _diode():
     dev, cfg = D.config1()
     P = O.OracleProblem(dev, cfg, O.golden_coupling(cfg.max_expansion_order))
     A = P.matrix(3)
-    return A.rp, A.ci, P.blocks()
+    return A.rp, A.ci, P.blocks(), A.v
 
 
 def _band(n=1500, width=300):
@@ -44,7 +44,9 @@ def _band(n=1500, width=300):
         rows.append(np.arange(max(0, i - width), min(n, i + 2)))
     rp = np.zeros(n + 1, np.int64)
     rp[1:] = np.cumsum([len(r) for r in rows])
-    return rp, np.concatenate(rows).astype(np.int32), None
+    ci = np.concatenate(rows).astype(np.int32)
+    v = np.where(ci == np.repeat(np.arange(n), np.diff(rp)), 4.0, -1.0 / width)
+    return rp, ci, None, v
 
 
 CASES = {
@@ -54,6 +56,7 @@ CASES = {
     "diode_ilu0_fp64_per_system": (_diode, dict(precond="ilu0", ordering="natural", trsv="per_system"), False, "fp64", 1),
     "band_per_system_mixed": (_band, dict(precond="ilu0", ordering="natural", trsv="per_system"), False, "mixed", 1),
     "band_per_system_fp64": (_band, dict(precond="ilu0", ordering="natural", trsv="per_system"), False, "fp64", 1),
+    "bar_slab_ilut_mixed": (_bar, dict(precond="ilut", ordering="natural", ilut_entries=20, ilut_drop=1e-3), True, "mixed", 2),
 }
 
 
@@ -64,13 +67,14 @@ def _stage_bytes(ns, nslot, r0, r1, lower, vb):
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_sweep_plan_fits_the_stages(name):
     make, kw, blocks, precision, kind = CASES[name]
-    rp, ci, bl = make()
+    rp, ci, bl, v = make()
     kw = dict(kw, precision=precision)
     if blocks:
         kw["blocks"] = bl
     n = len(rp) - 1
-    lay = gpu.layout(rp, ci, None, **kw)
-    plan = gpu.sweep_plan(rp, ci, None, **kw)
+    vals = v if kw["precond"] == "ilut" else None  # the ILUT pattern comes from the values
+    lay = gpu.layout(rp, ci, vals, **kw)
+    plan = gpu.sweep_plan(rp, ci, vals, **kw)
     assert plan["kind"] == kind
     vb = 4 if precision == "mixed" else 8
     chunks, sdesc = plan["chunks"], plan["sdesc"]
@@ -115,19 +119,20 @@ def test_sweep_plan_fits_the_stages(name):
         assert n_direct > 0
 
 
-@pytest.mark.parametrize("name", ["bar_block_ilu1_mixed", "diode_ilu0_mixed", "band_per_system_fp64"])
+@pytest.mark.parametrize("name", ["bar_block_ilu1_mixed", "diode_ilu0_mixed", "band_per_system_fp64", "bar_slab_ilut_mixed"])
 def test_sweep_plan_honours_every_dependency(name):
     """Every factor entry a chunk's row reads (a solved value of the same sweep) belongs to a row
     of the same task swept in an earlier level of that task: tasks never wait on each other, and
     a level's rows only read rows before the level barrier."""
     make, kw, blocks, precision, kind = CASES[name]
-    rp, ci, bl = make()
+    rp, ci, bl, v = make()
     kw = dict(kw, precision=precision)
     if blocks:
         kw["blocks"] = bl
     n = len(rp) - 1
-    lay = gpu.layout(rp, ci, None, **kw)
-    plan = gpu.sweep_plan(rp, ci, None, **kw)
+    vals = v if kw["precond"] == "ilut" else None  # the ILUT pattern comes from the values
+    lay = gpu.layout(rp, ci, vals, **kw)
+    plan = gpu.sweep_plan(rp, ci, vals, **kw)
     # backward slot of every solver row
     slot_of_row = np.empty(n, np.int64)
     slot_of_row[lay["urow"]] = np.arange(n)
